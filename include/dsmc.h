@@ -1,0 +1,244 @@
+/*
+ * dsmc.h - C ABI of the B200 DSMC engine.
+ *
+ * This is the drop-in boundary.  The reference solver exposes argument-less
+ * C++ functions over global state (include/Simulation.h:4,
+ * include/Initialization.h:4-5, include/Boundary.h:3-21, include/Geometry.h:14-22,
+ * include/Collision.h:4-6, include/Sampling.h:7-8).  Here the same operations
+ * take an explicit context, plain pointers and sizes; every call returns an
+ * int status and no exception crosses the boundary.  The C++ surface with the
+ * reference's own names (dsmc_reference_api.h) is a thin layer on top of
+ * these entry points.
+ *
+ * A context holds one or more independent cases (a batched ensemble).  All
+ * particle and cell storage lives in device memory owned by the context;
+ * host buffers are only touched by the explicit upload/download calls.
+ *
+ * Units are SI throughout, as in the reference.
+ */
+#ifndef DSMC_H
+#define DSMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------
+ * The reference aborts with MPI error codes; the same numbers are returned
+ * here (Geometry.cpp:82,120,157; MPIManager.cpp:628,792;
+ * Initialization.cpp:218).                                                 */
+enum {
+    DSMC_OK = 0,
+    DSMC_ERR_ARGUMENT = 2,        /* invalid argument or parameter           */
+    DSMC_ERR_OUT_OF_DOMAIN = 20,  /* particle outside the grid (Geometry.cpp:66-86) */
+    DSMC_ERR_CELL_OVERFLOW = 22,  /* > max_particles_in_cell (Geometry.cpp:142-161) */
+    DSMC_ERR_EXCHANGE = 30,       /* particle outside the domain at exchange  */
+    DSMC_ERR_CAPACITY = 31,       /* particle slots exhausted (Boundary.cpp:73-80,
+                                     MPIManager.cpp:782-796)                 */
+    DSMC_ERR_BAD_CLL = 40,        /* CLL coefficient outside [0, 1]
+                                     (Initialization.cpp:211-220, Boundary.cpp:247-250) */
+    DSMC_ERR_CUDA = 50,           /* a CUDA runtime call failed              */
+    DSMC_ERR_NO_DEVICE = 51,      /* no CUDA device                          */
+    DSMC_ERR_TIMEOUT = 60,        /* a bounded device-side wait gave up      */
+    DSMC_ERR_STATE = 61,          /* call out of order (e.g. step before init) */
+    DSMC_ERR_UNSUPPORTED = 62     /* feature not available in this build     */
+};
+
+/* WallModel, same enumerator order as the reference (include/Boundary.h:3). */
+enum {
+    DSMC_WALL_DIFFUSE = 0,
+    DSMC_WALL_SPECULAR = 1,
+    DSMC_WALL_CLL = 2
+};
+
+/* Storage precision of particle positions and velocities.  Hit times, inflow
+ * counts, cell indices and every moment accumulator are FP64 in both.     */
+enum {
+    DSMC_FP64 = 0,
+    DSMC_FP32 = 1
+};
+
+/* One case.  Field names follow the reference globals they replace
+ * (Geometry.cpp:11-24, Initialization.cpp:11-31, Boundary.cpp:11-13).     */
+typedef struct dsmc_params {
+    double x1, x2, y1, y2;   /* domain bounds X1 X2 Y1 Y2 [m]              */
+    double dz;               /* thickness DZ [m]                           */
+    double dl;               /* inflow strip width DL [m]                  */
+    int32_t nx, ny;          /* grid NX NY                                 */
+    double box_x, box_y;     /* obstacle centre BoxX BoxY [m]              */
+    double box_width, box_height;
+    double dt;               /* Dt [s]                                     */
+    int32_t n_step;          /* NStep                                      */
+    int32_t first_sampling_step; /* FirstSamplingStep                      */
+    int32_t sampling_period; /* SamplingPeriod                             */
+    int32_t wall_model;      /* DSMC_WALL_*  (WallInteraction)             */
+    double npc_free;         /* NPCFree                                    */
+    double molar_mass;       /* MolarMass [kg/mol]                         */
+    double ma_free;          /* MaFree                                     */
+    double n_free;           /* NFree [1/m^3]                              */
+    double t_free;           /* TFree [K]                                  */
+    double attack_angle;     /* AttackAngle [deg]                          */
+    double t_wall;           /* Tw [K]                                     */
+    double d_ref;            /* DRef [m]                                   */
+    double viscosity_index;  /* ViscosityIndex (omega)                     */
+    double t_ref;            /* Tref [K]                                   */
+    double cll_normal;       /* CLLNormalAccommodation                     */
+    double cll_tangential;   /* CLLTangentialAccommodation                 */
+    uint64_t seed;           /* Philox key of this case                    */
+    int32_t precision;       /* DSMC_FP64 or DSMC_FP32                     */
+    int32_t reserved1;       /* must be 0                                  */
+    int32_t max_particles_in_cell; /* 0: unlimited; >0: report
+                                DSMC_ERR_CELL_OVERFLOW above it as the
+                                reference's MAX_PCL_IN_CELL does            */
+    int32_t reserved0;
+    int64_t capacity;        /* particle slots; 0 = sized automatically    */
+} dsmc_params;
+
+/* Derived constants computed by Setup() (Initialization.cpp:221-265). */
+typedef struct dsmc_derived {
+    double molecule_mass;    /* MoleculeMass                               */
+    double p_free;           /* PFree                                      */
+    double u_free;           /* UFree                                      */
+    double ux_free, uy_free; /* UxFree UyFree                              */
+    double dx, dy, dv;       /* DX DY DV                                   */
+    double weight;           /* Weight                                     */
+    double sigma_ref;        /* SigmaRef                                   */
+    double omega;            /* Omega = 2 omega - 1                        */
+    double cr_ref;           /* CrRef                                      */
+    double mft_free;         /* MFTFree                                    */
+    double mfp_free;         /* MFPFree                                    */
+    double kn_free;          /* KnFree                                     */
+    double sc_max;           /* SCMax of Collision.cpp:23                  */
+} dsmc_derived;
+
+/* Run-time counters of one case. */
+typedef struct dsmc_counters {
+    int64_t np;                   /* NP after the last completed stage     */
+    int64_t step;                 /* Step                                  */
+    int64_t sample_step;          /* SampleStep                            */
+    int64_t collisions_last_step; /* NC returned by CollideParticles       */
+    int64_t collisions_total;
+    int64_t drag_collision_count; /* DragCollisionCount                    */
+    int64_t particle_steps;       /* sum of NP over completed steps        */
+    double drag_impulse_total;    /* DragImpulseTotal                      */
+    double time;                  /* Time                                  */
+    double sample_time;           /* SampleTime                            */
+    double drag_sampling_time;    /* DragSamplingTime                      */
+} dsmc_counters;
+
+/* Moments of one cell, laid out exactly as the reference's CELL
+ * (include/Cell.h:4-10), 17 doubles.                                       */
+typedef struct dsmc_cell {
+    double count_np;
+    double count_v[3];
+    double count_vv[3][3];
+    double count_v2v[3];
+    double count_nc;
+} dsmc_cell;
+
+typedef struct dsmc_ctx dsmc_ctx;
+
+/* ---- host-only helpers (no device needed) ------------------------------ */
+
+/* Reference defaults: Initialization.cpp:11-31, Geometry.cpp:11-24,
+ * Boundary.cpp:11-13 (CLL 0.8/0.8 walls). */
+void dsmc_default_params(dsmc_params *p);
+
+/* Setup() (Initialization.cpp:210-288): validates the case and fills *d.
+ * Returns DSMC_ERR_BAD_CLL for CLL coefficients outside [0, 1]. */
+int dsmc_setup(const dsmc_params *p, dsmc_derived *d);
+
+/* WallModelName() (Boundary.cpp:15-24); NULL for an unknown model. */
+const char *dsmc_wall_model_name(int wall_model);
+
+const char *dsmc_status_string(int status);
+
+/* Printing() (Sampling.cpp:36-268): writes <dir>/<wall>/DSMC2D_Field.plt and
+ * .json from a gathered field of nx*ny cells in x-major order (k*ny + l),
+ * exactly in the reference format.  `sample_step` is SampleStep. */
+int dsmc_write_field(const dsmc_params *p, const dsmc_derived *d, int64_t sample_step,
+                     const dsmc_cell *cells, const char *results_dir);
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Creates a context of n_cases independent cases on the current CUDA device.
+ * `derived` may be NULL (computed by dsmc_setup) or an array of n_cases
+ * overrides.  `cuda_stream` is a cudaStream_t to launch on, or NULL for a
+ * stream owned by the context. */
+int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n_cases,
+                    void *cuda_stream, dsmc_ctx **out);
+int dsmc_ctx_destroy(dsmc_ctx *ctx);
+
+/* InitialConditions() (Initialization.cpp:290-313) for every case, followed
+ * by the cell sort that leaves particles ordered by cell. */
+int dsmc_init_cold(dsmc_ctx *ctx);
+
+/* Runs n_steps complete time steps (Simulation.cpp:138-199) for every case:
+ * move, boundary conditions, indexing, collisions, sampling.  Launched as
+ * CUDA graphs; returns after enqueueing.  Errors raised on the device are
+ * reported by the next dsmc_synchronize(). */
+int dsmc_step(dsmc_ctx *ctx, int n_steps);
+
+/* The stages of one step, for callers of the per-function surface.  They
+ * must be called in this order; dsmc_stage_end_step advances Step. */
+int dsmc_stage_move(dsmc_ctx *ctx);      /* MoveParticles (Boundary.cpp:284-328) */
+int dsmc_stage_boundary(dsmc_ctx *ctx);  /* BoundaryConditions (Boundary.cpp:94-203) */
+int dsmc_stage_index(dsmc_ctx *ctx);     /* Indexing (Geometry.cpp:37-170)          */
+int dsmc_stage_collide(dsmc_ctx *ctx);   /* CollideParticles (Collision.cpp:45-56)  */
+int dsmc_stage_sample(dsmc_ctx *ctx);    /* Sampling (Sampling.cpp:14-31), in sampling steps */
+int dsmc_stage_end_step(dsmc_ctx *ctx);  /* Step++, Time += Dt (Simulation.cpp:160-161) */
+
+/* Waits for queued work and returns the first device-side error, if any. */
+int dsmc_synchronize(dsmc_ctx *ctx);
+
+int dsmc_get_counters(dsmc_ctx *ctx, int case_index, dsmc_counters *out);
+
+/* Accumulated moments of one case, nx*ny cells x-major, as GatherGlobalField
+ * (MPIManager.cpp:305-499) returns them. */
+int dsmc_get_fields(dsmc_ctx *ctx, int case_index, dsmc_cell *host_out);
+/* Same, into device memory (17 doubles per cell), e.g. for an all-reduce. */
+int dsmc_get_fields_device(dsmc_ctx *ctx, int case_index, double *device_out);
+/* Replaces the accumulators of a case (e.g. after a replica all-reduce). */
+int dsmc_set_fields_device(dsmc_ctx *ctx, int case_index, const double *device_in,
+                           int64_t sample_step);
+
+/* Particle state of one case in slot order, as FP64 host arrays. */
+int dsmc_download_particles(dsmc_ctx *ctx, int case_index, double *x, double *y, double *vx,
+                            double *vy, double *vz, int64_t capacity, int64_t *n_out);
+/* Replaces the particle state of one case and re-sorts it by cell. */
+int dsmc_upload_particles(dsmc_ctx *ctx, int case_index, const double *x, const double *y,
+                          const double *vx, const double *vy, const double *vz, int64_t n);
+/* Cell start offsets (nx*ny + 1 entries) of the last sort. */
+int dsmc_get_cell_starts(dsmc_ctx *ctx, int case_index, int32_t *host_out);
+
+/* Per-kernel device time of the stages, for profiling.  When enabled,
+ * dsmc_step brackets every kernel with CUDA events; dsmc_get_kernel_times
+ * returns the summed milliseconds per kernel since the last reset and the
+ * kernel names. */
+int dsmc_set_profiling(dsmc_ctx *ctx, int enabled);
+int dsmc_get_kernel_times(dsmc_ctx *ctx, double *ms_out, int64_t *launches_out, int max_kernels,
+                          int *n_kernels, const char **names_out);
+
+/* ---- unit kernels (parity tests of single device functions) ------------
+ * Pointers are device pointers of n elements. */
+
+/* IntersectBox (Geometry.cpp:179-229) over a batch of segments. */
+int dsmc_k_intersect(const dsmc_params *p, int64_t n, const double *x, const double *y,
+                     const double *dx, const double *dy, int32_t *hit, double *t_hit,
+                     double *nx, double *ny, void *cuda_stream);
+
+/* One wall interaction per element (Boundary.cpp:205-282) with the case's
+ * wall model; element i draws from stream (kind, step, entity[i]).  v is
+ * 3*n doubles, (vx, vy, vz) per element, updated in place. */
+int dsmc_k_scatter(const dsmc_params *p, const dsmc_derived *d, int64_t n, double *v,
+                   const double *nx, const double *ny, uint32_t kind, uint32_t step,
+                   const uint32_t *entity, void *cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DSMC_H */
