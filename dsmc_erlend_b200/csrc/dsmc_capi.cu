@@ -1,0 +1,1178 @@
+// dsmc_capi.cu - the C ABI of include/dsmc.h over the kernels of
+// dsmc_kernels.cuh: context and device memory, the launch sequence of a
+// step, its CUDA graphs, and the upload/download paths.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dsmc.h"
+#include "dsmc_kernels.cuh"
+
+using namespace dsmc;
+
+namespace {
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            std::fprintf(stderr, "dsmc: %s failed: %s (%s:%d)\n", #call,                  \
+                         cudaGetErrorString(e_), __FILE__, __LINE__);                     \
+            return DSMC_ERR_CUDA;                                                         \
+        }                                                                                 \
+    } while (0)
+
+enum KernelId {
+    KID_PLAN, KID_MOVE, KID_INJECT, KID_PLAN2, KID_TAIL, KID_CELL_SCAN, KID_TILE_SCAN,
+    KID_OLIST, KID_CELL_FIX, KID_SCATTER, KID_COLLIDE, KID_FINISH, KID_COUNT
+};
+const char *kKernelNames[KID_COUNT] = {"k_plan",     "k_move",      "k_inject",  "k_plan2",
+                                       "k_tail",     "k_cell_scan", "k_tile_scan", "k_olist",
+                                       "k_cell_fix", "k_scatter",   "k_collide", "k_finish"};
+
+struct Timed {
+    int kid;
+    cudaEvent_t a, b;
+};
+
+template <class T> size_t collide_smem() { return sizeof(T) * 3 * COLLIDE_SMEM_PCL; }
+
+} // namespace
+
+struct dsmc_ctx {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int ncase = 0;
+    int precision = DSMC_FP64;
+    std::vector<dsmc_params> params;
+    std::vector<dsmc_derived> derived;
+    std::vector<CaseDev> hcases;
+    int64_t total_slots = 0;
+    int total_cells = 0; // global cell ids, ncell + 1 per case
+    int max_slot_tiles = 0;
+    int total_cell_tiles = 0;
+
+    CaseDev *d_cases = nullptr;
+    CaseState *d_state = nullptr;
+    StepScratch *d_scratch = nullptr;
+    int *d_err = nullptr;
+    int32_t *d_tables = nullptr; // 7 x (ncase + 1)
+    int32_t *d_tmp = nullptr;    // 2 x ncase
+    int64_t *d_pbases = nullptr;
+    TileTables tt{};
+
+    void *buf[2][5] = {{nullptr}};
+    uint32_t *key = nullptr;
+    Cells cells{};
+    int32_t *tile_in = nullptr, *tile_prefix = nullptr;
+    uint64_t *lb = nullptr; // 4 chains: move, inject, tail, cell
+    size_t lb_words = 0;
+    int32_t *hole_pos = nullptr, *hole_oc = nullptr;
+    uint32_t *obuf = nullptr;
+    int32_t *olist = nullptr;
+
+    int cur = 0;
+    bool initialized = false;
+    int stage = 0; // staged calls: 0 idle, 1 moved, 2 boundary, 3 indexed, 4 collided, 5 sampled
+    bool sampled = false;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+
+    int grid_move = 0, grid_inject = 0, grid_tail = 0, grid_cell_scan = 0, grid_olist = 0;
+    int grid_cell_fix = 0, grid_scatter = 0, grid_collide = 0;
+
+    bool profiling = false;
+    std::vector<Timed> timed;
+    double kernel_ms[KID_COUNT] = {0};
+    int64_t kernel_launches[KID_COUNT] = {0};
+    std::vector<cudaEvent_t> event_pool;
+};
+
+namespace {
+
+cudaEvent_t take_event(dsmc_ctx *c)
+{
+    if (!c->event_pool.empty()) {
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one launch with events when profiling (eager mode only).
+struct Span {
+    dsmc_ctx *c;
+    int kid;
+    cudaEvent_t a = nullptr;
+    Span(dsmc_ctx *ctx, int k) : c(ctx), kid(k)
+    {
+        if (c->profiling) {
+            a = take_event(c);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    ~Span()
+    {
+        if (c->profiling) {
+            cudaEvent_t b = take_event(c);
+            cudaEventRecord(b, c->stream);
+            c->timed.push_back({kid, a, b});
+        }
+    }
+};
+
+template <class T> Slots<T> slots(dsmc_ctx *c, int side)
+{
+    Slots<T> s;
+    s.x = static_cast<T *>(c->buf[side][0]);
+    s.y = static_cast<T *>(c->buf[side][1]);
+    s.vx = static_cast<T *>(c->buf[side][2]);
+    s.vy = static_cast<T *>(c->buf[side][3]);
+    s.vz = static_cast<T *>(c->buf[side][4]);
+    return s;
+}
+
+uint64_t *lb_chain(dsmc_ctx *c, int i) { return c->lb + static_cast<size_t>(i) * c->lb_words / 4; }
+
+int clear_step_scratch(dsmc_ctx *c)
+{
+    CK(cudaMemsetAsync(c->d_scratch, 0, sizeof(StepScratch), c->stream));
+    CK(cudaMemsetAsync(c->lb, 0, c->lb_words * sizeof(uint64_t), c->stream));
+    return DSMC_OK;
+}
+
+// MoveParticles: plan + move.
+template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
+{
+    int s = clear_step_scratch(c);
+    if (s)
+        return s;
+    {
+        Span sp(c, KID_PLAN);
+        k_plan<<<1, 1024, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch, c->tt, c->d_tmp,
+                                          c->ncase, init_mode, c->d_err);
+    }
+    if (!init_mode) {
+        Span sp(c, KID_MOVE);
+        k_move<T><<<c->grid_move, TILE_THREADS, 0, c->stream>>>(
+            c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
+            c->tile_in, lb_chain(c, 0), c->hole_pos, c->hole_oc, c->obuf, c->ncase, c->d_err);
+    }
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+// BoundaryConditions: inflow strips, then the swap-with-last removal.
+template <class T> int enqueue_boundary(dsmc_ctx *c)
+{
+    {
+        Span sp(c, KID_INJECT);
+        k_inject<T><<<c->grid_inject, TILE_THREADS, 0, c->stream>>>(
+            c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
+            lb_chain(c, 1), c->hole_pos, c->hole_oc, c->obuf, c->ncase, c->d_err);
+    }
+    {
+        Span sp(c, KID_PLAN2);
+        k_plan2<<<1, 1024, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch, c->tt,
+                                           c->hole_pos, c->d_tmp, c->ncase);
+    }
+    {
+        Span sp(c, KID_TAIL);
+        k_tail<T><<<c->grid_tail, TILE_THREADS, 0, c->stream>>>(
+            c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
+            c->tile_in, lb_chain(c, 2), c->hole_pos, c->hole_oc, c->obuf, c->ncase, c->d_err);
+    }
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+// Indexing: the stable counting sort into the other buffer, then flip.
+template <class T> int enqueue_index(dsmc_ctx *c)
+{
+    const int side = c->cur;
+    {
+        Span sp(c, KID_CELL_SCAN);
+        k_cell_scan<<<c->grid_cell_scan, TILE_THREADS, 0, c->stream>>>(
+            c->d_cases, c->d_scratch, c->tt, c->cells, side ^ 1, lb_chain(c, 3), c->ncase,
+            c->d_err);
+    }
+    {
+        Span sp(c, KID_TILE_SCAN);
+        k_tile_scan<<<c->ncase, TILE_THREADS, 0, c->stream>>>(c->d_state, c->tile_in,
+                                                              c->tile_prefix);
+    }
+    {
+        Span sp(c, KID_OLIST);
+        k_olist<<<c->grid_olist, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch,
+                                                      c->obuf, c->key, c->cells, c->olist,
+                                                      c->d_pbases, c->ncase, c->d_err);
+    }
+    {
+        Span sp(c, KID_CELL_FIX);
+        k_cell_fix<T><<<c->grid_cell_fix, 256, 0, c->stream>>>(
+            c->d_cases, c->d_state, c->tt, c->cells, side, slots<T>(c, side),
+            slots<T>(c, side ^ 1), c->olist, c->total_cells, c->ncase, c->d_err);
+    }
+    {
+        Span sp(c, KID_SCATTER);
+        k_scatter<T><<<c->grid_scatter, TILE_THREADS, 0, c->stream>>>(
+            c->d_cases, c->d_state, c->tt, slots<T>(c, side), slots<T>(c, side ^ 1), c->key,
+            c->cells, c->tile_prefix, c->ncase, c->d_err);
+    }
+    CK(cudaGetLastError());
+    c->cur ^= 1;
+    return DSMC_OK;
+}
+
+template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sample)
+{
+    Span sp(c, KID_COLLIDE);
+    k_collide<T><<<c->grid_collide, COLLIDE_CELLS, collide_smem<T>(), c->stream>>>(
+        c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, do_collide,
+        do_sample, c->ncase);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+int enqueue_finish(dsmc_ctx *c, int init_mode, int did_sample, int end_step)
+{
+    Span sp(c, KID_FINISH);
+    k_finish<<<1, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->ncase, init_mode, did_sample,
+                                        end_step);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+template <class T> int enqueue_step(dsmc_ctx *c)
+{
+    int s;
+    if ((s = enqueue_move<T>(c, 0)))
+        return s;
+    if ((s = enqueue_boundary<T>(c)))
+        return s;
+    if ((s = enqueue_index<T>(c)))
+        return s;
+    if ((s = enqueue_collide<T>(c, 1, 1)))
+        return s;
+    return enqueue_finish(c, 0, 1, 1);
+}
+
+int dispatch_step(dsmc_ctx *c)
+{
+    return c->precision == DSMC_FP32 ? enqueue_step<float>(c) : enqueue_step<double>(c);
+}
+
+int build_graphs(dsmc_ctx *c)
+{
+    for (int side = 0; side < 2; ++side) {
+        const int saved = c->cur;
+        c->cur = side;
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int s = dispatch_step(c);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->cur = saved;
+        if (s)
+            return s;
+        if (e != cudaSuccess)
+            return DSMC_ERR_CUDA;
+        e = cudaGraphInstantiate(&c->graph[side], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess)
+            return DSMC_ERR_CUDA;
+    }
+    return DSMC_OK;
+}
+
+// Constants of one case, computed on the host with the reference expressions.
+CaseDev make_case(const dsmc_params &p, const dsmc_derived &d)
+{
+    CaseDev c{};
+    c.x1 = p.x1;
+    c.x2 = p.x2;
+    c.y1 = p.y1;
+    c.y2 = p.y2;
+    c.dz = p.dz;
+    c.dx = d.dx;
+    c.dy = d.dy;
+    c.dv = d.dv;
+    c.dt = p.dt;
+    c.inv_dx = 1.0 / d.dx;
+    c.inv_dy = 1.0 / d.dy;
+    {
+        double mag = 1.0;
+        const double v[] = {p.x1, p.x2, p.y1, p.y2, p.box_x - p.box_width / 2.0,
+                            p.box_x + p.box_width / 2.0, p.box_y - p.box_height / 2.0,
+                            p.box_y + p.box_height / 2.0};
+        for (double a : v)
+            mag = std::max(mag, std::fabs(a));
+        c.cull = 1e-9 * mag;
+    }
+    c.box_lo[0] = p.box_x - p.box_width / 2.0; // Geometry.cpp:184
+    c.box_lo[1] = p.box_y - p.box_height / 2.0;
+    c.box_hi[0] = p.box_x + p.box_width / 2.0; // Geometry.cpp:185
+    c.box_hi[1] = p.box_y + p.box_height / 2.0;
+    c.box_x = p.box_x;
+    c.box_y = p.box_y;
+    c.box_hw = p.box_width / 2.0; // Geometry.cpp:175-176
+    c.box_hh = p.box_height / 2.0;
+    const double m = d.molecule_mass;
+    c.rtw = K_BOLTZMANN * p.t_wall / m; // Boundary.cpp:213 (and :258)
+    c.sqrt_rtw = std::sqrt(c.rtw);
+    c.cll_an = p.cll_normal;
+    c.cll_at = p.cll_tangential;
+    c.cll_var_n = p.cll_normal * c.rtw; // Boundary.cpp:268
+    c.cll_var_t = p.cll_tangential * c.rtw; // Boundary.cpp:276
+    c.cll_keep_n = std::sqrt(1.0 - p.cll_normal);
+    c.cll_keep_t = std::sqrt(1.0 - p.cll_tangential);
+    c.mass = m;
+    c.drag_scale = d.weight * m; // Boundary.cpp:318
+    c.weight = d.weight;
+    c.sigma_ref = d.sigma_ref;
+    c.omega = d.omega;
+    c.cr_ref = d.cr_ref;
+    c.sc_max = d.sc_max;
+    c.ux_free = d.ux_free;
+    c.uy_free = d.uy_free;
+    c.rt_free = K_BOLTZMANN * p.t_free / m; // Boundary.cpp:53
+    // One rank owns all cells: LocalX1 = X1 + 0 * DX, LocalX2 = X1 + NX * DX
+    // (MPIManager.cpp:216-229).
+    const double lx1 = p.x1 + 0 * d.dx, lx2 = p.x1 + p.nx * d.dx;
+    const double ly1 = p.y1 + 0 * d.dy, ly2 = p.y1 + p.ny * d.dy;
+    const double strips[5][4] = {
+        {p.x1 - p.dl, ly1, p.x1, ly2},  // Boundary.cpp:100-113
+        {p.x2, ly1, p.x2 + p.dl, ly2},  // :120-133
+        {lx1, p.y1 - p.dl, lx2, p.y1},  // :140-153
+        {lx1, p.y2, lx2, p.y2 + p.dl},  // :160-173
+        {lx1, ly1, lx2, ly2},           // Initialization.cpp:302-310
+    };
+    for (int s = 0; s < 5; ++s) {
+        for (int k = 0; k < 4; ++k)
+            c.strip[s][k] = strips[s][k];
+        // Boundary.cpp:62-63
+        const double v = (strips[s][2] - strips[s][0]) * (strips[s][3] - strips[s][1]) * p.dz;
+        c.strip_navg[s] = p.n_free * v / d.weight;
+    }
+    c.nx = p.nx;
+    c.ny = p.ny;
+    c.wall_model = p.wall_model;
+    c.first_sampling_step = p.first_sampling_step;
+    c.sampling_period = p.sampling_period;
+    c.max_per_cell = p.max_particles_in_cell;
+    c.ncell = p.nx * p.ny;
+    c.key0 = static_cast<uint32_t>(p.seed);
+    c.key1 = static_cast<uint32_t>(p.seed >> 32);
+    return c;
+}
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+template <class T> int occupancy_grids(dsmc_ctx *c)
+{
+    int b = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_move<T>, TILE_THREADS, 0));
+    c->grid_move = std::max(1, b) * c->sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_inject<T>, TILE_THREADS, 0));
+    c->grid_inject = std::max(1, b) * c->sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_tail<T>, TILE_THREADS, 0));
+    c->grid_tail = std::max(1, b) * c->sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cell_scan, TILE_THREADS, 0));
+    c->grid_cell_scan = std::max(1, b) * c->sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, TILE_THREADS, 0));
+    c->grid_scatter = std::max(1, b) * c->sms;
+    CK(cudaFuncSetAttribute(k_collide<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(collide_smem<T>())));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_collide<T>, COLLIDE_CELLS,
+                                                     collide_smem<T>()));
+    c->grid_collide = std::max(1, b) * c->sms;
+    c->grid_olist = 4 * c->sms;
+    c->grid_cell_fix = 8 * c->sms;
+    return DSMC_OK;
+}
+
+void free_ctx(dsmc_ctx *c)
+{
+    for (auto &g : c->graph)
+        if (g)
+            cudaGraphExecDestroy(g);
+    for (auto &t : c->timed) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (auto e : c->event_pool)
+        cudaEventDestroy(e);
+    void *ptrs[] = {c->d_cases, c->d_state, c->d_scratch, c->d_err, c->d_tables, c->d_tmp,
+                    c->d_pbases, c->key, c->cells.n_in, c->cells.n_o, c->cells.o_fill,
+                    c->cells.fin, c->cells.ostart, c->cells.base_in, c->cells.start[0],
+                    c->cells.start[1], c->cells.acc, c->tile_in, c->tile_prefix, c->lb,
+                    c->hole_pos, c->hole_oc, c->obuf, c->olist};
+    for (void *p : ptrs)
+        if (p)
+            cudaFree(p);
+    for (auto &side : c->buf)
+        for (void *p : side)
+            if (p)
+                cudaFree(p);
+    if (c->own_stream && c->stream)
+        cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int read_state(dsmc_ctx *c, std::vector<CaseState> &st)
+{
+    st.resize(c->ncase);
+    CK(cudaMemcpyAsync(st.data(), c->d_state, sizeof(CaseState) * c->ncase,
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int device_error(dsmc_ctx *c)
+{
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return err;
+}
+
+// ---- upload: convert host FP64 state into one case's slots, then re-sort ---
+
+template <class T>
+__global__ void k_upload_case(const double *x, const double *y, const double *vx, const double *vy,
+                              const double *vz, int64_t n, Slots<T> p, int64_t pbase)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        p.x[pbase + i] = Store<T>::rn(x[i]);
+        p.y[pbase + i] = Store<T>::rn(y[i]);
+        p.vx[pbase + i] = Store<T>::rn(vx[i]);
+        p.vy[pbase + i] = Store<T>::rn(vy[i]);
+        p.vz[pbase + i] = Store<T>::rn(vz[i]);
+    }
+}
+
+// Every slot of every case becomes an out-of-range particle of its cell, so
+// the sort orders all cases from scratch (stable in slot order).
+template <class T>
+__global__ void k_rekey(const CaseDev *cases, CaseState *st, StepScratch *sc, Slots<T> p,
+                        uint32_t *key, Cells cells, uint32_t *obuf, int ncase, int *err)
+{
+    for (int ci = 0; ci < ncase; ++ci) {
+        const CaseDev &c = cases[ci];
+        const int64_t n = st[ci].n_old;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+             i += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t g = c.pbase + i;
+            const int32_t cl = cell_of(c, static_cast<double>(p.x[g]), static_cast<double>(p.y[g]));
+            if (cl < 0) {
+                report_error(err, DSMC_ERR_EXCHANGE);
+                key[g] = KEY_DEAD;
+                continue;
+            }
+            key[g] = static_cast<uint32_t>(c.cbase + cl);
+            atomicAdd(cells.n_o + c.cbase + cl, 1);
+            obuf[atomicAdd(&sc->obuf_count, 1u)] = static_cast<uint32_t>(g);
+        }
+    }
+}
+
+__global__ void k_resort_plan(CaseState *st, StepScratch *sc, TileTables tt, int ncase)
+{
+    if (threadIdx.x != 0)
+        return;
+    int32_t run = 0;
+    for (int i = 0; i < ncase; ++i) {
+        CaseState &s = st[i];
+        s.n_total = s.n_old;
+        s.dead_old = s.dead_total = 0;
+        s.n_keep = s.n_old;
+        s.n_holes = 0;
+        s.n_move_tiles = 0;
+        s.move_tile0 = 0;
+        s.n_tail_tiles = 0;
+        tt.scatter0[i] = run;
+        run += static_cast<int32_t>((s.n_keep + TILE - 1) / TILE);
+    }
+    tt.scatter0[ncase] = run;
+    sc->total_tail_tiles = 0;
+}
+
+template <class T> int resort_all(dsmc_ctx *c)
+{
+    int s = clear_step_scratch(c);
+    if (s)
+        return s;
+    const int side = c->cur;
+    CK(cudaMemsetAsync(c->cells.start[side], 0, sizeof(int32_t) * c->total_cells, c->stream));
+    k_resort_plan<<<1, 32, 0, c->stream>>>(c->d_state, c->d_scratch, c->tt, c->ncase);
+    k_rekey<T><<<4 * c->sms, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch,
+                                                   slots<T>(c, side), c->key, c->cells, c->obuf,
+                                                   c->ncase, c->d_err);
+    CK(cudaGetLastError());
+    if ((s = enqueue_index<T>(c)))
+        return s;
+    return enqueue_finish(c, 1, 0, 0);
+}
+
+__global__ void k_fields_out(const Cells cells, int cbase, int ncell, double *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncell; i += gridDim.x * blockDim.x) {
+        const int64_t cg = cbase + i;
+        const int64_t S = cells.acc_stride;
+        auto A = [&](int m) { return cells.acc[m * S + cg]; };
+        double *o = out + 17 * static_cast<int64_t>(i);
+        o[0] = A(ACC_NP);
+        o[1] = A(ACC_V0);
+        o[2] = A(ACC_V1);
+        o[3] = A(ACC_V2);
+        o[4] = A(ACC_VV00);
+        o[5] = A(ACC_VV01);
+        o[6] = A(ACC_VV02);
+        o[7] = A(ACC_VV01);
+        o[8] = A(ACC_VV11);
+        o[9] = A(ACC_VV12);
+        o[10] = A(ACC_VV02);
+        o[11] = A(ACC_VV12);
+        o[12] = A(ACC_VV22);
+        o[13] = A(ACC_V2V0);
+        o[14] = A(ACC_V2V1);
+        o[15] = A(ACC_V2V2);
+        o[16] = A(ACC_NC);
+    }
+}
+
+__global__ void k_fields_in(Cells cells, int cbase, int ncell, const double *in)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncell; i += gridDim.x * blockDim.x) {
+        const int64_t cg = cbase + i;
+        const int64_t S = cells.acc_stride;
+        const double *o = in + 17 * static_cast<int64_t>(i);
+        const int map[ACC_COUNT] = {0, 1, 2, 3, 4, 5, 6, 8, 9, 12, 13, 14, 15, 16};
+        for (int m = 0; m < ACC_COUNT; ++m)
+            cells.acc[m * S + cg] = o[map[m]];
+    }
+}
+
+__global__ void k_download_case(Slots<float> p, int64_t pbase, int64_t n, double *out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        out[i] = p.x[pbase + i];
+        out[n + i] = p.y[pbase + i];
+        out[2 * n + i] = p.vx[pbase + i];
+        out[3 * n + i] = p.vy[pbase + i];
+        out[4 * n + i] = p.vz[pbase + i];
+    }
+}
+
+// ---- unit kernels ------------------------------------------------------------
+
+__global__ void k_unit_intersect(CaseDev c, int64_t n, const double *x, const double *y,
+                                 const double *dx, const double *dy, int32_t *hit, double *t,
+                                 double *nx, double *ny)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double th = 0.0, a = 0.0, b = 0.0;
+        const bool h = intersect_box(c, x[i], y[i], dx[i], dy[i], th, a, b);
+        hit[i] = h ? 1 : 0;
+        t[i] = h ? th : 0.0;
+        nx[i] = h ? a : 0.0;
+        ny[i] = h ? b : 0.0;
+    }
+}
+
+__global__ void k_unit_scatter(CaseDev c, int64_t n, double *v, const double *nx,
+                               const double *ny, uint32_t kind, uint32_t step,
+                               const uint32_t *entity)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double w[3] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+        dsmc_stream r;
+        open_stream(r, c, kind, step, entity[i]);
+        wall_interaction(r, c, w, nx[i], ny[i]);
+        v[3 * i] = w[0];
+        v[3 * i + 1] = w[1];
+        v[3 * i + 2] = w[2];
+    }
+}
+
+int resolve_timings(dsmc_ctx *c)
+{
+    if (c->timed.empty())
+        return DSMC_OK;
+    CK(cudaStreamSynchronize(c->stream));
+    for (auto &t : c->timed) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, t.a, t.b));
+        c->kernel_ms[t.kid] += ms;
+        c->kernel_launches[t.kid] += 1;
+        c->event_pool.push_back(t.a);
+        c->event_pool.push_back(t.b);
+    }
+    c->timed.clear();
+    return DSMC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n_cases,
+                    void *cuda_stream, dsmc_ctx **out)
+{
+    if (cases == nullptr || out == nullptr || n_cases < 1)
+        return DSMC_ERR_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return DSMC_ERR_NO_DEVICE;
+    auto *c = new dsmc_ctx();
+    c->ncase = n_cases;
+    c->precision = cases[0].precision;
+    c->params.assign(cases, cases + n_cases);
+    c->derived.resize(n_cases);
+    for (int i = 0; i < n_cases; ++i) {
+        if (cases[i].precision != c->precision) {
+            delete c;
+            return DSMC_ERR_ARGUMENT; // one storage precision per context
+        }
+        const int s = dsmc_setup(&cases[i], &c->derived[i]);
+        if (s) {
+            delete c;
+            return s;
+        }
+        if (derived != nullptr)
+            c->derived[i] = derived[i];
+    }
+    cudaGetDevice(&c->device);
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+    if (cuda_stream != nullptr) {
+        c->stream = static_cast<cudaStream_t>(cuda_stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return DSMC_ERR_CUDA;
+        }
+        c->own_stream = true;
+    }
+
+    // Layout: each case owns a TILE-aligned slot range and ncell + 1 cell ids.
+    c->hcases.resize(n_cases);
+    int64_t slot = 0;
+    int cell = 0, cell_tiles = 0, cblocks = 0;
+    std::vector<int32_t> cell0(n_cases + 1), cblock0(n_cases + 1), cellbase(n_cases + 1);
+    std::vector<int64_t> pbases(n_cases);
+    int max_tiles = 0;
+    for (int i = 0; i < n_cases; ++i) {
+        const dsmc_params &p = cases[i];
+        CaseDev cd = make_case(p, c->derived[i]);
+        int64_t cap = p.capacity;
+        if (cap <= 0) {
+            // Freestream count plus room for compression near the box and
+            // one step of inflow per strip.
+            double inflow = 0.0;
+            for (int s = 0; s < 4; ++s)
+                inflow += cd.strip_navg[s] + 10.0 * std::sqrt(cd.strip_navg[s] + 1.0);
+            cap = static_cast<int64_t>(1.5 * p.npc_free * p.nx * p.ny + 2.0 * inflow +
+                                       cd.strip_navg[4] * 0.0) + 4096;
+            cap = std::max<int64_t>(cap, static_cast<int64_t>(
+                                              cd.strip_navg[4] + 10.0 * std::sqrt(cd.strip_navg[4]) +
+                                              4096));
+        }
+        cap = round_up(cap, TILE);
+        cd.pbase = slot;
+        cd.cap = cap;
+        cd.cbase = cell;
+        pbases[i] = slot;
+        cellbase[i] = cell;
+        cell0[i] = cell_tiles;
+        cblock0[i] = cblocks;
+        slot += cap;
+        cell += cd.ncell + 1;
+        cell_tiles += (cd.ncell + TILE - 1) / TILE;
+        cblocks += (cd.ncell + COLLIDE_CELLS - 1) / COLLIDE_CELLS;
+        max_tiles += static_cast<int>(cap / TILE) + 1;
+        c->hcases[i] = cd;
+    }
+    cellbase[n_cases] = cell;
+    cell0[n_cases] = cell_tiles;
+    cblock0[n_cases] = cblocks;
+    c->total_slots = slot;
+    c->total_cells = cell;
+    c->total_cell_tiles = cell_tiles;
+    c->max_slot_tiles = max_tiles;
+    if (slot >= (int64_t(1) << 32) - 1 || cell >= (1 << 30)) {
+        free_ctx(c);
+        return DSMC_ERR_ARGUMENT;
+    }
+
+    const size_t esz = c->precision == DSMC_FP32 ? sizeof(float) : sizeof(double);
+    auto alloc = [&](void **p, size_t bytes) -> bool {
+        return cudaMalloc(p, std::max<size_t>(bytes, 16)) == cudaSuccess;
+    };
+    bool ok = true;
+    ok &= alloc(reinterpret_cast<void **>(&c->d_cases), sizeof(CaseDev) * n_cases);
+    ok &= alloc(reinterpret_cast<void **>(&c->d_state), sizeof(CaseState) * n_cases);
+    ok &= alloc(reinterpret_cast<void **>(&c->d_scratch), sizeof(StepScratch));
+    ok &= alloc(reinterpret_cast<void **>(&c->d_err), sizeof(int));
+    ok &= alloc(reinterpret_cast<void **>(&c->d_tables), sizeof(int32_t) * 7 * (n_cases + 1));
+    ok &= alloc(reinterpret_cast<void **>(&c->d_tmp), sizeof(int32_t) * 2 * n_cases);
+    ok &= alloc(reinterpret_cast<void **>(&c->d_pbases), sizeof(int64_t) * n_cases);
+    for (auto &side : c->buf)
+        for (void *&p : side)
+            ok &= alloc(&p, esz * slot);
+    ok &= alloc(reinterpret_cast<void **>(&c->key), sizeof(uint32_t) * slot);
+    int32_t **cell_arrays[] = {&c->cells.n_in, &c->cells.n_o, &c->cells.o_fill, &c->cells.fin,
+                               &c->cells.ostart, &c->cells.base_in, &c->cells.start[0],
+                               &c->cells.start[1]};
+    for (auto pp : cell_arrays)
+        ok &= alloc(reinterpret_cast<void **>(pp), sizeof(int32_t) * cell);
+    ok &= alloc(reinterpret_cast<void **>(&c->cells.acc), sizeof(double) * ACC_COUNT * cell);
+    c->cells.acc_stride = cell;
+    ok &= alloc(reinterpret_cast<void **>(&c->tile_in), sizeof(int32_t) * max_tiles);
+    ok &= alloc(reinterpret_cast<void **>(&c->tile_prefix), sizeof(int32_t) * max_tiles);
+    const size_t chain = static_cast<size_t>(std::max(max_tiles, cell_tiles)) + 1;
+    c->lb_words = 4 * chain;
+    ok &= alloc(reinterpret_cast<void **>(&c->lb), sizeof(uint64_t) * c->lb_words);
+    ok &= alloc(reinterpret_cast<void **>(&c->hole_pos), sizeof(int32_t) * slot);
+    ok &= alloc(reinterpret_cast<void **>(&c->hole_oc), sizeof(int32_t) * slot);
+    // Appends per step and case: out-of-range moved slots + injected
+    // survivors (n_old + n_inj <= cap) + refilled holes (<= n_old): <= 2 cap.
+    ok &= alloc(reinterpret_cast<void **>(&c->obuf), sizeof(uint32_t) * 2 * slot);
+    ok &= alloc(reinterpret_cast<void **>(&c->olist), sizeof(int32_t) * slot);
+    if (!ok) {
+        free_ctx(c);
+        return DSMC_ERR_CUDA;
+    }
+    int32_t *t = c->d_tables;
+    const int w = n_cases + 1;
+    c->tt = TileTables{t, t + w, t + 2 * w, t + 3 * w, t + 4 * w, t + 5 * w, t + 6 * w};
+    auto fail = [&]() {
+        free_ctx(c);
+        return DSMC_ERR_CUDA;
+    };
+    if (cudaMemcpy(c->d_cases, c->hcases.data(), sizeof(CaseDev) * n_cases,
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->tt.cell0, cell0.data(), sizeof(int32_t) * w, cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(c->tt.cblock0, cblock0.data(), sizeof(int32_t) * w, cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(c->tt.cellbase, cellbase.data(), sizeof(int32_t) * w,
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_pbases, pbases.data(), sizeof(int64_t) * n_cases,
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail();
+    if (cudaMemset(c->d_state, 0, sizeof(CaseState) * n_cases) != cudaSuccess ||
+        cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->cells.n_in, 0, sizeof(int32_t) * cell) != cudaSuccess ||
+        cudaMemset(c->cells.n_o, 0, sizeof(int32_t) * cell) != cudaSuccess ||
+        cudaMemset(c->cells.o_fill, 0, sizeof(int32_t) * cell) != cudaSuccess ||
+        cudaMemset(c->cells.start[0], 0, sizeof(int32_t) * cell) != cudaSuccess ||
+        cudaMemset(c->cells.start[1], 0, sizeof(int32_t) * cell) != cudaSuccess ||
+        cudaMemset(c->cells.acc, 0, sizeof(double) * ACC_COUNT * cell) != cudaSuccess)
+        return fail();
+    const int g = c->precision == DSMC_FP32 ? occupancy_grids<float>(c) : occupancy_grids<double>(c);
+    if (g)
+        return fail();
+    *out = c;
+    return DSMC_OK;
+}
+
+int dsmc_ctx_destroy(dsmc_ctx *ctx)
+{
+    if (ctx == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    cudaStreamSynchronize(ctx->stream);
+    free_ctx(ctx);
+    return DSMC_OK;
+}
+
+int dsmc_init_cold(dsmc_ctx *c)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    CK(cudaMemsetAsync(c->d_state, 0, sizeof(CaseState) * c->ncase, c->stream));
+    CK(cudaMemsetAsync(c->cells.acc, 0, sizeof(double) * ACC_COUNT * c->total_cells, c->stream));
+    CK(cudaMemsetAsync(c->cells.start[c->cur], 0, sizeof(int32_t) * c->total_cells, c->stream));
+    int s;
+    if (c->precision == DSMC_FP32) {
+        if ((s = enqueue_move<float>(c, 1)) || (s = enqueue_boundary<float>(c)) ||
+            (s = enqueue_index<float>(c)))
+            return s;
+    } else {
+        if ((s = enqueue_move<double>(c, 1)) || (s = enqueue_boundary<double>(c)) ||
+            (s = enqueue_index<double>(c)))
+            return s;
+    }
+    if ((s = enqueue_finish(c, 1, 0, 0)))
+        return s;
+    c->initialized = true;
+    c->stage = 0;
+    return DSMC_OK;
+}
+
+int dsmc_step(dsmc_ctx *c, int n_steps)
+{
+    if (c == nullptr || n_steps < 0)
+        return DSMC_ERR_ARGUMENT;
+    if (!c->initialized || c->stage != 0)
+        return DSMC_ERR_STATE;
+    if (c->profiling) {
+        for (int i = 0; i < n_steps; ++i) {
+            const int s = dispatch_step(c);
+            if (s)
+                return s;
+        }
+        return DSMC_OK;
+    }
+    if (c->graph[0] == nullptr) {
+        const int s = build_graphs(c);
+        if (s)
+            return s;
+    }
+    for (int i = 0; i < n_steps; ++i) {
+        CK(cudaGraphLaunch(c->graph[c->cur], c->stream));
+        c->cur ^= 1;
+    }
+    return DSMC_OK;
+}
+
+#define STAGE_DISPATCH(fn, ...)                                                   \
+    (c->precision == DSMC_FP32 ? fn<float>(__VA_ARGS__) : fn<double>(__VA_ARGS__))
+
+int dsmc_stage_move(dsmc_ctx *c)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (!c->initialized || c->stage != 0)
+        return DSMC_ERR_STATE;
+    const int s = STAGE_DISPATCH(enqueue_move, c, 0);
+    c->stage = s ? c->stage : 1;
+    c->sampled = false;
+    return s;
+}
+
+int dsmc_stage_boundary(dsmc_ctx *c)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 1)
+        return DSMC_ERR_STATE;
+    const int s = STAGE_DISPATCH(enqueue_boundary, c);
+    c->stage = s ? c->stage : 2;
+    return s;
+}
+
+int dsmc_stage_index(dsmc_ctx *c)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 2)
+        return DSMC_ERR_STATE;
+    const int s = STAGE_DISPATCH(enqueue_index, c);
+    c->stage = s ? c->stage : 3;
+    return s;
+}
+
+int dsmc_stage_collide(dsmc_ctx *c)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 3)
+        return DSMC_ERR_STATE;
+    const int s = STAGE_DISPATCH(enqueue_collide, c, 1, 0);
+    c->stage = s ? c->stage : 4;
+    return s;
+}
+
+int dsmc_stage_sample(dsmc_ctx *c)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 4)
+        return DSMC_ERR_STATE;
+    const int s = STAGE_DISPATCH(enqueue_collide, c, 0, 1);
+    c->stage = s ? c->stage : 5;
+    c->sampled = s == 0;
+    return s;
+}
+
+int dsmc_stage_end_step(dsmc_ctx *c)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage < 3)
+        return DSMC_ERR_STATE;
+    const int s = enqueue_finish(c, 0, c->sampled ? 1 : 0, 1);
+    if (s == 0)
+        c->stage = 0;
+    return s;
+}
+
+int dsmc_synchronize(dsmc_ctx *c)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    return device_error(c);
+}
+
+int dsmc_get_counters(dsmc_ctx *c, int i, dsmc_counters *out)
+{
+    if (c == nullptr || out == nullptr || i < 0 || i >= c->ncase)
+        return DSMC_ERR_ARGUMENT;
+    std::vector<CaseState> st;
+    const int s = read_state(c, st);
+    if (s)
+        return s;
+    const CaseState &x = st[i];
+    // After BoundaryConditions the valid slots are the survivors [0, K).
+    out->np = c->stage >= 2 ? x.n_keep : x.n_old;
+    out->step = x.step;
+    out->sample_step = x.sample_step;
+    out->collisions_last_step = c->stage >= 4 ? x.nc_step : x.nc_last;
+    out->collisions_total = x.nc_total;
+    out->drag_collision_count = static_cast<int64_t>(x.drag_count);
+    out->particle_steps = x.particle_steps;
+    out->drag_impulse_total = x.drag_impulse;
+    out->time = x.time;
+    out->sample_time = x.sample_time;
+    out->drag_sampling_time = x.drag_time;
+    return DSMC_OK;
+}
+
+int dsmc_get_fields_device(dsmc_ctx *c, int i, double *device_out)
+{
+    if (c == nullptr || device_out == nullptr || i < 0 || i >= c->ncase)
+        return DSMC_ERR_ARGUMENT;
+    const CaseDev &cd = c->hcases[i];
+    k_fields_out<<<std::max(1, std::min(1024, (cd.ncell + 255) / 256)), 256, 0, c->stream>>>(
+        c->cells, cd.cbase, cd.ncell, device_out);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+int dsmc_get_fields(dsmc_ctx *c, int i, dsmc_cell *host_out)
+{
+    if (c == nullptr || host_out == nullptr || i < 0 || i >= c->ncase)
+        return DSMC_ERR_ARGUMENT;
+    const CaseDev &cd = c->hcases[i];
+    double *tmp = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(double) * 17 * cd.ncell, c->stream));
+    int s = dsmc_get_fields_device(c, i, tmp);
+    if (s == 0) {
+        CK(cudaMemcpyAsync(host_out, tmp, sizeof(double) * 17 * cd.ncell, cudaMemcpyDeviceToHost,
+                           c->stream));
+    }
+    CK(cudaFreeAsync(tmp, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return s;
+}
+
+int dsmc_set_fields_device(dsmc_ctx *c, int i, const double *device_in, int64_t sample_step)
+{
+    if (c == nullptr || device_in == nullptr || i < 0 || i >= c->ncase)
+        return DSMC_ERR_ARGUMENT;
+    const CaseDev &cd = c->hcases[i];
+    k_fields_in<<<std::max(1, std::min(1024, (cd.ncell + 255) / 256)), 256, 0, c->stream>>>(
+        c->cells, cd.cbase, cd.ncell, device_in);
+    CK(cudaGetLastError());
+    std::vector<CaseState> st;
+    int s = read_state(c, st);
+    if (s)
+        return s;
+    st[i].sample_step = sample_step;
+    CK(cudaMemcpyAsync(c->d_state + i, &st[i], sizeof(CaseState), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_download_particles(dsmc_ctx *c, int i, double *x, double *y, double *vx, double *vy,
+                            double *vz, int64_t capacity, int64_t *n_out)
+{
+    if (c == nullptr || i < 0 || i >= c->ncase || n_out == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    std::vector<CaseState> st;
+    int s = read_state(c, st);
+    if (s)
+        return s;
+    // Valid slots: [0, n_old) at rest and after MoveParticles, the survivors
+    // [0, K) from BoundaryConditions on.
+    const int64_t n = c->stage >= 2 ? st[i].n_keep : st[i].n_old;
+    *n_out = n;
+    if (n > capacity)
+        return DSMC_ERR_CAPACITY;
+    if (n == 0)
+        return DSMC_OK;
+    const CaseDev &cd = c->hcases[i];
+    double *tmp = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(double) * 5 * n, c->stream));
+    if (c->precision == DSMC_FP32) {
+        k_download_case<<<std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256)), 256, 0,
+                          c->stream>>>(slots<float>(c, c->cur), cd.pbase, n, tmp);
+    } else {
+        Slots<double> p = slots<double>(c, c->cur);
+        double *dsts[5] = {tmp, tmp + n, tmp + 2 * n, tmp + 3 * n, tmp + 4 * n};
+        double *srcs[5] = {p.x, p.y, p.vx, p.vy, p.vz};
+        for (int k = 0; k < 5; ++k)
+            CK(cudaMemcpyAsync(dsts[k], srcs[k] + cd.pbase, sizeof(double) * n,
+                               cudaMemcpyDeviceToDevice, c->stream));
+    }
+    double *outs[5] = {x, y, vx, vy, vz};
+    for (int k = 0; k < 5; ++k)
+        if (outs[k] != nullptr)
+            CK(cudaMemcpyAsync(outs[k], tmp + k * n, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                               c->stream));
+    CK(cudaFreeAsync(tmp, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_upload_particles(dsmc_ctx *c, int i, const double *x, const double *y, const double *vx,
+                          const double *vy, const double *vz, int64_t n)
+{
+    if (c == nullptr || i < 0 || i >= c->ncase || n < 0 || !x || !y || !vx || !vy || !vz)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 0)
+        return DSMC_ERR_STATE;
+    const CaseDev &cd = c->hcases[i];
+    if (n > cd.cap)
+        return DSMC_ERR_CAPACITY;
+    std::vector<CaseState> st;
+    int s = read_state(c, st);
+    if (s)
+        return s;
+    double *tmp = nullptr;
+    if (n > 0) {
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(double) * 5 * n, c->stream));
+        const double *ins[5] = {x, y, vx, vy, vz};
+        for (int k = 0; k < 5; ++k)
+            CK(cudaMemcpyAsync(tmp + k * n, ins[k], sizeof(double) * n, cudaMemcpyHostToDevice,
+                               c->stream));
+        const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256)));
+        if (c->precision == DSMC_FP32)
+            k_upload_case<float><<<grid, 256, 0, c->stream>>>(tmp, tmp + n, tmp + 2 * n,
+                                                              tmp + 3 * n, tmp + 4 * n, n,
+                                                              slots<float>(c, c->cur), cd.pbase);
+        else
+            k_upload_case<double><<<grid, 256, 0, c->stream>>>(tmp, tmp + n, tmp + 2 * n,
+                                                               tmp + 3 * n, tmp + 4 * n, n,
+                                                               slots<double>(c, c->cur), cd.pbase);
+        CK(cudaGetLastError());
+    }
+    st[i].n_old = n;
+    CK(cudaMemcpyAsync(c->d_state + i, &st[i], sizeof(CaseState), cudaMemcpyHostToDevice,
+                       c->stream));
+    s = c->precision == DSMC_FP32 ? resort_all<float>(c) : resort_all<double>(c);
+    if (tmp)
+        CK(cudaFreeAsync(tmp, c->stream));
+    if (s)
+        return s;
+    CK(cudaStreamSynchronize(c->stream));
+    c->initialized = true;
+    return device_error(c);
+}
+
+int dsmc_get_cell_starts(dsmc_ctx *c, int i, int32_t *host_out)
+{
+    if (c == nullptr || host_out == nullptr || i < 0 || i >= c->ncase)
+        return DSMC_ERR_ARGUMENT;
+    const CaseDev &cd = c->hcases[i];
+    CK(cudaMemcpyAsync(host_out, c->cells.start[c->cur] + cd.cbase,
+                       sizeof(int32_t) * (cd.ncell + 1), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
+int dsmc_set_profiling(dsmc_ctx *c, int enabled)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    int s = resolve_timings(c);
+    if (s)
+        return s;
+    c->profiling = enabled != 0;
+    for (int k = 0; k < KID_COUNT; ++k) {
+        c->kernel_ms[k] = 0.0;
+        c->kernel_launches[k] = 0;
+    }
+    return DSMC_OK;
+}
+
+int dsmc_get_kernel_times(dsmc_ctx *c, double *ms_out, int64_t *launches_out, int max_kernels,
+                          int *n_kernels, const char **names_out)
+{
+    if (c == nullptr || n_kernels == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    const int s = resolve_timings(c);
+    if (s)
+        return s;
+    *n_kernels = KID_COUNT;
+    for (int k = 0; k < KID_COUNT && k < max_kernels; ++k) {
+        if (ms_out)
+            ms_out[k] = c->kernel_ms[k];
+        if (launches_out)
+            launches_out[k] = c->kernel_launches[k];
+        if (names_out)
+            names_out[k] = kKernelNames[k];
+    }
+    return DSMC_OK;
+}
+
+int dsmc_k_intersect(const dsmc_params *p, int64_t n, const double *x, const double *y,
+                     const double *dx, const double *dy, int32_t *hit, double *t_hit, double *nx,
+                     double *ny, void *cuda_stream)
+{
+    if (p == nullptr || n < 0)
+        return DSMC_ERR_ARGUMENT;
+    dsmc_derived d;
+    const int s = dsmc_setup(p, &d);
+    if (s)
+        return s;
+    if (n == 0)
+        return DSMC_OK;
+    const CaseDev c = make_case(*p, d);
+    const int grid = static_cast<int>(std::min<int64_t>(4096, (n + 255) / 256));
+    k_unit_intersect<<<grid, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(c, n, x, y, dx, dy,
+                                                                               hit, t_hit, nx, ny);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+int dsmc_k_scatter(const dsmc_params *p, const dsmc_derived *d, int64_t n, double *v,
+                   const double *nx, const double *ny, uint32_t kind, uint32_t step,
+                   const uint32_t *entity, void *cuda_stream)
+{
+    if (p == nullptr || n < 0)
+        return DSMC_ERR_ARGUMENT;
+    dsmc_derived dd;
+    const int s = dsmc_setup(p, &dd);
+    if (s)
+        return s;
+    if (d != nullptr)
+        dd = *d;
+    if (n == 0)
+        return DSMC_OK;
+    const CaseDev c = make_case(*p, dd);
+    const int grid = static_cast<int>(std::min<int64_t>(4096, (n + 255) / 256));
+    k_unit_scatter<<<grid, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(c, n, v, nx, ny, kind,
+                                                                             step, entity);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+} // extern "C"

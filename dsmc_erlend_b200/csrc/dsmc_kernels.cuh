@@ -1,0 +1,1011 @@
+// dsmc_kernels.cuh - the kernels of one DSMC time step.
+//
+// A step over all cases of a context is this fixed launch sequence (every
+// size lives on the device, so the sequence is captured once in a CUDA graph):
+//
+//   k_plan      1 CTA    per case: sampling mode, inflow counts (the count
+//                        draws of GenerateNewParticles), tile tables
+//   k_move      tiles    MoveParticles + the new cell of every slot, removal
+//                        flag, in-range flag, per-cell counts, hole list
+//   k_inject    tiles    GenerateNewParticles for the four strips, appended
+//   k_plan2     1 CTA    survivors K, hole count H, tail tiles
+//   k_tail      tiles    swap-with-last: alive tail slots refill the holes
+//   k_cell_scan tiles    per-cell offsets (stable counting sort)
+//   k_tile_scan 1 CTA/case  prefix of in-range counts per tile
+//   k_olist     grid     lists of the particles that changed cell
+//   k_cell_fix  grid     orders those lists, places them, per-cell bases
+//   k_scatter   tiles    places every in-range particle
+//   k_collide   cells    NTC collisions and moment sampling, one thread/cell
+//   k_finish    1 CTA    Step++, NP = K
+//
+// Particle order contract (the reference's, made parallel):
+//   * at the start of a step slots [0, n_old) are sorted by cell, each cell
+//     keeping the order its particles had before the sort;
+//   * injected particles are appended in strip order L, R, B, T;
+//   * removal is the reference's swap-with-last loop (Boundary.cpp:181-202):
+//     survivors below K stay, and the m-th removed slot below K receives the
+//     m-th survivor at or above K counted from the end;
+//   * Indexing's lists are stable in slot order (Geometry.cpp:168), so the
+//     sort is a stable counting sort by cell.
+#pragma once
+
+#include <cstdint>
+
+#include "dsmc_device.cuh"
+#include "dsmc_scan.cuh"
+
+namespace dsmc {
+
+// Tile bases of every case for each tiled kernel: entry i is the first
+// global tile of case i, entry ncase the total.  The last three are static:
+// cell-scan tiles, collide blocks and global cell ids (ncell + 1 per case).
+struct TileTables {
+    int32_t *move0, *inject0, *tail0, *scatter0, *cell0, *cblock0, *cellbase;
+};
+
+// Particle arrays of one buffer.
+template <class T> struct Slots {
+    T *x, *y, *vx, *vy, *vz;
+};
+
+// Per-cell arrays, indexed by global cell id (each case owns ncell + 1 ids).
+struct Cells {
+    int32_t *n_in, *n_o, *o_fill;
+    int32_t *fin, *ostart, *base_in;
+    int32_t *start[2];   // cell start offsets, ping-pong: old and new
+    double *acc;         // 14 moment sums per cell, one array per moment
+    int64_t acc_stride;  // elements per moment array
+};
+
+// Moments kept per cell.  The reference's CELL (include/Cell.h:4-10) holds
+// CountVV as a 3x3 tensor; it is symmetric and stored once here.
+enum : int {
+    ACC_NP = 0,
+    ACC_V0, ACC_V1, ACC_V2,
+    ACC_VV00, ACC_VV01, ACC_VV02, ACC_VV11, ACC_VV12, ACC_VV22,
+    ACC_V2V0, ACC_V2V1, ACC_V2V2,
+    ACC_NC,
+    ACC_COUNT
+};
+
+__device__ __forceinline__ int case_of(const int32_t *base, int ncase, int t)
+{
+    int lo = 0, hi = ncase - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (base[mid] <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Exclusive scan over cases of one count per case (<= 1024 threads, any
+// number of cases); writes base[0..ncase] and returns nothing.
+__device__ __forceinline__ void case_scan(int32_t *base, const int32_t *count_of_case_smem,
+                                          int ncase)
+{
+    // Single-thread scan: the number of cases is at most a few thousand and
+    // this runs once per step in a 1-CTA kernel.
+    if (threadIdx.x == 0) {
+        int32_t run = 0;
+        for (int i = 0; i < ncase; ++i) {
+            base[i] = run;
+            run += count_of_case_smem[i];
+        }
+        base[ncase] = run;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_plan: start of a step (or of the cold start when init_mode is set).
+// ---------------------------------------------------------------------------
+__global__ void k_plan(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
+                       int32_t *tmp, int ncase, int init_mode, int *err)
+{
+    for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
+        const CaseDev &c = cases[i];
+        CaseState &s = st[i];
+        if (init_mode) {
+            s.n_old = 0;
+            s.sampling_mode = 0;
+        } else {
+            // Simulation.cpp:139-146
+            s.sampling_mode =
+                (s.step > c.first_sampling_step && s.step % c.sampling_period == 0) ? 1 : 0;
+            if (s.step > c.first_sampling_step)
+                s.drag_time += c.dt;
+        }
+        // The count draws of GenerateNewParticles (Boundary.cpp:62-71).
+        const int s0 = init_mode ? 4 : 0;
+        const int s1 = init_mode ? 5 : 4;
+        int64_t total = 0;
+        for (int k = 0; k < 5; ++k) {
+            s.inj_count[k] = 0;
+            s.inj_c0[k] = 0;
+        }
+        for (int k = s0; k < s1; ++k) {
+            dsmc_stream r;
+            if (init_mode)
+                open_stream(r, c, DSMC_RNG_INIT, 0, 0);
+            else
+                open_stream(r, c, DSMC_RNG_INJECT, s.step, static_cast<uint32_t>(k));
+            const double navg = c.strip_navg[k];
+            int n, draws;
+            if (navg > 20.0) {
+                n = static_cast<int>(navg);
+                if (uniform(r) < navg - n)
+                    n++;
+                draws = 1;
+            } else {
+                n = irand_poisson(r, navg, &draws);
+            }
+            s.inj_count[k] = n;
+            s.inj_c0[k] = draws;
+            total += n;
+        }
+        if (s.n_old + total > c.cap) {
+            // Boundary.cpp:73-80 exits; the step injects nothing and reports.
+            report_error(err, DSMC_ERR_CAPACITY);
+            for (int k = 0; k < 5; ++k)
+                s.inj_count[k] = 0;
+            total = 0;
+        }
+        s.inj_off[0] = 0;
+        for (int k = 0; k < 5; ++k)
+            s.inj_off[k + 1] = s.inj_off[k] + s.inj_count[k];
+        s.n_total = s.n_old + total;
+        s.dead_old = 0;
+        s.dead_total = 0;
+        s.nc_step = 0;
+        s.n_move_tiles = static_cast<int32_t>((s.n_old + TILE - 1) / TILE);
+        s.n_inject_tiles = static_cast<int32_t>((total + TILE - 1) / TILE);
+        tmp[i] = s.n_move_tiles;
+        tmp[ncase + i] = s.n_inject_tiles;
+    }
+    __syncthreads();
+    case_scan(tt.move0, tmp, ncase);
+    __syncthreads();
+    case_scan(tt.inject0, tmp + ncase, ncase);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sc->total_move_tiles = tt.move0[ncase];
+        sc->total_inject_tiles = tt.inject0[ncase];
+        sc->init_mode = init_mode;
+    }
+    for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
+        st[i].move_tile0 = tt.move0[i];
+        st[i].inject_tile0 = tt.inject0[i];
+    }
+}
+
+// The impact branch of MoveParticles (Boundary.cpp:301-326) for slot q (global
+// slot g): wall interaction drawn from the slot's stream, new velocity stored,
+// post-impact position returned; the result is the drag impulse of the hit.
+// Kept out of line: impacts are rare and the transcendental code would
+// otherwise set the register budget of the whole move loop.
+template <class T>
+__device__ __noinline__ double wall_hit(const CaseDev &c, int64_t step, int64_t q, int64_t g,
+                                        Slots<T> p, double x0, double y0, double dx, double dy,
+                                        double t_hit, double nx, double ny, T &xn, T &yn)
+{
+    const double x_hit = x0 + t_hit * dx;
+    const double y_hit = y0 + t_hit * dy;
+    double v[3] = {static_cast<double>(p.vx[g]), static_cast<double>(p.vy[g]),
+                   static_cast<double>(p.vz[g])};
+    const double vx_in = v[0];
+    dsmc_stream r;
+    open_stream(r, c, DSMC_RNG_MOVE, step, static_cast<uint32_t>(q));
+    wall_interaction(r, c, v, nx, ny);
+    p.vx[g] = Store<T>::rn(v[0]);
+    p.vy[g] = Store<T>::rn(v[1]);
+    p.vz[g] = Store<T>::rn(v[2]);
+    const double remaining = c.dt * (1.0 - t_hit);
+    constexpr double epsilon = 1e-12;
+    xn = round_out<T>(x_hit + remaining * v[0] + epsilon * nx, nx);
+    yn = round_out<T>(y_hit + remaining * v[1] + epsilon * ny, ny);
+    return c.drag_scale * (vx_in - v[0]);
+}
+
+// ---------------------------------------------------------------------------
+// k_move: MoveParticles (Boundary.cpp:284-328) over the sorted slots, plus the
+// per-slot bookkeeping of BoundaryConditions' removal and of Indexing.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS, 2)
+    k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+           Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
+           uint64_t *lb, int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc,
+           uint32_t *__restrict__ obuf, int ncase, int *err)
+{
+    __shared__ int s_tile;
+    __shared__ uint64_t s_excl;
+    __shared__ int32_t s_oc[TILE]; // old cell of removed slots, for the hole list
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_tile = static_cast<int>(atomicAdd(&sc->move_ticket, 1u));
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= sc->total_move_tiles)
+            return;
+        const int ci = case_of(tt.move0, ncase, t);
+        const CaseDev &c = cases[ci];
+        const int64_t n_old = st[ci].n_old;
+        const int64_t step = st[ci].step;
+        const int local_tile = t - tt.move0[ci];
+        // Each thread owns TILE_VEC consecutive slots, so ranks within the
+        // tile follow slot order.
+        const int64_t q0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
+        const int64_t g0 = c.pbase + q0;
+
+        int n_dead = 0, n_in = 0, n_hit = 0;
+        unsigned dead_mask = 0;
+        double impulse = 0.0;
+        T cx{}, cy{}, cvx{}, cvy{};
+        if (q0 < n_old) {
+            cx = p.x[g0];
+            cy = p.y[g0];
+            cvx = p.vx[g0];
+            cvy = p.vy[g0];
+        }
+#pragma unroll 1
+        for (int k = 0; k < TILE_VEC; ++k) {
+            const int64_t q = q0 + k;
+            const bool valid = q < n_old;
+            // Prefetch the next slot while this one is computed.
+            T nx_{}, ny_{}, nvx{}, nvy{};
+            if (k + 1 < TILE_VEC && q + 1 < n_old) {
+                nx_ = p.x[g0 + k + 1];
+                ny_ = p.y[g0 + k + 1];
+                nvx = p.vx[g0 + k + 1];
+                nvy = p.vy[g0 + k + 1];
+            }
+            uint32_t kk = KEY_DEAD;
+            if (valid) {
+                const double x0 = static_cast<double>(cx);
+                const double y0 = static_cast<double>(cy);
+                const int32_t oc = cell_of(c, x0, y0);
+                const double dx = c.dt * static_cast<double>(cvx);
+                const double dy = c.dt * static_cast<double>(cvy);
+                const double xe = x0 + dx;
+                const double ye = y0 + dy;
+                double t_hit, nx, ny;
+                T xn, yn;
+                if (may_hit_box(c, x0, y0, xe, ye) &&
+                    intersect_box(c, x0, y0, dx, dy, t_hit, nx, ny)) {
+                    impulse += wall_hit<T>(c, step, q, g0 + k, p, x0, y0, dx, dy, t_hit, nx, ny,
+                                           xn, yn);
+                    n_hit++;
+                } else {
+                    xn = Store<T>::rn(xe);
+                    yn = Store<T>::rn(ye);
+                    keep_outside<T>(c, xn, yn);
+                }
+                p.x[g0 + k] = xn;
+                p.y[g0 + k] = yn;
+                const double xd = static_cast<double>(xn);
+                const double yd = static_cast<double>(yn);
+                if (outside_domain(c, xd, yd)) {
+                    dead_mask |= 1u << k;
+                    s_oc[threadIdx.x * TILE_VEC + k] = oc < 0 ? NO_CELL : c.cbase + oc;
+                } else {
+                    const int32_t nc = cell_of(c, xd, yd);
+                    if (nc < 0) {
+                        // Inside the domain bounds but in no cell (rounding,
+                        // NaN): the reference aborts in ExchangeParticles, 30.
+                        report_error(err, DSMC_ERR_EXCHANGE);
+                        dead_mask |= 1u << k;
+                        s_oc[threadIdx.x * TILE_VEC + k] = NO_CELL;
+                    } else {
+                        kk = static_cast<uint32_t>(c.cbase + nc) | (nc == oc ? KEY_IN : 0u);
+                    }
+                }
+                key[g0 + k] = kk;
+            }
+            // Per-cell counts and the list of particles that changed cell.
+            const bool alive = kk != KEY_DEAD;
+            const bool in = alive && (kk & KEY_IN);
+            const bool out = alive && !in;
+            const int32_t cg = static_cast<int32_t>(kk & KEY_CELL);
+            n_in += in ? 1 : 0;
+            warp_aggregated_inc(cells.n_in, cg, in);
+            warp_aggregated_inc(cells.n_o, cg, out);
+            const unsigned m = __ballot_sync(0xffffffffu, out);
+            if (m) {
+                uint32_t base = 0;
+                if (lane == __ffs(m) - 1)
+                    base = atomicAdd(&sc->obuf_count, static_cast<uint32_t>(__popc(m)));
+                base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+                if (out)
+                    obuf[base + __popc(m & ((1u << lane) - 1u))] =
+                        static_cast<uint32_t>(g0 + k);
+            }
+            cx = nx_;
+            cy = ny_;
+            cvx = nvx;
+            cvy = nvy;
+        }
+        n_dead = __popc(dead_mask);
+        // Wall-hit diagnostics (Boundary.cpp:318-319).
+        {
+            double imp = impulse;
+            int hits = n_hit;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                imp += __shfl_xor_sync(0xffffffffu, imp, o);
+                hits += __shfl_xor_sync(0xffffffffu, hits, o);
+            }
+            if (lane == 0 && hits > 0) {
+                atomicAdd(&st[ci].drag_impulse, imp);
+                atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(hits));
+            }
+        }
+        // Tile totals: in-range count, and the removed-slot ranks (hole list).
+        int in_total;
+        (void)block_exclusive<int>(n_in, in_total);
+        int dead_total;
+        const int dead_excl = block_exclusive<int>(n_dead, dead_total);
+        if (threadIdx.x == 0) {
+            tile_in[t] = in_total;
+            const uint64_t excl = lookback(lb, t, local_tile == 0, dead_total, err);
+            s_excl = excl;
+            if (local_tile == st[ci].n_move_tiles - 1)
+                st[ci].dead_old = static_cast<int64_t>(excl) + dead_total;
+        }
+        __syncthreads();
+        int64_t rank = static_cast<int64_t>(s_excl) + dead_excl;
+        for (int k = 0; k < TILE_VEC; ++k) {
+            if (dead_mask & (1u << k)) {
+                hole_pos[c.pbase + rank] = static_cast<int32_t>(q0 + k);
+                hole_oc[c.pbase + rank] = s_oc[threadIdx.x * TILE_VEC + k];
+                ++rank;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_inject: GenerateNewParticles (Boundary.cpp:60-92) for every strip of every
+// case, written after the case's n_old slots.  In init mode the single strip
+// is the cold-start fill of InitialConditions (Initialization.cpp:302-310),
+// without the pre-move, and the removal predicate is InsideBox
+// (RemoveParticlesInsideBox, Geometry.cpp:231-247).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_inject(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+             Slots<T> p, uint32_t *__restrict__ key, Cells cells, uint64_t *lb,
+             int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc,
+             uint32_t *__restrict__ obuf, int ncase, int *err)
+{
+    __shared__ int s_tile;
+    __shared__ uint64_t s_excl;
+    const int init_mode = sc->init_mode;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_tile = static_cast<int>(atomicAdd(&sc->inject_ticket, 1u));
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= sc->total_inject_tiles)
+            return;
+        const int ci = case_of(tt.inject0, ncase, t);
+        const CaseDev &c = cases[ci];
+        const CaseState &s = st[ci];
+        const int64_t n_inj = s.inj_off[5];
+        const int local_tile = t - tt.inject0[ci];
+        const int64_t j0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
+        uint32_t keys[TILE_VEC];
+        int n_dead = 0;
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            keys[k] = KEY_DEAD;
+            const int64_t j = j0 + k;
+            if (j >= n_inj)
+                continue;
+            int strip = 0;
+            while (strip < 4 && j >= s.inj_off[strip + 1])
+                ++strip;
+            const int64_t js = j - s.inj_off[strip];
+            dsmc_stream r;
+            if (init_mode)
+                open_stream(r, c, DSMC_RNG_INIT, 0, 0);
+            else
+                open_stream(r, c, DSMC_RNG_INJECT, s.step, static_cast<uint32_t>(strip));
+            dsmc_stream_seek(&r, static_cast<uint64_t>(s.inj_c0[strip]) + 8ull * js);
+            const double *b = c.strip[strip];
+            // v2rand_uniform_rect (Boundary.cpp:44-47) and vrand_MB (:52-57).
+            double x = b[0] + (b[2] - b[0]) * uniform(r);
+            double y = b[1] + (b[3] - b[1]) * uniform(r);
+            const double vx = frand_gaussian(r, c.ux_free, c.rt_free);
+            const double vy = frand_gaussian(r, c.uy_free, c.rt_free);
+            const double vz = frand_gaussian(r, 0.0, c.rt_free);
+            if (!init_mode) {
+                x += c.dt * vx;
+                y += c.dt * vy;
+            }
+            const T xs = Store<T>::rn(x), ys = Store<T>::rn(y);
+            const int64_t q = s.n_old + j;
+            const int64_t g = c.pbase + q;
+            p.x[g] = xs;
+            p.y[g] = ys;
+            p.vx[g] = Store<T>::rn(vx);
+            p.vy[g] = Store<T>::rn(vy);
+            p.vz[g] = Store<T>::rn(vz);
+            const double xd = static_cast<double>(xs), yd = static_cast<double>(ys);
+            const bool dead = init_mode ? inside_box(c, xd, yd) : outside_domain(c, xd, yd);
+            if (dead) {
+                n_dead++;
+            } else {
+                const int32_t nc = cell_of(c, xd, yd);
+                if (nc < 0) {
+                    report_error(err, DSMC_ERR_EXCHANGE);
+                    n_dead++;
+                } else {
+                    keys[k] = static_cast<uint32_t>(c.cbase + nc);
+                }
+            }
+            key[g] = keys[k];
+        }
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            const bool alive = keys[k] != KEY_DEAD;
+            const int32_t cg = static_cast<int32_t>(keys[k] & KEY_CELL);
+            warp_aggregated_inc(cells.n_o, cg, alive);
+            const unsigned m = __ballot_sync(0xffffffffu, alive);
+            if (m) {
+                const int lane = threadIdx.x & 31;
+                uint32_t base = 0;
+                if (lane == __ffs(m) - 1)
+                    base = atomicAdd(&sc->obuf_count, static_cast<uint32_t>(__popc(m)));
+                base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+                if (alive)
+                    obuf[base + __popc(m & ((1u << lane) - 1u))] =
+                        static_cast<uint32_t>(c.pbase + s.n_old + j0 + k);
+            }
+        }
+        int dead_total;
+        const int dead_excl = block_exclusive<int>(n_dead, dead_total);
+        if (threadIdx.x == 0) {
+            // The chain of this case continues the removed count of its
+            // moved slots: the first inject tile starts at dead_old.
+            const bool first = local_tile == 0;
+            const uint64_t agg = static_cast<uint64_t>(dead_total) +
+                                 (first ? static_cast<uint64_t>(s.dead_old) : 0ull);
+            const uint64_t excl = lookback(lb, t, first, agg, err);
+            s_excl = first ? static_cast<uint64_t>(s.dead_old) : excl;
+            if (local_tile == s.n_inject_tiles - 1)
+                st[ci].dead_total = static_cast<int64_t>(excl + agg);
+        }
+        __syncthreads();
+        int64_t rank = static_cast<int64_t>(s_excl) + dead_excl;
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            if (j0 + k < n_inj && keys[k] == KEY_DEAD) {
+                hole_pos[c.pbase + rank] = static_cast<int32_t>(s.n_old + j0 + k);
+                hole_oc[c.pbase + rank] = NO_CELL;
+                ++rank;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_plan2: survivors, holes and the tail of every case.
+// ---------------------------------------------------------------------------
+__global__ void k_plan2(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
+                        const int32_t *hole_pos, int32_t *tmp, int ncase)
+{
+    for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
+        CaseState &s = st[i];
+        if (s.n_inject_tiles == 0)
+            s.dead_total = s.dead_old;
+        const int64_t keep = s.n_total - s.dead_total;
+        s.n_keep = keep;
+        // Holes are the removed slots below K; the list is in slot order.
+        const int32_t *hp = hole_pos + cases[i].pbase;
+        int64_t lo = 0, hi = s.dead_total;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (hp[mid] < keep)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        s.n_holes = lo;
+        s.n_tail_tiles = static_cast<int32_t>((s.n_total - keep + TILE - 1) / TILE);
+        tmp[i] = s.n_tail_tiles;
+        tmp[ncase + i] = static_cast<int32_t>((keep + TILE - 1) / TILE);
+    }
+    __syncthreads();
+    case_scan(tt.tail0, tmp, ncase);
+    __syncthreads();
+    case_scan(tt.scatter0, tmp + ncase, ncase);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        sc->total_tail_tiles = tt.tail0[ncase];
+    for (int i = threadIdx.x; i < ncase; i += blockDim.x)
+        st[i].tail_tile0 = tt.tail0[i];
+}
+
+// ---------------------------------------------------------------------------
+// k_tail: the swap-with-last removal (Boundary.cpp:181-202) as a permutation.
+// The r-th surviving slot of the tail [K, n_total), counted from its end,
+// moves into the r-th hole.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_tail(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+           Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
+           uint64_t *lb, const int32_t *__restrict__ hole_pos,
+           const int32_t *__restrict__ hole_oc, uint32_t *__restrict__ obuf, int ncase, int *err)
+{
+    __shared__ int s_tile;
+    __shared__ uint64_t s_excl;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_tile = static_cast<int>(atomicAdd(&sc->tail_ticket, 1u));
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= sc->total_tail_tiles)
+            return;
+        const int ci = case_of(tt.tail0, ncase, t);
+        const CaseDev &c = cases[ci];
+        const CaseState &s = st[ci];
+        const int local_tile = t - tt.tail0[ci];
+        const int64_t q0 = s.n_keep + static_cast<int64_t>(local_tile) * TILE +
+                           threadIdx.x * TILE_VEC;
+        uint32_t keys[TILE_VEC];
+        int n_alive = 0;
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            keys[k] = KEY_DEAD;
+            if (q0 + k < s.n_total)
+                keys[k] = key[c.pbase + q0 + k];
+            n_alive += keys[k] != KEY_DEAD ? 1 : 0;
+        }
+        int alive_total;
+        const int alive_excl = block_exclusive<int>(n_alive, alive_total);
+        if (threadIdx.x == 0)
+            s_excl = lookback(lb, t, local_tile == 0, alive_total, err);
+        __syncthreads();
+        int64_t r = static_cast<int64_t>(s_excl) + alive_excl;
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            if (keys[k] == KEY_DEAD)
+                continue;
+            const int64_t m = s.n_holes - 1 - r;
+            ++r;
+            if (m < 0) {
+                report_error(err, DSMC_ERR_STATE);
+                continue;
+            }
+            const int64_t h = hole_pos[c.pbase + m];
+            const int32_t hoc = hole_oc[c.pbase + m];
+            const int32_t cg = static_cast<int32_t>(keys[k] & KEY_CELL);
+            const bool was_in = (keys[k] & KEY_IN) != 0;
+            const bool now_in = hoc == cg;
+            if (was_in)
+                atomicSub(cells.n_in + cg, 1);
+            else if (now_in)
+                atomicSub(cells.n_o + cg, 1);
+            if (now_in) {
+                atomicAdd(cells.n_in + cg, 1);
+                atomicAdd(tile_in + s.move_tile0 + static_cast<int>(h / TILE), 1);
+            } else {
+                if (was_in)
+                    atomicAdd(cells.n_o + cg, 1);
+                obuf[atomicAdd(&sc->obuf_count, 1u)] = static_cast<uint32_t>(c.pbase + h);
+            }
+            const int64_t gs = c.pbase + q0 + k, gd = c.pbase + h;
+            p.x[gd] = p.x[gs];
+            p.y[gd] = p.y[gs];
+            p.vx[gd] = p.vx[gs];
+            p.vy[gd] = p.vy[gs];
+            p.vz[gd] = p.vz[gs];
+            key[gd] = static_cast<uint32_t>(cg) | (now_in ? KEY_IN : 0u);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_cell_scan: per case, exclusive sums over its cells of the in-range and
+// out-of-range counts (Fin, ostart) and the new cell starts.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_cell_scan(const CaseDev *__restrict__ cases, StepScratch *sc, TileTables tt, Cells cells,
+                int new_side, uint64_t *lb, int ncase, int *err)
+{
+    __shared__ int s_tile;
+    __shared__ uint64_t s_excl;
+    int32_t *start = cells.start[new_side];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_tile = static_cast<int>(atomicAdd(&sc->cell_ticket, 1u));
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= tt.cell0[ncase])
+            return;
+        const int ci = case_of(tt.cell0, ncase, t);
+        const CaseDev &c = cases[ci];
+        const int local_tile = t - tt.cell0[ci];
+        const int c0 = local_tile * TILE + threadIdx.x * TILE_VEC;
+        uint32_t a[TILE_VEC], b[TILE_VEC];
+        uint32_t sa = 0, sb = 0;
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            a[k] = b[k] = 0;
+            if (c0 + k < c.ncell) {
+                a[k] = static_cast<uint32_t>(cells.n_in[c.cbase + c0 + k]);
+                b[k] = static_cast<uint32_t>(cells.n_o[c.cbase + c0 + k]);
+            }
+            sa += a[k];
+            sb += b[k];
+        }
+        unsigned long long tot;
+        const unsigned long long ex =
+            block_exclusive<unsigned long long>(pack2(sa, sb), tot);
+        if (threadIdx.x == 0)
+            s_excl = lookback(lb, t, local_tile == 0, tot, err);
+        __syncthreads();
+        const uint64_t base = s_excl + ex;
+        uint32_t ra = pack2_a(base), rb = pack2_b(base);
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            const int cc = c0 + k;
+            if (cc < c.ncell) {
+                cells.fin[c.cbase + cc] = static_cast<int32_t>(ra);
+                cells.ostart[c.cbase + cc] = static_cast<int32_t>(rb);
+                start[c.cbase + cc] = static_cast<int32_t>(ra + rb);
+            }
+            ra += a[k];
+            rb += b[k];
+            if (cc == c.ncell - 1)
+                start[c.cbase + c.ncell] = static_cast<int32_t>(ra + rb);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_tile_scan: per case (one CTA each), exclusive prefix of the in-range
+// counts of its move tiles, in place into tile_prefix.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_tile_scan(const CaseState *st, const int32_t *tile_in, int32_t *tile_prefix)
+{
+    const CaseState &s = st[blockIdx.x];
+    int32_t carry = 0;
+    for (int b = 0; b < s.n_move_tiles; b += TILE_THREADS) {
+        const int i = b + threadIdx.x;
+        const int v = i < s.n_move_tiles ? tile_in[s.move_tile0 + i] : 0;
+        int tot;
+        const int ex = block_exclusive<int>(v, tot);
+        if (i < s.n_move_tiles)
+            tile_prefix[s.move_tile0 + i] = carry + ex;
+        carry += tot;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_olist: buckets the particles that are not in range (changed cell, were
+// injected, or refilled a hole) into per-cell lists; order is fixed later.
+// ---------------------------------------------------------------------------
+__global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
+                        const StepScratch *sc, const uint32_t *__restrict__ obuf,
+                        const uint32_t *__restrict__ key, Cells cells,
+                        int32_t *__restrict__ olist, const int64_t *__restrict__ pbases,
+                        int ncase, int *err)
+{
+    const uint32_t n = sc->obuf_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const uint32_t g = obuf[i];
+        int lo = 0, hi = ncase - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pbases[mid] <= static_cast<int64_t>(g))
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const int64_t q = static_cast<int64_t>(g) - pbases[lo];
+        if (q >= st[lo].n_keep)
+            continue; // a tail slot that moved into a hole; listed there
+        const uint32_t k = key[g];
+        if (k == KEY_DEAD || (k & KEY_IN))
+            continue;
+        const int32_t cg = static_cast<int32_t>(k & KEY_CELL);
+        const int32_t j = atomicAdd(cells.o_fill + cg, 1);
+        if (j >= cells.n_o[cg]) {
+            report_error(err, DSMC_ERR_STATE); // counts and list disagree
+            continue;
+        }
+        olist[pbases[lo] + cells.ostart[cg] + j] = static_cast<int32_t>(q);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_cell_fix: per cell, orders its out-of-range list by slot, places those
+// particles, and computes the base offset of its in-range particles.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *st,
+                           TileTables tt, Cells cells, int old_side, Slots<T> src, Slots<T> dst,
+                           int32_t *__restrict__ olist, int total_cells, int ncase, int *err)
+{
+    const int32_t *os = cells.start[old_side];
+    const int32_t *ns = cells.start[old_side ^ 1];
+    for (int cg = blockIdx.x * blockDim.x + threadIdx.x; cg < total_cells;
+         cg += gridDim.x * blockDim.x) {
+        const int ci = case_of(tt.cellbase, ncase, cg);
+        const CaseDev &c = cases[ci];
+        const int cl = cg - c.cbase;
+        if (cl >= c.ncell)
+            continue;
+        const int32_t n = cells.n_o[cg];
+        const int32_t ni = cells.n_in[cg];
+        const int32_t start = ns[cg];
+        const int32_t o_lo = os[cg], o_hi = os[cg + 1];
+        int32_t lo = 0;
+        if (n > 0) {
+            int32_t *seg = olist + c.pbase + cells.ostart[cg];
+            // Insertion sort by slot: lists are a few entries long.
+            for (int a = 1; a < n; ++a) {
+                const int32_t v = seg[a];
+                int b = a - 1;
+                while (b >= 0 && seg[b] > v) {
+                    seg[b + 1] = seg[b];
+                    --b;
+                }
+                seg[b + 1] = v;
+            }
+            const int64_t keep = st[ci].n_keep;
+            for (int j = 0; j < n; ++j) {
+                const int32_t q = seg[j];
+                if (q < o_lo)
+                    ++lo;
+                const int64_t fin = start + j + (q >= o_hi ? ni : 0);
+                if (q < 0 || q >= keep || fin < 0 || fin >= keep) {
+                    report_error(err, DSMC_ERR_STATE); // counts and list disagree
+                    continue;
+                }
+                const int64_t gs = c.pbase + q, gd = c.pbase + fin;
+                dst.x[gd] = src.x[gs];
+                dst.y[gd] = src.y[gs];
+                dst.vx[gd] = src.vx[gs];
+                dst.vy[gd] = src.vy[gs];
+                dst.vz[gd] = src.vz[gs];
+            }
+        }
+        cells.base_in[cg] = start + lo - cells.fin[cg];
+        cells.n_in[cg] = 0;
+        cells.n_o[cg] = 0;
+        cells.o_fill[cg] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_scatter: every in-range particle goes to base_in[cell] + (number of
+// in-range particles at lower slots of its case).
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_scatter(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt,
+              Slots<T> src, Slots<T> dst, const uint32_t *__restrict__ key, Cells cells,
+              const int32_t *__restrict__ tile_prefix, int ncase, int *err)
+{
+    const int total = tt.scatter0[ncase];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int ci = case_of(tt.scatter0, ncase, t);
+        const CaseDev &c = cases[ci];
+        const CaseState &s = st[ci];
+        const int local_tile = t - tt.scatter0[ci];
+        const int64_t q0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
+        uint32_t keys[TILE_VEC];
+        int n_in = 0;
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            keys[k] = 0;
+            if (q0 + k < s.n_keep)
+                keys[k] = key[c.pbase + q0 + k];
+            n_in += (keys[k] & KEY_IN) ? 1 : 0;
+        }
+        int tot;
+        const int ex = block_exclusive<int>(n_in, tot);
+        if (tot == 0)
+            continue;
+        int64_t f = tile_prefix[s.move_tile0 + local_tile] + ex;
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            if (!(keys[k] & KEY_IN))
+                continue;
+            const int32_t cg = static_cast<int32_t>(keys[k] & KEY_CELL);
+            const int64_t fin = cells.base_in[cg] + f;
+            ++f;
+            if (fin < 0 || fin >= s.n_keep) {
+                report_error(err, DSMC_ERR_STATE); // counts and keys disagree
+                continue;
+            }
+            const int64_t gd = c.pbase + fin;
+            const int64_t gs = c.pbase + q0 + k;
+            dst.x[gd] = src.x[gs];
+            dst.y[gd] = src.y[gs];
+            dst.vx[gd] = src.vx[gs];
+            dst.vy[gd] = src.vy[gs];
+            dst.vz[gd] = src.vz[gs];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_collide: per cell, BinaryCollisionsInCell (Collision.cpp:21-44) with one
+// stream per cell, then Sampling's accumulation (Sampling.cpp:14-31) in the
+// reference's order: one thread per cell walks its particles sequentially, so
+// every FP64 sum is bit-identical to the reference's.  A CTA stages the
+// velocities of its cells in shared memory when they fit.
+// ---------------------------------------------------------------------------
+constexpr int COLLIDE_CELLS = 128;
+constexpr int COLLIDE_SMEM_PCL = 3072;
+
+template <class T>
+__global__ void __launch_bounds__(COLLIDE_CELLS)
+    k_collide(const CaseDev *__restrict__ cases, CaseState *st, TileTables tt, Slots<T> p,
+              Cells cells, int side, int do_collide, int do_sample, int ncase)
+{
+    extern __shared__ unsigned char smem_raw[];
+    T *sv = reinterpret_cast<T *>(smem_raw);
+    const int32_t *start = cells.start[side];
+    const int nblocks = tt.cblock0[ncase];
+    for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+        const int ci = case_of(tt.cblock0, ncase, b);
+        const CaseDev &c = cases[ci];
+        CaseState &s = st[ci];
+        const int block_local = b - tt.cblock0[ci];
+        const int cl0 = block_local * COLLIDE_CELLS;
+        const int cl1 = min(cl0 + COLLIDE_CELLS, c.ncell);
+        const int64_t r0 = start[c.cbase + cl0], r1 = start[c.cbase + cl1];
+        const int64_t nr = r1 - r0;
+        const bool staged = nr <= COLLIDE_SMEM_PCL;
+        __syncthreads();
+        if (staged) {
+            for (int64_t i = threadIdx.x; i < nr; i += blockDim.x) {
+                sv[i] = p.vx[c.pbase + r0 + i];
+                sv[COLLIDE_SMEM_PCL + i] = p.vy[c.pbase + r0 + i];
+                sv[2 * COLLIDE_SMEM_PCL + i] = p.vz[c.pbase + r0 + i];
+            }
+        }
+        __syncthreads();
+        const int cl = cl0 + threadIdx.x;
+        int ncc = 0;
+        if (cl < cl1) {
+            const int cg = c.cbase + cl;
+            const int64_t a0 = start[cg];
+            const int n = static_cast<int>(start[cg + 1] - a0);
+            // Velocity access: shared memory when staged, else global.
+            auto vel = [&](int i, int m) -> double {
+                if (staged)
+                    return static_cast<double>(sv[m * COLLIDE_SMEM_PCL + (a0 - r0) + i]);
+                const int64_t g = c.pbase + a0 + i;
+                return static_cast<double>(m == 0 ? p.vx[g] : (m == 1 ? p.vy[g] : p.vz[g]));
+            };
+            auto set_vel = [&](int i, double v0, double v1, double v2) {
+                const int64_t g = c.pbase + a0 + i;
+                const T t0 = Store<T>::rn(v0), t1 = Store<T>::rn(v1), t2 = Store<T>::rn(v2);
+                p.vx[g] = t0;
+                p.vy[g] = t1;
+                p.vz[g] = t2;
+                if (staged) {
+                    const int64_t o = (a0 - r0) + i;
+                    sv[o] = t0;
+                    sv[COLLIDE_SMEM_PCL + o] = t1;
+                    sv[2 * COLLIDE_SMEM_PCL + o] = t2;
+                }
+            };
+            if (do_collide && n >= 2) {
+                dsmc_stream r;
+                open_stream(r, c, DSMC_RNG_COLLIDE, s.step, static_cast<uint32_t>(cl));
+                const double npair = 0.5 * n * (n - 1) * c.weight * c.sc_max * c.dt / c.dv;
+                int nn = static_cast<int>(npair);
+                const double frac = npair - nn;
+                nn = (uniform(r) < frac) ? nn + 1 : nn;
+                for (int kk = 0; kk < nn; ++kk) {
+                    const int i = irand_uniform(r, n);
+                    int j;
+                    do {
+                        j = irand_uniform(r, n);
+                    } while (j == i);
+                    const double vi0 = vel(i, 0), vi1 = vel(i, 1), vi2 = vel(i, 2);
+                    const double vj0 = vel(j, 0), vj1 = vel(j, 1), vj2 = vel(j, 2);
+                    const double vr0 = vj0 - vi0, vr1 = vj1 - vi1, vr2 = vj2 - vi2;
+                    const double cr = sqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
+                    const double sigma = c.sigma_ref * pow(c.cr_ref / cr, c.omega);
+                    if (uniform(r) < sigma * cr / c.sc_max) {
+                        // ElasticCollision, Collision.cpp:7-19, with
+                        // v3rand_isotropic (rng/IsotropicVectorRNG.cxx:11-19).
+                        const double cos_t = 1.0 - 2.0 * uniform(r);
+                        const double sin_t = sqrt(1.0 - cos_t * cos_t);
+                        const double e = 2.0 * PI_D * uniform(r);
+                        const double nv[3] = {cos_t, sin_t * cos(e), sin_t * sin(e)};
+                        const double half = cr * 0.5;
+                        const double vc0 = 0.5 * (vj0 + vi0), vc1 = 0.5 * (vj1 + vi1),
+                                     vc2 = 0.5 * (vj2 + vi2);
+                        const double d0 = half * nv[0], d1 = half * nv[1], d2 = half * nv[2];
+                        set_vel(i, vc0 + d0, vc1 + d1, vc2 + d2);
+                        set_vel(j, vc0 - d0, vc1 - d1, vc2 - d2);
+                        ncc++;
+                    }
+                }
+                if (s.sampling_mode == 1 && ncc > 0)
+                    cells.acc[ACC_NC * cells.acc_stride + cg] += ncc;
+            }
+            if (do_sample && s.sampling_mode == 1 && n > 0) {
+                double a[ACC_NC];
+#pragma unroll
+                for (int m = 0; m < ACC_NC; ++m)
+                    a[m] = cells.acc[m * cells.acc_stride + cg];
+                for (int i = 0; i < n; ++i) {
+                    const double v0 = vel(i, 0), v1 = vel(i, 1), v2 = vel(i, 2);
+                    a[ACC_NP] += 1.0;
+                    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
+                    a[ACC_V0] += v0;
+                    a[ACC_V1] += v1;
+                    a[ACC_V2] += v2;
+                    a[ACC_V2V0] += vv * v0;
+                    a[ACC_V2V1] += vv * v1;
+                    a[ACC_V2V2] += vv * v2;
+                    a[ACC_VV00] += v0 * v0;
+                    a[ACC_VV01] += v0 * v1;
+                    a[ACC_VV02] += v0 * v2;
+                    a[ACC_VV11] += v1 * v1;
+                    a[ACC_VV12] += v1 * v2;
+                    a[ACC_VV22] += v2 * v2;
+                }
+#pragma unroll
+                for (int m = 0; m < ACC_NC; ++m)
+                    cells.acc[m * cells.acc_stride + cg] = a[m];
+            }
+        }
+        if (do_collide) {
+            int tot = ncc;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                tot += __shfl_xor_sync(0xffffffffu, tot, o);
+            if ((threadIdx.x & 31) == 0 && tot > 0)
+                atomicAdd(reinterpret_cast<unsigned long long *>(&s.nc_step),
+                          static_cast<unsigned long long>(tot));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_finish: end of the step (Simulation.cpp:160-161), Sampling's counters
+// (Sampling.cpp:17-18) when the step sampled.
+// ---------------------------------------------------------------------------
+__global__ void k_finish(const CaseDev *cases, CaseState *st, int ncase, int init_mode,
+                         int did_sample, int end_step)
+{
+    for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
+        CaseState &s = st[i];
+        s.n_old = s.n_keep;
+        if (init_mode)
+            continue;
+        if (did_sample && s.sampling_mode == 1) {
+            s.sample_step++;
+            s.sample_time += cases[i].dt;
+        }
+        if (end_step) {
+            s.nc_last = s.nc_step;
+            s.nc_total += s.nc_step;
+            s.particle_steps += s.n_keep;
+            s.step++;
+            s.time += cases[i].dt;
+        }
+    }
+}
+
+} // namespace dsmc

@@ -1,0 +1,118 @@
+// dsmc_scan.cuh - block scans and the decoupled look-back chain used by the
+// single-pass kernels (Merrill and Garland, "Single-pass parallel prefix scan
+// with decoupled look-back", 2016).
+#pragma once
+
+#include <cstdint>
+
+#include "dsmc_device.cuh"
+
+namespace dsmc {
+
+// Status word of one tile of a chain: flag in bits 62-63, value below.
+constexpr uint64_t LB_AGG = 1ull << 62;  // tile aggregate published
+constexpr uint64_t LB_INC = 2ull << 62;  // inclusive prefix published
+constexpr uint64_t LB_FLAGS = 3ull << 62;
+constexpr uint64_t LB_VALUE = ~LB_FLAGS;
+
+// Two 31-bit counts packed into one value (for the pair scan of cells).
+__device__ __forceinline__ uint64_t pack2(uint32_t a, uint32_t b)
+{
+    return (static_cast<uint64_t>(a) << 31) | b;
+}
+__device__ __forceinline__ uint32_t pack2_a(uint64_t v) { return static_cast<uint32_t>(v >> 31); }
+__device__ __forceinline__ uint32_t pack2_b(uint64_t v)
+{
+    return static_cast<uint32_t>(v & 0x7FFFFFFFull);
+}
+
+__device__ __forceinline__ void report_error(int *err, int code) { atomicCAS(err, 0, code); }
+
+// Exclusive prefix of `agg` over the earlier tiles of one chain.  Tile
+// `t` is the chain's first when `first` is set.  Called by one thread.  Every
+// wait is bounded: after SPIN_LIMIT polls the chain is abandoned, the error
+// word gets DSMC_ERR_TIMEOUT and the prefix is returned as 0.
+__device__ __forceinline__ uint64_t lookback(uint64_t *status, int t, bool first, uint64_t agg,
+                                            int *err)
+{
+    volatile uint64_t *vs = status;
+    if (first) {
+        __threadfence();
+        vs[t] = LB_INC | agg;
+        return 0;
+    }
+    vs[t] = LB_AGG | agg;
+    __threadfence();
+    uint64_t excl = 0;
+    int j = t - 1;
+    for (;;) {
+        uint64_t w = vs[j];
+        uint32_t spins = 0;
+        while ((w & LB_FLAGS) == 0) {
+            if (++spins > SPIN_LIMIT) {
+                report_error(err, DSMC_ERR_TIMEOUT);
+                vs[t] = LB_INC | agg;
+                return 0;
+            }
+            __nanosleep(64);
+            w = vs[j];
+        }
+        excl += (w & LB_VALUE);
+        if ((w & LB_FLAGS) == LB_INC)
+            break;
+        --j;
+    }
+    __threadfence();
+    vs[t] = LB_INC | (excl + agg);
+    return excl;
+}
+
+// Block-wide exclusive sum over TILE_THREADS threads; also returns the total.
+template <class V> __device__ __forceinline__ V block_exclusive(V v, V &total)
+{
+    __shared__ V warp_tot[TILE_THREADS / 32];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    V inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const V n = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o)
+            inc += n;
+    }
+    if (lane == 31)
+        warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        V w = lane < TILE_THREADS / 32 ? warp_tot[lane] : V(0);
+#pragma unroll
+        for (int o = 1; o < TILE_THREADS / 32; o <<= 1) {
+            const V n = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o)
+                w += n;
+        }
+        if (lane < TILE_THREADS / 32)
+            warp_tot[lane] = w;
+    }
+    __syncthreads();
+    const V warp_excl = warp == 0 ? V(0) : warp_tot[warp - 1];
+    total = warp_tot[TILE_THREADS / 32 - 1];
+    __syncthreads();
+    return warp_excl + inc - v;
+}
+
+// Index of the case that owns tile `t`: the last i with tile0[i] <= t.
+__device__ __forceinline__ int case_of_tile(const int32_t *tile0, int stride, int ncase, int t)
+{
+    int lo = 0, hi = ncase - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile0[mid * stride] <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+} // namespace dsmc

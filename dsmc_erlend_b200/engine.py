@@ -1,0 +1,179 @@
+"""Python surface of the engine, mirroring the reference's stage functions.
+
+    sim = Engine([params])                # Setup()       (Initialization.cpp:210)
+    sim.InitialConditions()               # Initialization.cpp:290
+    for _ in range(n):                    # the loop of Simulation.cpp:138-199
+        sim.step()                        #   Move, Boundary, Index, Collide, Sample
+    cells = sim.GatherGlobalField()       # MPIManager.cpp:305, 17 moments per cell
+    sim.Printing("results")               # Sampling.cpp:36
+
+The stage functions (MoveParticles, BoundaryConditions, Indexing,
+CollideParticles, Sampling, end_step) run the same kernels as step(), one
+stage at a time.  Every call goes through the C ABI of include/dsmc.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import abi
+from ._lib import check, load
+from .abi import Counters, Derived, Params
+
+_D = C.POINTER(C.c_double)
+
+
+def setup(p: Params) -> Derived:
+    """Setup(): derived constants of one case (raises on invalid input)."""
+    d = Derived()
+    check(load().dsmc_setup(C.byref(p), C.byref(d)), "dsmc_setup")
+    return d
+
+
+def write_field(p: Params, d: Derived, sample_step: int, cells: np.ndarray, results_dir: str):
+    """Printing(): DSMC2D_Field.plt/.json under results_dir/<wall>/."""
+    cells = np.ascontiguousarray(cells, dtype=np.float64).reshape(-1, 17)
+    check(load().dsmc_write_field(C.byref(p), C.byref(d), int(sample_step),
+                                  cells.ctypes.data_as(C.c_void_p), str(results_dir).encode()),
+          "dsmc_write_field")
+
+
+class Engine:
+    """One device context holding one or more independent cases."""
+
+    def __init__(self, cases: Params | Sequence[Params], derived: Sequence[Derived] | None = None,
+                 stream: int | None = None):
+        lib = load()
+        if isinstance(cases, Params):
+            cases = [cases]
+        self.params = [p.copy() for p in cases]
+        n = len(self.params)
+        arr = (Params * n)(*self.params)
+        darr = None
+        if derived is not None:
+            darr = (Derived * n)(*derived)
+        h = C.c_void_p()
+        check(lib.dsmc_ctx_create(arr, darr, n, C.c_void_p(stream) if stream else None,
+                                  C.byref(h)), "dsmc_ctx_create")
+        self._h = h
+        self._lib = lib
+        self.derived = list(derived) if derived is not None else [setup(p) for p in self.params]
+        self.n_cases = n
+
+    # -- lifecycle ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.dsmc_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- the time loop --------------------------------------------------------
+    def InitialConditions(self):
+        check(self._lib.dsmc_init_cold(self._h), "dsmc_init_cold")
+
+    init_cold = InitialConditions
+
+    def step(self, n: int = 1):
+        check(self._lib.dsmc_step(self._h, int(n)), "dsmc_step")
+
+    def MoveParticles(self):
+        check(self._lib.dsmc_stage_move(self._h), "dsmc_stage_move")
+
+    def BoundaryConditions(self):
+        check(self._lib.dsmc_stage_boundary(self._h), "dsmc_stage_boundary")
+
+    def Indexing(self):
+        check(self._lib.dsmc_stage_index(self._h), "dsmc_stage_index")
+
+    def CollideParticles(self) -> int:
+        check(self._lib.dsmc_stage_collide(self._h), "dsmc_stage_collide")
+        return sum(self.counters(i)["collisions_last_step"] for i in range(self.n_cases))
+
+    def Sampling(self):
+        check(self._lib.dsmc_stage_sample(self._h), "dsmc_stage_sample")
+
+    def end_step(self):
+        check(self._lib.dsmc_stage_end_step(self._h), "dsmc_stage_end_step")
+
+    def synchronize(self):
+        check(self._lib.dsmc_synchronize(self._h), "device")
+
+    # -- state ----------------------------------------------------------------
+    def counters(self, case: int = 0) -> dict:
+        c = Counters()
+        check(self._lib.dsmc_get_counters(self._h, case, C.byref(c)), "dsmc_get_counters")
+        return c.as_dict()
+
+    def GatherGlobalField(self, case: int = 0) -> np.ndarray:
+        """Moments of every cell, shape (nx*ny, 17), CELL layout, x-major."""
+        p = self.params[case]
+        out = np.empty((p.nx * p.ny, 17), dtype=np.float64)
+        check(self._lib.dsmc_get_fields(self._h, case, out.ctypes.data_as(C.c_void_p)),
+              "dsmc_get_fields")
+        return out
+
+    fields = GatherGlobalField
+
+    def fields_to_device(self, case: int, device_ptr: int):
+        check(self._lib.dsmc_get_fields_device(self._h, case, C.c_void_p(device_ptr)),
+              "dsmc_get_fields_device")
+
+    def fields_from_device(self, case: int, device_ptr: int, sample_step: int):
+        check(self._lib.dsmc_set_fields_device(self._h, case, C.c_void_p(device_ptr),
+                                               int(sample_step)), "dsmc_set_fields_device")
+
+    def particles(self, case: int = 0) -> dict:
+        n = C.c_int64()
+        cap = int(self.counters(case)["np"]) + 16
+        arrs = [np.empty(cap, dtype=np.float64) for _ in range(5)]
+        check(self._lib.dsmc_download_particles(self._h, case, *[a.ctypes.data_as(_D)
+                                                                 for a in arrs],
+                                                cap, C.byref(n)), "dsmc_download_particles")
+        return {k: a[: n.value].copy() for k, a in zip(("x", "y", "vx", "vy", "vz"), arrs)}
+
+    def set_particles(self, st: dict, case: int = 0):
+        arrs = [np.ascontiguousarray(st[k], dtype=np.float64) for k in ("x", "y", "vx", "vy", "vz")]
+        check(self._lib.dsmc_upload_particles(self._h, case, *[a.ctypes.data_as(_D) for a in arrs],
+                                              len(arrs[0])), "dsmc_upload_particles")
+
+    def cell_starts(self, case: int = 0) -> np.ndarray:
+        p = self.params[case]
+        out = np.empty(p.nx * p.ny + 1, dtype=np.int32)
+        check(self._lib.dsmc_get_cell_starts(self._h, case,
+                                             out.ctypes.data_as(C.POINTER(C.c_int32))),
+              "dsmc_get_cell_starts")
+        return out
+
+    def Printing(self, results_dir: str, case: int = 0):
+        write_field(self.params[case], self.derived[case], self.counters(case)["sample_step"],
+                    self.GatherGlobalField(case), results_dir)
+
+    # -- profiling ------------------------------------------------------------
+    def set_profiling(self, on: bool):
+        check(self._lib.dsmc_set_profiling(self._h, 1 if on else 0), "dsmc_set_profiling")
+
+    def kernel_times(self) -> dict:
+        n = C.c_int()
+        ms = (C.c_double * 32)()
+        launches = (C.c_int64 * 32)()
+        names = (C.c_char_p * 32)()
+        check(self._lib.dsmc_get_kernel_times(self._h, ms, launches, 32, C.byref(n), names),
+              "dsmc_get_kernel_times")
+        return {names[i].decode(): (ms[i], launches[i]) for i in range(n.value)}
+
+
+def default_params() -> Params:
+    return abi.default_params()

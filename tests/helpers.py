@@ -1,0 +1,42 @@
+"""Shared case definitions and comparison helpers of the tests."""
+from __future__ import annotations
+
+import numpy as np
+
+from dsmc_erlend_b200.abi import (WALL_CLL, WALL_DIFFUSE, WALL_SPECULAR, Params, default_params)
+
+WALLS = {"specular": WALL_SPECULAR, "diffuse": WALL_DIFFUSE, "cll": WALL_CLL}
+
+
+def small_case(wall: int = WALL_CLL, seed: int = 7, **kw) -> Params:
+    """A 40x30 grid with an off-centre 6x3 m box, 8 particles per cell,
+    a 12 degree flow and sampling from step 2: every stage is exercised
+    (impacts, inflow, removal, cell changes, collisions, sampling) in a few
+    thousand particles."""
+    base = dict(nx=40, ny=30, npc_free=8.0, wall_model=wall, attack_angle=12.0,
+                first_sampling_step=2, box_width=6.0, box_height=3.0, box_x=1.0, box_y=-0.5,
+                seed=seed, dt=4e-5, n_step=1000)
+    base.update(kw)
+    return default_params().copy(**base)
+
+
+def assert_close(a: np.ndarray, b: np.ndarray, rtol: float, atol: float, what: str):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    assert a.shape == b.shape, f"{what}: shape {a.shape} != {b.shape}"
+    if a.size == 0:
+        return
+    bad = ~np.isclose(a, b, rtol=rtol, atol=atol, equal_nan=True)
+    if bad.any():
+        i = np.flatnonzero(bad)[:5]
+        raise AssertionError(
+            f"{what}: {bad.sum()} of {a.size} differ; first {i.tolist()}: "
+            f"{a.ravel()[i].tolist()} vs {b.ravel()[i].tolist()}")
+
+
+# Scales of the state: positions ~20 m, velocities ~1e3 m/s.  FP64 kernels
+# differ from the host's libm only in the last bits of log/cos/sin/pow/hypot,
+# so states agree to ~1e-13 relative over a few steps.
+def assert_state_close(gpu: dict, ref: dict, what: str, rtol: float = 1e-11):
+    for k, atol in (("x", 1e-9), ("y", 1e-9), ("vx", 1e-7), ("vy", 1e-7), ("vz", 1e-7)):
+        assert_close(gpu[k], ref[k], rtol, atol, f"{what} {k}")
