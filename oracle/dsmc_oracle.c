@@ -517,6 +517,18 @@ int dsmc_oracle_step(dsmc_oracle *o)
     return dsmc_oracle_stage_end_step(o);
 }
 
+/* RemoveParticlesInsideBox, src/Geometry.cpp:231-247 (swap-with-last). */
+int dsmc_oracle_remove_inside_box(dsmc_oracle *o)
+{
+    for (int64_t i = 0; i < o->np;) {
+        if (inside_box(o, o->x[i], o->y[i]))
+            swap_last(o, i);
+        else
+            i++;
+    }
+    return DSMC_OK;
+}
+
 /* InitialConditions, src/Initialization.cpp:290-313, with
  * RemoveParticlesInsideBox (src/Geometry.cpp:231-247), then the cell sort. */
 int dsmc_oracle_init_cold(dsmc_oracle *o)
@@ -531,12 +543,7 @@ int dsmc_oracle_init_cold(dsmc_oracle *o)
     int s = generate(o, o->local[0], o->local[1], o->local[2], o->local[3], 0);
     if (s != DSMC_OK)
         return s;
-    for (int64_t i = 0; i < o->np;) {
-        if (inside_box(o, o->x[i], o->y[i]))
-            swap_last(o, i);
-        else
-            i++;
-    }
+    dsmc_oracle_remove_inside_box(o);
     return dsmc_oracle_stage_index(o);
 }
 

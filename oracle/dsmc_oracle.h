@@ -36,6 +36,7 @@ dsmc_oracle *dsmc_oracle_create(const dsmc_params *p, const dsmc_derived *d, int
 void dsmc_oracle_destroy(dsmc_oracle *o);
 
 int dsmc_oracle_init_cold(dsmc_oracle *o);
+int dsmc_oracle_remove_inside_box(dsmc_oracle *o);
 int dsmc_oracle_stage_move(dsmc_oracle *o);
 int dsmc_oracle_stage_boundary(dsmc_oracle *o);
 int dsmc_oracle_stage_index(dsmc_oracle *o);

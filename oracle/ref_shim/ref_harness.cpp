@@ -125,6 +125,7 @@ int dsmc_ref_configure(const dsmc_params *p)
         CLLNormalAccommodation = p->cll_normal;
         CLLTangentialAccommodation = p->cll_tangential;
         dsmc_ref_rng_set_seed64(p->seed);
+        MPI_Comm_size(MPI_COMM_WORLD, &MPISize); // as RunSimulation does (Simulation.cpp:70-71)
         CreateMPICellType();
         CreateMPIParticleType();
         MPIRank = 1; // Setup() prints on rank 0 only; keep test output quiet

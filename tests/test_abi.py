@@ -1,0 +1,110 @@
+"""The C ABI without a GPU: the library loads, exports every entry point that
+include/dsmc.h declares, and its host-only functions (defaults, Setup(),
+WallModelName(), Printing()) agree with the reference."""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from dsmc_erlend_b200 import _lib
+from dsmc_erlend_b200.abi import (WALL_CLL, WALL_DIFFUSE, WALL_SPECULAR, Derived, Params,
+                                  default_params)
+from dsmc_erlend_b200.engine import setup, write_field
+from oracle.cpu import OracleEngine
+
+ROOT = Path(__file__).resolve().parent.parent
+GOLDEN = ROOT / "tests" / "golden"
+
+
+def declared_functions() -> set[str]:
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"\b(dsmc_\w+)\s*\(", text):
+            name = m.group(1)
+            if not name.startswith("dsmc_philox") and not name.startswith("dsmc_stream") \
+                    and name not in ("dsmc_mulhilo32", "dsmc_u32_to_unit"):
+                names.add(name)
+    return names
+
+
+def test_library_exports_every_declared_entry_point(engine_lib):
+    declared = declared_functions()
+    assert "dsmc_step" in declared and "dsmc_ctx_create" in declared
+    missing = [n for n in sorted(declared) if not hasattr(engine_lib, n)]
+    assert not missing, f"not exported: {missing}"
+    assert set(_lib.SIGNATURES) <= declared
+
+
+def test_defaults_match_reference_settings(engine_lib):
+    p = Params()
+    engine_lib.dsmc_default_params(C.byref(p))
+    assert p.as_dict() == default_params().as_dict()
+
+
+@pytest.mark.parametrize("kw", [{}, {"attack_angle": 10.0, "nx": 1000, "ny": 1000,
+                                     "npc_free": 20.0},
+                                {"ma_free": 6.0, "n_free": 3e17, "box_width": 3.0,
+                                 "box_height": 5.0, "attack_angle": 15.0}])
+def test_setup_matches_oracle(engine_lib, kw):
+    p = default_params().copy(**kw)
+    d = setup(p)
+    s, od = OracleEngine.setup(p)
+    assert s == 0
+    assert d.as_dict() == od.as_dict()
+
+
+def test_setup_rejects_bad_cll(engine_lib):
+    d = Derived()
+    for an, at in ((-0.1, 0.5), (0.5, 1.1), (float("nan"), 0.5)):
+        p = default_params().copy(wall_model=WALL_CLL, cll_normal=an, cll_tangential=at)
+        assert engine_lib.dsmc_setup(C.byref(p), C.byref(d)) == 40
+    # Coefficients are only checked for CLL walls (Initialization.cpp:211).
+    p = default_params().copy(wall_model=WALL_DIFFUSE, cll_normal=-1.0)
+    assert engine_lib.dsmc_setup(C.byref(p), C.byref(d)) == 0
+
+
+def test_wall_model_names(engine_lib):
+    assert engine_lib.dsmc_wall_model_name(WALL_SPECULAR) == b"specular"
+    assert engine_lib.dsmc_wall_model_name(WALL_DIFFUSE) == b"diffuse"
+    assert engine_lib.dsmc_wall_model_name(WALL_CLL) == b"cll"
+    assert engine_lib.dsmc_wall_model_name(7) is None
+    assert engine_lib.dsmc_status_string(22) == b"too many particles in cell"
+
+
+def test_context_without_device_fails_cleanly(engine_lib):
+    from tests.conftest import gpu_available
+
+    if gpu_available():
+        pytest.skip("a device is present")
+    h = C.c_void_p()
+    p = default_params()
+    assert engine_lib.dsmc_ctx_create(C.byref(p), None, 1, None, C.byref(h)) == 51
+
+
+@pytest.mark.parametrize("wall", ["specular", "diffuse", "cll"])
+def test_printing_is_byte_identical_to_reference(engine_lib, tmp_path, wall):
+    """The field of the golden case after 8 steps (reproduced bit for bit by
+    the oracle) written by dsmc_write_field equals the reference's Printing()
+    output of the same field."""
+    g = json.loads((GOLDEN / "reference_steps.json").read_text())
+    case = g["cases"][wall]
+    p, d = Params(), Derived()
+    for k, v in case["params"].items():
+        setattr(p, k, v)
+    for k, v in case["derived"].items():
+        setattr(d, k, v)
+    o = OracleEngine(p, d)
+    o.init_cold()
+    o.step(8)
+    write_field(p, d, o.counters()["sample_step"], o.fields(), str(tmp_path))
+    for f in ("DSMC2D_Field.plt", "DSMC2D_Field.json"):
+        got = (tmp_path / wall / f).read_bytes()
+        want = (GOLDEN / f"printing_{wall}_{f}").read_bytes()
+        assert got == want, f
