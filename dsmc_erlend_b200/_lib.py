@@ -52,6 +52,8 @@ SIGNATURES = {
     "dsmc_k_intersect": (C.c_int, [_P, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p]),
+    "dsmc_k_inside_box": (C.c_int, [_P, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]),
     "dsmc_k_scatter": (C.c_int, [_P, _DV, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
 }

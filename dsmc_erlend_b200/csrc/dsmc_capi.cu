@@ -592,6 +592,14 @@ __global__ void k_unit_intersect(CaseDev c, int64_t n, const double *x, const do
     }
 }
 
+__global__ void k_unit_inside(CaseDev c, int64_t n, const double *x, const double *y,
+                              int32_t *inside)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        inside[i] = inside_box(c, x[i], y[i]) ? 1 : 0;
+}
+
 __global__ void k_unit_scatter(CaseDev c, int64_t n, double *v, const double *nx,
                                const double *ny, uint32_t kind, uint32_t step,
                                const uint32_t *entity)
@@ -1149,6 +1157,24 @@ int dsmc_k_intersect(const dsmc_params *p, int64_t n, const double *x, const dou
     const int grid = static_cast<int>(std::min<int64_t>(4096, (n + 255) / 256));
     k_unit_intersect<<<grid, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(c, n, x, y, dx, dy,
                                                                                hit, t_hit, nx, ny);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+int dsmc_k_inside_box(const dsmc_params *p, int64_t n, const double *x, const double *y,
+                      int32_t *inside, void *cuda_stream)
+{
+    if (p == nullptr || n < 0)
+        return DSMC_ERR_ARGUMENT;
+    dsmc_derived d;
+    const int s = dsmc_setup(p, &d);
+    if (s)
+        return s;
+    if (n == 0)
+        return DSMC_OK;
+    const CaseDev c = make_case(*p, d);
+    const int grid = static_cast<int>(std::min<int64_t>(4096, (n + 255) / 256));
+    k_unit_inside<<<grid, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(c, n, x, y, inside);
     CK(cudaGetLastError());
     return DSMC_OK;
 }

@@ -339,6 +339,21 @@ template <class T> __device__ __forceinline__ T round_out(double v, double n)
     return n < 0.0 ? Store<T>::down(v) : (n > 0.0 ? Store<T>::up(v) : Store<T>::rn(v));
 }
 
+// Keeps a stored coordinate inside [lo, hi).  The cold-start fill draws in
+// [X1, X2) in FP64; rounded to FP32 a draw just below X2 can become X2
+// itself, which lies in no cell.  In FP64 the largest draw stays ~1e-8 m
+// inside (u <= 1 - 4.7e-10), so the double version is the identity.
+template <class T> __device__ __forceinline__ T clamp_into(T v, double, double) { return v; }
+
+template <> __device__ __forceinline__ float clamp_into<float>(float v, double lo, double hi)
+{
+    if (static_cast<double>(v) < lo)
+        v = __double2float_ru(lo);
+    for (int i = 0; i < 4 && static_cast<double>(v) >= hi; ++i)
+        v = nextafterf(v, -INFINITY);
+    return v;
+}
+
 // FP32 only: a free-flight end point rounded to float can fall inside a box
 // whose faces are not floats.  Push it to the nearest face's outside.
 template <class T>

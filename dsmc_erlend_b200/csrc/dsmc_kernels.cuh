@@ -427,7 +427,11 @@ __global__ void __launch_bounds__(TILE_THREADS)
                 x += c.dt * vx;
                 y += c.dt * vy;
             }
-            const T xs = Store<T>::rn(x), ys = Store<T>::rn(y);
+            T xs = Store<T>::rn(x), ys = Store<T>::rn(y);
+            if (init_mode) {
+                xs = clamp_into<T>(xs, b[0], b[2]);
+                ys = clamp_into<T>(ys, b[1], b[3]);
+            }
             const int64_t q = s.n_old + j;
             const int64_t g = c.pbase + q;
             p.x[g] = xs;

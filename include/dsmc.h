@@ -230,6 +230,10 @@ int dsmc_k_intersect(const dsmc_params *p, int64_t n, const double *x, const dou
                      const double *dx, const double *dy, int32_t *hit, double *t_hit,
                      double *nx, double *ny, void *cuda_stream);
 
+/* InsideBox (Geometry.cpp:173-177) over a batch of points; inside[i] = 0/1. */
+int dsmc_k_inside_box(const dsmc_params *p, int64_t n, const double *x, const double *y,
+                      int32_t *inside, void *cuda_stream);
+
 /* One wall interaction per element (Boundary.cpp:205-282) with the case's
  * wall model; element i draws from stream (kind, step, entity[i]).  v is
  * 3*n doubles, (vx, vy, vz) per element, updated in place. */

@@ -10,12 +10,15 @@
 // reference fixes at compile time are set through its globals before Setup().
 //
 // usage: dsmc_ref_baseline NX NY NPCFREE WARMUP STEPS WALL AN AT AOA DT SEED
-//        [FIRST_SAMPLING_STEP]
+//        [FIRST_SAMPLING_STEP [FIELD_OUT]]
 //   WALL: 0 diffuse, 1 specular, 2 cll (the reference's WallModel order)
+//   FIELD_OUT: file receiving GatherGlobalField() as raw doubles (17 per
+//   cell, x-major) followed by SampleStep as one double
 // prints one JSON line: {"particle_steps": ..., "seconds": ..., ...}
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <vector>
 
 #include "Boundary.h"
 #include "Collision.h"
@@ -94,6 +97,16 @@ int main(int argc, char **argv)
     }
     const auto t1 = std::chrono::steady_clock::now();
     const double seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (argc > 13) {
+        const std::vector<CELL> field = GatherGlobalField();
+        std::FILE *f = std::fopen(argv[13], "wb");
+        if (f == nullptr)
+            return 3;
+        const double ss = SampleStep;
+        std::fwrite(field.data(), sizeof(CELL), field.size(), f);
+        std::fwrite(&ss, sizeof ss, 1, f);
+        std::fclose(f);
+    }
     std::printf("{\"particle_steps\": %lld, \"seconds\": %.6f, \"np\": %d, \"collisions\": %lld, "
                 "\"nx\": %d, \"ny\": %d, \"steps\": %d}\n",
                 particle_steps, seconds, NP, collisions, NX, NY, steps);

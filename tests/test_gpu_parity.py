@@ -219,6 +219,36 @@ def test_upload_sorts_like_indexing(cuda, engine_lib):
         assert np.array_equal(pg[k], po[k]), k
 
 
+@pytest.mark.parametrize("wall", ["diffuse", "cll"])
+def test_fp32_state_keeps_the_sort_invariant(cuda, engine_lib, wall):
+    """FP32 storage: after the cold start and after every step the particles
+    lie in their cells' slot ranges (cells recomputed on the host from the
+    stored FP32 positions with the reference's Indexing arithmetic), none is
+    inside the box, and none outside the domain."""
+    from dsmc_erlend_b200.abi import FP32
+
+    p = small_case(WALLS[wall], seed=61, precision=FP32, nx=64, ny=48, npc_free=12.0)
+    d = setup(p)
+    g = Engine(p, derived=[d])
+    g.InitialConditions()
+    for s in range(25):
+        if s:
+            g.step(1)
+        g.synchronize()
+        st = g.particles()
+        starts = g.cell_starts()
+        k = np.floor((st["x"] - p.x1) / d.dx).astype(np.int64)
+        l = np.floor((st["y"] - p.y1) / d.dy).astype(np.int64)
+        assert k.min() >= 0 and k.max() < p.nx and l.min() >= 0 and l.max() < p.ny
+        cells = k * p.ny + l
+        assert np.all(np.diff(cells) >= 0), f"step {s}: not in cell order"
+        np.testing.assert_array_equal(np.searchsorted(cells, np.arange(p.nx * p.ny + 1)),
+                                      starts)
+        inside = (np.abs(st["x"] - p.box_x) < p.box_width / 2) & \
+                 (np.abs(st["y"] - p.box_y) < p.box_height / 2)
+        assert not inside.any(), f"step {s}: {inside.sum()} particles inside the box"
+
+
 def test_upload_then_steps_match(cuda, engine_lib):
     """From one shared state, full steps agree (in-range fast path and the
     out-of-range lists both exercised)."""

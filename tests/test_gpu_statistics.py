@@ -1,0 +1,110 @@
+"""Statistical agreement of full GPU runs with the reference and with theory.
+
+  * the equilibrium NTC collision rate equals the analytic VHS rate of the
+    reference's Setup() (src/Initialization.cpp:231-253) within 1%;
+  * the sampled field of the plain reference case agrees with the unmodified
+    reference solver's (its own RNG, 64 seeds; tests/golden/
+    reference_case_field.npz) to relative L2 <= 2% on n, ux, uy and T
+    outside the wall cells;
+  * FP32 particle state agrees with FP64 to the same bar.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from dsmc_erlend_b200 import Engine, setup
+from dsmc_erlend_b200.abi import FP32, FP64, WALL_SPECULAR, default_params, reference_case
+from dsmc_erlend_b200.ensemble import replicas
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "reference_case_field.npz"
+K_B = 1.380662e-23
+
+
+def merged_fields(eng: Engine, n_cases: int):
+    p = eng.params[0]
+    d = eng.derived[0]
+    m = sum(eng.GatherGlobalField(i) for i in range(n_cases))
+    ss = sum(eng.counters(i)["sample_step"] for i in range(n_cases))
+    npc = m[:, 0]
+    n = d.weight * npc / ss / d.dv
+    with np.errstate(invalid="ignore", divide="ignore"):
+        u = m[:, 1:4] / npc[:, None]
+        vv = m[:, [4, 8, 12]] / npc[:, None]
+        t = d.molecule_mass * (vv - u * u) / K_B
+    return {"n": n, "ux": u[:, 0], "uy": u[:, 1], "t": t.mean(axis=1), "count": npc}
+
+
+def field_errors(a: dict, b: dict, p, u_free: float) -> dict:
+    """Relative L2 over cells outside the wall cells (cells whose centre lies
+    within one cell of the box) that both runs sampled.  Velocities are
+    normalised by the freestream speed, n by ||n_b||, T by ||T_b||."""
+    dx = (p.x2 - p.x1) / p.nx
+    dy = (p.y2 - p.y1) / p.ny
+    k, l = np.meshgrid(np.arange(p.nx), np.arange(p.ny), indexing="ij")
+    xc = p.x1 + (k.ravel() + 0.5) * dx
+    yc = p.y1 + (l.ravel() + 0.5) * dy
+    wall = (np.abs(xc - p.box_x) < p.box_width / 2 + dx) & \
+           (np.abs(yc - p.box_y) < p.box_height / 2 + dy)
+    ok = ~wall & (a["count"] > 0) & (b["count"] > 0)
+    out = {}
+    for key in ("n", "t"):
+        out[key] = np.linalg.norm(a[key][ok] - b[key][ok]) / np.linalg.norm(b[key][ok])
+    for key in ("ux", "uy"):
+        out[key] = np.linalg.norm(a[key][ok] - b[key][ok]) / (u_free * np.sqrt(ok.sum()))
+    return out
+
+
+def test_equilibrium_collision_rate(cuda, engine_lib):
+    # Gas at rest, no obstacle, inflow at the equilibrium flux: the NTC
+    # count per step must equal 1/2 n nu V Dt / W with nu = 1/MFT.
+    p = default_params().copy(ma_free=0.0, box_width=0.0, box_height=0.0, n_free=1e19,
+                              npc_free=50.0, nx=100, ny=100, dt=1e-5,
+                              wall_model=WALL_SPECULAR, first_sampling_step=10 ** 6, seed=77)
+    d = setup(p)
+    eng = Engine(p)
+    eng.InitialConditions()
+    eng.step(10)
+    eng.synchronize()
+    c0 = eng.counters()["collisions_total"]
+    steps = 200
+    eng.step(steps)
+    eng.synchronize()
+    nc = eng.counters()["collisions_total"] - c0
+    volume = (p.x2 - p.x1) * (p.y2 - p.y1) * p.dz
+    expected = 0.5 * p.n_free * (1.0 / d.mft_free) * volume * p.dt / d.weight * steps
+    assert nc > 1e6
+    assert abs(nc / expected - 1.0) < 0.01, (nc, expected)
+
+
+def test_reference_case_field_matches_reference_solver(cuda, engine_lib):
+    ref = np.load(GOLDEN)
+    base = reference_case(seed=1)
+    cases = replicas(base, 64, seed=11)
+    eng = Engine(cases)
+    eng.InitialConditions()
+    eng.step(base.n_step)
+    eng.synchronize()
+    got = merged_fields(eng, len(cases))
+    want = {k: ref[k].astype(np.float64) for k in ("n", "ux", "uy", "t", "count")}
+    err = field_errors(got, want, base, eng.derived[0].u_free)
+    assert all(v <= 0.02 for v in err.values()), err
+
+
+def test_fp32_state_matches_fp64(cuda, engine_lib):
+    base = reference_case(seed=1)
+    res = {}
+    for prec in (FP64, FP32):
+        cases = replicas(base.copy(precision=prec), 64, seed=23)
+        eng = Engine(cases)
+        eng.InitialConditions()
+        eng.step(base.n_step)
+        eng.synchronize()
+        res[prec] = merged_fields(eng, len(cases))
+        eng.close()
+    err = field_errors(res[FP32], res[FP64], base, setup(base).u_free)
+    assert all(v <= 0.02 for v in err.values()), err

@@ -1,0 +1,72 @@
+"""Replica reduction on two ranks over gloo (CPU).  Each rank runs the CPU
+oracle of the same case with its own Philox key; the merged moments must be
+the sum of both replicas' moments and the merged SampleStep their total."""
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+
+def _free_port() -> int:
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _case(rank: int):
+    from tests.helpers import small_case
+
+    return small_case(seed=500 + rank, nx=20, ny=16, npc_free=5.0, first_sampling_step=0)
+
+
+def _run(rank: int):
+    from oracle.cpu import OracleEngine
+
+    o = OracleEngine(_case(rank))
+    o.init_cold()
+    o.step(6)
+    return o.fields(), o.counters()["sample_step"]
+
+
+def _worker(rank, world, port, out):
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+    import torch.distributed as dist
+
+    from dsmc_erlend_b200.replicas import reduce_replica_fields
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        f, ss = _run(rank)
+        t = torch.from_numpy(f.copy())
+        merged, total = reduce_replica_fields(t, ss)
+        if rank == 0:
+            np.save(out, merged.numpy())
+            with open(out + ".ss", "w") as fh:
+                fh.write(str(total))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_replicas_sum_over_gloo(tmp_path):
+    out = str(tmp_path / "merged.npy")
+    mp.start_processes(_worker, args=(2, _free_port(), out), nprocs=2, join=True,
+                       start_method="spawn")
+    merged = np.load(out)
+    total = int(open(out + ".ss").read())
+    f0, s0 = _run(0)
+    f1, s1 = _run(1)
+    assert total == s0 + s1
+    np.testing.assert_array_equal(merged, f0 + f1)
+    assert not np.array_equal(f0, f1)  # distinct keys, distinct replicas
