@@ -290,6 +290,11 @@ void Sampling()
     SampleTime += Dt;
 }
 
+// ExchangeParticles, src/MPIManager.cpp:592-824: with one device owning every
+// cell no particle changes owner; the out-of-domain check it performs is made
+// by the device sort (status 30).
+void ExchangeParticles() { ctx(); }
+
 // GatherGlobalField, src/MPIManager.cpp:305-499 (one process holds it all)
 std::vector<CELL> GatherGlobalField()
 {

@@ -61,7 +61,10 @@ int CollideParticles();
 void Sampling();
 void Printing(const std::vector<CELL> &GlobalField);
 
-// include/MPIManager.h (single process: the whole field)
+// include/MPIManager.h: one device owns the whole domain, so the exchange
+// between BoundaryConditions() and Indexing() moves nothing; the field is
+// gathered from the device.
+void ExchangeParticles();
 std::vector<CELL> GatherGlobalField();
 
 // include/Simulation.h
