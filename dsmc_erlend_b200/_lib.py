@@ -41,6 +41,7 @@ SIGNATURES = {
     "dsmc_get_counters": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Counters)]),
     "dsmc_get_fields": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dsmc_get_fields_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "dsmc_get_fields_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dsmc_set_fields_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
     "dsmc_download_particles": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, C.c_int64,
                                           _I64]),

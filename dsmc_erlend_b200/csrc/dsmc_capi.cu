@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -987,6 +988,79 @@ int dsmc_get_fields(dsmc_ctx *c, int i, dsmc_cell *host_out)
     }
     CK(cudaFreeAsync(tmp, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return s;
+}
+
+} // extern "C"
+
+// Staging array of dsmc_get_fields_noalloc: 17 doubles per cell.
+static __device__ __align__(256) double g_fields_noalloc[17 * DSMC_FIELDS_NOALLOC_MAX_CELLS];
+
+namespace {
+// Device address of g_fields_noalloc on each device.  In host code the name
+// g_fields_noalloc is a host-side stand-in, not a device address, so the
+// kernel receives the address cudaGetSymbolAddress reports, looked up once
+// per device with that device current.
+constexpr int kMaxDevices = 64;
+double *g_fields_noalloc_addr[kMaxDevices] = {nullptr};
+std::mutex g_fields_noalloc_lock;
+
+int fields_noalloc_address(int device, double **out)
+{
+    if (device < 0 || device >= kMaxDevices)
+        return DSMC_ERR_ARGUMENT;
+    std::lock_guard<std::mutex> guard(g_fields_noalloc_lock);
+    if (g_fields_noalloc_addr[device] == nullptr) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_fields_noalloc);
+        if (e != cudaSuccess || p == nullptr) {
+            std::fprintf(stderr, "dsmc: cudaGetSymbolAddress failed: %s\n",
+                         cudaGetErrorString(e));
+            return DSMC_ERR_CUDA;
+        }
+        g_fields_noalloc_addr[device] = static_cast<double *>(p);
+    }
+    *out = g_fields_noalloc_addr[device];
+    return DSMC_OK;
+}
+} // namespace
+
+extern "C" {
+
+int dsmc_get_fields_noalloc(dsmc_ctx *c, int i, dsmc_cell *host_out)
+{
+    if (c == nullptr || host_out == nullptr || i < 0 || i >= c->ncase)
+        return DSMC_ERR_ARGUMENT;
+    const CaseDev &cd = c->hcases[i];
+    if (cd.ncell > DSMC_FIELDS_NOALLOC_MAX_CELLS) {
+        std::fprintf(stderr,
+                     "dsmc_get_fields_noalloc: %d cells exceed the static maximum of %d; "
+                     "use dsmc_get_fields\n",
+                     cd.ncell, DSMC_FIELDS_NOALLOC_MAX_CELLS);
+        return DSMC_ERR_TOO_LARGE;
+    }
+    int prev = 0;
+    CK(cudaGetDevice(&prev));
+    if (prev != c->device)
+        CK(cudaSetDevice(c->device));
+    double *staging = nullptr;
+    int s = fields_noalloc_address(c->device, &staging);
+    if (s == DSMC_OK) {
+        k_fields_out<<<std::max(1, std::min(1024, (cd.ncell + 255) / 256)), 256, 0, c->stream>>>(
+            c->cells, cd.cbase, cd.ncell, staging);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host_out, staging, sizeof(double) * 17 * cd.ncell,
+                                cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            std::fprintf(stderr, "dsmc_get_fields_noalloc: %s\n", cudaGetErrorString(e));
+            s = DSMC_ERR_CUDA;
+        }
+    }
+    if (prev != c->device)
+        cudaSetDevice(prev);
     return s;
 }
 

@@ -132,6 +132,7 @@ const char *dsmc_status_string(int status)
     case DSMC_ERR_TIMEOUT: return "device-side wait timed out";
     case DSMC_ERR_STATE: return "call out of order";
     case DSMC_ERR_UNSUPPORTED: return "unsupported";
+    case DSMC_ERR_TOO_LARGE: return "input larger than the fixed maximum of this entry point";
     }
     return "unknown status";
 }

@@ -44,7 +44,8 @@ enum {
     DSMC_ERR_NO_DEVICE = 51,      /* no CUDA device                          */
     DSMC_ERR_TIMEOUT = 60,        /* a bounded device-side wait gave up      */
     DSMC_ERR_STATE = 61,          /* call out of order (e.g. step before init) */
-    DSMC_ERR_UNSUPPORTED = 62     /* feature not available in this build     */
+    DSMC_ERR_UNSUPPORTED = 62,    /* feature not available in this build     */
+    DSMC_ERR_TOO_LARGE = 63       /* input beyond a fixed maximum size       */
 };
 
 /* WallModel, same enumerator order as the reference (include/Boundary.h:3). */
@@ -199,6 +200,26 @@ int dsmc_get_counters(dsmc_ctx *ctx, int case_index, dsmc_counters *out);
 /* Accumulated moments of one case, nx*ny cells x-major, as GatherGlobalField
  * (MPIManager.cpp:305-499) returns them. */
 int dsmc_get_fields(dsmc_ctx *ctx, int case_index, dsmc_cell *host_out);
+/* dsmc_get_fields without any allocation.  No counterpart in the reference:
+ * it exists for callers that cannot allocate device memory at read-out time,
+ * for example a thread reading results while another thread captures a CUDA
+ * graph in global capture mode (cudaMalloc then fails), an application whose
+ * device memory is already reserved by its own pool, or a monitor that must
+ * not stall the device (cudaFree synchronizes it).  dsmc_get_fields stages the
+ * expanded moments in a temporary device buffer; this variant stages them in
+ * one static device array of DSMC_FIELDS_NOALLOC_MAX_CELLS cells (8.9 MB,
+ * held by every GPU that loads the library until the process exits).
+ *   - A case with more cells returns DSMC_ERR_TOO_LARGE and touches nothing.
+ *   - The first call on a device looks up the array's device address (with
+ *     the context's device current); make that first call before any stream
+ *     capture begins.
+ *   - All calls share the array and return only after the copy to host_out
+ *     completed.  Calls from several host threads that overlap on the GPU
+ *     race on the array: serialize them.  Every element the call reads is
+ *     written by the same call, so no clearing is needed. */
+#define DSMC_FIELDS_NOALLOC_MAX_CELLS 65536
+int dsmc_get_fields_noalloc(dsmc_ctx *ctx, int case_index, dsmc_cell *host_out);
+
 /* Same, into device memory (17 doubles per cell), e.g. for an all-reduce. */
 int dsmc_get_fields_device(dsmc_ctx *ctx, int case_index, double *device_out);
 /* Replaces the accumulators of a case (e.g. after a replica all-reduce). */
