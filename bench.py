@@ -155,10 +155,11 @@ def run_reference(args):
 
 
 def workload_config(args) -> dict:
-    return {"workload": "1000x1000 cells, NPCFree 20 (~2e7 particles), angle 10 deg, "
-                        f"{args.wall} walls, Dt 1e-6 s, {args.precision} state with FP64 "
+    g = getattr(args, "grid", 1000)
+    return {"workload": f"{g}x{g} cells, NPCFree 20 (~{20 * g * g:.1e} particles), angle 10 "
+                        f"deg, {args.wall} walls, Dt 1e-6 s, {args.precision} state with FP64 "
                         "accumulators",
-            "grid": [1000, 1000], "npc_free": 20, "attack_angle": 10, "wall": args.wall,
+            "grid": [g, g], "npc_free": 20, "attack_angle": 10, "wall": args.wall,
             "dt": 1e-6, "precision": args.precision, "sampling": "every timed step",
             "l2": "inputs larger than L2 (particle state ~400 MB)",
             "parallelism": f"replicas x{args.gpus}"}
@@ -175,6 +176,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=10)
+    ap.add_argument("--grid", type=int, default=1000,
+                    help="cells per side; smaller grids are for profiler captures only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -203,6 +206,7 @@ def main():
     wall = {"diffuse": WALL_DIFFUSE, "cll": WALL_CLL, "specular": WALL_SPECULAR}[args.wall]
     prec = FP32 if args.precision == "fp32" else FP64
     p = large_case(wall_model=wall, precision=prec, seed=20251 + rank)
+    p.nx = p.ny = args.grid
     p.first_sampling_step = 0  # every timed step samples
     stream = torch.cuda.Stream()
 

@@ -220,9 +220,9 @@ template <class T> int enqueue_index(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_CELL_FIX);
-        k_cell_fix<T><<<c->grid_cell_fix, 256, 0, c->stream>>>(
-            c->d_cases, c->d_state, c->tt, c->cells, side, slots<T>(c, side),
-            slots<T>(c, side ^ 1), c->olist, c->total_cells, c->ncase, c->d_err);
+        k_cell_fix<<<c->grid_cell_fix, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->tt,
+                                                             c->cells, side, c->key, c->olist,
+                                                             c->total_cells, c->ncase, c->d_err);
     }
     {
         Span sp(c, KID_SCATTER);
@@ -515,6 +515,7 @@ template <class T> int resort_all(dsmc_ctx *c)
         return s;
     const int side = c->cur;
     CK(cudaMemsetAsync(c->cells.start[side], 0, sizeof(int32_t) * c->total_cells, c->stream));
+    CK(cudaMemsetAsync(c->cells.n_in, 0, sizeof(int32_t) * c->total_cells, c->stream));
     k_resort_plan<<<1, 32, 0, c->stream>>>(c->d_state, c->d_scratch, c->tt, c->ncase);
     k_rekey<T><<<4 * c->sms, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch,
                                                    slots<T>(c, side), c->key, c->cells, c->obuf,
@@ -815,6 +816,8 @@ int dsmc_init_cold(dsmc_ctx *c)
     CK(cudaMemsetAsync(c->d_state, 0, sizeof(CaseState) * c->ncase, c->stream));
     CK(cudaMemsetAsync(c->cells.acc, 0, sizeof(double) * ACC_COUNT * c->total_cells, c->stream));
     CK(cudaMemsetAsync(c->cells.start[c->cur], 0, sizeof(int32_t) * c->total_cells, c->stream));
+    // Every particle of the cold start is out of range (no previous sort).
+    CK(cudaMemsetAsync(c->cells.n_in, 0, sizeof(int32_t) * c->total_cells, c->stream));
     int s;
     if (c->precision == DSMC_FP32) {
         if ((s = enqueue_move<float>(c, 1)) || (s = enqueue_boundary<float>(c)) ||

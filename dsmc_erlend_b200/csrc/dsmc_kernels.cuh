@@ -212,6 +212,66 @@ __device__ __noinline__ double wall_hit(const CaseDev &c, int64_t step, int64_t 
 // k_move: MoveParticles (Boundary.cpp:284-328) over the sorted slots, plus the
 // per-slot bookkeeping of BoundaryConditions' removal and of Indexing.
 // ---------------------------------------------------------------------------
+// Four consecutive slots, 16-byte aligned (case bases and tiles are
+// multiples of TILE).
+__device__ __forceinline__ void load4(const float *p, float v[4])
+{
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+}
+__device__ __forceinline__ void load4(const double *p, double v[4])
+{
+    const double2 a = *reinterpret_cast<const double2 *>(p);
+    const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+}
+__device__ __forceinline__ void store4(float *p, const float v[4])
+{
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store4(double *p, const double v[4])
+{
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void store4(uint32_t *p, const uint32_t v[4])
+{
+    *reinterpret_cast<uint4 *>(p) = make_uint4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void load4(const uint32_t *p, uint32_t v[4])
+{
+    const uint4 t = *reinterpret_cast<const uint4 *>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+}
+
+// The slab test of IntersectBox, out of line: only segments that pass
+// may_hit_box reach it.
+__device__ __noinline__ bool intersect_box_ool(const CaseDev &c, double x, double y, double dx,
+                                               double dy, double &t_hit, double &nx, double &ny)
+{
+    return intersect_box(c, x, y, dx, dy, t_hit, nx, ny);
+}
+
+// Per-tile counts packed for one block scan: in-range, removed, changed cell.
+__device__ __forceinline__ unsigned long long pack3(unsigned a, unsigned b, unsigned c)
+{
+    return static_cast<unsigned long long>(a) | (static_cast<unsigned long long>(b) << 21) |
+           (static_cast<unsigned long long>(c) << 42);
+}
+__device__ __forceinline__ unsigned unpack3(unsigned long long v, int i)
+{
+    return static_cast<unsigned>((v >> (21 * i)) & 0x1FFFFFull);
+}
+
 template <class T>
 __global__ void __launch_bounds__(TILE_THREADS, 2)
     k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
@@ -221,7 +281,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
 {
     __shared__ int s_tile;
     __shared__ uint64_t s_excl;
-    __shared__ int32_t s_oc[TILE]; // old cell of removed slots, for the hole list
+    __shared__ uint32_t s_obase;
     const int lane = threadIdx.x & 31;
     for (;;) {
         __syncthreads();
@@ -240,95 +300,106 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
         // tile follow slot order.
         const int64_t q0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
         const int64_t g0 = c.pbase + q0;
+        const bool full = q0 + TILE_VEC <= n_old;
 
-        int n_dead = 0, n_in = 0, n_hit = 0;
-        unsigned dead_mask = 0;
+        T xs[TILE_VEC], ys[TILE_VEC], vxs[TILE_VEC], vys[TILE_VEC];
+        if (full) {
+            load4(p.x + g0, xs);
+            load4(p.y + g0, ys);
+            load4(p.vx + g0, vxs);
+            load4(p.vy + g0, vys);
+        } else {
+#pragma unroll
+            for (int k = 0; k < TILE_VEC; ++k) {
+                const bool v = q0 + k < n_old;
+                xs[k] = v ? p.x[g0 + k] : T(0);
+                ys[k] = v ? p.y[g0 + k] : T(0);
+                vxs[k] = v ? p.vx[g0 + k] : T(0);
+                vys[k] = v ? p.vy[g0 + k] : T(0);
+            }
+        }
+
+        uint32_t keys[TILE_VEC];
+        int32_t ocs[TILE_VEC];
+        unsigned dead_mask = 0, out_mask = 0, n_in = 0;
+        int n_hit = 0;
         double impulse = 0.0;
-        T cx{}, cy{}, cvx{}, cvy{};
-        if (q0 < n_old) {
-            cx = p.x[g0];
-            cy = p.y[g0];
-            cvx = p.vx[g0];
-            cvy = p.vy[g0];
-        }
-#pragma unroll 1
+#pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            const int64_t q = q0 + k;
-            const bool valid = q < n_old;
-            // Prefetch the next slot while this one is computed.
-            T nx_{}, ny_{}, nvx{}, nvy{};
-            if (k + 1 < TILE_VEC && q + 1 < n_old) {
-                nx_ = p.x[g0 + k + 1];
-                ny_ = p.y[g0 + k + 1];
-                nvx = p.vx[g0 + k + 1];
-                nvy = p.vy[g0 + k + 1];
+            keys[k] = KEY_DEAD;
+            ocs[k] = NO_CELL;
+            if (q0 + k >= n_old)
+                continue;
+            const double x0 = static_cast<double>(xs[k]);
+            const double y0 = static_cast<double>(ys[k]);
+            const int32_t oc = cell_of(c, x0, y0);
+            ocs[k] = oc < 0 ? NO_CELL : c.cbase + oc;
+            const double dx = c.dt * static_cast<double>(vxs[k]);
+            const double dy = c.dt * static_cast<double>(vys[k]);
+            const double xe = x0 + dx;
+            const double ye = y0 + dy;
+            double t_hit = 0.0, nx = 0.0, ny = 0.0;
+            T xn, yn;
+            if (may_hit_box(c, x0, y0, xe, ye) &&
+                intersect_box_ool(c, x0, y0, dx, dy, t_hit, nx, ny)) {
+                impulse += wall_hit<T>(c, step, q0 + k, g0 + k, p, x0, y0, dx, dy, t_hit, nx, ny,
+                                       xn, yn);
+                n_hit++;
+            } else {
+                xn = Store<T>::rn(xe);
+                yn = Store<T>::rn(ye);
+                keep_outside<T>(c, xn, yn);
             }
-            uint32_t kk = KEY_DEAD;
-            if (valid) {
-                const double x0 = static_cast<double>(cx);
-                const double y0 = static_cast<double>(cy);
-                const int32_t oc = cell_of(c, x0, y0);
-                const double dx = c.dt * static_cast<double>(cvx);
-                const double dy = c.dt * static_cast<double>(cvy);
-                const double xe = x0 + dx;
-                const double ye = y0 + dy;
-                double t_hit, nx, ny;
-                T xn, yn;
-                if (may_hit_box(c, x0, y0, xe, ye) &&
-                    intersect_box(c, x0, y0, dx, dy, t_hit, nx, ny)) {
-                    impulse += wall_hit<T>(c, step, q, g0 + k, p, x0, y0, dx, dy, t_hit, nx, ny,
-                                           xn, yn);
-                    n_hit++;
-                } else {
-                    xn = Store<T>::rn(xe);
-                    yn = Store<T>::rn(ye);
-                    keep_outside<T>(c, xn, yn);
-                }
-                p.x[g0 + k] = xn;
-                p.y[g0 + k] = yn;
-                const double xd = static_cast<double>(xn);
-                const double yd = static_cast<double>(yn);
-                if (outside_domain(c, xd, yd)) {
-                    dead_mask |= 1u << k;
-                    s_oc[threadIdx.x * TILE_VEC + k] = oc < 0 ? NO_CELL : c.cbase + oc;
-                } else {
-                    const int32_t nc = cell_of(c, xd, yd);
-                    if (nc < 0) {
-                        // Inside the domain bounds but in no cell (rounding,
-                        // NaN): the reference aborts in ExchangeParticles, 30.
-                        report_error(err, DSMC_ERR_EXCHANGE);
-                        dead_mask |= 1u << k;
-                        s_oc[threadIdx.x * TILE_VEC + k] = NO_CELL;
-                    } else {
-                        kk = static_cast<uint32_t>(c.cbase + nc) | (nc == oc ? KEY_IN : 0u);
-                    }
-                }
-                key[g0 + k] = kk;
+            xs[k] = xn;
+            ys[k] = yn;
+            const double xd = static_cast<double>(xn);
+            const double yd = static_cast<double>(yn);
+            if (outside_domain(c, xd, yd)) {
+                dead_mask |= 1u << k;
+                continue;
             }
-            // Per-cell counts and the list of particles that changed cell.
-            const bool alive = kk != KEY_DEAD;
-            const bool in = alive && (kk & KEY_IN);
-            const bool out = alive && !in;
-            const int32_t cg = static_cast<int32_t>(kk & KEY_CELL);
-            n_in += in ? 1 : 0;
-            warp_aggregated_inc(cells.n_in, cg, in);
-            warp_aggregated_inc(cells.n_o, cg, out);
-            const unsigned m = __ballot_sync(0xffffffffu, out);
-            if (m) {
-                uint32_t base = 0;
-                if (lane == __ffs(m) - 1)
-                    base = atomicAdd(&sc->obuf_count, static_cast<uint32_t>(__popc(m)));
-                base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-                if (out)
-                    obuf[base + __popc(m & ((1u << lane) - 1u))] =
-                        static_cast<uint32_t>(g0 + k);
+            const int32_t nc = cell_of(c, xd, yd);
+            if (nc < 0) {
+                // Inside the domain bounds but in no cell (rounding, NaN):
+                // the reference aborts in ExchangeParticles with code 30.
+                report_error(err, DSMC_ERR_EXCHANGE);
+                dead_mask |= 1u << k;
+                continue;
             }
-            cx = nx_;
-            cy = ny_;
-            cvx = nvx;
-            cvy = nvy;
+            if (nc == oc) {
+                keys[k] = static_cast<uint32_t>(c.cbase + nc) | KEY_IN;
+                ++n_in;
+            } else {
+                keys[k] = static_cast<uint32_t>(c.cbase + nc);
+                out_mask |= 1u << k;
+            }
         }
-        n_dead = __popc(dead_mask);
+        if (full) {
+            store4(p.x + g0, xs);
+            store4(p.y + g0, ys);
+            store4(key + g0, keys);
+        } else {
+#pragma unroll
+            for (int k = 0; k < TILE_VEC; ++k)
+                if (q0 + k < n_old) {
+                    p.x[g0 + k] = xs[k];
+                    p.y[g0 + k] = ys[k];
+                    key[g0 + k] = keys[k];
+                }
+        }
+        // Cell counts.  Every cell starts the step with its old count as its
+        // in-range count, so only the few slots that leave a cell (or the
+        // domain) touch the counters.
+        const unsigned leave = dead_mask | out_mask;
+        if (leave) {
+#pragma unroll
+            for (int k = 0; k < TILE_VEC; ++k) {
+                if (((leave >> k) & 1u) && ocs[k] != NO_CELL)
+                    atomicSub(cells.n_in + ocs[k], 1);
+                if ((out_mask >> k) & 1u)
+                    atomicAdd(cells.n_o + (keys[k] & KEY_CELL), 1);
+            }
+        }
         // Wall-hit diagnostics (Boundary.cpp:318-319).
         {
             double imp = impulse;
@@ -343,26 +414,33 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
                 atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(hits));
             }
         }
-        // Tile totals: in-range count, and the removed-slot ranks (hole list).
-        int in_total;
-        (void)block_exclusive<int>(n_in, in_total);
-        int dead_total;
-        const int dead_excl = block_exclusive<int>(n_dead, dead_total);
-        if (threadIdx.x == 0) {
-            tile_in[t] = in_total;
-            const uint64_t excl = lookback(lb, t, local_tile == 0, dead_total, err);
-            s_excl = excl;
-            if (local_tile == st[ci].n_move_tiles - 1)
-                st[ci].dead_old = static_cast<int64_t>(excl) + dead_total;
+        // One block scan for the three tile counts.
+        unsigned long long tot;
+        const unsigned long long ex = block_exclusive<unsigned long long>(
+            pack3(n_in, __popc(dead_mask), __popc(out_mask)), tot);
+        if (threadIdx.x < 32) {
+            const unsigned dead_tile = unpack3(tot, 1), out_tile = unpack3(tot, 2);
+            const uint64_t excl = lookback_warp(lb, t, t - local_tile, dead_tile, err);
+            if (threadIdx.x == 0) {
+                tile_in[t] = static_cast<int32_t>(unpack3(tot, 0));
+                s_excl = excl;
+                if (local_tile == st[ci].n_move_tiles - 1)
+                    st[ci].dead_old = static_cast<int64_t>(excl) + dead_tile;
+                s_obase = out_tile ? atomicAdd(&sc->obuf_count, out_tile) : 0u;
+            }
         }
         __syncthreads();
-        int64_t rank = static_cast<int64_t>(s_excl) + dead_excl;
+        int64_t rank = static_cast<int64_t>(s_excl) + unpack3(ex, 1);
+        uint32_t ob = s_obase + unpack3(ex, 2);
+#pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if (dead_mask & (1u << k)) {
+            if ((dead_mask >> k) & 1u) {
                 hole_pos[c.pbase + rank] = static_cast<int32_t>(q0 + k);
-                hole_oc[c.pbase + rank] = s_oc[threadIdx.x * TILE_VEC + k];
+                hole_oc[c.pbase + rank] = ocs[k];
                 ++rank;
             }
+            if ((out_mask >> k) & 1u)
+                obuf[ob++] = static_cast<uint32_t>(g0 + k);
         }
     }
 }
@@ -473,16 +551,18 @@ __global__ void __launch_bounds__(TILE_THREADS)
         }
         int dead_total;
         const int dead_excl = block_exclusive<int>(n_dead, dead_total);
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 32) {
             // The chain of this case continues the removed count of its
             // moved slots: the first inject tile starts at dead_old.
             const bool first = local_tile == 0;
             const uint64_t agg = static_cast<uint64_t>(dead_total) +
                                  (first ? static_cast<uint64_t>(s.dead_old) : 0ull);
-            const uint64_t excl = lookback(lb, t, first, agg, err);
-            s_excl = first ? static_cast<uint64_t>(s.dead_old) : excl;
-            if (local_tile == s.n_inject_tiles - 1)
-                st[ci].dead_total = static_cast<int64_t>(excl + agg);
+            const uint64_t excl = lookback_warp(lb, t, t - local_tile, agg, err);
+            if (threadIdx.x == 0) {
+                s_excl = first ? static_cast<uint64_t>(s.dead_old) : excl;
+                if (local_tile == s.n_inject_tiles - 1)
+                    st[ci].dead_total = static_cast<int64_t>(excl + agg);
+            }
         }
         __syncthreads();
         int64_t rank = static_cast<int64_t>(s_excl) + dead_excl;
@@ -574,8 +654,11 @@ __global__ void __launch_bounds__(TILE_THREADS)
         }
         int alive_total;
         const int alive_excl = block_exclusive<int>(n_alive, alive_total);
-        if (threadIdx.x == 0)
-            s_excl = lookback(lb, t, local_tile == 0, alive_total, err);
+        if (threadIdx.x < 32) {
+            const uint64_t excl = lookback_warp(lb, t, t - local_tile, alive_total, err);
+            if (threadIdx.x == 0)
+                s_excl = excl;
+        }
         __syncthreads();
         int64_t r = static_cast<int64_t>(s_excl) + alive_excl;
 #pragma unroll
@@ -654,8 +737,11 @@ __global__ void __launch_bounds__(TILE_THREADS)
         unsigned long long tot;
         const unsigned long long ex =
             block_exclusive<unsigned long long>(pack2(sa, sb), tot);
-        if (threadIdx.x == 0)
-            s_excl = lookback(lb, t, local_tile == 0, tot, err);
+        if (threadIdx.x < 32) {
+            const uint64_t excl = lookback_warp(lb, t, t - local_tile, tot, err);
+            if (threadIdx.x == 0)
+                s_excl = excl;
+        }
         __syncthreads();
         const uint64_t base = s_excl + ex;
         uint32_t ra = pack2_a(base), rb = pack2_b(base);
@@ -682,15 +768,29 @@ __global__ void __launch_bounds__(TILE_THREADS)
 __global__ void __launch_bounds__(TILE_THREADS)
     k_tile_scan(const CaseState *st, const int32_t *tile_in, int32_t *tile_prefix)
 {
+    constexpr int PER = 8; // consecutive tiles per thread
     const CaseState &s = st[blockIdx.x];
+    const int n = s.n_move_tiles;
+    const int32_t *in = tile_in + s.move_tile0;
+    int32_t *out = tile_prefix + s.move_tile0;
     int32_t carry = 0;
-    for (int b = 0; b < s.n_move_tiles; b += TILE_THREADS) {
-        const int i = b + threadIdx.x;
-        const int v = i < s.n_move_tiles ? tile_in[s.move_tile0 + i] : 0;
+    for (int b = 0; b < n; b += TILE_THREADS * PER) {
+        const int i0 = b + threadIdx.x * PER;
+        int v[PER];
+        int sum = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            v[k] = i0 + k < n ? in[i0 + k] : 0;
+            sum += v[k];
+        }
         int tot;
-        const int ex = block_exclusive<int>(v, tot);
-        if (i < s.n_move_tiles)
-            tile_prefix[s.move_tile0 + i] = carry + ex;
+        int run = carry + block_exclusive<int>(sum, tot);
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            if (i0 + k < n)
+                out[i0 + k] = run;
+            run += v[k];
+        }
         carry += tot;
     }
 }
@@ -734,12 +834,12 @@ __global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
 }
 
 // ---------------------------------------------------------------------------
-// k_cell_fix: per cell, orders its out-of-range list by slot, places those
-// particles, and computes the base offset of its in-range particles.
+// k_cell_fix: per cell, orders its out-of-range list by slot, gives each of
+// those particles its final slot (written into its key word, bit 31 clear),
+// and computes the base offset of the cell's in-range particles.
 // ---------------------------------------------------------------------------
-template <class T>
 __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *st,
-                           TileTables tt, Cells cells, int old_side, Slots<T> src, Slots<T> dst,
+                           TileTables tt, Cells cells, int old_side, uint32_t *__restrict__ key,
                            int32_t *__restrict__ olist, int total_cells, int ncase, int *err)
 {
     const int32_t *os = cells.start[old_side];
@@ -778,24 +878,23 @@ __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *s
                     report_error(err, DSMC_ERR_STATE); // counts and list disagree
                     continue;
                 }
-                const int64_t gs = c.pbase + q, gd = c.pbase + fin;
-                dst.x[gd] = src.x[gs];
-                dst.y[gd] = src.y[gs];
-                dst.vx[gd] = src.vx[gs];
-                dst.vy[gd] = src.vy[gs];
-                dst.vz[gd] = src.vz[gs];
+                key[c.pbase + q] = static_cast<uint32_t>(fin);
             }
         }
         cells.base_in[cg] = start + lo - cells.fin[cg];
-        cells.n_in[cg] = 0;
+        // The next step starts with every particle of the cell counted as
+        // in range; k_move subtracts the ones that leave.
+        cells.n_in[cg] = ns[cg + 1] - start;
         cells.n_o[cg] = 0;
         cells.o_fill[cg] = 0;
     }
 }
 
 // ---------------------------------------------------------------------------
-// k_scatter: every in-range particle goes to base_in[cell] + (number of
-// in-range particles at lower slots of its case).
+// k_scatter: moves every particle of slots [0, K) to its sorted slot.  An
+// in-range particle goes to base_in[cell] + (number of in-range particles at
+// lower slots of its case); any other particle's key word already holds its
+// slot (k_cell_fix).  Reads are whole coalesced tiles.
 // ---------------------------------------------------------------------------
 template <class T>
 __global__ void __launch_bounds__(TILE_THREADS)
@@ -810,38 +909,58 @@ __global__ void __launch_bounds__(TILE_THREADS)
         const CaseState &s = st[ci];
         const int local_tile = t - tt.scatter0[ci];
         const int64_t q0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
+        const int64_t g0 = c.pbase + q0;
+        const int64_t keep = s.n_keep;
+        const bool full = q0 + TILE_VEC <= keep;
         uint32_t keys[TILE_VEC];
+        T x[TILE_VEC], y[TILE_VEC], vx[TILE_VEC], vy[TILE_VEC], vz[TILE_VEC];
+        if (full) {
+            load4(key + g0, keys);
+            load4(src.x + g0, x);
+            load4(src.y + g0, y);
+            load4(src.vx + g0, vx);
+            load4(src.vy + g0, vy);
+            load4(src.vz + g0, vz);
+        } else {
+#pragma unroll
+            for (int k = 0; k < TILE_VEC; ++k) {
+                const bool v = q0 + k < keep;
+                keys[k] = v ? key[g0 + k] : KEY_DEAD;
+                x[k] = v ? src.x[g0 + k] : T(0);
+                y[k] = v ? src.y[g0 + k] : T(0);
+                vx[k] = v ? src.vx[g0 + k] : T(0);
+                vy[k] = v ? src.vy[g0 + k] : T(0);
+                vz[k] = v ? src.vz[g0 + k] : T(0);
+            }
+        }
         int n_in = 0;
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            keys[k] = 0;
-            if (q0 + k < s.n_keep)
-                keys[k] = key[c.pbase + q0 + k];
-            n_in += (keys[k] & KEY_IN) ? 1 : 0;
-        }
+        for (int k = 0; k < TILE_VEC; ++k)
+            n_in += (keys[k] != KEY_DEAD && (keys[k] & KEY_IN)) ? 1 : 0;
         int tot;
         const int ex = block_exclusive<int>(n_in, tot);
-        if (tot == 0)
-            continue;
-        int64_t f = tile_prefix[s.move_tile0 + local_tile] + ex;
+        int64_t f = (tot > 0 ? tile_prefix[s.move_tile0 + local_tile] : 0) + ex;
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if (!(keys[k] & KEY_IN))
+            if (keys[k] == KEY_DEAD)
                 continue;
-            const int32_t cg = static_cast<int32_t>(keys[k] & KEY_CELL);
-            const int64_t fin = cells.base_in[cg] + f;
-            ++f;
-            if (fin < 0 || fin >= s.n_keep) {
+            int64_t fin;
+            if (keys[k] & KEY_IN) {
+                fin = cells.base_in[keys[k] & KEY_CELL] + f;
+                ++f;
+            } else {
+                fin = keys[k];
+            }
+            if (fin < 0 || fin >= keep) {
                 report_error(err, DSMC_ERR_STATE); // counts and keys disagree
                 continue;
             }
             const int64_t gd = c.pbase + fin;
-            const int64_t gs = c.pbase + q0 + k;
-            dst.x[gd] = src.x[gs];
-            dst.y[gd] = src.y[gs];
-            dst.vx[gd] = src.vx[gs];
-            dst.vy[gd] = src.vy[gs];
-            dst.vz[gd] = src.vz[gs];
+            dst.x[gd] = x[k];
+            dst.y[gd] = y[k];
+            dst.vx[gd] = vx[k];
+            dst.vy[gd] = vy[k];
+            dst.vz[gd] = vz[k];
         }
     }
 }

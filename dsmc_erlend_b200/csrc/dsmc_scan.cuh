@@ -67,6 +67,74 @@ __device__ __forceinline__ uint64_t lookback(uint64_t *status, int t, bool first
     return excl;
 }
 
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Warp-wide form of lookback(): called by all 32 lanes of one warp.  Each
+// poll reads the 32 predecessors t-1 .. t-32 at once, so the walk over tiles
+// that have published only their aggregate advances 32 tiles per poll
+// instead of one.  `chain0` is the chain's first tile: predecessors before
+// it belong to another case and count as zero.  Returns the exclusive prefix
+// in every lane.
+__device__ __forceinline__ uint64_t lookback_warp(uint64_t *status, int t, int chain0,
+                                                  uint64_t agg, int *err)
+{
+    volatile uint64_t *vs = status;
+    const int lane = threadIdx.x & 31;
+    if (t == chain0) {
+        if (lane == 0) {
+            __threadfence();
+            vs[t] = LB_INC | agg;
+        }
+        __syncwarp();
+        return 0;
+    }
+    if (lane == 0)
+        vs[t] = LB_AGG | agg;
+    __threadfence();
+    __syncwarp();
+    uint64_t excl = 0;
+    int base = t - 1;
+    uint32_t spins = 0;
+    for (;;) {
+        const int j = base - lane;
+        uint64_t w = 2ull << 62; // LB_INC with value 0 before the chain
+        if (j >= chain0)
+            w = vs[j];
+        if (!__all_sync(0xffffffffu, (w & LB_FLAGS) != 0)) {
+            if (++spins > SPIN_LIMIT) {
+                if (lane == 0) {
+                    report_error(err, DSMC_ERR_TIMEOUT);
+                    vs[t] = LB_INC | agg;
+                }
+                __syncwarp();
+                return 0;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        const unsigned inc = __ballot_sync(0xffffffffu, (w & LB_FLAGS) == LB_INC);
+        if (inc) {
+            const int closest = __ffs(inc) - 1; // lowest lane = nearest tile
+            excl += warp_sum_u64(lane <= closest ? (w & LB_VALUE) : 0ull);
+            break;
+        }
+        excl += warp_sum_u64(w & LB_VALUE);
+        base -= 32;
+    }
+    if (lane == 0) {
+        __threadfence();
+        vs[t] = LB_INC | (excl + agg);
+    }
+    __syncwarp();
+    return excl;
+}
+
 // Block-wide exclusive sum over TILE_THREADS threads; also returns the total.
 template <class V> __device__ __forceinline__ V block_exclusive(V v, V &total)
 {

@@ -40,9 +40,17 @@ def merged_fields(eng: Engine, n_cases: int):
 
 
 def field_errors(a: dict, b: dict, p, u_free: float) -> dict:
-    """Relative L2 over cells outside the wall cells (cells whose centre lies
-    within one cell of the box) that both runs sampled.  Velocities are
-    normalised by the freestream speed, n by ||n_b||, T by ||T_b||."""
+    """Relative L2 errors of field a against field b over the cells outside
+    the wall cells (centre within one cell of the box).
+
+    n is compared over every such cell both runs sampled.  Velocity and
+    temperature are moments per sampled particle, undefined where almost
+    nothing is sampled: the near-vacuum wake right behind the box (about half
+    a percent of the cells here) holds tens of samples in a whole run, and
+    there even independent runs of the reference itself differ by O(100%).
+    ux, uy and T therefore leave out cells whose sample count in b is below
+    5% of b's median.  Velocities are normalised by the freestream speed,
+    n by ||n_b||, T by ||T_b||."""
     dx = (p.x2 - p.x1) / p.nx
     dy = (p.y2 - p.y1) / p.ny
     k, l = np.meshgrid(np.arange(p.nx), np.arange(p.ny), indexing="ij")
@@ -50,12 +58,14 @@ def field_errors(a: dict, b: dict, p, u_free: float) -> dict:
     yc = p.y1 + (l.ravel() + 0.5) * dy
     wall = (np.abs(xc - p.box_x) < p.box_width / 2 + dx) & \
            (np.abs(yc - p.box_y) < p.box_height / 2 + dy)
-    ok = ~wall & (a["count"] > 0) & (b["count"] > 0)
-    out = {}
-    for key in ("n", "t"):
-        out[key] = np.linalg.norm(a[key][ok] - b[key][ok]) / np.linalg.norm(b[key][ok])
+    sampled = ~wall & (a["count"] > 0) & (b["count"] > 0)
+    dense = sampled & (b["count"] >= 0.05 * np.median(b["count"][b["count"] > 0]))
+    out = {"n": np.linalg.norm(a["n"][sampled] - b["n"][sampled]) /
+                np.linalg.norm(b["n"][sampled]),
+           "t": np.linalg.norm(a["t"][dense] - b["t"][dense]) / np.linalg.norm(b["t"][dense])}
     for key in ("ux", "uy"):
-        out[key] = np.linalg.norm(a[key][ok] - b[key][ok]) / (u_free * np.sqrt(ok.sum()))
+        out[key] = np.linalg.norm(a[key][dense] - b[key][dense]) / \
+            (u_free * np.sqrt(dense.sum()))
     return out
 
 
