@@ -29,12 +29,16 @@ namespace {
     } while (0)
 
 enum KernelId {
-    KID_PLAN, KID_MOVE, KID_INJECT, KID_PLAN2, KID_TAIL, KID_CELL_SCAN, KID_TILE_SCAN,
-    KID_OLIST, KID_CELL_FIX, KID_SCATTER, KID_COLLIDE, KID_FINISH, KID_COUNT
+    KID_PLAN, KID_MOVE, KID_INJECT, KID_DEAD_SCAN, KID_HOLES, KID_PLAN2, KID_TAIL,
+    KID_CELL_SCAN, KID_TILE_SCAN,
+    KID_OLIST, KID_CELL_FIX, KID_SCATTER, KID_COLLIDE_SELECT, KID_COLLIDE, KID_SAMPLE,
+    KID_FINISH, KID_COUNT
 };
-const char *kKernelNames[KID_COUNT] = {"k_plan",     "k_move",      "k_inject",  "k_plan2",
-                                       "k_tail",     "k_cell_scan", "k_tile_scan", "k_olist",
-                                       "k_cell_fix", "k_scatter",   "k_collide", "k_finish"};
+const char *kKernelNames[KID_COUNT] = {
+    "k_plan",      "k_move",   "k_inject",         "k_dead_scan",     "k_holes",
+    "k_plan2",     "k_tail",
+    "k_cell_scan", "k_tile_scan", "k_olist",       "k_cell_fix",      "k_scatter",
+    "k_collide_select", "k_collide_pairs", "k_sample", "k_finish"};
 
 struct Timed {
     int kid;
@@ -73,11 +77,14 @@ struct dsmc_ctx {
     uint32_t *key = nullptr;
     Cells cells{};
     int32_t *tile_in = nullptr, *tile_prefix = nullptr;
+    int32_t *tile_dead = nullptr, *tile_dprefix = nullptr;   // removed slots per move tile
+    int32_t *itile_dead = nullptr, *itile_dprefix = nullptr; // ... per inject tile
     uint64_t *lb = nullptr; // 4 chains: move, inject, tail, cell
     size_t lb_words = 0;
     int32_t *hole_pos = nullptr, *hole_oc = nullptr;
     uint32_t *obuf = nullptr;
     int32_t *olist = nullptr;
+    uint32_t *coll_list = nullptr; // cells with candidate pairs, per step
 
     int cur = 0;
     bool initialized = false;
@@ -87,7 +94,7 @@ struct dsmc_ctx {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
     int grid_move = 0, grid_inject = 0, grid_tail = 0, grid_cell_scan = 0, grid_olist = 0;
-    int grid_cell_fix = 0, grid_scatter = 0, grid_collide = 0;
+    int grid_cell_fix = 0, grid_scatter = 0, grid_collide = 0, grid_select = 0;
 
     bool profiling = false;
     std::vector<Timed> timed;
@@ -167,7 +174,7 @@ template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
         Span sp(c, KID_MOVE);
         k_move<T><<<c->grid_move, TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
-            c->tile_in, lb_chain(c, 0), c->hole_pos, c->hole_oc, c->obuf, c->ncase, c->d_err);
+            c->tile_in, c->tile_dead, c->obuf, c->ncase, c->d_err);
     }
     CK(cudaGetLastError());
     return DSMC_OK;
@@ -180,7 +187,19 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
         Span sp(c, KID_INJECT);
         k_inject<T><<<c->grid_inject, TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
-            lb_chain(c, 1), c->hole_pos, c->hole_oc, c->obuf, c->ncase, c->d_err);
+            c->itile_dead, c->obuf, c->ncase, c->d_err);
+    }
+    {
+        Span sp(c, KID_DEAD_SCAN);
+        k_dead_scan<<<c->ncase, TILE_THREADS, 0, c->stream>>>(c->d_state, c->tile_dead,
+                                                              c->tile_dprefix, c->itile_dead,
+                                                              c->itile_dprefix);
+    }
+    {
+        Span sp(c, KID_HOLES);
+        k_holes<<<c->grid_scatter, TILE_THREADS, 0, c->stream>>>(
+            c->d_cases, c->d_state, c->d_scratch, c->tt, c->key, c->tile_dead, c->tile_dprefix,
+            c->itile_dead, c->itile_dprefix, c->hole_pos, c->hole_oc, c->ncase);
     }
     {
         Span sp(c, KID_PLAN2);
@@ -237,10 +256,25 @@ template <class T> int enqueue_index(dsmc_ctx *c)
 
 template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sample)
 {
-    Span sp(c, KID_COLLIDE);
-    k_collide<T><<<c->grid_collide, COLLIDE_CELLS, collide_smem<T>(), c->stream>>>(
-        c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, do_collide,
-        do_sample, c->ncase);
+    if (do_collide) {
+        {
+            Span sp(c, KID_COLLIDE_SELECT);
+            k_collide_select<<<c->grid_select, 256, 0, c->stream>>>(
+                c->d_cases, c->d_state, c->d_scratch, c->tt, c->cells, c->cur, c->coll_list,
+                c->total_cells, c->ncase);
+        }
+        {
+            Span sp(c, KID_COLLIDE);
+            k_collide_pairs<T><<<2 * c->sms, 128, 0, c->stream>>>(
+                c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->cells,
+                c->cur, c->coll_list, c->ncase);
+        }
+    }
+    if (do_sample) {
+        Span sp(c, KID_SAMPLE);
+        k_sample<T><<<c->grid_collide, COLLIDE_CELLS, collide_smem<T>(), c->stream>>>(
+            c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, c->ncase);
+    }
     CK(cudaGetLastError());
     return DSMC_OK;
 }
@@ -391,11 +425,13 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
     c->grid_cell_scan = std::max(1, b) * c->sms;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, TILE_THREADS, 0));
     c->grid_scatter = std::max(1, b) * c->sms;
-    CK(cudaFuncSetAttribute(k_collide<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(k_sample<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(collide_smem<T>())));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_collide<T>, COLLIDE_CELLS,
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sample<T>, COLLIDE_CELLS,
                                                      collide_smem<T>()));
     c->grid_collide = std::max(1, b) * c->sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_collide_select, 256, 0));
+    c->grid_select = std::max(1, b) * c->sms;
     c->grid_olist = 4 * c->sms;
     c->grid_cell_fix = 8 * c->sms;
     return DSMC_OK;
@@ -415,8 +451,9 @@ void free_ctx(dsmc_ctx *c)
     void *ptrs[] = {c->d_cases, c->d_state, c->d_scratch, c->d_err, c->d_tables, c->d_tmp,
                     c->d_pbases, c->key, c->cells.n_in, c->cells.n_o, c->cells.o_fill,
                     c->cells.fin, c->cells.ostart, c->cells.base_in, c->cells.start[0],
-                    c->cells.start[1], c->cells.acc, c->tile_in, c->tile_prefix, c->lb,
-                    c->hole_pos, c->hole_oc, c->obuf, c->olist};
+                    c->cells.start[1], c->cells.acc, c->tile_in, c->tile_prefix, c->tile_dead,
+                    c->tile_dprefix, c->itile_dead, c->itile_dprefix, c->lb,
+                    c->hole_pos, c->hole_oc, c->obuf, c->olist, c->coll_list};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -477,7 +514,7 @@ __global__ void k_rekey(const CaseDev *cases, CaseState *st, StepScratch *sc, Sl
             const int32_t cl = cell_of(c, static_cast<double>(p.x[g]), static_cast<double>(p.y[g]));
             if (cl < 0) {
                 report_error(err, DSMC_ERR_EXCHANGE);
-                key[g] = KEY_DEAD;
+                key[g] = KEY_DEAD | KEY_CELL;
                 continue;
             }
             key[g] = static_cast<uint32_t>(c.cbase + cl);
@@ -685,6 +722,7 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     std::vector<int32_t> cell0(n_cases + 1), cblock0(n_cases + 1), cellbase(n_cases + 1);
     std::vector<int64_t> pbases(n_cases);
     int max_tiles = 0;
+    int64_t max_cap = 0;
     for (int i = 0; i < n_cases; ++i) {
         const dsmc_params &p = cases[i];
         CaseDev cd = make_case(p, c->derived[i]);
@@ -702,6 +740,7 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
                                               4096));
         }
         cap = round_up(cap, TILE);
+        max_cap = std::max(max_cap, cap);
         cd.pbase = slot;
         cd.cap = cap;
         cd.cbase = cell;
@@ -723,7 +762,8 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     c->total_cells = cell;
     c->total_cell_tiles = cell_tiles;
     c->max_slot_tiles = max_tiles;
-    if (slot >= (int64_t(1) << 32) - 1 || cell >= (1 << 30)) {
+    // Keys hold cell ids and slots in 30 bits; global slots fit 32 bits.
+    if (slot >= (int64_t(1) << 32) - 1 || cell >= (1 << 30) - 1 || max_cap >= (int64_t(1) << 30)) {
         free_ctx(c);
         return DSMC_ERR_ARGUMENT;
     }
@@ -753,6 +793,10 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     c->cells.acc_stride = cell;
     ok &= alloc(reinterpret_cast<void **>(&c->tile_in), sizeof(int32_t) * max_tiles);
     ok &= alloc(reinterpret_cast<void **>(&c->tile_prefix), sizeof(int32_t) * max_tiles);
+    ok &= alloc(reinterpret_cast<void **>(&c->tile_dead), sizeof(int32_t) * max_tiles);
+    ok &= alloc(reinterpret_cast<void **>(&c->tile_dprefix), sizeof(int32_t) * max_tiles);
+    ok &= alloc(reinterpret_cast<void **>(&c->itile_dead), sizeof(int32_t) * max_tiles);
+    ok &= alloc(reinterpret_cast<void **>(&c->itile_dprefix), sizeof(int32_t) * max_tiles);
     const size_t chain = static_cast<size_t>(std::max(max_tiles, cell_tiles)) + 1;
     c->lb_words = 4 * chain;
     ok &= alloc(reinterpret_cast<void **>(&c->lb), sizeof(uint64_t) * c->lb_words);
@@ -762,6 +806,7 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     // survivors (n_old + n_inj <= cap) + refilled holes (<= n_old): <= 2 cap.
     ok &= alloc(reinterpret_cast<void **>(&c->obuf), sizeof(uint32_t) * 2 * slot);
     ok &= alloc(reinterpret_cast<void **>(&c->olist), sizeof(int32_t) * slot);
+    ok &= alloc(reinterpret_cast<void **>(&c->coll_list), sizeof(uint32_t) * cell);
     if (!ok) {
         free_ctx(c);
         return DSMC_ERR_CUDA;

@@ -24,11 +24,12 @@ constexpr int TILE_VEC = 4;
 constexpr int TILE = TILE_THREADS * TILE_VEC;
 
 // Sort key of a slot: bit 31 marks an "in-range" particle (still inside the
-// slot range its cell owned after the previous sort), bits 0-30 hold the
-// global cell id.  Removed particles carry KEY_DEAD.
+// slot range its cell owned after the previous sort), bit 30 a removed one,
+// bits 0-29 hold the global cell id (for a removed particle its old cell, or
+// all ones when it had none).  Cell ids and slots stay below 2^30.
 constexpr uint32_t KEY_IN = 0x80000000u;
-constexpr uint32_t KEY_CELL = 0x7FFFFFFFu;
-constexpr uint32_t KEY_DEAD = 0x7FFFFFFFu;
+constexpr uint32_t KEY_DEAD = 0x40000000u;
+constexpr uint32_t KEY_CELL = 0x3FFFFFFFu;
 constexpr int32_t NO_CELL = -1;
 
 // Bounded spin for the decoupled look-back chains (iterations of ~100 ns).
@@ -88,8 +89,8 @@ struct StepScratch {
     int32_t total_move_tiles, total_inject_tiles, total_tail_tiles;
     int32_t total_cell_tiles, total_otiles;
     uint32_t obuf_count;
+    uint32_t coll_count;  // cells listed by k_collide_select
     int32_t init_mode;
-    int32_t pad;
 };
 
 // ---- random numbers --------------------------------------------------------

@@ -15,7 +15,9 @@
 //   k_olist     grid     lists of the particles that changed cell
 //   k_cell_fix  grid     orders those lists, places them, per-cell bases
 //   k_scatter   tiles    places every in-range particle
-//   k_collide   cells    NTC collisions and moment sampling, one thread/cell
+//   k_collide_select  cells  NTC pair counts, list of cells with candidates
+//   k_collide_pairs   list   NTC + VHS collisions of the listed cells
+//   k_sample    cells    moment sampling, one thread per cell
 //   k_finish    1 CTA    Step++, NP = K
 //
 // Particle order contract (the reference's, made parallel):
@@ -272,17 +274,26 @@ __device__ __forceinline__ unsigned unpack3(unsigned long long v, int i)
     return static_cast<unsigned>((v >> (21 * i)) & 0x1FFFFFull);
 }
 
+// Slot mapping of a move tile: iteration k of thread t handles slot
+// tile + k * TILE_THREADS + t, so every load and store of a warp is one
+// contiguous 128-byte (FP32) access, and ranks in slot order come from warp
+// ballots: (iteration, warp) pairs are in slot order.
+constexpr int MOVE_WARPS = TILE_THREADS / 32;
+static_assert(TILE_VEC * MOVE_WARPS == 32, "one warp scans the (iteration, warp) counts");
+
 template <class T>
-__global__ void __launch_bounds__(TILE_THREADS, 2)
+__global__ void __launch_bounds__(TILE_THREADS, 4)
     k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
            Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
-           uint64_t *lb, int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc,
-           uint32_t *__restrict__ obuf, int ncase, int *err)
+           int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf, int ncase, int *err)
 {
     __shared__ int s_tile;
-    __shared__ uint64_t s_excl;
     __shared__ uint32_t s_obase;
+    __shared__ unsigned s_dead[32], s_out[32], s_in[32]; // ballots per (iteration, warp)
+    __shared__ unsigned s_opre[32];                      // exclusive prefix of s_out
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const unsigned lanes_below = (1u << lane) - 1u;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0)
@@ -296,109 +307,97 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
         const int64_t n_old = st[ci].n_old;
         const int64_t step = st[ci].step;
         const int local_tile = t - tt.move0[ci];
-        // Each thread owns TILE_VEC consecutive slots, so ranks within the
-        // tile follow slot order.
-        const int64_t q0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
-        const int64_t g0 = c.pbase + q0;
-        const bool full = q0 + TILE_VEC <= n_old;
+        const int64_t tile0 = static_cast<int64_t>(local_tile) * TILE;
+        const int64_t gt = c.pbase + tile0;
 
-        T xs[TILE_VEC], ys[TILE_VEC], vxs[TILE_VEC], vys[TILE_VEC];
-        if (full) {
-            load4(p.x + g0, xs);
-            load4(p.y + g0, ys);
-            load4(p.vx + g0, vxs);
-            load4(p.vy + g0, vys);
-        } else {
-#pragma unroll
-            for (int k = 0; k < TILE_VEC; ++k) {
-                const bool v = q0 + k < n_old;
-                xs[k] = v ? p.x[g0 + k] : T(0);
-                ys[k] = v ? p.y[g0 + k] : T(0);
-                vxs[k] = v ? p.vx[g0 + k] : T(0);
-                vys[k] = v ? p.vy[g0 + k] : T(0);
-            }
-        }
-
-        uint32_t keys[TILE_VEC];
-        int32_t ocs[TILE_VEC];
-        unsigned dead_mask = 0, out_mask = 0, n_in = 0;
-        int n_hit = 0;
         double impulse = 0.0;
-#pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            keys[k] = KEY_DEAD;
-            ocs[k] = NO_CELL;
-            if (q0 + k >= n_old)
-                continue;
-            const double x0 = static_cast<double>(xs[k]);
-            const double y0 = static_cast<double>(ys[k]);
-            const int32_t oc = cell_of(c, x0, y0);
-            ocs[k] = oc < 0 ? NO_CELL : c.cbase + oc;
-            const double dx = c.dt * static_cast<double>(vxs[k]);
-            const double dy = c.dt * static_cast<double>(vys[k]);
-            const double xe = x0 + dx;
-            const double ye = y0 + dy;
-            double t_hit = 0.0, nx = 0.0, ny = 0.0;
-            T xn, yn;
-            if (may_hit_box(c, x0, y0, xe, ye) &&
-                intersect_box_ool(c, x0, y0, dx, dy, t_hit, nx, ny)) {
-                impulse += wall_hit<T>(c, step, q0 + k, g0 + k, p, x0, y0, dx, dy, t_hit, nx, ny,
-                                       xn, yn);
-                n_hit++;
-            } else {
-                xn = Store<T>::rn(xe);
-                yn = Store<T>::rn(ye);
-                keep_outside<T>(c, xn, yn);
-            }
-            xs[k] = xn;
-            ys[k] = yn;
-            const double xd = static_cast<double>(xn);
-            const double yd = static_cast<double>(yn);
-            if (outside_domain(c, xd, yd)) {
-                dead_mask |= 1u << k;
-                continue;
-            }
-            const int32_t nc = cell_of(c, xd, yd);
-            if (nc < 0) {
-                // Inside the domain bounds but in no cell (rounding, NaN):
-                // the reference aborts in ExchangeParticles with code 30.
-                report_error(err, DSMC_ERR_EXCHANGE);
-                dead_mask |= 1u << k;
-                continue;
-            }
-            if (nc == oc) {
-                keys[k] = static_cast<uint32_t>(c.cbase + nc) | KEY_IN;
-                ++n_in;
-            } else {
-                keys[k] = static_cast<uint32_t>(c.cbase + nc);
-                out_mask |= 1u << k;
-            }
+        int n_hit = 0;
+        int64_t q = tile0 + threadIdx.x;
+        T cx{}, cy{}, cvx{}, cvy{};
+        if (q < n_old) {
+            cx = p.x[gt + threadIdx.x];
+            cy = p.y[gt + threadIdx.x];
+            cvx = p.vx[gt + threadIdx.x];
+            cvy = p.vy[gt + threadIdx.x];
         }
-        if (full) {
-            store4(p.x + g0, xs);
-            store4(p.y + g0, ys);
-            store4(key + g0, keys);
-        } else {
-#pragma unroll
-            for (int k = 0; k < TILE_VEC; ++k)
-                if (q0 + k < n_old) {
-                    p.x[g0 + k] = xs[k];
-                    p.y[g0 + k] = ys[k];
-                    key[g0 + k] = keys[k];
+#pragma unroll 1
+        for (int k = 0; k < TILE_VEC; ++k, q += TILE_THREADS) {
+            const int e = k * TILE_THREADS + threadIdx.x;
+            const int64_t g = gt + e;
+            T nx_{}, ny_{}, nvx{}, nvy{};
+            if (k + 1 < TILE_VEC && q + TILE_THREADS < n_old) {
+                nx_ = p.x[g + TILE_THREADS];
+                ny_ = p.y[g + TILE_THREADS];
+                nvx = p.vx[g + TILE_THREADS];
+                nvy = p.vy[g + TILE_THREADS];
+            }
+            bool dead = false, out = false, in = false;
+            int32_t ocg = NO_CELL;
+            uint32_t kk = KEY_DEAD;
+            if (q < n_old) {
+                const double x0 = static_cast<double>(cx);
+                const double y0 = static_cast<double>(cy);
+                const int32_t oc = cell_of(c, x0, y0);
+                ocg = oc < 0 ? NO_CELL : c.cbase + oc;
+                const double dx = c.dt * static_cast<double>(cvx);
+                const double dy = c.dt * static_cast<double>(cvy);
+                const double xe = x0 + dx;
+                const double ye = y0 + dy;
+                double t_hit = 0.0, hnx = 0.0, hny = 0.0;
+                T xn, yn;
+                if (may_hit_box(c, x0, y0, xe, ye) &&
+                    intersect_box_ool(c, x0, y0, dx, dy, t_hit, hnx, hny)) {
+                    impulse += wall_hit<T>(c, step, q, g, p, x0, y0, dx, dy, t_hit, hnx, hny, xn,
+                                           yn);
+                    n_hit++;
+                } else {
+                    xn = Store<T>::rn(xe);
+                    yn = Store<T>::rn(ye);
+                    keep_outside<T>(c, xn, yn);
                 }
-        }
-        // Cell counts.  Every cell starts the step with its old count as its
-        // in-range count, so only the few slots that leave a cell (or the
-        // domain) touch the counters.
-        const unsigned leave = dead_mask | out_mask;
-        if (leave) {
-#pragma unroll
-            for (int k = 0; k < TILE_VEC; ++k) {
-                if (((leave >> k) & 1u) && ocs[k] != NO_CELL)
-                    atomicSub(cells.n_in + ocs[k], 1);
-                if ((out_mask >> k) & 1u)
-                    atomicAdd(cells.n_o + (keys[k] & KEY_CELL), 1);
+                p.x[g] = xn;
+                p.y[g] = yn;
+                const double xd = static_cast<double>(xn);
+                const double yd = static_cast<double>(yn);
+                if (outside_domain(c, xd, yd)) {
+                    dead = true;
+                } else {
+                    const int32_t nc = cell_of(c, xd, yd);
+                    if (nc < 0) {
+                        // Inside the domain bounds but in no cell (rounding,
+                        // NaN): the reference aborts in ExchangeParticles, 30.
+                        report_error(err, DSMC_ERR_EXCHANGE);
+                        dead = true;
+                    } else if (nc == oc) {
+                        kk = static_cast<uint32_t>(c.cbase + nc) | KEY_IN;
+                        in = true;
+                    } else {
+                        kk = static_cast<uint32_t>(c.cbase + nc);
+                        out = true;
+                    }
+                }
+                if (dead)
+                    kk = KEY_DEAD | (ocg == NO_CELL ? KEY_CELL : static_cast<uint32_t>(ocg));
+                key[g] = kk;
+                // Every cell starts the step with its old count as its
+                // in-range count: only slots that leave it touch a counter.
+                if ((dead || out) && ocg != NO_CELL)
+                    atomicSub(cells.n_in + ocg, 1);
+                if (out)
+                    atomicAdd(cells.n_o + (kk & KEY_CELL), 1);
             }
+            const unsigned bd = __ballot_sync(0xffffffffu, dead);
+            const unsigned bo = __ballot_sync(0xffffffffu, out);
+            const unsigned bi = __ballot_sync(0xffffffffu, in);
+            if (lane == 0) {
+                s_dead[k * MOVE_WARPS + warp] = bd;
+                s_out[k * MOVE_WARPS + warp] = bo;
+                s_in[k * MOVE_WARPS + warp] = bi;
+            }
+            cx = nx_;
+            cy = ny_;
+            cvx = nvx;
+            cvy = nvy;
         }
         // Wall-hit diagnostics (Boundary.cpp:318-319).
         {
@@ -414,33 +413,37 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
                 atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(hits));
             }
         }
-        // One block scan for the three tile counts.
-        unsigned long long tot;
-        const unsigned long long ex = block_exclusive<unsigned long long>(
-            pack3(n_in, __popc(dead_mask), __popc(out_mask)), tot);
-        if (threadIdx.x < 32) {
-            const unsigned dead_tile = unpack3(tot, 1), out_tile = unpack3(tot, 2);
-            const uint64_t excl = lookback_warp(lb, t, t - local_tile, dead_tile, err);
-            if (threadIdx.x == 0) {
-                tile_in[t] = static_cast<int32_t>(unpack3(tot, 0));
-                s_excl = excl;
-                if (local_tile == st[ci].n_move_tiles - 1)
-                    st[ci].dead_old = static_cast<int64_t>(excl) + dead_tile;
+        __syncthreads();
+        if (warp == 0) {
+            // Lane i holds the counts of (iteration, warp) pair i; pairs are
+            // in slot order, so an exclusive scan gives list ranks in slot
+            // order.  Removed slots are only counted here: their ranks come
+            // from k_dead_scan and k_holes, so no tile waits on another.
+            const unsigned o = __popc(s_out[lane]);
+            unsigned oi = o;
+#pragma unroll
+            for (int sft = 1; sft < 32; sft <<= 1) {
+                const unsigned b = __shfl_up_sync(0xffffffffu, oi, sft);
+                if (lane >= sft)
+                    oi += b;
+            }
+            s_opre[lane] = oi - o;
+            const unsigned out_tile = __shfl_sync(0xffffffffu, oi, 31);
+            const unsigned dead_tile = static_cast<unsigned>(warp_sum_u64(__popc(s_dead[lane])));
+            const unsigned in_tile = static_cast<unsigned>(warp_sum_u64(__popc(s_in[lane])));
+            if (lane == 0) {
+                tile_in[t] = static_cast<int32_t>(in_tile);
+                tile_dead[t] = static_cast<int32_t>(dead_tile);
                 s_obase = out_tile ? atomicAdd(&sc->obuf_count, out_tile) : 0u;
             }
         }
         __syncthreads();
-        int64_t rank = static_cast<int64_t>(s_excl) + unpack3(ex, 1);
-        uint32_t ob = s_obase + unpack3(ex, 2);
-#pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if ((dead_mask >> k) & 1u) {
-                hole_pos[c.pbase + rank] = static_cast<int32_t>(q0 + k);
-                hole_oc[c.pbase + rank] = ocs[k];
-                ++rank;
-            }
-            if ((out_mask >> k) & 1u)
-                obuf[ob++] = static_cast<uint32_t>(g0 + k);
+            const int i = k * MOVE_WARPS + warp;
+            const unsigned bo = s_out[i];
+            if ((bo >> lane) & 1u)
+                obuf[s_obase + s_opre[i] + __popc(bo & lanes_below)] =
+                    static_cast<uint32_t>(gt + k * TILE_THREADS + threadIdx.x);
         }
     }
 }
@@ -455,12 +458,10 @@ __global__ void __launch_bounds__(TILE_THREADS, 2)
 template <class T>
 __global__ void __launch_bounds__(TILE_THREADS)
     k_inject(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
-             Slots<T> p, uint32_t *__restrict__ key, Cells cells, uint64_t *lb,
-             int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc,
-             uint32_t *__restrict__ obuf, int ncase, int *err)
+             Slots<T> p, uint32_t *__restrict__ key, Cells cells,
+             int32_t *__restrict__ itile_dead, uint32_t *__restrict__ obuf, int ncase, int *err)
 {
     __shared__ int s_tile;
-    __shared__ uint64_t s_excl;
     const int init_mode = sc->init_mode;
     for (;;) {
         __syncthreads();
@@ -480,7 +481,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
         int n_dead = 0;
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            keys[k] = KEY_DEAD;
+            keys[k] = KEY_DEAD | KEY_CELL;
             const int64_t j = j0 + k;
             if (j >= n_inj)
                 continue;
@@ -534,7 +535,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
         }
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            const bool alive = keys[k] != KEY_DEAD;
+            const bool alive = !(keys[k] & KEY_DEAD);
             const int32_t cg = static_cast<int32_t>(keys[k] & KEY_CELL);
             warp_aggregated_inc(cells.n_o, cg, alive);
             const unsigned m = __ballot_sync(0xffffffffu, alive);
@@ -550,29 +551,100 @@ __global__ void __launch_bounds__(TILE_THREADS)
             }
         }
         int dead_total;
-        const int dead_excl = block_exclusive<int>(n_dead, dead_total);
-        if (threadIdx.x < 32) {
-            // The chain of this case continues the removed count of its
-            // moved slots: the first inject tile starts at dead_old.
-            const bool first = local_tile == 0;
-            const uint64_t agg = static_cast<uint64_t>(dead_total) +
-                                 (first ? static_cast<uint64_t>(s.dead_old) : 0ull);
-            const uint64_t excl = lookback_warp(lb, t, t - local_tile, agg, err);
-            if (threadIdx.x == 0) {
-                s_excl = first ? static_cast<uint64_t>(s.dead_old) : excl;
-                if (local_tile == s.n_inject_tiles - 1)
-                    st[ci].dead_total = static_cast<int64_t>(excl + agg);
+        (void)block_exclusive<int>(n_dead, dead_total);
+        if (threadIdx.x == 0)
+            itile_dead[t] = dead_total;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_dead_scan: per case (one CTA each), exclusive prefix of the removed-slot
+// counts of its move tiles, then of its inject tiles, in slot order; sets
+// dead_old and dead_total.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_dead_scan(CaseState *st, const int32_t *tile_dead, int32_t *tile_dprefix,
+                const int32_t *itile_dead, int32_t *itile_dprefix)
+{
+    constexpr int PER = 8;
+    CaseState &s = st[blockIdx.x];
+    int32_t carry = 0;
+    for (int part = 0; part < 2; ++part) {
+        const int n = part == 0 ? s.n_move_tiles : s.n_inject_tiles;
+        const int t0 = part == 0 ? s.move_tile0 : s.inject_tile0;
+        const int32_t *in = (part == 0 ? tile_dead : itile_dead) + t0;
+        int32_t *out = (part == 0 ? tile_dprefix : itile_dprefix) + t0;
+        for (int b = 0; b < n; b += TILE_THREADS * PER) {
+            const int i0 = b + threadIdx.x * PER;
+            int v[PER];
+            int sum = 0;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                v[k] = i0 + k < n ? in[i0 + k] : 0;
+                sum += v[k];
             }
+            int tot;
+            int run = carry + block_exclusive<int>(sum, tot);
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                if (i0 + k < n)
+                    out[i0 + k] = run;
+                run += v[k];
+            }
+            carry += tot;
         }
-        __syncthreads();
-        int64_t rank = static_cast<int64_t>(s_excl) + dead_excl;
+        if (threadIdx.x == 0) {
+            if (part == 0)
+                s.dead_old = carry;
+            else
+                s.dead_total = carry;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_holes: the removed-slot list in slot order (hole_pos, and the old cell of
+// each removed slot in hole_oc), from the tiles that have removed slots.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_holes(const CaseDev *__restrict__ cases, const CaseState *st, const StepScratch *sc,
+            TileTables tt, const uint32_t *__restrict__ key, const int32_t *tile_dead,
+            const int32_t *tile_dprefix, const int32_t *itile_dead, const int32_t *itile_dprefix,
+            int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc, int ncase)
+{
+    const int n_move = sc->total_move_tiles;
+    const int total = n_move + sc->total_inject_tiles;
+    for (int T = blockIdx.x; T < total; T += gridDim.x) {
+        const bool moved = T < n_move;
+        const int t = moved ? T : T - n_move;
+        const int count = moved ? tile_dead[t] : itile_dead[t];
+        if (count == 0)
+            continue; // uniform over the block
+        const int ci = case_of(moved ? tt.move0 : tt.inject0, ncase, t);
+        const CaseDev &c = cases[ci];
+        const CaseState &s = st[ci];
+        const int local_tile = t - (moved ? tt.move0[ci] : tt.inject0[ci]);
+        const int64_t first = moved ? 0 : s.n_old;
+        const int64_t end = moved ? s.n_old : s.n_total;
+        const int64_t q0 = first + static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
+        uint32_t keys[TILE_VEC];
+        int n_dead = 0;
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if (j0 + k < n_inj && keys[k] == KEY_DEAD) {
-                hole_pos[c.pbase + rank] = static_cast<int32_t>(s.n_old + j0 + k);
-                hole_oc[c.pbase + rank] = NO_CELL;
-                ++rank;
-            }
+            keys[k] = q0 + k < end ? key[c.pbase + q0 + k] : 0u;
+            n_dead += (keys[k] & KEY_DEAD) ? 1 : 0;
+        }
+        int tot;
+        int64_t rank = (moved ? tile_dprefix[t] : itile_dprefix[t]) +
+                       block_exclusive<int>(n_dead, tot);
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            if (!(keys[k] & KEY_DEAD))
+                continue;
+            const uint32_t oc = keys[k] & KEY_CELL;
+            hole_pos[c.pbase + rank] = static_cast<int32_t>(q0 + k);
+            hole_oc[c.pbase + rank] = oc == KEY_CELL ? NO_CELL : static_cast<int32_t>(oc);
+            ++rank;
         }
     }
 }
@@ -585,9 +657,7 @@ __global__ void k_plan2(const CaseDev *cases, CaseState *st, StepScratch *sc, Ti
 {
     for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
         CaseState &s = st[i];
-        if (s.n_inject_tiles == 0)
-            s.dead_total = s.dead_old;
-        const int64_t keep = s.n_total - s.dead_total;
+        const int64_t keep = s.n_total - s.dead_total; // dead_total: k_dead_scan
         s.n_keep = keep;
         // Holes are the removed slots below K; the list is in slot order.
         const int32_t *hp = hole_pos + cases[i].pbase;
@@ -650,7 +720,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
             keys[k] = KEY_DEAD;
             if (q0 + k < s.n_total)
                 keys[k] = key[c.pbase + q0 + k];
-            n_alive += keys[k] != KEY_DEAD ? 1 : 0;
+            n_alive += (keys[k] & KEY_DEAD) ? 0 : 1;
         }
         int alive_total;
         const int alive_excl = block_exclusive<int>(n_alive, alive_total);
@@ -663,7 +733,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
         int64_t r = static_cast<int64_t>(s_excl) + alive_excl;
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if (keys[k] == KEY_DEAD)
+            if (keys[k] & KEY_DEAD)
                 continue;
             const int64_t m = s.n_holes - 1 - r;
             ++r;
@@ -821,7 +891,7 @@ __global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
         if (q >= st[lo].n_keep)
             continue; // a tail slot that moved into a hole; listed there
         const uint32_t k = key[g];
-        if (k == KEY_DEAD || (k & KEY_IN))
+        if (k & (KEY_DEAD | KEY_IN))
             continue;
         const int32_t cg = static_cast<int32_t>(k & KEY_CELL);
         const int32_t j = atomicAdd(cells.o_fill + cg, 1);
@@ -936,13 +1006,13 @@ __global__ void __launch_bounds__(TILE_THREADS)
         int n_in = 0;
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k)
-            n_in += (keys[k] != KEY_DEAD && (keys[k] & KEY_IN)) ? 1 : 0;
+            n_in += (keys[k] & KEY_IN) ? 1 : 0;
         int tot;
         const int ex = block_exclusive<int>(n_in, tot);
         int64_t f = (tot > 0 ? tile_prefix[s.move_tile0 + local_tile] : 0) + ex;
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if (keys[k] == KEY_DEAD)
+            if (keys[k] & KEY_DEAD)
                 continue;
             int64_t fin;
             if (keys[k] & KEY_IN) {
@@ -966,19 +1036,134 @@ __global__ void __launch_bounds__(TILE_THREADS)
 }
 
 // ---------------------------------------------------------------------------
-// k_collide: per cell, BinaryCollisionsInCell (Collision.cpp:21-44) with one
-// stream per cell, then Sampling's accumulation (Sampling.cpp:14-31) in the
-// reference's order: one thread per cell walks its particles sequentially, so
-// every FP64 sum is bit-identical to the reference's.  A CTA stages the
-// velocities of its cells in shared memory when they fit.
+// Collisions, BinaryCollisionsInCell (Collision.cpp:21-44) with one stream
+// per cell, in two passes.  k_collide_select makes every cell's first draw
+// (the Bernoulli rounding of the pair count) and lists the cells that have
+// candidate pairs; at the reference's rarefaction that is about one cell in
+// a thousand.  k_collide_pairs then runs the candidate loop of the listed
+// cells only, continuing each cell's stream at draw 1.  The expensive code
+// (pow, sin, cos, the elastic collision) thus sets neither the register
+// budget nor the occupancy of the passes that touch every cell.
 // ---------------------------------------------------------------------------
 constexpr int COLLIDE_CELLS = 128;
 constexpr int COLLIDE_SMEM_PCL = 3072;
 
+// NTC pair count of a cell with n particles (Collision.cpp:23-27) and the
+// draw that rounds it.
+__device__ __forceinline__ int ntc_pairs(const CaseDev &c, int n, dsmc_stream &r)
+{
+    const double npair = 0.5 * n * (n - 1) * c.weight * c.sc_max * c.dt / c.dv;
+    int nn = static_cast<int>(npair);
+    const double frac = npair - nn;
+    return (uniform(r) < frac) ? nn + 1 : nn;
+}
+
+__global__ void __launch_bounds__(256)
+    k_collide_select(const CaseDev *__restrict__ cases, const CaseState *st, StepScratch *sc,
+                     TileTables tt, Cells cells, int side, uint32_t *__restrict__ coll_list,
+                     int total_cells, int ncase)
+{
+    const int32_t *start = cells.start[side];
+    for (int base = blockIdx.x * blockDim.x; base < total_cells; base += gridDim.x * blockDim.x) {
+        const int cg = base + threadIdx.x;
+        bool listed = false;
+        if (cg < total_cells) {
+            const int ci = case_of(tt.cellbase, ncase, cg);
+            const CaseDev &c = cases[ci];
+            const int cl = cg - c.cbase;
+            if (cl < c.ncell) {
+                const int n = start[cg + 1] - start[cg];
+                if (n >= 2) {
+                    dsmc_stream r;
+                    open_stream(r, c, DSMC_RNG_COLLIDE, st[ci].step, static_cast<uint32_t>(cl));
+                    listed = ntc_pairs(c, n, r) > 0;
+                }
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, listed);
+        if (m) {
+            const int lane = threadIdx.x & 31;
+            uint32_t b = 0;
+            if (lane == __ffs(m) - 1)
+                b = atomicAdd(&sc->coll_count, static_cast<uint32_t>(__popc(m)));
+            b = __shfl_sync(0xffffffffu, b, __ffs(m) - 1);
+            if (listed)
+                coll_list[b + __popc(m & ((1u << lane) - 1u))] = static_cast<uint32_t>(cg);
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(128)
+    k_collide_pairs(const CaseDev *__restrict__ cases, CaseState *st, const StepScratch *sc,
+                    TileTables tt, Slots<T> p, Cells cells, int side,
+                    const uint32_t *__restrict__ coll_list, int ncase)
+{
+    const int32_t *start = cells.start[side];
+    const uint32_t count = sc->coll_count;
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
+         w += gridDim.x * blockDim.x) {
+        const int cg = static_cast<int>(coll_list[w]);
+        const int ci = case_of(tt.cellbase, ncase, cg);
+        const CaseDev &c = cases[ci];
+        CaseState &s = st[ci];
+        const int cl = cg - c.cbase;
+        const int64_t a0 = c.pbase + start[cg];
+        const int n = start[cg + 1] - start[cg];
+        dsmc_stream r;
+        open_stream(r, c, DSMC_RNG_COLLIDE, s.step, static_cast<uint32_t>(cl));
+        const int nn = ntc_pairs(c, n, r); // draw 0 again: the same value
+        int ncc = 0;
+        for (int kk = 0; kk < nn; ++kk) {
+            const int i = irand_uniform(r, n);
+            int j;
+            do {
+                j = irand_uniform(r, n);
+            } while (j == i);
+            const double vi0 = p.vx[a0 + i], vi1 = p.vy[a0 + i], vi2 = p.vz[a0 + i];
+            const double vj0 = p.vx[a0 + j], vj1 = p.vy[a0 + j], vj2 = p.vz[a0 + j];
+            const double vr0 = vj0 - vi0, vr1 = vj1 - vi1, vr2 = vj2 - vi2;
+            const double cr = sqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
+            const double sigma = c.sigma_ref * pow(c.cr_ref / cr, c.omega);
+            if (uniform(r) < sigma * cr / c.sc_max) {
+                // ElasticCollision, Collision.cpp:7-19, with v3rand_isotropic
+                // (rng/IsotropicVectorRNG.cxx:11-19).
+                const double cos_t = 1.0 - 2.0 * uniform(r);
+                const double sin_t = sqrt(1.0 - cos_t * cos_t);
+                const double e = 2.0 * PI_D * uniform(r);
+                const double nv[3] = {cos_t, sin_t * cos(e), sin_t * sin(e)};
+                const double half = cr * 0.5;
+                const double vc0 = 0.5 * (vj0 + vi0), vc1 = 0.5 * (vj1 + vi1),
+                             vc2 = 0.5 * (vj2 + vi2);
+                const double d0 = half * nv[0], d1 = half * nv[1], d2 = half * nv[2];
+                p.vx[a0 + i] = Store<T>::rn(vc0 + d0);
+                p.vy[a0 + i] = Store<T>::rn(vc1 + d1);
+                p.vz[a0 + i] = Store<T>::rn(vc2 + d2);
+                p.vx[a0 + j] = Store<T>::rn(vc0 - d0);
+                p.vy[a0 + j] = Store<T>::rn(vc1 - d1);
+                p.vz[a0 + j] = Store<T>::rn(vc2 - d2);
+                ncc++;
+            }
+        }
+        if (ncc > 0) {
+            if (s.sampling_mode == 1) // CollideParticles, Collision.cpp:53
+                cells.acc[ACC_NC * cells.acc_stride + cg] += ncc;
+            atomicAdd(reinterpret_cast<unsigned long long *>(&s.nc_step),
+                      static_cast<unsigned long long>(ncc));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_sample: Sampling's accumulation (Sampling.cpp:14-31) in the reference's
+// order: one thread per cell walks its particles sequentially, so every FP64
+// sum is bit-identical to the reference's.  A CTA stages the velocities of its
+// cells in shared memory when they fit.
+// ---------------------------------------------------------------------------
 template <class T>
 __global__ void __launch_bounds__(COLLIDE_CELLS)
-    k_collide(const CaseDev *__restrict__ cases, CaseState *st, TileTables tt, Slots<T> p,
-              Cells cells, int side, int do_collide, int do_sample, int ncase)
+    k_sample(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt, Slots<T> p,
+             Cells cells, int side, int ncase)
 {
     extern __shared__ unsigned char smem_raw[];
     T *sv = reinterpret_cast<T *>(smem_raw);
@@ -986,122 +1171,67 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
     const int nblocks = tt.cblock0[ncase];
     for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int ci = case_of(tt.cblock0, ncase, b);
+        if (st[ci].sampling_mode != 1)
+            continue;
         const CaseDev &c = cases[ci];
-        CaseState &s = st[ci];
-        const int block_local = b - tt.cblock0[ci];
-        const int cl0 = block_local * COLLIDE_CELLS;
+        const int cl0 = (b - tt.cblock0[ci]) * COLLIDE_CELLS;
         const int cl1 = min(cl0 + COLLIDE_CELLS, c.ncell);
         const int64_t r0 = start[c.cbase + cl0], r1 = start[c.cbase + cl1];
         const int64_t nr = r1 - r0;
         const bool staged = nr <= COLLIDE_SMEM_PCL;
         __syncthreads();
         if (staged) {
+            const T *gx = p.vx + c.pbase + r0, *gy = p.vy + c.pbase + r0,
+                    *gz = p.vz + c.pbase + r0;
             for (int64_t i = threadIdx.x; i < nr; i += blockDim.x) {
-                sv[i] = p.vx[c.pbase + r0 + i];
-                sv[COLLIDE_SMEM_PCL + i] = p.vy[c.pbase + r0 + i];
-                sv[2 * COLLIDE_SMEM_PCL + i] = p.vz[c.pbase + r0 + i];
+                sv[i] = gx[i];
+                sv[COLLIDE_SMEM_PCL + i] = gy[i];
+                sv[2 * COLLIDE_SMEM_PCL + i] = gz[i];
             }
         }
         __syncthreads();
         const int cl = cl0 + threadIdx.x;
-        int ncc = 0;
-        if (cl < cl1) {
-            const int cg = c.cbase + cl;
-            const int64_t a0 = start[cg];
-            const int n = static_cast<int>(start[cg + 1] - a0);
-            // Velocity access: shared memory when staged, else global.
-            auto vel = [&](int i, int m) -> double {
-                if (staged)
-                    return static_cast<double>(sv[m * COLLIDE_SMEM_PCL + (a0 - r0) + i]);
-                const int64_t g = c.pbase + a0 + i;
-                return static_cast<double>(m == 0 ? p.vx[g] : (m == 1 ? p.vy[g] : p.vz[g]));
-            };
-            auto set_vel = [&](int i, double v0, double v1, double v2) {
-                const int64_t g = c.pbase + a0 + i;
-                const T t0 = Store<T>::rn(v0), t1 = Store<T>::rn(v1), t2 = Store<T>::rn(v2);
-                p.vx[g] = t0;
-                p.vy[g] = t1;
-                p.vz[g] = t2;
-                if (staged) {
-                    const int64_t o = (a0 - r0) + i;
-                    sv[o] = t0;
-                    sv[COLLIDE_SMEM_PCL + o] = t1;
-                    sv[2 * COLLIDE_SMEM_PCL + o] = t2;
-                }
-            };
-            if (do_collide && n >= 2) {
-                dsmc_stream r;
-                open_stream(r, c, DSMC_RNG_COLLIDE, s.step, static_cast<uint32_t>(cl));
-                const double npair = 0.5 * n * (n - 1) * c.weight * c.sc_max * c.dt / c.dv;
-                int nn = static_cast<int>(npair);
-                const double frac = npair - nn;
-                nn = (uniform(r) < frac) ? nn + 1 : nn;
-                for (int kk = 0; kk < nn; ++kk) {
-                    const int i = irand_uniform(r, n);
-                    int j;
-                    do {
-                        j = irand_uniform(r, n);
-                    } while (j == i);
-                    const double vi0 = vel(i, 0), vi1 = vel(i, 1), vi2 = vel(i, 2);
-                    const double vj0 = vel(j, 0), vj1 = vel(j, 1), vj2 = vel(j, 2);
-                    const double vr0 = vj0 - vi0, vr1 = vj1 - vi1, vr2 = vj2 - vi2;
-                    const double cr = sqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
-                    const double sigma = c.sigma_ref * pow(c.cr_ref / cr, c.omega);
-                    if (uniform(r) < sigma * cr / c.sc_max) {
-                        // ElasticCollision, Collision.cpp:7-19, with
-                        // v3rand_isotropic (rng/IsotropicVectorRNG.cxx:11-19).
-                        const double cos_t = 1.0 - 2.0 * uniform(r);
-                        const double sin_t = sqrt(1.0 - cos_t * cos_t);
-                        const double e = 2.0 * PI_D * uniform(r);
-                        const double nv[3] = {cos_t, sin_t * cos(e), sin_t * sin(e)};
-                        const double half = cr * 0.5;
-                        const double vc0 = 0.5 * (vj0 + vi0), vc1 = 0.5 * (vj1 + vi1),
-                                     vc2 = 0.5 * (vj2 + vi2);
-                        const double d0 = half * nv[0], d1 = half * nv[1], d2 = half * nv[2];
-                        set_vel(i, vc0 + d0, vc1 + d1, vc2 + d2);
-                        set_vel(j, vc0 - d0, vc1 - d1, vc2 - d2);
-                        ncc++;
-                    }
-                }
-                if (s.sampling_mode == 1 && ncc > 0)
-                    cells.acc[ACC_NC * cells.acc_stride + cg] += ncc;
-            }
-            if (do_sample && s.sampling_mode == 1 && n > 0) {
-                double a[ACC_NC];
-#pragma unroll
-                for (int m = 0; m < ACC_NC; ++m)
-                    a[m] = cells.acc[m * cells.acc_stride + cg];
-                for (int i = 0; i < n; ++i) {
-                    const double v0 = vel(i, 0), v1 = vel(i, 1), v2 = vel(i, 2);
-                    a[ACC_NP] += 1.0;
-                    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
-                    a[ACC_V0] += v0;
-                    a[ACC_V1] += v1;
-                    a[ACC_V2] += v2;
-                    a[ACC_V2V0] += vv * v0;
-                    a[ACC_V2V1] += vv * v1;
-                    a[ACC_V2V2] += vv * v2;
-                    a[ACC_VV00] += v0 * v0;
-                    a[ACC_VV01] += v0 * v1;
-                    a[ACC_VV02] += v0 * v2;
-                    a[ACC_VV11] += v1 * v1;
-                    a[ACC_VV12] += v1 * v2;
-                    a[ACC_VV22] += v2 * v2;
-                }
-#pragma unroll
-                for (int m = 0; m < ACC_NC; ++m)
-                    cells.acc[m * cells.acc_stride + cg] = a[m];
-            }
+        if (cl >= cl1)
+            continue;
+        const int cg = c.cbase + cl;
+        const int64_t a0 = start[cg];
+        const int n = static_cast<int>(start[cg + 1] - a0);
+        if (n == 0)
+            continue;
+        const T *vx, *vy, *vz;
+        if (staged) {
+            vx = sv + (a0 - r0);
+            vy = sv + COLLIDE_SMEM_PCL + (a0 - r0);
+            vz = sv + 2 * COLLIDE_SMEM_PCL + (a0 - r0);
+        } else {
+            vx = p.vx + c.pbase + a0;
+            vy = p.vy + c.pbase + a0;
+            vz = p.vz + c.pbase + a0;
         }
-        if (do_collide) {
-            int tot = ncc;
+        double a[ACC_NC];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                tot += __shfl_xor_sync(0xffffffffu, tot, o);
-            if ((threadIdx.x & 31) == 0 && tot > 0)
-                atomicAdd(reinterpret_cast<unsigned long long *>(&s.nc_step),
-                          static_cast<unsigned long long>(tot));
+        for (int m = 0; m < ACC_NC; ++m)
+            a[m] = cells.acc[m * cells.acc_stride + cg];
+        for (int i = 0; i < n; ++i) {
+            const double v0 = vx[i], v1 = vy[i], v2 = vz[i];
+            a[ACC_NP] += 1.0;
+            const double vv = v0 * v0 + v1 * v1 + v2 * v2;
+            a[ACC_V0] += v0;
+            a[ACC_V1] += v1;
+            a[ACC_V2] += v2;
+            a[ACC_V2V0] += vv * v0;
+            a[ACC_V2V1] += vv * v1;
+            a[ACC_V2V2] += vv * v2;
+            a[ACC_VV00] += v0 * v0;
+            a[ACC_VV01] += v0 * v1;
+            a[ACC_VV02] += v0 * v2;
+            a[ACC_VV11] += v1 * v1;
+            a[ACC_VV12] += v1 * v2;
+            a[ACC_VV22] += v2 * v2;
         }
+#pragma unroll
+        for (int m = 0; m < ACC_NC; ++m)
+            cells.acc[m * cells.acc_stride + cg] = a[m];
     }
 }
 
