@@ -191,7 +191,7 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_DEAD_SCAN);
-        k_dead_scan<<<c->ncase, TILE_THREADS, 0, c->stream>>>(c->d_state, c->tile_dead,
+        k_dead_scan<<<c->ncase, SCAN_THREADS, 0, c->stream>>>(c->d_state, c->tile_dead,
                                                               c->tile_dprefix, c->itile_dead,
                                                               c->itile_dprefix);
     }
@@ -228,7 +228,7 @@ template <class T> int enqueue_index(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_TILE_SCAN);
-        k_tile_scan<<<c->ncase, TILE_THREADS, 0, c->stream>>>(c->d_state, c->tile_in,
+        k_tile_scan<<<c->ncase, SCAN_THREADS, 0, c->stream>>>(c->d_state, c->tile_in,
                                                               c->tile_prefix);
     }
     {
@@ -344,6 +344,7 @@ CaseDev make_case(const dsmc_params &p, const dsmc_derived &d)
     c.dt = p.dt;
     c.inv_dx = 1.0 / d.dx;
     c.inv_dy = 1.0 / d.dy;
+    double near_margin;
     {
         double mag = 1.0;
         const double v[] = {p.x1, p.x2, p.y1, p.y2, p.box_x - p.box_width / 2.0,
@@ -352,11 +353,19 @@ CaseDev make_case(const dsmc_params &p, const dsmc_derived &d)
         for (double a : v)
             mag = std::max(mag, std::fabs(a));
         c.cull = 1e-9 * mag;
+        near_margin = c.cull + std::ldexp(mag, -20);
     }
     c.box_lo[0] = p.box_x - p.box_width / 2.0; // Geometry.cpp:184
     c.box_lo[1] = p.box_y - p.box_height / 2.0;
     c.box_hi[0] = p.box_x + p.box_width / 2.0; // Geometry.cpp:185
     c.box_hi[1] = p.box_y + p.box_height / 2.0;
+    {
+        const double m = near_margin;
+        c.near_lo[0] = c.box_lo[0] - m;
+        c.near_lo[1] = c.box_lo[1] - m;
+        c.near_hi[0] = c.box_hi[0] + m;
+        c.near_hi[1] = c.box_hi[1] + m;
+    }
     c.box_x = p.box_x;
     c.box_y = p.box_y;
     c.box_hw = p.box_width / 2.0; // Geometry.cpp:175-176

@@ -41,6 +41,7 @@ struct CaseDev {
     double dx, dy, dv, dt;
     double inv_dx, inv_dy;         // 1 / DX, 1 / DY (fast path of the cell index)
     double cull;                   // margin of the box pre-test (may_hit_box)
+    double near_lo[2], near_hi[2]; // box widened by cull + 2^-20 of the coordinates
     double box_lo[2], box_hi[2];   // IntersectBox bounds (Geometry.cpp:184-185)
     double box_x, box_y;           // InsideBox centre (Geometry.cpp:175-176)
     double box_hw, box_hh;         // BoxWidth / 2.0, BoxHeight / 2.0
@@ -303,6 +304,26 @@ __device__ __forceinline__ int32_t cell_of(const CaseDev &c, double x, double y)
     return static_cast<int32_t>(fk) * c.ny + static_cast<int32_t>(fl);
 }
 
+// Estimate-only form of cell_of for the free-flight pass: false when either
+// floor is not certain from the estimate (the exact form then decides), else
+// the cell (NO_CELL outside the grid) in `cell`.
+__device__ __forceinline__ bool cell_of_fast(const CaseDev &c, double x, double y, int32_t &cell)
+{
+    const double qk = (x - c.x1) * c.inv_dx;
+    const double ql = (y - c.y1) * c.inv_dy;
+    const double fk = floor(qk);
+    const double fl = floor(ql);
+    const double rk = qk - fk;
+    const double rl = ql - fl;
+    if (!(rk > 1e-9 && rk < 1.0 - 1e-9 && rl > 1e-9 && rl < 1.0 - 1e-9 && fabs(qk) < 1e6 &&
+          fabs(ql) < 1e6))
+        return false;
+    cell = (fk >= 0.0 && fk < c.nx && fl >= 0.0 && fl < c.ny)
+               ? static_cast<int32_t>(fk) * c.ny + static_cast<int32_t>(fl)
+               : NO_CELL;
+    return true;
+}
+
 // False only when IntersectBox cannot report an impact: the segment's
 // bounding box is more than `cull` clear of the box.  An impact needs the
 // slab entry time <= 1 and the exit time >= 0, i.e. the segment reaching the
@@ -314,6 +335,18 @@ __device__ __forceinline__ bool may_hit_box(const CaseDev &c, double x0, double 
 {
     return fmax(x0, x1) > c.box_lo[0] - c.cull && fmin(x0, x1) < c.box_hi[0] + c.cull &&
            fmax(y0, y1) > c.box_lo[1] - c.cull && fmin(y0, y1) < c.box_hi[1] + c.cull;
+}
+
+// False when the segment's bounding box is clear of the box widened to
+// near_lo / near_hi.  The widening (cull plus 2^-20 of the largest coordinate)
+// covers both the margin of may_hit_box and the FP32 rounding of the end
+// point (at most 2^-24 of it), so a segment that is not near the box neither
+// hits it nor ends, rounded to storage precision, inside it.
+__device__ __forceinline__ bool near_box(const CaseDev &c, double x0, double y0, double x1,
+                                         double y1)
+{
+    return fmax(x0, x1) > c.near_lo[0] && fmin(x0, x1) < c.near_hi[0] &&
+           fmax(y0, y1) > c.near_lo[1] && fmin(y0, y1) < c.near_hi[1];
 }
 
 // ---- storage precision ---------------------------------------------------------

@@ -255,23 +255,97 @@ __device__ __forceinline__ void load4(const uint32_t *p, uint32_t v[4])
     v[3] = t.w;
 }
 
-// The slab test of IntersectBox, out of line: only segments that pass
-// may_hit_box reach it.
-__device__ __noinline__ bool intersect_box_ool(const CaseDev &c, double x, double y, double dx,
-                                               double dy, double &t_hit, double &nx, double &ny)
+// Classification of a moved slot: the key, the old and new global cells and
+// whether it is removed, in range (same cell) or out of range (new cell).
+struct MoveClass {
+    uint32_t key;
+    int32_t ocg;
+    bool dead, out, in;
+};
+
+// Removal (Boundary.cpp:183-188) and the new cell of a slot that moved from
+// (x0, y0) to the stored (xn, yn), given the old cell `oc` and the new cell
+// `nc` (NO_CELL outside the grid).
+template <class T>
+__device__ __forceinline__ MoveClass classify_cells(const CaseDev &c, int32_t oc, int32_t nc, T xn,
+                                                    T yn, int *err)
 {
-    return intersect_box(c, x, y, dx, dy, t_hit, nx, ny);
+    MoveClass m;
+    m.dead = m.out = m.in = false;
+    m.key = KEY_DEAD;
+    m.ocg = oc < 0 ? NO_CELL : c.cbase + oc;
+    if (outside_domain(c, static_cast<double>(xn), static_cast<double>(yn))) {
+        m.dead = true;
+    } else if (nc < 0) {
+        // Inside the domain bounds but in no cell (rounding, NaN): the
+        // reference aborts in ExchangeParticles, status 30.
+        report_error(err, DSMC_ERR_EXCHANGE);
+        m.dead = true;
+    } else if (nc == oc) {
+        m.key = static_cast<uint32_t>(c.cbase + nc) | KEY_IN;
+        m.in = true;
+    } else {
+        m.key = static_cast<uint32_t>(c.cbase + nc);
+        m.out = true;
+    }
+    if (m.dead)
+        m.key = KEY_DEAD | (m.ocg == NO_CELL ? KEY_CELL : static_cast<uint32_t>(m.ocg));
+    return m;
 }
 
-// Per-tile counts packed for one block scan: in-range, removed, changed cell.
-__device__ __forceinline__ unsigned long long pack3(unsigned a, unsigned b, unsigned c)
+template <class T>
+__device__ __forceinline__ MoveClass classify(const CaseDev &c, double x0, double y0, T xn, T yn,
+                                              int *err)
 {
-    return static_cast<unsigned long long>(a) | (static_cast<unsigned long long>(b) << 21) |
-           (static_cast<unsigned long long>(c) << 42);
+    const int32_t oc = cell_of(c, x0, y0);
+    const bool gone = outside_domain(c, static_cast<double>(xn), static_cast<double>(yn));
+    const int32_t nc = gone ? NO_CELL
+                            : cell_of(c, static_cast<double>(xn), static_cast<double>(yn));
+    return classify_cells<T>(c, oc, nc, xn, yn, err);
 }
-__device__ __forceinline__ unsigned unpack3(unsigned long long v, int i)
+
+// Stores the key of a classified slot and moves the cell counters: every
+// cell starts the step with its old count as its in-range count, so only
+// slots that leave it touch a counter.
+__device__ __forceinline__ void commit_class(const MoveClass &m, uint32_t *key, int64_t g,
+                                             Cells cells)
 {
-    return static_cast<unsigned>((v >> (21 * i)) & 0x1FFFFFull);
+    key[g] = m.key;
+    if ((m.dead || m.out) && m.ocg != NO_CELL)
+        atomicSub(cells.n_in + m.ocg, 1);
+    if (m.out)
+        atomicAdd(cells.n_o + (m.key & KEY_CELL), 1);
+}
+
+// The full MoveParticles body (Boundary.cpp:284-328) for one slot: impact
+// test, wall interaction, FP32 placement outside the box, exact cell index.
+// Out of line, so its register demand stays out of the free-flight loop.
+template <class T>
+__device__ __noinline__ MoveClass move_near_box(const CaseDev &c, int64_t step, int64_t q,
+                                                int64_t g, Slots<T> p, uint32_t *key, Cells cells,
+                                                double &impulse, int &n_hit, int *err)
+{
+    const double x0 = static_cast<double>(p.x[g]);
+    const double y0 = static_cast<double>(p.y[g]);
+    const double dx = c.dt * static_cast<double>(p.vx[g]);
+    const double dy = c.dt * static_cast<double>(p.vy[g]);
+    const double xe = x0 + dx;
+    const double ye = y0 + dy;
+    double t_hit = 0.0, hnx = 0.0, hny = 0.0;
+    T xn, yn;
+    if (may_hit_box(c, x0, y0, xe, ye) && intersect_box(c, x0, y0, dx, dy, t_hit, hnx, hny)) {
+        impulse += wall_hit<T>(c, step, q, g, p, x0, y0, dx, dy, t_hit, hnx, hny, xn, yn);
+        n_hit++;
+    } else {
+        xn = Store<T>::rn(xe);
+        yn = Store<T>::rn(ye);
+        keep_outside<T>(c, xn, yn);
+    }
+    p.x[g] = xn;
+    p.y[g] = yn;
+    const MoveClass m = classify<T>(c, x0, y0, xn, yn, err);
+    commit_class(m, key, g, cells);
+    return m;
 }
 
 // Slot mapping of a move tile: iteration k of thread t handles slot
@@ -281,6 +355,12 @@ __device__ __forceinline__ unsigned unpack3(unsigned long long v, int i)
 constexpr int MOVE_WARPS = TILE_THREADS / 32;
 static_assert(TILE_VEC * MOVE_WARPS == 32, "one warp scans the (iteration, warp) counts");
 
+// Two passes per tile.  The first moves every slot whose segment is not near
+// the box (free flight: no impact, and the stored end point cannot fall inside
+// the box) and whose old and new cells are certain from the reciprocal
+// estimate, with all four loads of a thread in flight at once; the second
+// runs the full body for the other few.  Both give the same result as the
+// full body for every slot.
 template <class T>
 __global__ void __launch_bounds__(TILE_THREADS, 4)
     k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
@@ -304,113 +384,91 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
             return;
         const int ci = case_of(tt.move0, ncase, t);
         const CaseDev &c = cases[ci];
-        const int64_t n_old = st[ci].n_old;
-        const int64_t step = st[ci].step;
         const int local_tile = t - tt.move0[ci];
         const int64_t tile0 = static_cast<int64_t>(local_tile) * TILE;
+        const int64_t left = st[ci].n_old - tile0;
+        const int n_here = left < TILE ? static_cast<int>(left) : TILE;
         const int64_t gt = c.pbase + tile0;
+        T *px = p.x + gt;
+        T *py = p.y + gt;
+        const T *pvx = p.vx + gt;
+        const T *pvy = p.vy + gt;
+        uint32_t *pkey = key + gt;
 
-        double impulse = 0.0;
-        int n_hit = 0;
-        int64_t q = tile0 + threadIdx.x;
-        T cx{}, cy{}, cvx{}, cvy{};
-        if (q < n_old) {
-            cx = p.x[gt + threadIdx.x];
-            cy = p.y[gt + threadIdx.x];
-            cvx = p.vx[gt + threadIdx.x];
-            cvy = p.vy[gt + threadIdx.x];
-        }
-#pragma unroll 1
-        for (int k = 0; k < TILE_VEC; ++k, q += TILE_THREADS) {
+        T x[TILE_VEC], y[TILE_VEC], vx[TILE_VEC], vy[TILE_VEC];
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
             const int e = k * TILE_THREADS + threadIdx.x;
-            const int64_t g = gt + e;
-            T nx_{}, ny_{}, nvx{}, nvy{};
-            if (k + 1 < TILE_VEC && q + TILE_THREADS < n_old) {
-                nx_ = p.x[g + TILE_THREADS];
-                ny_ = p.y[g + TILE_THREADS];
-                nvx = p.vx[g + TILE_THREADS];
-                nvy = p.vy[g + TILE_THREADS];
+            if (e < n_here) {
+                x[k] = px[e];
+                y[k] = py[e];
+                vx[k] = pvx[e];
+                vy[k] = pvy[e];
             }
-            bool dead = false, out = false, in = false;
-            int32_t ocg = NO_CELL;
-            uint32_t kk = KEY_DEAD;
-            if (q < n_old) {
-                const double x0 = static_cast<double>(cx);
-                const double y0 = static_cast<double>(cy);
-                const int32_t oc = cell_of(c, x0, y0);
-                ocg = oc < 0 ? NO_CELL : c.cbase + oc;
-                const double dx = c.dt * static_cast<double>(cvx);
-                const double dy = c.dt * static_cast<double>(cvy);
-                const double xe = x0 + dx;
-                const double ye = y0 + dy;
-                double t_hit = 0.0, hnx = 0.0, hny = 0.0;
-                T xn, yn;
-                if (may_hit_box(c, x0, y0, xe, ye) &&
-                    intersect_box_ool(c, x0, y0, dx, dy, t_hit, hnx, hny)) {
-                    impulse += wall_hit<T>(c, step, q, g, p, x0, y0, dx, dy, t_hit, hnx, hny, xn,
-                                           yn);
-                    n_hit++;
+        }
+        unsigned near = 0; // bit k: slot of iteration k is near the box
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            const int e = k * TILE_THREADS + threadIdx.x;
+            MoveClass m;
+            m.dead = m.out = m.in = false;
+            if (e < n_here) {
+                const double x0 = static_cast<double>(x[k]);
+                const double y0 = static_cast<double>(y[k]);
+                const double xe = x0 + c.dt * static_cast<double>(vx[k]);
+                const double ye = y0 + c.dt * static_cast<double>(vy[k]);
+                const T xn = Store<T>::rn(xe);
+                const T yn = Store<T>::rn(ye);
+                int32_t oc, nc;
+                if (near_box(c, x0, y0, xe, ye) || !cell_of_fast(c, x0, y0, oc) ||
+                    !cell_of_fast(c, static_cast<double>(xn), static_cast<double>(yn), nc)) {
+                    near |= 1u << k;
                 } else {
-                    xn = Store<T>::rn(xe);
-                    yn = Store<T>::rn(ye);
-                    keep_outside<T>(c, xn, yn);
+                    px[e] = xn;
+                    py[e] = yn;
+                    m = classify_cells<T>(c, oc, nc, xn, yn, err);
+                    commit_class(m, pkey, e, cells);
                 }
-                p.x[g] = xn;
-                p.y[g] = yn;
-                const double xd = static_cast<double>(xn);
-                const double yd = static_cast<double>(yn);
-                if (outside_domain(c, xd, yd)) {
-                    dead = true;
-                } else {
-                    const int32_t nc = cell_of(c, xd, yd);
-                    if (nc < 0) {
-                        // Inside the domain bounds but in no cell (rounding,
-                        // NaN): the reference aborts in ExchangeParticles, 30.
-                        report_error(err, DSMC_ERR_EXCHANGE);
-                        dead = true;
-                    } else if (nc == oc) {
-                        kk = static_cast<uint32_t>(c.cbase + nc) | KEY_IN;
-                        in = true;
-                    } else {
-                        kk = static_cast<uint32_t>(c.cbase + nc);
-                        out = true;
-                    }
-                }
-                if (dead)
-                    kk = KEY_DEAD | (ocg == NO_CELL ? KEY_CELL : static_cast<uint32_t>(ocg));
-                key[g] = kk;
-                // Every cell starts the step with its old count as its
-                // in-range count: only slots that leave it touch a counter.
-                if ((dead || out) && ocg != NO_CELL)
-                    atomicSub(cells.n_in + ocg, 1);
-                if (out)
-                    atomicAdd(cells.n_o + (kk & KEY_CELL), 1);
             }
-            const unsigned bd = __ballot_sync(0xffffffffu, dead);
-            const unsigned bo = __ballot_sync(0xffffffffu, out);
-            const unsigned bi = __ballot_sync(0xffffffffu, in);
+            const unsigned bd = __ballot_sync(0xffffffffu, m.dead);
+            const unsigned bo = __ballot_sync(0xffffffffu, m.out);
+            const unsigned bi = __ballot_sync(0xffffffffu, m.in);
             if (lane == 0) {
                 s_dead[k * MOVE_WARPS + warp] = bd;
                 s_out[k * MOVE_WARPS + warp] = bo;
                 s_in[k * MOVE_WARPS + warp] = bi;
             }
-            cx = nx_;
-            cy = ny_;
-            cvx = nvx;
-            cvy = nvy;
         }
-        // Wall-hit diagnostics (Boundary.cpp:318-319).
-        {
-            double imp = impulse;
-            int hits = n_hit;
+        if (__any_sync(0xffffffffu, near != 0)) {
+            double impulse = 0.0;
+            int n_hit = 0;
+            const int64_t step = st[ci].step;
+#pragma unroll 1
+            for (int k = 0; k < TILE_VEC; ++k) {
+                const int e = k * TILE_THREADS + threadIdx.x;
+                MoveClass m;
+                m.dead = m.out = m.in = false;
+                if ((near >> k) & 1u)
+                    m = move_near_box<T>(c, step, tile0 + e, gt + e, p, key, cells, impulse,
+                                         n_hit, err);
+                const unsigned bd = __ballot_sync(0xffffffffu, m.dead);
+                const unsigned bo = __ballot_sync(0xffffffffu, m.out);
+                const unsigned bi = __ballot_sync(0xffffffffu, m.in);
+                if (lane == 0) {
+                    s_dead[k * MOVE_WARPS + warp] |= bd;
+                    s_out[k * MOVE_WARPS + warp] |= bo;
+                    s_in[k * MOVE_WARPS + warp] |= bi;
+                }
+            }
+            // Wall-hit diagnostics (Boundary.cpp:318-319).
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
-                imp += __shfl_xor_sync(0xffffffffu, imp, o);
-                hits += __shfl_xor_sync(0xffffffffu, hits, o);
+                impulse += __shfl_xor_sync(0xffffffffu, impulse, o);
+                n_hit += __shfl_xor_sync(0xffffffffu, n_hit, o);
             }
-            if (lane == 0 && hits > 0) {
-                atomicAdd(&st[ci].drag_impulse, imp);
-                atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(hits));
+            if (lane == 0 && n_hit > 0) {
+                atomicAdd(&st[ci].drag_impulse, impulse);
+                atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(n_hit));
             }
         }
         __syncthreads();
@@ -558,11 +616,14 @@ __global__ void __launch_bounds__(TILE_THREADS)
 }
 
 // ---------------------------------------------------------------------------
+// Threads of the one-CTA-per-case tile scans (k_dead_scan, k_tile_scan).
+constexpr int SCAN_THREADS = 1024;
+
 // k_dead_scan: per case (one CTA each), exclusive prefix of the removed-slot
 // counts of its move tiles, then of its inject tiles, in slot order; sets
 // dead_old and dead_total.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TILE_THREADS)
+__global__ void __launch_bounds__(SCAN_THREADS)
     k_dead_scan(CaseState *st, const int32_t *tile_dead, int32_t *tile_dprefix,
                 const int32_t *itile_dead, int32_t *itile_dprefix)
 {
@@ -574,7 +635,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
         const int t0 = part == 0 ? s.move_tile0 : s.inject_tile0;
         const int32_t *in = (part == 0 ? tile_dead : itile_dead) + t0;
         int32_t *out = (part == 0 ? tile_dprefix : itile_dprefix) + t0;
-        for (int b = 0; b < n; b += TILE_THREADS * PER) {
+        for (int b = 0; b < n; b += SCAN_THREADS * PER) {
             const int i0 = b + threadIdx.x * PER;
             int v[PER];
             int sum = 0;
@@ -584,7 +645,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
                 sum += v[k];
             }
             int tot;
-            int run = carry + block_exclusive<int>(sum, tot);
+            int run = carry + block_exclusive<int, SCAN_THREADS>(sum, tot);
 #pragma unroll
             for (int k = 0; k < PER; ++k) {
                 if (i0 + k < n)
@@ -835,7 +896,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
 // k_tile_scan: per case (one CTA each), exclusive prefix of the in-range
 // counts of its move tiles, in place into tile_prefix.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TILE_THREADS)
+__global__ void __launch_bounds__(SCAN_THREADS)
     k_tile_scan(const CaseState *st, const int32_t *tile_in, int32_t *tile_prefix)
 {
     constexpr int PER = 8; // consecutive tiles per thread
@@ -844,7 +905,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
     const int32_t *in = tile_in + s.move_tile0;
     int32_t *out = tile_prefix + s.move_tile0;
     int32_t carry = 0;
-    for (int b = 0; b < n; b += TILE_THREADS * PER) {
+    for (int b = 0; b < n; b += SCAN_THREADS * PER) {
         const int i0 = b + threadIdx.x * PER;
         int v[PER];
         int sum = 0;
@@ -854,7 +915,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
             sum += v[k];
         }
         int tot;
-        int run = carry + block_exclusive<int>(sum, tot);
+        int run = carry + block_exclusive<int, SCAN_THREADS>(sum, tot);
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
             if (i0 + k < n)

@@ -135,10 +135,13 @@ __device__ __forceinline__ uint64_t lookback_warp(uint64_t *status, int t, int c
     return excl;
 }
 
-// Block-wide exclusive sum over TILE_THREADS threads; also returns the total.
-template <class V> __device__ __forceinline__ V block_exclusive(V v, V &total)
+// Block-wide exclusive sum over NT threads; also returns the total.
+template <class V, int NT = TILE_THREADS>
+__device__ __forceinline__ V block_exclusive(V v, V &total)
 {
-    __shared__ V warp_tot[TILE_THREADS / 32];
+    static_assert(NT % 32 == 0 && NT <= 1024, "block of whole warps");
+    constexpr int NW = NT / 32;
+    __shared__ V warp_tot[NW];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     V inc = v;
@@ -152,19 +155,19 @@ template <class V> __device__ __forceinline__ V block_exclusive(V v, V &total)
         warp_tot[warp] = inc;
     __syncthreads();
     if (warp == 0) {
-        V w = lane < TILE_THREADS / 32 ? warp_tot[lane] : V(0);
+        V w = lane < NW ? warp_tot[lane] : V(0);
 #pragma unroll
-        for (int o = 1; o < TILE_THREADS / 32; o <<= 1) {
+        for (int o = 1; o < NW; o <<= 1) {
             const V n = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o)
                 w += n;
         }
-        if (lane < TILE_THREADS / 32)
+        if (lane < NW)
             warp_tot[lane] = w;
     }
     __syncthreads();
     const V warp_excl = warp == 0 ? V(0) : warp_tot[warp - 1];
-    total = warp_tot[TILE_THREADS / 32 - 1];
+    total = warp_tot[NW - 1];
     __syncthreads();
     return warp_excl + inc - v;
 }

@@ -8,7 +8,7 @@ Independent seeds are run in parallel and their moments summed (replica
 statistics), so the fixture's own sampling noise is small next to the 2%
 field tolerance of the statistical test.
 
-    python tests/golden/make_reference_field.py [--seeds 64]
+    python tests/golden/make_reference_field.py [--seeds 256]
 """
 from __future__ import annotations
 
@@ -58,7 +58,7 @@ def run_one(seed: int) -> tuple[np.ndarray, int]:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--seeds", type=int, default=64)
+    ap.add_argument("--seeds", type=int, default=256)
     args = ap.parse_args()
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
         results = list(ex.map(run_one, range(1, args.seeds + 1)))

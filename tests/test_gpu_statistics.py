@@ -3,7 +3,7 @@
   * the equilibrium NTC collision rate equals the analytic VHS rate of the
     reference's Setup() (src/Initialization.cpp:231-253) within 1%;
   * the sampled field of the plain reference case agrees with the unmodified
-    reference solver's (its own RNG, 64 seeds; tests/golden/
+    reference solver's (its own RNG, 256 seeds; tests/golden/
     reference_case_field.npz) to relative L2 <= 2% on n, ux, uy and T
     outside the wall cells;
   * FP32 particle state agrees with FP64 to the same bar.
