@@ -94,7 +94,7 @@ struct dsmc_ctx {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
     int grid_move = 0, grid_inject = 0, grid_tail = 0, grid_cell_scan = 0, grid_olist = 0;
-    int grid_cell_fix = 0, grid_scatter = 0, grid_collide = 0, grid_select = 0;
+    int grid_cell_fix = 0, grid_scatter = 0, grid_collide = 0, grid_select = 0, grid_holes = 0;
 
     bool profiling = false;
     std::vector<Timed> timed;
@@ -172,7 +172,7 @@ template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
     }
     if (!init_mode) {
         Span sp(c, KID_MOVE);
-        k_move<T><<<c->grid_move, TILE_THREADS, 0, c->stream>>>(
+        k_move<T><<<c->grid_move, TILE_THREADS, move_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
             c->tile_in, c->tile_dead, c->obuf, c->ncase, c->d_err);
     }
@@ -197,7 +197,7 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_HOLES);
-        k_holes<<<c->grid_scatter, TILE_THREADS, 0, c->stream>>>(
+        k_holes<<<c->grid_holes, TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, c->key, c->tile_dead, c->tile_dprefix,
             c->itile_dead, c->itile_dprefix, c->hole_pos, c->hole_oc, c->ncase);
     }
@@ -245,7 +245,7 @@ template <class T> int enqueue_index(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_SCATTER);
-        k_scatter<T><<<c->grid_scatter, TILE_THREADS, 0, c->stream>>>(
+        k_scatter<T><<<c->grid_scatter, TILE_THREADS, scatter_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->tt, slots<T>(c, side), slots<T>(c, side ^ 1), c->key,
             c->cells, c->tile_prefix, c->ncase, c->d_err);
     }
@@ -330,6 +330,47 @@ int build_graphs(dsmc_ctx *c)
 }
 
 // Constants of one case, computed on the host with the reference expressions.
+// Largest float <= v and smallest float >= v.
+float float_down(double v)
+{
+    float f = static_cast<float>(v);
+    if (static_cast<double>(f) > v)
+        f = std::nextafter(f, -INFINITY);
+    return f;
+}
+float float_up(double v)
+{
+    float f = static_cast<float>(v);
+    if (static_cast<double>(f) < v)
+        f = std::nextafter(f, INFINITY);
+    return f;
+}
+
+// FP32 constants of the free-flight pass (see CaseDev).  fcell_eps bounds
+// |q' - (x - X1) / DX| for the float estimate q' inside the grid: the float
+// difference, the product and 1/DX each round by at most 2^-24 relative
+// (3 |q| 2^-24 in all), and X1 rounded to float adds 2^-24 |X1| / DX; the
+// bound is doubled, plus 1e-9 for the FP64 quotient of the reference.
+void set_float_bounds(CaseDev &c, const dsmc_params &p)
+{
+    c.fx1 = static_cast<float>(c.x1);
+    c.fy1 = static_cast<float>(c.y1);
+    c.finv_dx = static_cast<float>(c.inv_dx);
+    c.finv_dy = static_cast<float>(c.inv_dy);
+    const double qmax = static_cast<double>(std::max(p.nx, p.ny)) + 1.0;
+    const double shift = std::max(std::fabs(c.x1) / c.dx, std::fabs(c.y1) / c.dy);
+    const double err = std::ldexp(3.01 * qmax + 1.01 * shift + 1.0, -24);
+    c.fcell_eps = static_cast<float>(2.0 * err + 1e-9);
+    c.dom_lo[0] = float_down(c.x1);
+    c.dom_lo[1] = float_down(c.y1);
+    c.dom_hi[0] = float_up(c.x2);
+    c.dom_hi[1] = float_up(c.y2);
+    c.fnear_lo[0] = float_down(c.near_lo[0]);
+    c.fnear_lo[1] = float_down(c.near_lo[1]);
+    c.fnear_hi[0] = float_up(c.near_hi[0]);
+    c.fnear_hi[1] = float_up(c.near_hi[1]);
+}
+
 CaseDev make_case(const dsmc_params &p, const dsmc_derived &d)
 {
     CaseDev c{};
@@ -416,6 +457,7 @@ CaseDev make_case(const dsmc_params &p, const dsmc_derived &d)
     c.ncell = p.nx * p.ny;
     c.key0 = static_cast<uint32_t>(p.seed);
     c.key1 = static_cast<uint32_t>(p.seed >> 32);
+    set_float_bounds(c, p);
     return c;
 }
 
@@ -424,7 +466,10 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 template <class T> int occupancy_grids(dsmc_ctx *c)
 {
     int b = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_move<T>, TILE_THREADS, 0));
+    CK(cudaFuncSetAttribute(k_move<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(move_smem<T>())));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_move<T>, TILE_THREADS,
+                                                     move_smem<T>()));
     c->grid_move = std::max(1, b) * c->sms;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_inject<T>, TILE_THREADS, 0));
     c->grid_inject = std::max(1, b) * c->sms;
@@ -432,7 +477,12 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
     c->grid_tail = std::max(1, b) * c->sms;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cell_scan, TILE_THREADS, 0));
     c->grid_cell_scan = std::max(1, b) * c->sms;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, TILE_THREADS, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_holes, TILE_THREADS, 0));
+    c->grid_holes = std::max(1, b) * c->sms;
+    CK(cudaFuncSetAttribute(k_scatter<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(scatter_smem<T>())));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, TILE_THREADS,
+                                                     scatter_smem<T>()));
     c->grid_scatter = std::max(1, b) * c->sms;
     CK(cudaFuncSetAttribute(k_sample<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(collide_smem<T>())));

@@ -42,6 +42,13 @@ struct CaseDev {
     double inv_dx, inv_dy;         // 1 / DX, 1 / DY (fast path of the cell index)
     double cull;                   // margin of the box pre-test (may_hit_box)
     double near_lo[2], near_hi[2]; // box widened by cull + 2^-20 of the coordinates
+    // FP32 forms for the free-flight pass of FP32 slots: X1, Y1 and 1/DX, 1/DY
+    // rounded to float; the bound on the error of the float cell estimate;
+    // the domain bounds rounded inwards-exclusive (a float x is <= X1 iff it
+    // is <= dom_lo[0], >= X2 iff >= dom_hi[0]); the near bounds rounded out.
+    float fx1, fy1, finv_dx, finv_dy, fcell_eps;
+    float dom_lo[2], dom_hi[2];
+    float fnear_lo[2], fnear_hi[2];
     double box_lo[2], box_hi[2];   // IntersectBox bounds (Geometry.cpp:184-185)
     double box_x, box_y;           // InsideBox centre (Geometry.cpp:175-176)
     double box_hw, box_hh;         // BoxWidth / 2.0, BoxHeight / 2.0
@@ -322,6 +329,54 @@ __device__ __forceinline__ bool cell_of_fast(const CaseDev &c, double x, double 
                ? static_cast<int32_t>(fk) * c.ny + static_cast<int32_t>(fl)
                : NO_CELL;
     return true;
+}
+
+// FP32 estimate of the cell of a float position for the free-flight pass.
+// The estimate q' = (x - fx1) * finv_dx differs from (x - X1) / DX by less
+// than fcell_eps inside the grid (float rounding of X1, 1/DX, the difference
+// and the product), so when q' is more than fcell_eps from an integer its
+// floor is the reference's FP64 floor.  Returns false when not certain.
+// Floors use the 1.5 * 2^23 rounding constant (|q'| < 2^21 checked).
+__device__ __forceinline__ bool floor_fast_f(float q, float eps, int32_t &n)
+{
+    if (!(fabsf(q) < 2097152.0f))
+        return false;
+    const float t = q + 12582912.0f;
+    float f = t - 12582912.0f;
+    int32_t i = __float_as_int(t) - 0x4B400000;
+    if (f > q) {
+        f -= 1.0f;
+        i -= 1;
+    }
+    const float r = q - f;
+    n = i;
+    return r > eps && r < 1.0f - eps;
+}
+
+__device__ __forceinline__ bool cell_of_fast_f(const CaseDev &c, float x, float y, int32_t &cell)
+{
+    int32_t k, l;
+    if (!floor_fast_f((x - c.fx1) * c.finv_dx, c.fcell_eps, k) ||
+        !floor_fast_f((y - c.fy1) * c.finv_dy, c.fcell_eps, l))
+        return false;
+    cell = (k >= 0 && k < c.nx && l >= 0 && l < c.ny) ? k * c.ny + l : NO_CELL;
+    return true;
+}
+
+// Removal predicate of BoundaryConditions (Boundary.cpp:183-188) for a float
+// position, exact: compares against the float bounds described in CaseDev.
+__device__ __forceinline__ bool outside_domain_f(const CaseDev &c, float x, float y)
+{
+    return x <= c.dom_lo[0] || x >= c.dom_hi[0] || y <= c.dom_lo[1] || y >= c.dom_hi[1];
+}
+
+// near_box for a float segment (start, rounded end): the float near bounds
+// contain the FP64 ones, and the end point's rounding (2^-24 of it) is far
+// inside the 2^-20 widening, so "not near" here implies "not near" in FP64.
+__device__ __forceinline__ bool near_box_f(const CaseDev &c, float x0, float y0, float x1, float y1)
+{
+    return fmaxf(x0, x1) > c.fnear_lo[0] && fminf(x0, x1) < c.fnear_hi[0] &&
+           fmaxf(y0, y1) > c.fnear_lo[1] && fminf(y0, y1) < c.fnear_hi[1];
 }
 
 // False only when IntersectBox cannot report an impact: the segment's

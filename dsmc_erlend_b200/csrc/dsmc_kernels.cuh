@@ -34,6 +34,7 @@
 #include <cstdint>
 
 #include "dsmc_device.cuh"
+#include "dsmc_bulk.cuh"
 #include "dsmc_scan.cuh"
 
 namespace dsmc {
@@ -263,18 +264,17 @@ struct MoveClass {
     bool dead, out, in;
 };
 
-// Removal (Boundary.cpp:183-188) and the new cell of a slot that moved from
-// (x0, y0) to the stored (xn, yn), given the old cell `oc` and the new cell
-// `nc` (NO_CELL outside the grid).
-template <class T>
-__device__ __forceinline__ MoveClass classify_cells(const CaseDev &c, int32_t oc, int32_t nc, T xn,
-                                                    T yn, int *err)
+// Removal (Boundary.cpp:183-188) and the new cell of a slot, given its old
+// cell `oc`, whether its new position lies outside the domain (`gone`) and
+// otherwise its new cell `nc` (NO_CELL outside the grid).
+__device__ __forceinline__ MoveClass classify_cells(const CaseDev &c, int32_t oc, bool gone,
+                                                    int32_t nc, int *err)
 {
     MoveClass m;
     m.dead = m.out = m.in = false;
     m.key = KEY_DEAD;
     m.ocg = oc < 0 ? NO_CELL : c.cbase + oc;
-    if (outside_domain(c, static_cast<double>(xn), static_cast<double>(yn))) {
+    if (gone) {
         m.dead = true;
     } else if (nc < 0) {
         // Inside the domain bounds but in no cell (rounding, NaN): the
@@ -293,6 +293,7 @@ __device__ __forceinline__ MoveClass classify_cells(const CaseDev &c, int32_t oc
     return m;
 }
 
+// Exact form: the cells by the reference's FP64 expressions.
 template <class T>
 __device__ __forceinline__ MoveClass classify(const CaseDev &c, double x0, double y0, T xn, T yn,
                                               int *err)
@@ -301,7 +302,47 @@ __device__ __forceinline__ MoveClass classify(const CaseDev &c, double x0, doubl
     const bool gone = outside_domain(c, static_cast<double>(xn), static_cast<double>(yn));
     const int32_t nc = gone ? NO_CELL
                             : cell_of(c, static_cast<double>(xn), static_cast<double>(yn));
-    return classify_cells<T>(c, oc, nc, xn, yn, err);
+    return classify_cells(c, oc, gone, nc, err);
+}
+
+// Free flight of one slot, without the impact test and with estimated cell
+// indices: false when the segment is near the box or a cell index is not
+// certain from its estimate (the slot then takes the exact body), else the
+// stored end point, the old cell, whether the end point left the domain and
+// otherwise its new cell.  Same results as the exact body for every slot it
+// accepts.
+__device__ __forceinline__ bool free_flight(const CaseDev &c, double x0, double y0, double vx,
+                                            double vy, double &xn, double &yn, int32_t &oc,
+                                            bool &gone, int32_t &nc)
+{
+    xn = x0 + c.dt * vx;
+    yn = y0 + c.dt * vy;
+    if (near_box(c, x0, y0, xn, yn) || !cell_of_fast(c, x0, y0, oc))
+        return false;
+    gone = outside_domain(c, xn, yn);
+    nc = NO_CELL;
+    return gone || cell_of_fast(c, xn, yn, nc);
+}
+
+// FP32 slots: the end point is rounded from the FP64 sum as in the exact
+// body; the box, domain and cell tests run on floats (exact or conservative,
+// as their helpers state), with the FP64 estimate as a second chance for a
+// cell the float estimate leaves open.
+__device__ __forceinline__ bool free_flight(const CaseDev &c, float x0, float y0, float vx,
+                                            float vy, float &xn, float &yn, int32_t &oc,
+                                            bool &gone, int32_t &nc)
+{
+    xn = __double2float_rn(static_cast<double>(x0) + c.dt * static_cast<double>(vx));
+    yn = __double2float_rn(static_cast<double>(y0) + c.dt * static_cast<double>(vy));
+    if (near_box_f(c, x0, y0, xn, yn))
+        return false;
+    if (!cell_of_fast_f(c, x0, y0, oc) &&
+        !cell_of_fast(c, static_cast<double>(x0), static_cast<double>(y0), oc))
+        return false;
+    gone = outside_domain_f(c, xn, yn);
+    nc = NO_CELL;
+    return gone || cell_of_fast_f(c, xn, yn, nc) ||
+           cell_of_fast(c, static_cast<double>(xn), static_cast<double>(yn), nc);
 }
 
 // Stores the key of a classified slot and moves the cell counters: every
@@ -355,88 +396,109 @@ __device__ __noinline__ MoveClass move_near_box(const CaseDev &c, int64_t step, 
 constexpr int MOVE_WARPS = TILE_THREADS / 32;
 static_assert(TILE_VEC * MOVE_WARPS == 32, "one warp scans the (iteration, warp) counts");
 
-// Two passes per tile.  The first moves every slot whose segment is not near
-// the box (free flight: no impact, and the stored end point cannot fall inside
-// the box) and whose old and new cells are certain from the reciprocal
-// estimate, with all four loads of a thread in flight at once; the second
-// runs the full body for the other few.  Both give the same result as the
-// full body for every slot.
+// Tiles are staged in shared memory by bulk asynchronous copies, MOVE
+// stages deep, so the loads of the next tiles of a CTA are in flight while it
+// moves the current one.  Two passes per tile: the first moves every slot that
+// free_flight accepts, the second runs the exact body for the other few.
+// Both give the exact body's result for every slot.
+template <class T> struct MoveStage {
+    T v[4][TILE]; // x, y, vx, vy
+};
+template <class T> __host__ __device__ constexpr int move_stages() { return sizeof(T) == 4 ? 3 : 2; }
+template <class T> __host__ __device__ constexpr size_t move_smem()
+{
+    return sizeof(MoveStage<T>) * move_stages<T>();
+}
+
 template <class T>
 __global__ void __launch_bounds__(TILE_THREADS, 4)
     k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
            Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
            int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf, int ncase, int *err)
 {
-    __shared__ int s_tile;
-    __shared__ uint32_t s_obase;
-    __shared__ unsigned s_dead[32], s_out[32], s_in[32]; // ballots per (iteration, warp)
-    __shared__ unsigned s_opre[32];                      // exclusive prefix of s_out
+    constexpr int S = move_stages<T>();
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    MoveStage<T> *stage = reinterpret_cast<MoveStage<T> *>(smem_raw);
+    __shared__ uint64_t bar[S];
+    __shared__ int s_t[S];                        // tile of each stage
+    __shared__ unsigned s_dead[2][32], s_out[2][32], s_in[2][32]; // ballots per (iteration, warp)
+    __shared__ unsigned s_opre[2][32];            // exclusive prefix of s_out
+    __shared__ uint32_t s_obase[2];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
-    for (;;) {
-        __syncthreads();
-        if (threadIdx.x == 0)
-            s_tile = static_cast<int>(atomicAdd(&sc->move_ticket, 1u));
-        __syncthreads();
-        const int t = s_tile;
-        if (t >= sc->total_move_tiles)
+    const int total = sc->total_move_tiles;
+
+    // Thread 0 only: the copies of tile t into stage sidx.
+    auto issue = [&](int t, int sidx) {
+        const int ci = case_of(tt.move0, ncase, t);
+        const int64_t g0 = cases[ci].pbase + static_cast<int64_t>(t - tt.move0[ci]) * TILE;
+        constexpr uint32_t vb = TILE * sizeof(T);
+        mbar_arrive_expect_tx(&bar[sidx], 4 * vb);
+        bulk_g2s(stage[sidx].v[0], p.x + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[1], p.y + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[2], p.vx + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[3], p.vy + g0, vb, &bar[sidx]);
+    };
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S; ++i)
+            mbar_init(&bar[i], 1);
+        fence_mbar_init();
+        for (int i = 0; i < S; ++i) {
+            const int t = static_cast<int>(atomicAdd(&sc->move_ticket, 1u));
+            s_t[i] = t;
+            if (t < total)
+                issue(t, i);
+        }
+    }
+    __syncthreads();
+
+    for (int it = 0;; ++it) {
+        const int sidx = it % S;
+        const int par = it & 1;
+        const int t = s_t[sidx];
+        if (t >= total)
             return;
+        const bool ok = mbar_wait(&bar[sidx], static_cast<uint32_t>((it / S) & 1));
         const int ci = case_of(tt.move0, ncase, t);
         const CaseDev &c = cases[ci];
         const int local_tile = t - tt.move0[ci];
         const int64_t tile0 = static_cast<int64_t>(local_tile) * TILE;
         const int64_t left = st[ci].n_old - tile0;
-        const int n_here = left < TILE ? static_cast<int>(left) : TILE;
+        const int n_here = ok ? (left < TILE ? static_cast<int>(left) : TILE) : 0;
         const int64_t gt = c.pbase + tile0;
         T *px = p.x + gt;
         T *py = p.y + gt;
-        const T *pvx = p.vx + gt;
-        const T *pvy = p.vy + gt;
         uint32_t *pkey = key + gt;
+        const MoveStage<T> &sg = stage[sidx];
 
-        T x[TILE_VEC], y[TILE_VEC], vx[TILE_VEC], vy[TILE_VEC];
-#pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            const int e = k * TILE_THREADS + threadIdx.x;
-            if (e < n_here) {
-                x[k] = px[e];
-                y[k] = py[e];
-                vx[k] = pvx[e];
-                vy[k] = pvy[e];
-            }
-        }
-        unsigned near = 0; // bit k: slot of iteration k is near the box
+        unsigned near = 0; // bit k: the slot of iteration k takes the exact body
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
             const int e = k * TILE_THREADS + threadIdx.x;
             MoveClass m;
             m.dead = m.out = m.in = false;
             if (e < n_here) {
-                const double x0 = static_cast<double>(x[k]);
-                const double y0 = static_cast<double>(y[k]);
-                const double xe = x0 + c.dt * static_cast<double>(vx[k]);
-                const double ye = y0 + c.dt * static_cast<double>(vy[k]);
-                const T xn = Store<T>::rn(xe);
-                const T yn = Store<T>::rn(ye);
+                T xn, yn;
                 int32_t oc, nc;
-                if (near_box(c, x0, y0, xe, ye) || !cell_of_fast(c, x0, y0, oc) ||
-                    !cell_of_fast(c, static_cast<double>(xn), static_cast<double>(yn), nc)) {
-                    near |= 1u << k;
-                } else {
+                bool gone;
+                if (free_flight(c, sg.v[0][e], sg.v[1][e], sg.v[2][e], sg.v[3][e], xn, yn, oc,
+                                gone, nc)) {
                     px[e] = xn;
                     py[e] = yn;
-                    m = classify_cells<T>(c, oc, nc, xn, yn, err);
+                    m = classify_cells(c, oc, gone, nc, err);
                     commit_class(m, pkey, e, cells);
+                } else {
+                    near |= 1u << k;
                 }
             }
             const unsigned bd = __ballot_sync(0xffffffffu, m.dead);
             const unsigned bo = __ballot_sync(0xffffffffu, m.out);
             const unsigned bi = __ballot_sync(0xffffffffu, m.in);
             if (lane == 0) {
-                s_dead[k * MOVE_WARPS + warp] = bd;
-                s_out[k * MOVE_WARPS + warp] = bo;
-                s_in[k * MOVE_WARPS + warp] = bi;
+                s_dead[par][k * MOVE_WARPS + warp] = bd;
+                s_out[par][k * MOVE_WARPS + warp] = bo;
+                s_in[par][k * MOVE_WARPS + warp] = bi;
             }
         }
         if (__any_sync(0xffffffffu, near != 0)) {
@@ -455,9 +517,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
                 const unsigned bo = __ballot_sync(0xffffffffu, m.out);
                 const unsigned bi = __ballot_sync(0xffffffffu, m.in);
                 if (lane == 0) {
-                    s_dead[k * MOVE_WARPS + warp] |= bd;
-                    s_out[k * MOVE_WARPS + warp] |= bo;
-                    s_in[k * MOVE_WARPS + warp] |= bi;
+                    s_dead[par][k * MOVE_WARPS + warp] |= bd;
+                    s_out[par][k * MOVE_WARPS + warp] |= bo;
+                    s_in[par][k * MOVE_WARPS + warp] |= bi;
                 }
             }
             // Wall-hit diagnostics (Boundary.cpp:318-319).
@@ -471,13 +533,31 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
                 atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(n_hit));
             }
         }
-        __syncthreads();
+        // Every thread is done with the stage (its values are in registers or
+        // consumed): refill it with this CTA's next tile.
+        if (__syncthreads_or(!ok)) {
+            // A copy never completed (nothing of this tile was written).
+            if (threadIdx.x == 0) {
+                report_error(err, DSMC_ERR_TIMEOUT);
+                for (int j = it; j < it + S; ++j)
+                    if (s_t[j % S] < total)
+                        mbar_wait(&bar[j % S], static_cast<uint32_t>((j / S) & 1));
+            }
+            return;
+        }
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            const int tn = static_cast<int>(atomicAdd(&sc->move_ticket, 1u));
+            s_t[sidx] = tn;
+            if (tn < total)
+                issue(tn, sidx);
+        }
         if (warp == 0) {
             // Lane i holds the counts of (iteration, warp) pair i; pairs are
             // in slot order, so an exclusive scan gives list ranks in slot
             // order.  Removed slots are only counted here: their ranks come
             // from k_dead_scan and k_holes, so no tile waits on another.
-            const unsigned o = __popc(s_out[lane]);
+            const unsigned o = __popc(s_out[par][lane]);
             unsigned oi = o;
 #pragma unroll
             for (int sft = 1; sft < 32; sft <<= 1) {
@@ -485,22 +565,23 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
                 if (lane >= sft)
                     oi += b;
             }
-            s_opre[lane] = oi - o;
+            s_opre[par][lane] = oi - o;
             const unsigned out_tile = __shfl_sync(0xffffffffu, oi, 31);
-            const unsigned dead_tile = static_cast<unsigned>(warp_sum_u64(__popc(s_dead[lane])));
-            const unsigned in_tile = static_cast<unsigned>(warp_sum_u64(__popc(s_in[lane])));
+            const unsigned dead_tile =
+                static_cast<unsigned>(warp_sum_u64(__popc(s_dead[par][lane])));
+            const unsigned in_tile = static_cast<unsigned>(warp_sum_u64(__popc(s_in[par][lane])));
             if (lane == 0) {
                 tile_in[t] = static_cast<int32_t>(in_tile);
                 tile_dead[t] = static_cast<int32_t>(dead_tile);
-                s_obase = out_tile ? atomicAdd(&sc->obuf_count, out_tile) : 0u;
+                s_obase[par] = out_tile ? atomicAdd(&sc->obuf_count, out_tile) : 0u;
             }
         }
         __syncthreads();
         for (int k = 0; k < TILE_VEC; ++k) {
             const int i = k * MOVE_WARPS + warp;
-            const unsigned bo = s_out[i];
+            const unsigned bo = s_out[par][i];
             if ((bo >> lane) & 1u)
-                obuf[s_obase + s_opre[i] + __popc(bo & lanes_below)] =
+                obuf[s_obase[par] + s_opre[par][i] + __popc(bo & lanes_below)] =
                     static_cast<uint32_t>(gt + k * TILE_THREADS + threadIdx.x);
         }
     }
@@ -1025,73 +1106,157 @@ __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *s
 // k_scatter: moves every particle of slots [0, K) to its sorted slot.  An
 // in-range particle goes to base_in[cell] + (number of in-range particles at
 // lower slots of its case); any other particle's key word already holds its
-// slot (k_cell_fix).  Reads are whole coalesced tiles.
+// slot (k_cell_fix).
+//
+// Tiles are staged whole in shared memory by bulk asynchronous copies, SCATTER
+// stages deep: while the warps place tile i, the copies of the next tiles of
+// this CTA are in flight, so the kernel keeps HBM busy without holding the
+// loads in registers.  One barrier per tile: it publishes the per-warp
+// in-range counts and frees the stage for its refill.
 // ---------------------------------------------------------------------------
+template <class T> struct ScatterStage {
+    uint32_t key[TILE];
+    T v[5][TILE];
+};
+template <class T> __host__ __device__ constexpr int scatter_stages() { return sizeof(T) == 4 ? 3 : 2; }
+template <class T> __host__ __device__ constexpr size_t scatter_smem()
+{
+    return sizeof(ScatterStage<T>) * scatter_stages<T>();
+}
+
 template <class T>
 __global__ void __launch_bounds__(TILE_THREADS)
     k_scatter(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt,
               Slots<T> src, Slots<T> dst, const uint32_t *__restrict__ key, Cells cells,
               const int32_t *__restrict__ tile_prefix, int ncase, int *err)
 {
+    constexpr int S = scatter_stages<T>();
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    ScatterStage<T> *stage = reinterpret_cast<ScatterStage<T> *>(smem_raw);
+    __shared__ uint64_t bar[S];
+    __shared__ int s_wcnt[2][MOVE_WARPS];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const int total = tt.scatter0[ncase];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+
+    // Thread 0 only: starts the copies of tile t into stage sidx.
+    auto issue = [&](int t, int sidx) {
+        const int ci = case_of(tt.scatter0, ncase, t);
+        const int64_t g0 = cases[ci].pbase + static_cast<int64_t>(t - tt.scatter0[ci]) * TILE;
+        constexpr uint32_t kb = TILE * sizeof(uint32_t), vb = TILE * sizeof(T);
+        mbar_arrive_expect_tx(&bar[sidx], kb + 5 * vb);
+        bulk_g2s(stage[sidx].key, key + g0, kb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[0], src.x + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[1], src.y + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[2], src.vx + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[3], src.vy + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[4], src.vz + g0, vb, &bar[sidx]);
+    };
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S; ++i)
+            mbar_init(&bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    int issued = 0;
+    if (threadIdx.x == 0)
+        for (; issued < S && blockIdx.x + issued * gridDim.x < total; ++issued)
+            issue(blockIdx.x + issued * gridDim.x, issued);
+
+    int it = 0;
+    bool failed = false;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
+        const int sidx = it % S;
+        const bool ok = mbar_wait(&bar[sidx], static_cast<uint32_t>((it / S) & 1));
         const int ci = case_of(tt.scatter0, ncase, t);
         const CaseDev &c = cases[ci];
         const CaseState &s = st[ci];
         const int local_tile = t - tt.scatter0[ci];
         const int64_t q0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
-        const int64_t g0 = c.pbase + q0;
         const int64_t keep = s.n_keep;
-        const bool full = q0 + TILE_VEC <= keep;
+        const ScatterStage<T> &sg = stage[sidx];
+        const int e0 = threadIdx.x * TILE_VEC;
         uint32_t keys[TILE_VEC];
         T x[TILE_VEC], y[TILE_VEC], vx[TILE_VEC], vy[TILE_VEC], vz[TILE_VEC];
-        if (full) {
-            load4(key + g0, keys);
-            load4(src.x + g0, x);
-            load4(src.y + g0, y);
-            load4(src.vx + g0, vx);
-            load4(src.vy + g0, vy);
-            load4(src.vz + g0, vz);
-        } else {
-#pragma unroll
-            for (int k = 0; k < TILE_VEC; ++k) {
-                const bool v = q0 + k < keep;
-                keys[k] = v ? key[g0 + k] : KEY_DEAD;
-                x[k] = v ? src.x[g0 + k] : T(0);
-                y[k] = v ? src.y[g0 + k] : T(0);
-                vx[k] = v ? src.vx[g0 + k] : T(0);
-                vy[k] = v ? src.vy[g0 + k] : T(0);
-                vz[k] = v ? src.vz[g0 + k] : T(0);
-            }
-        }
+        load4(sg.key + e0, keys);
+        load4(sg.v[0] + e0, x);
+        load4(sg.v[1] + e0, y);
+        load4(sg.v[2] + e0, vx);
+        load4(sg.v[3] + e0, vy);
+        load4(sg.v[4] + e0, vz);
         int n_in = 0;
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k)
+        for (int k = 0; k < TILE_VEC; ++k) {
+            if (q0 + k >= keep)
+                keys[k] = KEY_DEAD;
             n_in += (keys[k] & KEY_IN) ? 1 : 0;
-        int tot;
-        const int ex = block_exclusive<int>(n_in, tot);
-        int64_t f = (tot > 0 ? tile_prefix[s.move_tile0 + local_tile] : 0) + ex;
+        }
+        int winc = n_in;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, winc, o);
+            if (lane >= o)
+                winc += v;
+        }
+        if (lane == 31)
+            s_wcnt[it & 1][warp] = winc;
+        // Every thread has copied its part of the stage into registers.
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            const int tn = t + S * gridDim.x;
+            if (tn < total) {
+                issue(tn, sidx);
+                ++issued;
+            }
+        }
+        int wpre = 0, tile_total = 0;
+#pragma unroll
+        for (int w = 0; w < MOVE_WARPS; ++w) {
+            const int v = s_wcnt[it & 1][w];
+            wpre += w < warp ? v : 0;
+            tile_total += v;
+        }
+        int64_t f = (tile_total > 0 ? tile_prefix[s.move_tile0 + local_tile] : 0) + wpre + winc -
+                    n_in;
+        int64_t fin[TILE_VEC];
+#pragma unroll
+        for (int k = 0; k < TILE_VEC; ++k) {
+            if (keys[k] & KEY_DEAD) {
+                fin[k] = -1;
+            } else if (keys[k] & KEY_IN) {
+                fin[k] = cells.base_in[keys[k] & KEY_CELL] + f;
+                ++f;
+            } else {
+                fin[k] = keys[k];
+            }
+        }
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
             if (keys[k] & KEY_DEAD)
                 continue;
-            int64_t fin;
-            if (keys[k] & KEY_IN) {
-                fin = cells.base_in[keys[k] & KEY_CELL] + f;
-                ++f;
-            } else {
-                fin = keys[k];
-            }
-            if (fin < 0 || fin >= keep) {
+            if (fin[k] < 0 || fin[k] >= keep) {
                 report_error(err, DSMC_ERR_STATE); // counts and keys disagree
                 continue;
             }
-            const int64_t gd = c.pbase + fin;
+            const int64_t gd = c.pbase + fin[k];
             dst.x[gd] = x[k];
             dst.y[gd] = y[k];
             dst.vx[gd] = vx[k];
             dst.vy[gd] = vy[k];
             dst.vz[gd] = vz[k];
+        }
+    }
+    if (failed) {
+        // A copy never completed: report, then wait (bounded) for the copies
+        // this CTA still has in flight before its shared memory goes away.
+        if (threadIdx.x == 0) {
+            report_error(err, DSMC_ERR_TIMEOUT);
+            for (int j = it; j < issued; ++j)
+                mbar_wait(&bar[j % S], static_cast<uint32_t>((j / S) & 1));
         }
     }
 }
