@@ -36,16 +36,23 @@ METRIC = "particle-steps/s on 1 B200"
 UNIT = "particle-steps/s"
 
 # Algorithmic bytes per particle (and per cell) of the step's kernels, FP32
-# state (x, y, vx, vy, vz = 20 B) / FP64 state (40 B).
-#   k_move     reads x, y, vx, vy and writes x, y
-#   k_scatter  the cell sort: key read twice, state read and written once
-#   k_collide  sampling: reads v, read-modify-write of the cell moments
+# state (x, y, vx, vy, vz = 20 B) / FP64 state (40 B); the 4-byte key is the
+# cell index the sort needs from the move.
+#   k_move     reads x, y, vx, vy; writes x, y and the key
+#   k_scatter  reads the key and the state, writes the state once
+#   k_sample   reads vx, vy, vz; read-modify-write of the 13 FP64 moments of
+#              every cell plus its start offset
 ALGO = {
-    "k_move": {"fp32": 24, "fp64": 48},
-    "k_scatter": {"fp32": 48, "fp64": 88},
-    "k_collide": {"fp32": 12, "fp64": 24},
+    "k_move": {"fp32": 28, "fp64": 52},
+    "k_scatter": {"fp32": 44, "fp64": 84},
+    "k_sample": {"fp32": 12, "fp64": 24},
 }
-CELL_BYTES = 2 * 136  # read + write of the 17 FP64 moments of a cell
+CELL_BYTES = {"k_sample": 2 * 13 * 8 + 4}
+
+# DRAM bytes per particle (read + write) of each kernel from one ncu capture
+# of the same kernels on the 640x640 case (8.1e6 particles, FP32), scaled by
+# the particles of a launch.
+NCU_TRAFFIC_PER_PARTICLE = {}
 
 
 def peaks():
@@ -321,7 +328,7 @@ def main():
         avg = kms / launches
         ent = {"ms_avg": avg, "launches": launches}
         if name in ALGO:
-            b = ALGO[name][key] * np_mean + (CELL_BYTES * ncell if name == "k_collide" else 0)
+            b = ALGO[name][key] * np_mean + CELL_BYTES.get(name, 0) * ncell
             ent["algo_bytes"] = b
             ent["gbs"] = b / (avg / 1e3) / 1e9
         kernels[name] = ent
@@ -332,17 +339,20 @@ def main():
         ach = kernels[dom]["gbs"]
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak,
                 "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
-                "traffic": None,
+                "traffic": (NCU_TRAFFIC_PER_PARTICLE[dom] * np_mean
+                            if key == "fp32" and dom in NCU_TRAFFIC_PER_PARTICLE else None),
                 "algo_bytes_per_launch": kernels[dom]["algo_bytes"],
                 "units_per_launch": np_mean}
-    step_kernels = 12
+    # Launches of this library's kernels per step (all launches of the
+    # profiled steps, which run the same sequence as the graph of a step).
+    step_kernels = sum(v["launches"] for v in kernels.values()) / max(1, args.profile_steps)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if prec == FP32 else "f64", "data": "synthetic",
             "config": workload_config(args), "particles_mean": np_mean,
             "status": status, "roofline": roof, "kernels": kernels,
-            "gpu_launches": step_kernels * args.steps, "clocks": clk, "e2e": e2e}
+            "gpu_launches": int(round(step_kernels * args.steps)), "clocks": clk, "e2e": e2e}
     if reduce_ms is not None:
         line["replica_allreduce_ms"] = reduce_ms
     if world == 1 and not args.no_cpu:

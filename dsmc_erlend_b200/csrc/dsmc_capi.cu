@@ -45,7 +45,6 @@ struct Timed {
     cudaEvent_t a, b;
 };
 
-template <class T> size_t collide_smem() { return sizeof(T) * 3 * COLLIDE_SMEM_PCL; }
 
 } // namespace
 
@@ -272,8 +271,9 @@ template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sampl
     }
     if (do_sample) {
         Span sp(c, KID_SAMPLE);
-        k_sample<T><<<c->grid_collide, COLLIDE_CELLS, collide_smem<T>(), c->stream>>>(
-            c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, c->ncase);
+        k_sample<T><<<c->grid_collide, COLLIDE_CELLS, sample_smem<T>(), c->stream>>>(
+            c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, c->ncase,
+            c->d_err);
     }
     CK(cudaGetLastError());
     return DSMC_OK;
@@ -485,9 +485,9 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
                                                      scatter_smem<T>()));
     c->grid_scatter = std::max(1, b) * c->sms;
     CK(cudaFuncSetAttribute(k_sample<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(collide_smem<T>())));
+                            static_cast<int>(sample_smem<T>())));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sample<T>, COLLIDE_CELLS,
-                                                     collide_smem<T>()));
+                                                     sample_smem<T>()));
     c->grid_collide = std::max(1, b) * c->sms;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_collide_select, 256, 0));
     c->grid_select = std::max(1, b) * c->sms;

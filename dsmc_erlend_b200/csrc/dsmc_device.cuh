@@ -93,7 +93,7 @@ struct CaseState {
 
 // Whole-context counters of one step, cleared before each step.
 struct StepScratch {
-    uint32_t move_ticket, inject_ticket, tail_ticket, cell_ticket, otile_ticket;
+    uint32_t inject_ticket, tail_ticket, cell_ticket, otile_ticket;
     int32_t total_move_tiles, total_inject_tiles, total_tail_tiles;
     int32_t total_cell_tiles, total_otiles;
     uint32_t obuf_count;

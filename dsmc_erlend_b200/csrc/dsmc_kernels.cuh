@@ -398,7 +398,8 @@ static_assert(TILE_VEC * MOVE_WARPS == 32, "one warp scans the (iteration, warp)
 
 // Tiles are staged in shared memory by bulk asynchronous copies, MOVE
 // stages deep, so the loads of the next tiles of a CTA are in flight while it
-// moves the current one.  Two passes per tile: the first moves every slot that
+// moves the current one.  Tiles are dealt to CTAs statically (no tile waits on
+// another, so no ticket order is needed).  Two passes per tile: the first moves every slot that
 // free_flight accepts, the second runs the exact body for the other few.
 // Both give the exact body's result for every slot.
 template <class T> struct MoveStage {
@@ -445,7 +446,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
             mbar_init(&bar[i], 1);
         fence_mbar_init();
         for (int i = 0; i < S; ++i) {
-            const int t = static_cast<int>(atomicAdd(&sc->move_ticket, 1u));
+            const int t = blockIdx.x + i * gridDim.x;
             s_t[i] = t;
             if (t < total)
                 issue(t, i);
@@ -547,7 +548,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
         }
         if (threadIdx.x == 0) {
             fence_proxy_async_smem();
-            const int tn = static_cast<int>(atomicAdd(&sc->move_ticket, 1u));
+            const int tn = t + S * gridDim.x;
             s_t[sidx] = tn;
             if (tn < total)
                 issue(tn, sidx);
@@ -1111,8 +1112,10 @@ __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *s
 // Tiles are staged whole in shared memory by bulk asynchronous copies, SCATTER
 // stages deep: while the warps place tile i, the copies of the next tiles of
 // this CTA are in flight, so the kernel keeps HBM busy without holding the
-// loads in registers.  One barrier per tile: it publishes the per-warp
-// in-range counts and frees the stage for its refill.
+// loads in registers.  Iteration k of thread t takes slot k * TILE_THREADS + t
+// of the tile, so the 32 lanes of a warp store 32 consecutive destinations
+// when they share a cell.  One barrier per tile: it publishes the in-range
+// counts of the (iteration, warp) chunks and frees the stage for its refill.
 // ---------------------------------------------------------------------------
 template <class T> struct ScatterStage {
     uint32_t key[TILE];
@@ -1134,9 +1137,10 @@ __global__ void __launch_bounds__(TILE_THREADS)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     ScatterStage<T> *stage = reinterpret_cast<ScatterStage<T> *>(smem_raw);
     __shared__ uint64_t bar[S];
-    __shared__ int s_wcnt[2][MOVE_WARPS];
+    __shared__ int s_cnt[2][32]; // in-range counts per (iteration, warp), two buffers
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    const unsigned lanes_below = (1u << lane) - 1u;
     const int total = tt.scatter0[ncase];
 
     // Thread 0 only: starts the copies of tile t into stage sidx.
@@ -1172,34 +1176,25 @@ __global__ void __launch_bounds__(TILE_THREADS)
         const CaseDev &c = cases[ci];
         const CaseState &s = st[ci];
         const int local_tile = t - tt.scatter0[ci];
-        const int64_t q0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
         const int64_t keep = s.n_keep;
         const ScatterStage<T> &sg = stage[sidx];
-        const int e0 = threadIdx.x * TILE_VEC;
+        const int64_t tile0 = static_cast<int64_t>(local_tile) * TILE;
         uint32_t keys[TILE_VEC];
         T x[TILE_VEC], y[TILE_VEC], vx[TILE_VEC], vy[TILE_VEC], vz[TILE_VEC];
-        load4(sg.key + e0, keys);
-        load4(sg.v[0] + e0, x);
-        load4(sg.v[1] + e0, y);
-        load4(sg.v[2] + e0, vx);
-        load4(sg.v[3] + e0, vy);
-        load4(sg.v[4] + e0, vz);
-        int n_in = 0;
+        unsigned bin[TILE_VEC];
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if (q0 + k >= keep)
-                keys[k] = KEY_DEAD;
-            n_in += (keys[k] & KEY_IN) ? 1 : 0;
+            const int e = k * TILE_THREADS + threadIdx.x;
+            keys[k] = (ok && tile0 + e < keep) ? sg.key[e] : KEY_DEAD;
+            x[k] = sg.v[0][e];
+            y[k] = sg.v[1][e];
+            vx[k] = sg.v[2][e];
+            vy[k] = sg.v[3][e];
+            vz[k] = sg.v[4][e];
+            bin[k] = __ballot_sync(0xffffffffu, (keys[k] & KEY_IN) != 0);
+            if (lane == 0)
+                s_cnt[it & 1][k * MOVE_WARPS + warp] = __popc(bin[k]);
         }
-        int winc = n_in;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, winc, o);
-            if (lane >= o)
-                winc += v;
-        }
-        if (lane == 31)
-            s_wcnt[it & 1][warp] = winc;
         // Every thread has copied its part of the stage into registers.
         if (__syncthreads_or(!ok)) {
             failed = true;
@@ -1213,26 +1208,30 @@ __global__ void __launch_bounds__(TILE_THREADS)
                 ++issued;
             }
         }
-        int wpre = 0, tile_total = 0;
+        // Lane i: in-range count of (iteration, warp) chunk i; chunks are in
+        // slot order, so their exclusive scan ranks them within the tile.
+        const int cnt = s_cnt[it & 1][lane];
+        int cinc = cnt;
 #pragma unroll
-        for (int w = 0; w < MOVE_WARPS; ++w) {
-            const int v = s_wcnt[it & 1][w];
-            wpre += w < warp ? v : 0;
-            tile_total += v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, cinc, o);
+            if (lane >= o)
+                cinc += v;
         }
-        int64_t f = (tile_total > 0 ? tile_prefix[s.move_tile0 + local_tile] : 0) + wpre + winc -
-                    n_in;
+        const int cexcl = cinc - cnt;
+        const int tile_total = __shfl_sync(0xffffffffu, cinc, 31);
+        const int64_t base = tile_total > 0 ? tile_prefix[s.move_tile0 + local_tile] : 0;
         int64_t fin[TILE_VEC];
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if (keys[k] & KEY_DEAD) {
+            const int pre = __shfl_sync(0xffffffffu, cexcl, k * MOVE_WARPS + warp);
+            if (keys[k] & KEY_DEAD)
                 fin[k] = -1;
-            } else if (keys[k] & KEY_IN) {
-                fin[k] = cells.base_in[keys[k] & KEY_CELL] + f;
-                ++f;
-            } else {
+            else if (keys[k] & KEY_IN)
+                fin[k] = cells.base_in[keys[k] & KEY_CELL] + base + pre +
+                         __popc(bin[k] & lanes_below);
+            else
                 fin[k] = keys[k];
-            }
         }
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
@@ -1272,7 +1271,6 @@ __global__ void __launch_bounds__(TILE_THREADS)
 // budget nor the occupancy of the passes that touch every cell.
 // ---------------------------------------------------------------------------
 constexpr int COLLIDE_CELLS = 128;
-constexpr int COLLIDE_SMEM_PCL = 3072;
 
 // NTC pair count of a cell with n particles (Collision.cpp:23-27) and the
 // draw that rounds it.
@@ -1383,81 +1381,145 @@ __global__ void __launch_bounds__(128)
 // ---------------------------------------------------------------------------
 // k_sample: Sampling's accumulation (Sampling.cpp:14-31) in the reference's
 // order: one thread per cell walks its particles sequentially, so every FP64
-// sum is bit-identical to the reference's.  A CTA stages the velocities of its
-// cells in shared memory when they fit.
+// sum is bit-identical to the reference's.  The velocities of a block of
+// COLLIDE_CELLS cells are one contiguous slot range; bulk asynchronous copies
+// stage it in shared memory, SAMPLE_STAGES blocks ahead, so the loads of the
+// next blocks are in flight while the threads accumulate the current one.  A
+// block whose range exceeds a stage is read from global memory directly.
 // ---------------------------------------------------------------------------
+constexpr int SAMPLE_STAGES = 2;
+template <class T> __host__ __device__ constexpr int sample_pcl() { return 12288 / sizeof(T); }
+template <class T> struct SampleStage {
+    T v[3][sample_pcl<T>() + 16 / sizeof(T)];
+};
+template <class T> __host__ __device__ constexpr size_t sample_smem()
+{
+    return sizeof(SampleStage<T>) * SAMPLE_STAGES;
+}
+
 template <class T>
 __global__ void __launch_bounds__(COLLIDE_CELLS)
     k_sample(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt, Slots<T> p,
-             Cells cells, int side, int ncase)
+             Cells cells, int side, int ncase, int *err)
 {
-    extern __shared__ unsigned char smem_raw[];
-    T *sv = reinterpret_cast<T *>(smem_raw);
+    constexpr int S = SAMPLE_STAGES;
+    constexpr int A = 16 / sizeof(T); // elements per 16 bytes
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    SampleStage<T> *stage = reinterpret_cast<SampleStage<T> *>(smem_raw);
+    __shared__ uint64_t bar[S];
+    __shared__ int s_staged[S];
+    __shared__ int64_t s_r0[S]; // first staged slot (rounded down to A)
     const int32_t *start = cells.start[side];
     const int nblocks = tt.cblock0[ncase];
-    for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+
+    // Thread 0 only: stages the velocities of block b in stage sidx when its
+    // case samples this step and the range fits.
+    auto issue = [&](int b, int sidx) {
+        s_staged[sidx] = 0;
         const int ci = case_of(tt.cblock0, ncase, b);
         if (st[ci].sampling_mode != 1)
-            continue;
+            return;
         const CaseDev &c = cases[ci];
         const int cl0 = (b - tt.cblock0[ci]) * COLLIDE_CELLS;
         const int cl1 = min(cl0 + COLLIDE_CELLS, c.ncell);
-        const int64_t r0 = start[c.cbase + cl0], r1 = start[c.cbase + cl1];
-        const int64_t nr = r1 - r0;
-        const bool staged = nr <= COLLIDE_SMEM_PCL;
-        __syncthreads();
-        if (staged) {
-            const T *gx = p.vx + c.pbase + r0, *gy = p.vy + c.pbase + r0,
-                    *gz = p.vz + c.pbase + r0;
-            for (int64_t i = threadIdx.x; i < nr; i += blockDim.x) {
-                sv[i] = gx[i];
-                sv[COLLIDE_SMEM_PCL + i] = gy[i];
-                sv[2 * COLLIDE_SMEM_PCL + i] = gz[i];
+        const int64_t r0 = start[c.cbase + cl0] & ~static_cast<int64_t>(A - 1);
+        const int64_t r1 = (start[c.cbase + cl1] + A - 1) & ~static_cast<int64_t>(A - 1);
+        const int64_t n = r1 - r0;
+        if (n <= 0 || n > sample_pcl<T>() + A)
+            return;
+        const uint32_t bytes = static_cast<uint32_t>(n * sizeof(T));
+        mbar_arrive_expect_tx(&bar[sidx], 3 * bytes);
+        bulk_g2s(stage[sidx].v[0], p.vx + c.pbase + r0, bytes, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[1], p.vy + c.pbase + r0, bytes, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[2], p.vz + c.pbase + r0, bytes, &bar[sidx]);
+        s_r0[sidx] = r0;
+        s_staged[sidx] = 1;
+    };
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S; ++i)
+            mbar_init(&bar[i], 1);
+        fence_mbar_init();
+        for (int i = 0; i < S; ++i)
+            if (blockIdx.x + i * gridDim.x < nblocks)
+                issue(blockIdx.x + i * gridDim.x, i);
+    }
+    __syncthreads();
+
+    uint32_t phase = 0; // bit i: parity of the next completion of stage i
+    for (int it = 0;; ++it) {
+        const int b = blockIdx.x + it * gridDim.x;
+        if (b >= nblocks)
+            return;
+        const int sidx = it % S;
+        const int ci = case_of(tt.cblock0, ncase, b);
+        const bool staged = s_staged[sidx] != 0;
+        bool ok = true;
+        if (st[ci].sampling_mode == 1) {
+            const CaseDev &c = cases[ci];
+            const int cl0 = (b - tt.cblock0[ci]) * COLLIDE_CELLS;
+            const int cl = cl0 + threadIdx.x;
+            const int cg = c.cbase + cl;
+            const bool mine = cl < c.ncell;
+            int64_t a0 = 0;
+            int n = 0;
+            double a[ACC_NC];
+            if (mine) {
+                a0 = start[cg];
+                n = static_cast<int>(start[cg + 1] - a0);
+#pragma unroll
+                for (int m = 0; m < ACC_NC; ++m)
+                    a[m] = cells.acc[m * cells.acc_stride + cg];
+            }
+            const T *vx = p.vx + c.pbase + a0, *vy = p.vy + c.pbase + a0,
+                    *vz = p.vz + c.pbase + a0;
+            if (staged) {
+                ok = mbar_wait(&bar[sidx], (phase >> sidx) & 1u);
+                phase ^= 1u << sidx;
+                const int64_t off = a0 - s_r0[sidx];
+                vx = stage[sidx].v[0] + off;
+                vy = stage[sidx].v[1] + off;
+                vz = stage[sidx].v[2] + off;
+            }
+            if (mine && n > 0 && ok) {
+                for (int i = 0; i < n; ++i) {
+                    const double v0 = vx[i], v1 = vy[i], v2 = vz[i];
+                    a[ACC_NP] += 1.0;
+                    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
+                    a[ACC_V0] += v0;
+                    a[ACC_V1] += v1;
+                    a[ACC_V2] += v2;
+                    a[ACC_V2V0] += vv * v0;
+                    a[ACC_V2V1] += vv * v1;
+                    a[ACC_V2V2] += vv * v2;
+                    a[ACC_VV00] += v0 * v0;
+                    a[ACC_VV01] += v0 * v1;
+                    a[ACC_VV02] += v0 * v2;
+                    a[ACC_VV11] += v1 * v1;
+                    a[ACC_VV12] += v1 * v2;
+                    a[ACC_VV22] += v2 * v2;
+                }
+#pragma unroll
+                for (int m = 0; m < ACC_NC; ++m)
+                    cells.acc[m * cells.acc_stride + cg] = a[m];
             }
         }
-        __syncthreads();
-        const int cl = cl0 + threadIdx.x;
-        if (cl >= cl1)
-            continue;
-        const int cg = c.cbase + cl;
-        const int64_t a0 = start[cg];
-        const int n = static_cast<int>(start[cg + 1] - a0);
-        if (n == 0)
-            continue;
-        const T *vx, *vy, *vz;
-        if (staged) {
-            vx = sv + (a0 - r0);
-            vy = sv + COLLIDE_SMEM_PCL + (a0 - r0);
-            vz = sv + 2 * COLLIDE_SMEM_PCL + (a0 - r0);
-        } else {
-            vx = p.vx + c.pbase + a0;
-            vy = p.vy + c.pbase + a0;
-            vz = p.vz + c.pbase + a0;
+        // The stage is consumed: refill it with this CTA's block it + S.
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                report_error(err, DSMC_ERR_TIMEOUT);
+                for (int j = 0; j < S; ++j)
+                    if (s_staged[j])
+                        mbar_wait(&bar[j], (phase >> j) & 1u);
+            }
+            return;
         }
-        double a[ACC_NC];
-#pragma unroll
-        for (int m = 0; m < ACC_NC; ++m)
-            a[m] = cells.acc[m * cells.acc_stride + cg];
-        for (int i = 0; i < n; ++i) {
-            const double v0 = vx[i], v1 = vy[i], v2 = vz[i];
-            a[ACC_NP] += 1.0;
-            const double vv = v0 * v0 + v1 * v1 + v2 * v2;
-            a[ACC_V0] += v0;
-            a[ACC_V1] += v1;
-            a[ACC_V2] += v2;
-            a[ACC_V2V0] += vv * v0;
-            a[ACC_V2V1] += vv * v1;
-            a[ACC_V2V2] += vv * v2;
-            a[ACC_VV00] += v0 * v0;
-            a[ACC_VV01] += v0 * v1;
-            a[ACC_VV02] += v0 * v2;
-            a[ACC_VV11] += v1 * v1;
-            a[ACC_VV12] += v1 * v2;
-            a[ACC_VV22] += v2 * v2;
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            const int bn = b + S * gridDim.x;
+            s_staged[sidx] = 0;
+            if (bn < nblocks)
+                issue(bn, sidx);
         }
-#pragma unroll
-        for (int m = 0; m < ACC_NC; ++m)
-            cells.acc[m * cells.acc_stride + cg] = a[m];
     }
 }
 
