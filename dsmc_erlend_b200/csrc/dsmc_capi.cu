@@ -29,13 +29,13 @@ namespace {
     } while (0)
 
 enum KernelId {
-    KID_PLAN, KID_MOVE, KID_INJECT, KID_DEAD_SCAN, KID_HOLES, KID_PLAN2, KID_TAIL,
+    KID_PLAN, KID_MOVE, KID_MOVE_NEAR, KID_INJECT, KID_DEAD_SCAN, KID_HOLES, KID_PLAN2, KID_TAIL,
     KID_CELL_SCAN, KID_TILE_SCAN,
     KID_OLIST, KID_CELL_FIX, KID_SCATTER, KID_COLLIDE_SELECT, KID_COLLIDE, KID_SAMPLE,
     KID_FINISH, KID_COUNT
 };
 const char *kKernelNames[KID_COUNT] = {
-    "k_plan",      "k_move",   "k_inject",         "k_dead_scan",     "k_holes",
+    "k_plan",      "k_move",   "k_move_near",      "k_inject",         "k_dead_scan",     "k_holes",
     "k_plan2",     "k_tail",
     "k_cell_scan", "k_tile_scan", "k_olist",       "k_cell_fix",      "k_scatter",
     "k_collide_select", "k_collide_pairs", "k_sample", "k_finish"};
@@ -82,6 +82,7 @@ struct dsmc_ctx {
     size_t lb_words = 0;
     int32_t *hole_pos = nullptr, *hole_oc = nullptr;
     uint32_t *obuf = nullptr;
+    uint32_t *near_list = nullptr; // slots queued by k_move for k_move_near
     int32_t *olist = nullptr;
     uint32_t *coll_list = nullptr; // cells with candidate pairs, per step
 
@@ -173,7 +174,13 @@ template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
         Span sp(c, KID_MOVE);
         k_move<T><<<c->grid_move, TILE_THREADS, move_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
-            c->tile_in, c->tile_dead, c->obuf, c->ncase, c->d_err);
+            c->tile_in, c->tile_dead, c->obuf, c->near_list, c->ncase, c->d_err);
+    }
+    if (!init_mode) {
+        Span sp(c, KID_MOVE_NEAR);
+        k_move_near<T><<<c->sms, TILE_THREADS, 0, c->stream>>>(
+            c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
+            c->tile_in, c->tile_dead, c->obuf, c->near_list, c->ncase, c->d_err);
     }
     CK(cudaGetLastError());
     return DSMC_OK;
@@ -346,11 +353,11 @@ float float_up(double v)
     return f;
 }
 
-// FP32 constants of the free-flight pass (see CaseDev).  fcell_eps bounds
-// |q' - (x - X1) / DX| for the float estimate q' inside the grid: the float
-// difference, the product and 1/DX each round by at most 2^-24 relative
-// (3 |q| 2^-24 in all), and X1 rounded to float adds 2^-24 |X1| / DX; the
-// bound is doubled, plus 1e-9 for the FP64 quotient of the reference.
+// FP32 constants of the free-flight pass (see CaseDev).  The float cell
+// estimate q' differs from (x - X1) / DX by at most e inside the grid: the
+// float difference, the product and 1/DX each round by at most 2^-24
+// relative (3 |q| 2^-24 in all), and X1 rounded to float adds 2^-24 |X1| / DX;
+// e is doubled, plus 1e-9 for the FP64 quotient of the reference.
 void set_float_bounds(CaseDev &c, const dsmc_params &p)
 {
     c.fx1 = static_cast<float>(c.x1);
@@ -360,7 +367,12 @@ void set_float_bounds(CaseDev &c, const dsmc_params &p)
     const double qmax = static_cast<double>(std::max(p.nx, p.ny)) + 1.0;
     const double shift = std::max(std::fabs(c.x1) / c.dx, std::fabs(c.y1) / c.dy);
     const double err = std::ldexp(3.01 * qmax + 1.01 * shift + 1.0, -24);
-    c.fcell_eps = static_cast<float>(2.0 * err + 1e-9);
+    // Half-width of the certain window of r - 0.5, less 2^-20 for the
+    // rounding of that difference; off (negative) for grids of 2^20 cells or
+    // more per side, where the rounding constant's range is not assured.
+    c.fcell_hw = std::max(p.nx, p.ny) < (1 << 20)
+                     ? static_cast<float>(0.5 - (2.0 * err + 1e-9) - std::ldexp(1.0, -20))
+                     : -1.0f;
     c.dom_lo[0] = float_down(c.x1);
     c.dom_lo[1] = float_down(c.y1);
     c.dom_hi[0] = float_up(c.x2);
@@ -512,7 +524,8 @@ void free_ctx(dsmc_ctx *c)
                     c->cells.fin, c->cells.ostart, c->cells.base_in, c->cells.start[0],
                     c->cells.start[1], c->cells.acc, c->tile_in, c->tile_prefix, c->tile_dead,
                     c->tile_dprefix, c->itile_dead, c->itile_dprefix, c->lb,
-                    c->hole_pos, c->hole_oc, c->obuf, c->olist, c->coll_list};
+                    c->hole_pos, c->hole_oc, c->obuf, c->olist, c->coll_list,
+                    c->near_list};
     for (void *p : ptrs)
         if (p)
             cudaFree(p);
@@ -864,6 +877,7 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     // Appends per step and case: out-of-range moved slots + injected
     // survivors (n_old + n_inj <= cap) + refilled holes (<= n_old): <= 2 cap.
     ok &= alloc(reinterpret_cast<void **>(&c->obuf), sizeof(uint32_t) * 2 * slot);
+    ok &= alloc(reinterpret_cast<void **>(&c->near_list), sizeof(uint32_t) * slot);
     ok &= alloc(reinterpret_cast<void **>(&c->olist), sizeof(int32_t) * slot);
     ok &= alloc(reinterpret_cast<void **>(&c->coll_list), sizeof(uint32_t) * cell);
     if (!ok) {

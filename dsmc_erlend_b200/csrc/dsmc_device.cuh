@@ -46,7 +46,7 @@ struct CaseDev {
     // rounded to float; the bound on the error of the float cell estimate;
     // the domain bounds rounded inwards-exclusive (a float x is <= X1 iff it
     // is <= dom_lo[0], >= X2 iff >= dom_hi[0]); the near bounds rounded out.
-    float fx1, fy1, finv_dx, finv_dy, fcell_eps;
+    float fx1, fy1, finv_dx, finv_dy, fcell_hw; // fcell_hw: half-width of the certain window
     float dom_lo[2], dom_hi[2];
     float fnear_lo[2], fnear_hi[2];
     double box_lo[2], box_hi[2];   // IntersectBox bounds (Geometry.cpp:184-185)
@@ -97,6 +97,7 @@ struct StepScratch {
     int32_t total_move_tiles, total_inject_tiles, total_tail_tiles;
     int32_t total_cell_tiles, total_otiles;
     uint32_t obuf_count;
+    uint32_t near_count;  // slots queued by k_move for k_move_near
     uint32_t coll_count;  // cells listed by k_collide_select
     int32_t init_mode;
 };
@@ -333,41 +334,43 @@ __device__ __forceinline__ bool cell_of_fast(const CaseDev &c, double x, double 
 
 // FP32 estimate of the cell of a float position for the free-flight pass.
 // The estimate q' = (x - fx1) * finv_dx differs from (x - X1) / DX by less
-// than fcell_eps inside the grid (float rounding of X1, 1/DX, the difference
-// and the product), so when q' is more than fcell_eps from an integer its
-// floor is the reference's FP64 floor.  Returns false when not certain.
-// Floors use the 1.5 * 2^23 rounding constant (|q'| < 2^21 checked).
-__device__ __forceinline__ bool floor_fast_f(float q, float eps, int32_t &n)
+// than a bound e inside the grid (float rounding of X1, 1/DX, the difference
+// and the product; computed on the host), so when q' is more than e from an
+// integer its floor is the reference's FP64 floor.  Returns false when not
+// certain.
+//
+// floor(q') comes from rounding q' - 0.5 to an integer with the 1.5 * 2^23
+// constant; r = q' - floor is then certain when |r - 0.5| < fcell_hw
+// (= 0.5 - e, less a margin for the rounding of r - 0.5).  A tie or
+// any |q'| >= 2^21 gives r outside that window, so no separate range check
+// is needed; the host keeps the grid below 2^20 cells per side for this
+// path (fcell_hw < 0 turns it off).
+__device__ __forceinline__ bool floor_fast_f(float q, float hw, int32_t &n)
 {
-    if (!(fabsf(q) < 2097152.0f))
-        return false;
-    const float t = q + 12582912.0f;
-    float f = t - 12582912.0f;
-    int32_t i = __float_as_int(t) - 0x4B400000;
-    if (f > q) {
-        f -= 1.0f;
-        i -= 1;
-    }
-    const float r = q - f;
-    n = i;
-    return r > eps && r < 1.0f - eps;
+    const float t = (q - 0.5f) + 12582912.0f;
+    const float f = t - 12582912.0f;
+    n = __float_as_int(t) - 0x4B400000;
+    return fabsf((q - f) - 0.5f) < hw;
 }
 
 __device__ __forceinline__ bool cell_of_fast_f(const CaseDev &c, float x, float y, int32_t &cell)
 {
     int32_t k, l;
-    if (!floor_fast_f((x - c.fx1) * c.finv_dx, c.fcell_eps, k) ||
-        !floor_fast_f((y - c.fy1) * c.finv_dy, c.fcell_eps, l))
-        return false;
-    cell = (k >= 0 && k < c.nx && l >= 0 && l < c.ny) ? k * c.ny + l : NO_CELL;
-    return true;
+    const bool ok = floor_fast_f((x - c.fx1) * c.finv_dx, c.fcell_hw, k) &
+                    floor_fast_f((y - c.fy1) * c.finv_dy, c.fcell_hw, l);
+    const bool in = (static_cast<uint32_t>(k) < static_cast<uint32_t>(c.nx)) &
+                    (static_cast<uint32_t>(l) < static_cast<uint32_t>(c.ny));
+    cell = in ? static_cast<int32_t>(static_cast<uint32_t>(k) * static_cast<uint32_t>(c.ny) +
+                                     static_cast<uint32_t>(l))
+              : NO_CELL;
+    return ok;
 }
 
 // Removal predicate of BoundaryConditions (Boundary.cpp:183-188) for a float
 // position, exact: compares against the float bounds described in CaseDev.
 __device__ __forceinline__ bool outside_domain_f(const CaseDev &c, float x, float y)
 {
-    return x <= c.dom_lo[0] || x >= c.dom_hi[0] || y <= c.dom_lo[1] || y >= c.dom_hi[1];
+    return (x <= c.dom_lo[0]) | (x >= c.dom_hi[0]) | (y <= c.dom_lo[1]) | (y >= c.dom_hi[1]);
 }
 
 // near_box for a float segment (start, rounded end): the float near bounds
@@ -375,8 +378,8 @@ __device__ __forceinline__ bool outside_domain_f(const CaseDev &c, float x, floa
 // inside the 2^-20 widening, so "not near" here implies "not near" in FP64.
 __device__ __forceinline__ bool near_box_f(const CaseDev &c, float x0, float y0, float x1, float y1)
 {
-    return fmaxf(x0, x1) > c.fnear_lo[0] && fminf(x0, x1) < c.fnear_hi[0] &&
-           fmaxf(y0, y1) > c.fnear_lo[1] && fminf(y0, y1) < c.fnear_hi[1];
+    return (fmaxf(x0, x1) > c.fnear_lo[0]) & (fminf(x0, x1) < c.fnear_hi[0]) &
+           (fmaxf(y0, y1) > c.fnear_lo[1]) & (fminf(y0, y1) < c.fnear_hi[1]);
 }
 
 // False only when IntersectBox cannot report an impact: the segment's

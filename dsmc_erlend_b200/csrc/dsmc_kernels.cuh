@@ -334,15 +334,15 @@ __device__ __forceinline__ bool free_flight(const CaseDev &c, float x0, float y0
 {
     xn = __double2float_rn(static_cast<double>(x0) + c.dt * static_cast<double>(vx));
     yn = __double2float_rn(static_cast<double>(y0) + c.dt * static_cast<double>(vy));
-    if (near_box_f(c, x0, y0, xn, yn))
-        return false;
-    if (!cell_of_fast_f(c, x0, y0, oc) &&
-        !cell_of_fast(c, static_cast<double>(x0), static_cast<double>(y0), oc))
-        return false;
+    const bool near = near_box_f(c, x0, y0, xn, yn);
+    bool ok_o = cell_of_fast_f(c, x0, y0, oc);
     gone = outside_domain_f(c, xn, yn);
-    nc = NO_CELL;
-    return gone || cell_of_fast_f(c, xn, yn, nc) ||
-           cell_of_fast(c, static_cast<double>(xn), static_cast<double>(yn), nc);
+    bool ok_n = cell_of_fast_f(c, xn, yn, nc) | gone;
+    if (!ok_o)
+        ok_o = cell_of_fast(c, static_cast<double>(x0), static_cast<double>(y0), oc);
+    if (!ok_n)
+        ok_n = cell_of_fast(c, static_cast<double>(xn), static_cast<double>(yn), nc);
+    return !near & ok_o & ok_n;
 }
 
 // Stores the key of a classified slot and moves the cell counters: every
@@ -360,9 +360,9 @@ __device__ __forceinline__ void commit_class(const MoveClass &m, uint32_t *key, 
 
 // The full MoveParticles body (Boundary.cpp:284-328) for one slot: impact
 // test, wall interaction, FP32 placement outside the box, exact cell index.
-// Out of line, so its register demand stays out of the free-flight loop.
+// Runs in its own kernel, so its register demand stays out of k_move.
 template <class T>
-__device__ __noinline__ MoveClass move_near_box(const CaseDev &c, int64_t step, int64_t q,
+__device__ __forceinline__ MoveClass move_near_box(const CaseDev &c, int64_t step, int64_t q,
                                                 int64_t g, Slots<T> p, uint32_t *key, Cells cells,
                                                 double &impulse, int &n_hit, int *err)
 {
@@ -399,9 +399,9 @@ static_assert(TILE_VEC * MOVE_WARPS == 32, "one warp scans the (iteration, warp)
 // Tiles are staged in shared memory by bulk asynchronous copies, MOVE
 // stages deep, so the loads of the next tiles of a CTA are in flight while it
 // moves the current one.  Tiles are dealt to CTAs statically (no tile waits on
-// another, so no ticket order is needed).  Two passes per tile: the first moves every slot that
-// free_flight accepts, the second runs the exact body for the other few.
-// Both give the exact body's result for every slot.
+// another, so no ticket order is needed).  k_move moves every slot that
+// free_flight accepts and queues the other few for k_move_near, which runs
+// the exact body; both give the exact body's result for every slot.
 template <class T> struct MoveStage {
     T v[4][TILE]; // x, y, vx, vy
 };
@@ -415,16 +415,19 @@ template <class T>
 __global__ void __launch_bounds__(TILE_THREADS, 4)
     k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
            Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
-           int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf, int ncase, int *err)
+           int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf,
+           uint32_t *__restrict__ near_list, int ncase, int *err)
 {
+    static_assert(TILE == 1024, "near_list packs the slot in tile into 10 bits");
     constexpr int S = move_stages<T>();
+    constexpr int NB = 3; // ballot buffers: a tile's are read until the next tile's barrier
     extern __shared__ __align__(128) unsigned char smem_raw[];
     MoveStage<T> *stage = reinterpret_cast<MoveStage<T> *>(smem_raw);
     __shared__ uint64_t bar[S];
-    __shared__ int s_t[S];                        // tile of each stage
-    __shared__ unsigned s_dead[2][32], s_out[2][32], s_in[2][32]; // ballots per (iteration, warp)
-    __shared__ unsigned s_opre[2][32];            // exclusive prefix of s_out
-    __shared__ uint32_t s_obase[2];
+    __shared__ CaseDev s_case; // constants of the current tile's case
+    __shared__ unsigned s_dead[NB][32], s_out[NB][32], s_in[NB][32]; // per (iteration, warp)
+    __shared__ unsigned s_opre[NB][32];                              // exclusive prefix of s_out
+    __shared__ uint32_t s_obase[NB];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
@@ -441,28 +444,49 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
         bulk_g2s(stage[sidx].v[2], p.vx + g0, vb, &bar[sidx]);
         bulk_g2s(stage[sidx].v[3], p.vy + g0, vb, &bar[sidx]);
     };
+    // All threads: the out-of-range list entries of the tile at global slot
+    // gt whose ballots are in buffer nb (counted by warp 0 after its barrier).
+    auto append = [&](int nb, int64_t gt) {
+        for (int k = 0; k < TILE_VEC; ++k) {
+            const int i = k * MOVE_WARPS + warp;
+            const unsigned bo = s_out[nb][i];
+            if ((bo >> lane) & 1u)
+                obuf[s_obase[nb] + s_opre[nb][i] + __popc(bo & lanes_below)] =
+                    static_cast<uint32_t>(gt + k * TILE_THREADS + threadIdx.x);
+        }
+    };
     if (threadIdx.x == 0) {
         for (int i = 0; i < S; ++i)
             mbar_init(&bar[i], 1);
         fence_mbar_init();
-        for (int i = 0; i < S; ++i) {
-            const int t = blockIdx.x + i * gridDim.x;
-            s_t[i] = t;
-            if (t < total)
-                issue(t, i);
-        }
+        for (int i = 0; i < S; ++i)
+            if (blockIdx.x + i * gridDim.x < total)
+                issue(blockIdx.x + i * gridDim.x, i);
     }
     __syncthreads();
 
-    for (int it = 0;; ++it) {
-        const int sidx = it % S;
-        const int par = it & 1;
-        const int t = s_t[sidx];
+    int cur_case = -1;
+    int64_t prev_gt = 0;
+    int it = 0;
+    for (;; ++it) {
+        const int t = blockIdx.x + it * gridDim.x;
         if (t >= total)
-            return;
-        const bool ok = mbar_wait(&bar[sidx], static_cast<uint32_t>((it / S) & 1));
+            break;
+        const int sidx = it % S;
+        const int nb = it % NB;
         const int ci = case_of(tt.move0, ncase, t);
-        const CaseDev &c = cases[ci];
+        if (ci != cur_case) {
+            // No thread reads s_case between a tile's barrier and the next
+            // tile's top, so the copy needs only the barrier after it.
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(cases + ci);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&s_case);
+            for (int w = threadIdx.x; w < static_cast<int>(sizeof(CaseDev) / 4); w += TILE_THREADS)
+                dst[w] = src[w];
+            __syncthreads();
+            cur_case = ci;
+        }
+        const CaseDev &c = s_case;
+        const bool ok = mbar_wait(&bar[sidx], static_cast<uint32_t>((it / S) & 1));
         const int local_tile = t - tt.move0[ci];
         const int64_t tile0 = static_cast<int64_t>(local_tile) * TILE;
         const int64_t left = st[ci].n_old - tile0;
@@ -497,51 +521,40 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
             const unsigned bo = __ballot_sync(0xffffffffu, m.out);
             const unsigned bi = __ballot_sync(0xffffffffu, m.in);
             if (lane == 0) {
-                s_dead[par][k * MOVE_WARPS + warp] = bd;
-                s_out[par][k * MOVE_WARPS + warp] = bo;
-                s_in[par][k * MOVE_WARPS + warp] = bi;
+                s_dead[nb][k * MOVE_WARPS + warp] = bd;
+                s_out[nb][k * MOVE_WARPS + warp] = bo;
+                s_in[nb][k * MOVE_WARPS + warp] = bi;
             }
         }
-        if (__any_sync(0xffffffffu, near != 0)) {
-            double impulse = 0.0;
-            int n_hit = 0;
-            const int64_t step = st[ci].step;
-#pragma unroll 1
-            for (int k = 0; k < TILE_VEC; ++k) {
-                const int e = k * TILE_THREADS + threadIdx.x;
-                MoveClass m;
-                m.dead = m.out = m.in = false;
-                if ((near >> k) & 1u)
-                    m = move_near_box<T>(c, step, tile0 + e, gt + e, p, key, cells, impulse,
-                                         n_hit, err);
-                const unsigned bd = __ballot_sync(0xffffffffu, m.dead);
-                const unsigned bo = __ballot_sync(0xffffffffu, m.out);
-                const unsigned bi = __ballot_sync(0xffffffffu, m.in);
-                if (lane == 0) {
-                    s_dead[par][k * MOVE_WARPS + warp] |= bd;
-                    s_out[par][k * MOVE_WARPS + warp] |= bo;
-                    s_in[par][k * MOVE_WARPS + warp] |= bi;
-                }
-            }
-            // Wall-hit diagnostics (Boundary.cpp:318-319).
+        // Slots for the exact body go to k_move_near's queue as (tile, slot
+        // in tile); their ballots, counts and list entries are added there.
+        const unsigned nq = __ballot_sync(0xffffffffu, near != 0);
+        if (nq) {
+            int n_mine = __popc(near);
+            int incl = n_mine;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                impulse += __shfl_xor_sync(0xffffffffu, impulse, o);
-                n_hit += __shfl_xor_sync(0xffffffffu, n_hit, o);
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o)
+                    incl += v;
             }
-            if (lane == 0 && n_hit > 0) {
-                atomicAdd(&st[ci].drag_impulse, impulse);
-                atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(n_hit));
-            }
+            uint32_t qbase = 0;
+            if (lane == 31)
+                qbase = atomicAdd(&sc->near_count, static_cast<uint32_t>(incl));
+            qbase = __shfl_sync(0xffffffffu, qbase, 31) + static_cast<uint32_t>(incl - n_mine);
+            for (int k = 0; k < TILE_VEC; ++k)
+                if ((near >> k) & 1u)
+                    near_list[qbase++] = (static_cast<uint32_t>(t) << 10) |
+                                         static_cast<uint32_t>(k * TILE_THREADS + threadIdx.x);
         }
-        // Every thread is done with the stage (its values are in registers or
-        // consumed): refill it with this CTA's next tile.
+        // The one barrier of the tile: the stage is consumed, this tile's
+        // ballots are complete and the previous tile's list base is visible.
         if (__syncthreads_or(!ok)) {
             // A copy never completed (nothing of this tile was written).
             if (threadIdx.x == 0) {
                 report_error(err, DSMC_ERR_TIMEOUT);
                 for (int j = it; j < it + S; ++j)
-                    if (s_t[j % S] < total)
+                    if (blockIdx.x + j * gridDim.x < total)
                         mbar_wait(&bar[j % S], static_cast<uint32_t>((j / S) & 1));
             }
             return;
@@ -549,7 +562,6 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
         if (threadIdx.x == 0) {
             fence_proxy_async_smem();
             const int tn = t + S * gridDim.x;
-            s_t[sidx] = tn;
             if (tn < total)
                 issue(tn, sidx);
         }
@@ -558,7 +570,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
             // in slot order, so an exclusive scan gives list ranks in slot
             // order.  Removed slots are only counted here: their ranks come
             // from k_dead_scan and k_holes, so no tile waits on another.
-            const unsigned o = __popc(s_out[par][lane]);
+            const unsigned o = __popc(s_out[nb][lane]);
             unsigned oi = o;
 #pragma unroll
             for (int sft = 1; sft < 32; sft <<= 1) {
@@ -566,24 +578,61 @@ __global__ void __launch_bounds__(TILE_THREADS, 4)
                 if (lane >= sft)
                     oi += b;
             }
-            s_opre[par][lane] = oi - o;
+            s_opre[nb][lane] = oi - o;
             const unsigned out_tile = __shfl_sync(0xffffffffu, oi, 31);
             const unsigned dead_tile =
-                static_cast<unsigned>(warp_sum_u64(__popc(s_dead[par][lane])));
-            const unsigned in_tile = static_cast<unsigned>(warp_sum_u64(__popc(s_in[par][lane])));
+                static_cast<unsigned>(warp_sum_u64(__popc(s_dead[nb][lane])));
+            const unsigned in_tile = static_cast<unsigned>(warp_sum_u64(__popc(s_in[nb][lane])));
             if (lane == 0) {
                 tile_in[t] = static_cast<int32_t>(in_tile);
                 tile_dead[t] = static_cast<int32_t>(dead_tile);
-                s_obase[par] = out_tile ? atomicAdd(&sc->obuf_count, out_tile) : 0u;
+                s_obase[nb] = out_tile ? atomicAdd(&sc->obuf_count, out_tile) : 0u;
             }
         }
+        // The previous tile's list entries (its base was set before this
+        // tile's barrier).
+        if (it > 0)
+            append((it + NB - 1) % NB, prev_gt);
+        prev_gt = gt;
+    }
+    if (it > 0) {
         __syncthreads();
-        for (int k = 0; k < TILE_VEC; ++k) {
-            const int i = k * MOVE_WARPS + warp;
-            const unsigned bo = s_out[par][i];
-            if ((bo >> lane) & 1u)
-                obuf[s_obase[par] + s_opre[par][i] + __popc(bo & lanes_below)] =
-                    static_cast<uint32_t>(gt + k * TILE_THREADS + threadIdx.x);
+        append((it + NB - 1) % NB, prev_gt);
+    }
+}
+
+// k_move_near: the exact MoveParticles body for the slots k_move queued
+// (near the box, or a cell index not certain from its estimate), then their
+// share of the tile counts, the out-of-range list and the drag diagnostics.
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_move_near(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc,
+                TileTables tt, Slots<T> p, uint32_t *__restrict__ key, Cells cells,
+                int32_t *__restrict__ tile_in, int32_t *__restrict__ tile_dead,
+                uint32_t *__restrict__ obuf, const uint32_t *__restrict__ near_list, int ncase,
+                int *err)
+{
+    const uint32_t n = sc->near_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t w = near_list[i];
+        const int t = static_cast<int>(w >> 10);
+        const int e = static_cast<int>(w & 1023u);
+        const int ci = case_of(tt.move0, ncase, t);
+        const CaseDev &c = cases[ci];
+        const int64_t q = static_cast<int64_t>(t - tt.move0[ci]) * TILE + e;
+        double impulse = 0.0;
+        int n_hit = 0;
+        const MoveClass m = move_near_box<T>(c, st[ci].step, q, c.pbase + q, p, key, cells,
+                                             impulse, n_hit, err);
+        if (m.in)
+            atomicAdd(tile_in + t, 1);
+        if (m.dead)
+            atomicAdd(tile_dead + t, 1);
+        if (m.out)
+            obuf[atomicAdd(&sc->obuf_count, 1u)] = static_cast<uint32_t>(c.pbase + q);
+        if (n_hit) {
+            atomicAdd(&st[ci].drag_impulse, impulse);
+            atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(n_hit));
         }
     }
 }
