@@ -9,7 +9,7 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from .abi import Counters, Derived, Params
+from .abi import Counters, Derived, Drag, Params
 
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libdsmc_b200.so"
 
@@ -30,6 +30,7 @@ SIGNATURES = {
     "dsmc_ctx_create": (C.c_int, [_P, _DV, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dsmc_ctx_destroy": (C.c_int, [C.c_void_p]),
     "dsmc_init_cold": (C.c_int, [C.c_void_p]),
+    "dsmc_init_warm": (C.c_int, [C.c_void_p, _D]),
     "dsmc_step": (C.c_int, [C.c_void_p, C.c_int]),
     "dsmc_stage_move": (C.c_int, [C.c_void_p]),
     "dsmc_stage_boundary": (C.c_int, [C.c_void_p]),
@@ -47,7 +48,14 @@ SIGNATURES = {
                                           _I64]),
     "dsmc_upload_particles": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, C.c_int64]),
     "dsmc_get_cell_starts": (C.c_int, [C.c_void_p, C.c_int, _I32]),
+    "dsmc_checkpoint_save": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "dsmc_checkpoint_load": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "dsmc_drag_report": (C.c_int, [_P, _DV, C.POINTER(Counters), C.POINTER(Drag)]),
     "dsmc_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "dsmc_get_launch_config": (C.c_int, [C.c_void_p, _I32, _I32, C.c_int, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_char_p)]),
+    "dsmc_set_launch_config": (C.c_int, [C.c_void_p, _I32, C.c_int]),
+    "dsmc_autotune": (C.c_int, [C.c_void_p, C.c_int]),
     "dsmc_get_kernel_times": (C.c_int, [C.c_void_p, _D, _I64, C.c_int, C.POINTER(C.c_int),
                                         C.POINTER(C.c_char_p)]),
     "dsmc_k_intersect": (C.c_int, [_P, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -77,6 +77,19 @@ class Params(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class Drag(C.Structure):
+    """dsmc_drag of include/dsmc.h: the drag block of RunSimulation."""
+    _fields_ = [
+        ("sampling_time", C.c_double), ("rho_free", C.c_double), ("area_ref", C.c_double),
+        ("mean_force_total", C.c_double), ("cd_total", C.c_double),
+        ("box_collisions", C.c_int64), ("mean_force", C.c_double), ("cd", C.c_double),
+        ("box_collisions_window", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class Derived(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "molecule_mass", "p_free", "u_free", "ux_free", "uy_free", "dx", "dy", "dv",
@@ -94,6 +107,7 @@ class Counters(C.Structure):
         ("drag_collision_count", C.c_int64), ("particle_steps", C.c_int64),
         ("drag_impulse_total", C.c_double), ("time", C.c_double),
         ("sample_time", C.c_double), ("drag_sampling_time", C.c_double),
+        ("drag_collision_count_window", C.c_int64), ("drag_impulse_window", C.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -1,6 +1,7 @@
 """Build recipe of the engine library (sm_100a) and the command-line program.
 
-    python -m dsmc_erlend_b200.build          # builds lib/libdsmc_b200.so and lib/dsmc
+    python -m dsmc_erlend_b200.build          # lib/libdsmc_b200.so, lib/dsmc and
+                                              # lib/libdsmc_surrogate.so
 
 The CUDA sources are compiled for sm_100a only, with --fmad=false (no
 contraction of a*b+c, so FP64 arithmetic is the reference's operation
@@ -26,7 +27,13 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler",
               "-fPIC,-ffp-contract=off,-O2", "-I", str(ROOT / "include")]
 
 LIB_SOURCES = ["dsmc_capi.cu", "host_api.cpp", "surface.cpp"]
-DEPENDS = ["dsmc_device.cuh", "dsmc_scan.cuh", "dsmc_kernels.cuh"]
+DEPENDS = ["dsmc_device.cuh", "dsmc_scan.cuh", "dsmc_kernels.cuh", "dsmc_bulk.cuh"]
+
+# The surrogate's kernels: ordinary FP32 contraction is fine there (a neural
+# network, not the reference's arithmetic).
+SG_LIB = LIB_DIR / "libdsmc_surrogate.so"
+SG_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-I",
+            str(ROOT / "include")]
 
 
 def nvcc() -> str:
@@ -50,6 +57,12 @@ def build(force: bool = False, verbose: bool = False) -> Path:
                                                  ROOT / "include" / "dsmc_philox.h"]
     if force or _stale(LIB, deps):
         cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-shared", "-o", str(LIB), *map(str, srcs)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    sg = CSRC / "surrogate.cu"
+    if sg.exists() and (force or _stale(SG_LIB, [sg, ROOT / "include" / "dsmc_surrogate.h"])):
+        cmd = [nvcc(), *ARCH, *SG_FLAGS, "-shared", "-o", str(SG_LIB), str(sg)]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

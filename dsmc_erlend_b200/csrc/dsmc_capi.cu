@@ -93,8 +93,10 @@ struct dsmc_ctx {
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
 
-    int grid_move = 0, grid_inject = 0, grid_tail = 0, grid_cell_scan = 0, grid_olist = 0;
-    int grid_cell_fix = 0, grid_scatter = 0, grid_collide = 0, grid_select = 0, grid_holes = 0;
+    // CTAs per SM of each kernel's grid (the tunable launch shape), and the
+    // most that fit (occupancy); zero for kernels with a fixed grid.
+    int ctas[KID_COUNT] = {0};
+    int ctas_max[KID_COUNT] = {0};
 
     bool profiling = false;
     std::vector<Timed> timed;
@@ -139,6 +141,8 @@ struct Span {
     }
 };
 
+int grid(const dsmc_ctx *c, int kid) { return std::max(1, c->ctas[kid]) * c->sms; }
+
 template <class T> Slots<T> slots(dsmc_ctx *c, int side)
 {
     Slots<T> s;
@@ -172,7 +176,7 @@ template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
     }
     if (!init_mode) {
         Span sp(c, KID_MOVE);
-        k_move<T><<<c->grid_move, TILE_THREADS, move_smem<T>(), c->stream>>>(
+        k_move<T><<<grid(c, KID_MOVE), TILE_THREADS, move_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
             c->tile_in, c->tile_dead, c->obuf, c->near_list, c->ncase, c->d_err);
     }
@@ -191,7 +195,7 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
 {
     {
         Span sp(c, KID_INJECT);
-        k_inject<T><<<c->grid_inject, TILE_THREADS, 0, c->stream>>>(
+        k_inject<T><<<grid(c, KID_INJECT), TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
             c->itile_dead, c->obuf, c->ncase, c->d_err);
     }
@@ -203,7 +207,7 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_HOLES);
-        k_holes<<<c->grid_holes, TILE_THREADS, 0, c->stream>>>(
+        k_holes<<<grid(c, KID_HOLES), TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, c->key, c->tile_dead, c->tile_dprefix,
             c->itile_dead, c->itile_dprefix, c->hole_pos, c->hole_oc, c->ncase);
     }
@@ -214,7 +218,7 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_TAIL);
-        k_tail<T><<<c->grid_tail, TILE_THREADS, 0, c->stream>>>(
+        k_tail<T><<<grid(c, KID_TAIL), TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
             c->tile_in, lb_chain(c, 2), c->hole_pos, c->hole_oc, c->obuf, c->ncase, c->d_err);
     }
@@ -228,7 +232,7 @@ template <class T> int enqueue_index(dsmc_ctx *c)
     const int side = c->cur;
     {
         Span sp(c, KID_CELL_SCAN);
-        k_cell_scan<<<c->grid_cell_scan, TILE_THREADS, 0, c->stream>>>(
+        k_cell_scan<<<grid(c, KID_CELL_SCAN), TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_scratch, c->tt, c->cells, side ^ 1, lb_chain(c, 3), c->ncase,
             c->d_err);
     }
@@ -239,19 +243,19 @@ template <class T> int enqueue_index(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_OLIST);
-        k_olist<<<c->grid_olist, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch,
+        k_olist<<<grid(c, KID_OLIST), 256, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch,
                                                       c->obuf, c->key, c->cells, c->olist,
                                                       c->d_pbases, c->ncase, c->d_err);
     }
     {
         Span sp(c, KID_CELL_FIX);
-        k_cell_fix<<<c->grid_cell_fix, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->tt,
+        k_cell_fix<<<grid(c, KID_CELL_FIX), 256, 0, c->stream>>>(c->d_cases, c->d_state, c->tt,
                                                              c->cells, side, c->key, c->olist,
                                                              c->total_cells, c->ncase, c->d_err);
     }
     {
         Span sp(c, KID_SCATTER);
-        k_scatter<T><<<c->grid_scatter, TILE_THREADS, scatter_smem<T>(), c->stream>>>(
+        k_scatter<T><<<grid(c, KID_SCATTER), TILE_THREADS, scatter_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->tt, slots<T>(c, side), slots<T>(c, side ^ 1), c->key,
             c->cells, c->tile_prefix, c->ncase, c->d_err);
     }
@@ -265,7 +269,7 @@ template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sampl
     if (do_collide) {
         {
             Span sp(c, KID_COLLIDE_SELECT);
-            k_collide_select<<<c->grid_select, 256, 0, c->stream>>>(
+            k_collide_select<<<grid(c, KID_COLLIDE_SELECT), 256, 0, c->stream>>>(
                 c->d_cases, c->d_state, c->d_scratch, c->tt, c->cells, c->cur, c->coll_list,
                 c->total_cells, c->ncase);
         }
@@ -278,7 +282,7 @@ template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sampl
     }
     if (do_sample) {
         Span sp(c, KID_SAMPLE);
-        k_sample<T><<<c->grid_collide, COLLIDE_CELLS, sample_smem<T>(), c->stream>>>(
+        k_sample<T><<<grid(c, KID_SAMPLE), COLLIDE_CELLS, sample_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, c->ncase,
             c->d_err);
     }
@@ -478,33 +482,41 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 template <class T> int occupancy_grids(dsmc_ctx *c)
 {
     int b = 0;
+    auto occ = [&](int kid, int occupancy) {
+        c->ctas_max[kid] = std::max(1, occupancy);
+        c->ctas[kid] = c->ctas_max[kid];
+    };
     CK(cudaFuncSetAttribute(k_move<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(move_smem<T>())));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_move<T>, TILE_THREADS,
                                                      move_smem<T>()));
-    c->grid_move = std::max(1, b) * c->sms;
+    occ(KID_MOVE, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_inject<T>, TILE_THREADS, 0));
-    c->grid_inject = std::max(1, b) * c->sms;
+    occ(KID_INJECT, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_tail<T>, TILE_THREADS, 0));
-    c->grid_tail = std::max(1, b) * c->sms;
+    occ(KID_TAIL, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cell_scan, TILE_THREADS, 0));
-    c->grid_cell_scan = std::max(1, b) * c->sms;
+    occ(KID_CELL_SCAN, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_holes, TILE_THREADS, 0));
-    c->grid_holes = std::max(1, b) * c->sms;
+    occ(KID_HOLES, b);
     CK(cudaFuncSetAttribute(k_scatter<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(scatter_smem<T>())));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, TILE_THREADS,
                                                      scatter_smem<T>()));
-    c->grid_scatter = std::max(1, b) * c->sms;
+    occ(KID_SCATTER, b);
     CK(cudaFuncSetAttribute(k_sample<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(sample_smem<T>())));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sample<T>, COLLIDE_CELLS,
                                                      sample_smem<T>()));
-    c->grid_collide = std::max(1, b) * c->sms;
+    occ(KID_SAMPLE, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_collide_select, 256, 0));
-    c->grid_select = std::max(1, b) * c->sms;
-    c->grid_olist = 4 * c->sms;
-    c->grid_cell_fix = 8 * c->sms;
+    occ(KID_COLLIDE_SELECT, b);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_olist, 256, 0));
+    occ(KID_OLIST, b);
+    c->ctas[KID_OLIST] = std::min(4, c->ctas_max[KID_OLIST]);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cell_fix, 256, 0));
+    occ(KID_CELL_FIX, b);
+    c->ctas[KID_CELL_FIX] = std::min(8, c->ctas_max[KID_CELL_FIX]);
     return DSMC_OK;
 }
 
@@ -635,6 +647,150 @@ template <class T> int resort_all(dsmc_ctx *c)
     return enqueue_finish(c, 1, 0, 0);
 }
 
+// ---- warm start: particles from the local Maxwellian of a field ------------
+//
+// Cell l of a case (x-major, k * NY + m) with field (n, ux, uy, T) gets
+// floor(n DV / W) + Bernoulli(rest) candidates (draw 0 of the cell's WARM
+// stream, step 0); candidate j sits at X1 + (k + u) DX, Y1 + (m + u') DY
+// (draws 1 + 2j, 2 + 2j) and moves with ux, uy, 0 plus Gaussians of variance
+// k T / m (the cell's WARM stream at step 1, as vrand_MB draws them).  A
+// candidate whose stored position is inside the box is dropped, as
+// RemoveParticlesInsideBox does after the cold fill.
+
+__device__ __forceinline__ int warm_candidates(const CaseDev &c, const double *f, int cl)
+{
+    const double lam = f[0] * c.dv / c.weight;
+    if (!(lam > 0.0) || !(lam < 1e9))
+        return 0;
+    dsmc_stream r;
+    open_stream(r, c, DSMC_RNG_WARM, 0, static_cast<uint32_t>(cl));
+    const double fl = floor(lam);
+    return static_cast<int>(fl) + (uniform(r) < lam - fl ? 1 : 0);
+}
+
+template <class T>
+__device__ __forceinline__ void warm_position(const CaseDev &c, int cl, dsmc_stream &r, T &x, T &y)
+{
+    const int k = cl / c.ny, m = cl % c.ny;
+    x = clamp_into<T>(Store<T>::rn(c.x1 + (k + uniform(r)) * c.dx), c.x1, c.x2);
+    y = clamp_into<T>(Store<T>::rn(c.y1 + (m + uniform(r)) * c.dy), c.y1, c.y2);
+}
+
+// Survivors per cell into cnt[global cell].
+template <class T>
+__global__ void k_warm_count(const CaseDev *cases, int ncase, const double *field, int32_t *cnt)
+{
+    int64_t f0 = 0;
+    for (int ci = 0; ci < ncase; ++ci) {
+        const CaseDev &c = cases[ci];
+        for (int cl = blockIdx.x * blockDim.x + threadIdx.x; cl < c.ncell;
+             cl += gridDim.x * blockDim.x) {
+            const double *f = field + 4 * (f0 + cl);
+            const int nc = warm_candidates(c, f, cl);
+            dsmc_stream r;
+            open_stream(r, c, DSMC_RNG_WARM, 0, static_cast<uint32_t>(cl));
+            uniform(r); // the count draw
+            int keep = 0;
+            for (int j = 0; j < nc; ++j) {
+                T x, y;
+                warm_position<T>(c, cl, r, x, y);
+                keep += inside_box(c, static_cast<double>(x), static_cast<double>(y)) ? 0 : 1;
+            }
+            cnt[c.cbase + cl] = keep;
+        }
+        f0 += c.ncell;
+    }
+}
+
+// Per case (one CTA each): exclusive prefix of the survivors and n_old.
+__global__ void __launch_bounds__(SCAN_THREADS)
+    k_warm_scan(const CaseDev *cases, CaseState *st, const int32_t *cnt, int32_t *off, int *err)
+{
+    constexpr int PER = 8;
+    const CaseDev &c = cases[blockIdx.x];
+    int64_t carry = 0;
+    for (int b = 0; b < c.ncell; b += SCAN_THREADS * PER) {
+        const int i0 = b + threadIdx.x * PER;
+        int v[PER];
+        int sum = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            v[k] = i0 + k < c.ncell ? cnt[c.cbase + i0 + k] : 0;
+            sum += v[k];
+        }
+        int tot;
+        int64_t run = carry + block_exclusive<int, SCAN_THREADS>(sum, tot);
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            if (i0 + k < c.ncell)
+                off[c.cbase + i0 + k] = static_cast<int32_t>(run);
+            run += v[k];
+        }
+        carry += tot;
+    }
+    if (threadIdx.x == 0) {
+        if (carry > c.cap) {
+            report_error(err, DSMC_ERR_CAPACITY);
+            carry = 0;
+        }
+        st[blockIdx.x].n_old = carry;
+    }
+}
+
+// Writes the survivors of every cell from its offset, in cell order.
+template <class T>
+__global__ void k_warm_fill(const CaseDev *cases, const CaseState *st, int ncase,
+                            const double *field, const int32_t *off, Slots<T> p)
+{
+    int64_t f0 = 0;
+    for (int ci = 0; ci < ncase; ++ci) {
+        const CaseDev &c = cases[ci];
+        const bool fits = st[ci].n_old > 0;
+        for (int cl = blockIdx.x * blockDim.x + threadIdx.x; fits && cl < c.ncell;
+             cl += gridDim.x * blockDim.x) {
+            const double *f = field + 4 * (f0 + cl);
+            const int nc = warm_candidates(c, f, cl);
+            if (nc == 0)
+                continue;
+            const double ux = f[1], uy = f[2];
+            const double var = K_BOLTZMANN * fmax(f[3], 0.0) / c.mass;
+            dsmc_stream r, rv;
+            open_stream(r, c, DSMC_RNG_WARM, 0, static_cast<uint32_t>(cl));
+            open_stream(rv, c, DSMC_RNG_WARM, 1, static_cast<uint32_t>(cl));
+            uniform(r);
+            int64_t g = c.pbase + off[c.cbase + cl];
+            for (int j = 0; j < nc; ++j) {
+                T x, y;
+                warm_position<T>(c, cl, r, x, y);
+                const double vx = frand_gaussian(rv, ux, var);
+                const double vy = frand_gaussian(rv, uy, var);
+                const double vz = frand_gaussian(rv, 0.0, var);
+                if (inside_box(c, static_cast<double>(x), static_cast<double>(y)))
+                    continue;
+                p.x[g] = x;
+                p.y[g] = y;
+                p.vx[g] = Store<T>::rn(vx);
+                p.vy[g] = Store<T>::rn(vy);
+                p.vz[g] = Store<T>::rn(vz);
+                ++g;
+            }
+        }
+        f0 += c.ncell;
+    }
+}
+
+template <class T> int warm_fill(dsmc_ctx *c, const double *dfield, int32_t *cnt, int32_t *off)
+{
+    const int grid = 4 * c->sms;
+    k_warm_count<T><<<grid, 256, 0, c->stream>>>(c->d_cases, c->ncase, dfield, cnt);
+    k_warm_scan<<<c->ncase, SCAN_THREADS, 0, c->stream>>>(c->d_cases, c->d_state, cnt, off,
+                                                           c->d_err);
+    k_warm_fill<T><<<grid, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->ncase, dfield, off,
+                                                slots<T>(c, c->cur));
+    CK(cudaGetLastError());
+    return resort_all<T>(c);
+}
+
 __global__ void k_fields_out(const Cells cells, int cbase, int ncell, double *out)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncell; i += gridDim.x * blockDim.x) {
@@ -742,6 +898,16 @@ int resolve_timings(dsmc_ctx *c)
     }
     c->timed.clear();
     return DSMC_OK;
+}
+
+
+void drop_graphs(dsmc_ctx *c)
+{
+    for (auto &g : c->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
 }
 
 } // namespace
@@ -932,6 +1098,7 @@ int dsmc_init_cold(dsmc_ctx *c)
     if (c == nullptr)
         return DSMC_ERR_ARGUMENT;
     CK(cudaMemsetAsync(c->d_state, 0, sizeof(CaseState) * c->ncase, c->stream));
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream)); // a new run starts clean
     CK(cudaMemsetAsync(c->cells.acc, 0, sizeof(double) * ACC_COUNT * c->total_cells, c->stream));
     CK(cudaMemsetAsync(c->cells.start[c->cur], 0, sizeof(int32_t) * c->total_cells, c->stream));
     // Every particle of the cold start is out of range (no previous sort).
@@ -951,6 +1118,36 @@ int dsmc_init_cold(dsmc_ctx *c)
     c->initialized = true;
     c->stage = 0;
     return DSMC_OK;
+}
+
+int dsmc_init_warm(dsmc_ctx *c, const double *host_field)
+{
+    if (c == nullptr || host_field == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    int64_t cells = 0;
+    for (const CaseDev &cd : c->hcases)
+        cells += cd.ncell;
+    CK(cudaMemsetAsync(c->d_state, 0, sizeof(CaseState) * c->ncase, c->stream));
+    CK(cudaMemsetAsync(c->cells.acc, 0, sizeof(double) * ACC_COUNT * c->total_cells, c->stream));
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    double *dfield = nullptr;
+    int32_t *tmp = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&dfield), sizeof(double) * 4 * cells, c->stream));
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(int32_t) * 2 * c->total_cells,
+                       c->stream));
+    CK(cudaMemcpyAsync(dfield, host_field, sizeof(double) * 4 * cells, cudaMemcpyHostToDevice,
+                       c->stream));
+    const int s = c->precision == DSMC_FP32 ? warm_fill<float>(c, dfield, tmp, tmp + c->total_cells)
+                                            : warm_fill<double>(c, dfield, tmp,
+                                                                tmp + c->total_cells);
+    CK(cudaFreeAsync(dfield, c->stream));
+    CK(cudaFreeAsync(tmp, c->stream));
+    if (s)
+        return s;
+    CK(cudaStreamSynchronize(c->stream));
+    c->initialized = true;
+    c->stage = 0;
+    return device_error(c);
 }
 
 int dsmc_step(dsmc_ctx *c, int n_steps)
@@ -1081,6 +1278,8 @@ int dsmc_get_counters(dsmc_ctx *c, int i, dsmc_counters *out)
     out->time = x.time;
     out->sample_time = x.sample_time;
     out->drag_sampling_time = x.drag_time;
+    out->drag_collision_count_window = static_cast<int64_t>(x.drag_count_window);
+    out->drag_impulse_window = x.drag_impulse_window;
     return DSMC_OK;
 }
 
@@ -1144,6 +1343,33 @@ int fields_noalloc_address(int device, double **out)
     *out = g_fields_noalloc_addr[device];
     return DSMC_OK;
 }
+} // namespace
+
+// ---- checkpoint ----------------------------------------------------------------
+
+namespace {
+
+constexpr char kCheckpointMagic[8] = {'D', 'S', 'M', 'C', 'C', 'K', 'P', '1'};
+
+// The run counters of one case, as stored in a checkpoint.
+struct CheckpointCase {
+    int64_t n, step, sample_step, nc_last, nc_total, particle_steps;
+    uint64_t drag_count, drag_count_window;
+    double drag_impulse, drag_impulse_window, time, sample_time, drag_time;
+};
+
+struct File {
+    FILE *f = nullptr;
+    ~File()
+    {
+        if (f)
+            std::fclose(f);
+    }
+};
+
+bool put(FILE *f, const void *p, size_t n) { return std::fwrite(p, 1, n, f) == n; }
+bool get(FILE *f, void *p, size_t n) { return std::fread(p, 1, n, f) == n; }
+
 } // namespace
 
 extern "C" {
@@ -1290,6 +1516,117 @@ int dsmc_upload_particles(dsmc_ctx *c, int i, const double *x, const double *y, 
     return device_error(c);
 }
 
+
+int dsmc_checkpoint_save(dsmc_ctx *c, const char *path)
+{
+    if (c == nullptr || path == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 0 || !c->initialized)
+        return DSMC_ERR_STATE;
+    std::vector<CaseState> st;
+    int s = read_state(c, st);
+    if (s)
+        return s;
+    File out;
+    out.f = std::fopen(path, "wb");
+    if (out.f == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    const int32_t head[4] = {1, c->ncase, c->precision, static_cast<int32_t>(sizeof(dsmc_params))};
+    bool ok = put(out.f, kCheckpointMagic, 8) && put(out.f, head, sizeof(head));
+    for (int i = 0; i < c->ncase && ok; ++i) {
+        const CaseDev &cd = c->hcases[i];
+        const CaseState &x = st[i];
+        const CheckpointCase k{x.n_old,        x.step,         x.sample_step,      x.nc_last,
+                               x.nc_total,     x.particle_steps, x.drag_count,      x.drag_count_window,
+                               x.drag_impulse, x.drag_impulse_window, x.time,       x.sample_time,
+                               x.drag_time};
+        ok = put(out.f, &c->params[i], sizeof(dsmc_params)) && put(out.f, &k, sizeof(k));
+        std::vector<double> v(5 * static_cast<size_t>(std::max<int64_t>(k.n, 1)));
+        int64_t n = 0;
+        s = dsmc_download_particles(c, i, v.data(), v.data() + k.n, v.data() + 2 * k.n,
+                                    v.data() + 3 * k.n, v.data() + 4 * k.n, k.n, &n);
+        if (s)
+            return s;
+        ok = ok && put(out.f, v.data(), sizeof(double) * 5 * k.n);
+        std::vector<double> acc(static_cast<size_t>(ACC_COUNT) * cd.ncell);
+        for (int m = 0; m < ACC_COUNT; ++m)
+            CK(cudaMemcpyAsync(acc.data() + static_cast<size_t>(m) * cd.ncell,
+                               c->cells.acc + static_cast<size_t>(m) * c->cells.acc_stride + cd.cbase,
+                               sizeof(double) * cd.ncell, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        ok = ok && put(out.f, acc.data(), sizeof(double) * acc.size());
+    }
+    return ok ? DSMC_OK : DSMC_ERR_ARGUMENT;
+}
+
+int dsmc_checkpoint_load(dsmc_ctx *c, const char *path)
+{
+    if (c == nullptr || path == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 0)
+        return DSMC_ERR_STATE;
+    File in;
+    in.f = std::fopen(path, "rb");
+    if (in.f == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    char magic[8];
+    int32_t head[4];
+    if (!get(in.f, magic, 8) || std::memcmp(magic, kCheckpointMagic, 8) != 0 ||
+        !get(in.f, head, sizeof(head)) || head[0] != 1 || head[1] != c->ncase ||
+        head[2] != c->precision || head[3] != static_cast<int32_t>(sizeof(dsmc_params)))
+        return DSMC_ERR_ARGUMENT;
+    std::vector<CheckpointCase> ks(c->ncase);
+    for (int i = 0; i < c->ncase; ++i) {
+        const CaseDev &cd = c->hcases[i];
+        dsmc_params p;
+        CheckpointCase &k = ks[i];
+        if (!get(in.f, &p, sizeof(p)))
+            return DSMC_ERR_ARGUMENT;
+        p.n_step = c->params[i].n_step; // the run length may grow on a restart
+        if (std::memcmp(&p, &c->params[i], sizeof(p)) != 0 || !get(in.f, &k, sizeof(k)) ||
+            k.n < 0 || k.n > cd.cap)
+            return DSMC_ERR_ARGUMENT;
+        std::vector<double> v(5 * static_cast<size_t>(std::max<int64_t>(k.n, 1)));
+        std::vector<double> acc(static_cast<size_t>(ACC_COUNT) * cd.ncell);
+        if (!get(in.f, v.data(), sizeof(double) * 5 * k.n) ||
+            !get(in.f, acc.data(), sizeof(double) * acc.size()))
+            return DSMC_ERR_ARGUMENT;
+        int s = dsmc_upload_particles(c, i, v.data(), v.data() + k.n, v.data() + 2 * k.n,
+                                      v.data() + 3 * k.n, v.data() + 4 * k.n, k.n);
+        if (s)
+            return s;
+        for (int m = 0; m < ACC_COUNT; ++m)
+            CK(cudaMemcpyAsync(c->cells.acc + static_cast<size_t>(m) * c->cells.acc_stride + cd.cbase,
+                               acc.data() + static_cast<size_t>(m) * cd.ncell,
+                               sizeof(double) * cd.ncell, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    std::vector<CaseState> st;
+    int s = read_state(c, st);
+    if (s)
+        return s;
+    for (int i = 0; i < c->ncase; ++i) {
+        const CheckpointCase &k = ks[i];
+        CaseState &x = st[i];
+        x.step = k.step;
+        x.sample_step = k.sample_step;
+        x.nc_last = k.nc_last;
+        x.nc_total = k.nc_total;
+        x.particle_steps = k.particle_steps;
+        x.drag_count = k.drag_count;
+        x.drag_count_window = k.drag_count_window;
+        x.drag_impulse = k.drag_impulse;
+        x.drag_impulse_window = k.drag_impulse_window;
+        x.time = k.time;
+        x.sample_time = k.sample_time;
+        x.drag_time = k.drag_time;
+    }
+    CK(cudaMemcpyAsync(c->d_state, st.data(), sizeof(CaseState) * c->ncase,
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DSMC_OK;
+}
+
 int dsmc_get_cell_starts(dsmc_ctx *c, int i, int32_t *host_out)
 {
     if (c == nullptr || host_out == nullptr || i < 0 || i >= c->ncase)
@@ -1334,6 +1671,81 @@ int dsmc_get_kernel_times(dsmc_ctx *c, double *ms_out, int64_t *launches_out, in
             names_out[k] = kKernelNames[k];
     }
     return DSMC_OK;
+}
+
+int dsmc_get_launch_config(dsmc_ctx *c, int32_t *ctas_per_sm, int32_t *max_ctas_per_sm,
+                           int max_kernels, int *n_kernels, const char **names_out)
+{
+    if (c == nullptr || n_kernels == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    *n_kernels = KID_COUNT;
+    for (int k = 0; k < KID_COUNT && k < max_kernels; ++k) {
+        if (ctas_per_sm)
+            ctas_per_sm[k] = c->ctas[k];
+        if (max_ctas_per_sm)
+            max_ctas_per_sm[k] = c->ctas_max[k];
+        if (names_out)
+            names_out[k] = kKernelNames[k];
+    }
+    return DSMC_OK;
+}
+
+int dsmc_set_launch_config(dsmc_ctx *c, const int32_t *ctas_per_sm, int n)
+{
+    if (c == nullptr || ctas_per_sm == nullptr || n < 0 || n > KID_COUNT)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 0)
+        return DSMC_ERR_STATE;
+    for (int k = 0; k < n; ++k)
+        if (c->ctas_max[k] > 0 && ctas_per_sm[k] > 0)
+            c->ctas[k] = std::min(ctas_per_sm[k], c->ctas_max[k]);
+    drop_graphs(c); // rebuilt with the new shapes at the next dsmc_step
+    return DSMC_OK;
+}
+
+int dsmc_autotune(dsmc_ctx *c, int steps_per_trial)
+{
+    if (c == nullptr || steps_per_trial < 1)
+        return DSMC_ERR_ARGUMENT;
+    if (!c->initialized || c->stage != 0)
+        return DSMC_ERR_STATE;
+    const bool was_profiling = c->profiling;
+    int s = dsmc_set_profiling(c, 1);
+    if (s)
+        return s;
+    for (int k = 0; k < KID_COUNT; ++k) {
+        if (c->ctas_max[k] <= 0)
+            continue;
+        const int mx = c->ctas_max[k];
+        std::vector<int> cand;
+        for (int v : {mx, mx / 2, mx / 4, 1, 2, 4, 8, 16})
+            if (v >= 1 && v <= mx && std::find(cand.begin(), cand.end(), v) == cand.end())
+                cand.push_back(v);
+        int best = c->ctas[k];
+        double best_ms = 1e300;
+        for (int v : cand) {
+            c->ctas[k] = v;
+            if ((s = resolve_timings(c)))
+                return s;
+            c->kernel_ms[k] = 0.0;
+            c->kernel_launches[k] = 0;
+            for (int i = 0; i < steps_per_trial; ++i)
+                if ((s = dispatch_step(c)))
+                    return s;
+            if ((s = resolve_timings(c)))
+                return s;
+            const double ms = c->kernel_launches[k] ? c->kernel_ms[k] / c->kernel_launches[k] : 0.0;
+            if (ms < best_ms * 0.98) { // keep the larger grid unless clearly slower
+                best_ms = ms;
+                best = v;
+            }
+        }
+        c->ctas[k] = best;
+    }
+    drop_graphs(c);
+    if ((s = dsmc_set_profiling(c, was_profiling ? 1 : 0)))
+        return s;
+    return device_error(c);
 }
 
 int dsmc_k_intersect(const dsmc_params *p, int64_t n, const double *x, const double *y,

@@ -76,6 +76,8 @@ struct CaseState {
     int64_t particle_steps;
     unsigned long long drag_count;
     double drag_impulse;
+    unsigned long long drag_count_window; // impacts of moves after FirstSamplingStep
+    double drag_impulse_window;
     double time, sample_time, drag_time;
     int32_t sampling_mode;
     int32_t inj_count[5], inj_c0[5], inj_off[6];

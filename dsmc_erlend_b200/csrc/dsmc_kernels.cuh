@@ -633,6 +633,10 @@ __global__ void __launch_bounds__(TILE_THREADS)
         if (n_hit) {
             atomicAdd(&st[ci].drag_impulse, impulse);
             atomicAdd(&st[ci].drag_count, static_cast<unsigned long long>(n_hit));
+            if (st[ci].step > c.first_sampling_step) { // the DragSamplingTime window
+                atomicAdd(&st[ci].drag_impulse_window, impulse);
+                atomicAdd(&st[ci].drag_count_window, static_cast<unsigned long long>(n_hit));
+            }
         }
     }
 }

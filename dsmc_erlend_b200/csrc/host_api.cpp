@@ -5,6 +5,7 @@
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <filesystem>
 #include <fstream>
 #include <iomanip>
@@ -135,6 +136,30 @@ const char *dsmc_status_string(int status)
     case DSMC_ERR_TOO_LARGE: return "input larger than the fixed maximum of this entry point";
     }
     return "unknown status";
+}
+
+// The drag block of RunSimulation (src/Simulation.cpp:210-237, commented out
+// in the reference): mean force over DragSamplingTime and the drag
+// coefficient on the box's frontal area BoxHeight * DZ.
+int dsmc_drag_report(const dsmc_params *p, const dsmc_derived *d, const dsmc_counters *c,
+                     dsmc_drag *out)
+{
+    if (p == nullptr || d == nullptr || c == nullptr || out == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    out->sampling_time = c->drag_sampling_time;
+    out->rho_free = p->n_free * d->molecule_mass;
+    out->area_ref = p->box_height * p->dz;
+    out->box_collisions = c->drag_collision_count;
+    out->box_collisions_window = c->drag_collision_count_window;
+    if (!(c->drag_sampling_time > 0.0))
+        return DSMC_ERR_STATE;
+    const double q = 0.5 * out->rho_free * d->u_free * d->u_free * out->area_ref;
+    out->mean_force_total = c->drag_impulse_total / c->drag_sampling_time;
+    out->cd_total = out->mean_force_total / q;
+    out->mean_force = c->drag_impulse_window / c->drag_sampling_time;
+    out->cd = out->mean_force / q;
+    return DSMC_OK;
 }
 
 // Printing(), src/Sampling.cpp:36-268: the Tecplot-style field and its JSON

@@ -450,6 +450,16 @@ bool parse_number(const char *s, double &out)
 
 // The reference's flags (--angle-of-attack/--aoa, -h/--help, exit codes 0/2)
 // plus run-time settings it fixes at compile time; defaults are its values.
+// Run controls beyond the reference's flags.
+struct RunControls {
+    int print_period = 0;      // intermediate fields (the reference's commented PrintPeriod)
+    int checkpoint_period = 0; // checkpoints during the run
+    std::string checkpoint;    // checkpoint file
+    std::string restart;       // resume from this checkpoint
+    bool drag = false;         // print the drag block at the end
+};
+RunControls g_run;
+
 ArgumentResult ParseArguments(int argc, char **argv)
 {
     for (int i = 1; i < argc; ++i) {
@@ -465,7 +475,14 @@ ArgumentResult ParseArguments(int argc, char **argv)
                 << "  --nx N, --ny N, --npc N       grid and particles per cell\n"
                 << "  --dt S, --steps N, --first-sampling-step N\n"
                 << "  --box-width W, --box-height H, --mach M, --density N\n"
-                << "  --seed N, --precision fp64|fp32, --results DIR\n";
+                << "  --seed N, --precision fp64|fp32, --results DIR\n"
+                << "  --print-period N      also write the field every N steps after\n"
+                << "                        FirstSamplingStep, into DIR/step_<Step>\n"
+                << "  --checkpoint FILE     write a checkpoint at the end (and every\n"
+                << "  --checkpoint-period N   N steps)\n"
+                << "  --restart FILE        resume from a checkpoint instead of\n"
+                << "                        InitialConditions\n"
+                << "  --drag                print the drag block (mean force, Cd)\n";
             return ArgumentResult::Help;
         }
         const bool known =
@@ -474,7 +491,12 @@ ArgumentResult ParseArguments(int argc, char **argv)
             option == "--npc" || option == "--dt" || option == "--steps" ||
             option == "--first-sampling-step" || option == "--seed" || option == "--precision" ||
             option == "--results" || option == "--box-width" || option == "--box-height" ||
-            option == "--mach" || option == "--density";
+            option == "--mach" || option == "--density" || option == "--print-period" ||
+            option == "--checkpoint" || option == "--checkpoint-period" || option == "--restart";
+        if (option == "--drag") {
+            g_run.drag = true;
+            continue;
+        }
         if (!known) {
             std::cerr << "Unknown option: " << option << ". Use --help.\n";
             return ArgumentResult::Error;
@@ -514,6 +536,10 @@ ArgumentResult ParseArguments(int argc, char **argv)
             }
         } else if (option == "--results") {
             dsmc::ResultsDirectory = value;
+        } else if (option == "--checkpoint") {
+            g_run.checkpoint = value;
+        } else if (option == "--restart") {
+            g_run.restart = value;
         } else {
             if (!parse_number(argv[i], x)) {
                 std::cerr << "Invalid value for " << option << ": " << value << '\n';
@@ -534,6 +560,14 @@ ArgumentResult ParseArguments(int argc, char **argv)
             else if (option == "--box-height") BoxHeight = x;
             else if (option == "--mach") MaFree = x;
             else if (option == "--density") NFree = x;
+            else if (option == "--print-period" || option == "--checkpoint-period") {
+                if (x < 1.0 || x != std::floor(x)) {
+                    std::cerr << "Invalid value for " << option << ": " << value << '\n';
+                    return ArgumentResult::Error;
+                }
+                (option == "--print-period" ? g_run.print_period : g_run.checkpoint_period) =
+                    static_cast<int>(x);
+            }
         }
     }
     return ArgumentResult::Run;
@@ -548,12 +582,22 @@ int RunSimulation(int argc, char **argv)
     try {
         Setup();
         std::cout << "Setup\n";
-        InitialConditions();
-        std::cout << "Total particles across all ranks = " << NP << "\nInitialConditions\n";
+        if (!g_run.restart.empty()) {
+            check(dsmc_checkpoint_load(ctx(), g_run.restart.c_str()), "restart");
+            pull_counters();
+            std::cout << "Restarted from " << g_run.restart << " at step " << Step << '\n';
+        } else {
+            InitialConditions();
+            std::cout << "Total particles across all ranks = " << NP << "\nInitialConditions\n";
+        }
+        const std::string results = dsmc::ResultsDirectory;
         // The loop of src/Simulation.cpp:138-199 as CUDA graphs, with the
         // reference's progress line every 100 steps.
         while (Step < NStep) {
-            const int chunk = std::min(100 - Step % 100, NStep - Step);
+            int chunk = std::min(100 - Step % 100, NStep - Step);
+            for (int period : {g_run.print_period, g_run.checkpoint_period})
+                if (period > 0)
+                    chunk = std::min(chunk, period - Step % period);
             check(dsmc_step(ctx(), chunk), "time step");
             const int s = dsmc_synchronize(ctx());
             if (s != DSMC_OK)
@@ -565,8 +609,37 @@ int RunSimulation(int argc, char **argv)
                 std::cout << "Time step " << Step << ", Number of particles " << NP
                           << ", Number of collisions " << c.collisions_last_step << '\n';
             }
+            // The reference's commented-out intermediate output
+            // (Simulation.cpp:198), one directory per output step.
+            if (g_run.print_period > 0 && Step > FirstSamplingStep &&
+                Step % g_run.print_period == 0 && Step < NStep) {
+                dsmc::ResultsDirectory = results + "/step_" + std::to_string(Step);
+                Printing(GatherGlobalField());
+                dsmc::ResultsDirectory = results;
+            }
+            if (g_run.checkpoint_period > 0 && !g_run.checkpoint.empty() &&
+                Step % g_run.checkpoint_period == 0 && Step < NStep)
+                check(dsmc_checkpoint_save(ctx(), g_run.checkpoint.c_str()), "checkpoint");
         }
         Printing(GatherGlobalField());
+        if (!g_run.checkpoint.empty())
+            check(dsmc_checkpoint_save(ctx(), g_run.checkpoint.c_str()), "checkpoint");
+        if (g_run.drag) {
+            // Simulation.cpp:210-237 (commented out in the reference).
+            dsmc_counters c;
+            dsmc_drag dr;
+            check(dsmc_get_counters(ctx(), 0, &c), "dsmc_get_counters");
+            if (dsmc_drag_report(&g_params, &g_derived, &c, &dr) == DSMC_OK) {
+                std::cout << "\n====================================\n"
+                          << "Box collisions = " << dr.box_collisions_window << "\n"
+                          << "Sampling time = " << dr.sampling_time << " s\n"
+                          << "Mean drag force = " << dr.mean_force << " N\n"
+                          << "Drag coefficient Cd = " << dr.cd << "\n"
+                          << "====================================\n";
+            } else {
+                std::cout << "No drag sampling time yet (Step <= FirstSamplingStep)\n";
+            }
+        }
     } catch (const dsmc::Error &e) {
         std::cerr << "ERROR: " << e.what() << '\n';
         return e.code();

@@ -20,9 +20,18 @@ import numpy as np
 
 from . import abi
 from ._lib import check, load
-from .abi import Counters, Derived, Params
+from .abi import Counters, Derived, Drag, Params
 
 _D = C.POINTER(C.c_double)
+
+
+def drag_report(p: Params, d: Derived, counters: dict) -> dict:
+    """dsmc_drag_report over a counters dict (as Engine.counters returns)."""
+    c = Counters(**counters)
+    out = Drag()
+    check(load().dsmc_drag_report(C.byref(p), C.byref(d), C.byref(c), C.byref(out)),
+          "dsmc_drag_report")
+    return out.as_dict()
 
 
 def setup(p: Params) -> Derived:
@@ -85,6 +94,15 @@ class Engine:
         check(self._lib.dsmc_init_cold(self._h), "dsmc_init_cold")
 
     init_cold = InitialConditions
+
+    def init_warm(self, field: np.ndarray):
+        """Fills every case from the local Maxwellian of `field`: (n, ux, uy,
+        T) per cell, cells x-major, cases one after another (dsmc_init_warm)."""
+        f = np.ascontiguousarray(field, dtype=np.float64)
+        need = sum(p.nx * p.ny for p in self.params)
+        if f.shape != (need, 4):
+            raise ValueError(f"field must have shape ({need}, 4), not {f.shape}")
+        check(self._lib.dsmc_init_warm(self._h, f.ctypes.data_as(_D)), "dsmc_init_warm")
 
     def step(self, n: int = 1):
         check(self._lib.dsmc_step(self._h, int(n)), "dsmc_step")
@@ -160,6 +178,52 @@ class Engine:
     def Printing(self, results_dir: str, case: int = 0):
         write_field(self.params[case], self.derived[case], self.counters(case)["sample_step"],
                     self.GatherGlobalField(case), results_dir)
+
+    def drag_report(self, case: int = 0) -> dict:
+        """Mean drag force and Cd (Simulation.cpp:210-237): over all steps as
+        the reference's expression has it, and over the sampling window."""
+        return drag_report(self.params[case], self.derived[case], self.counters(case))
+
+    def checkpoint_save(self, path: str):
+        """Counters, particles and moments of every case, between steps."""
+        check(self._lib.dsmc_checkpoint_save(self._h, str(path).encode()),
+              "dsmc_checkpoint_save")
+
+    def checkpoint_load(self, path: str):
+        """Resumes a checkpoint of a context with the same cases."""
+        check(self._lib.dsmc_checkpoint_load(self._h, str(path).encode()),
+              "dsmc_checkpoint_load")
+
+    # -- launch shapes ----------------------------------------------------------
+    def launch_config(self) -> dict:
+        """{kernel: (CTAs per SM, maximum)} of the tunable step kernels."""
+        cur = (C.c_int32 * 32)()
+        mx = (C.c_int32 * 32)()
+        names = (C.c_char_p * 32)()
+        n = C.c_int()
+        check(self._lib.dsmc_get_launch_config(self._h, cur, mx, 32, C.byref(n), names),
+              "dsmc_get_launch_config")
+        return {names[i].decode(): (cur[i], mx[i]) for i in range(n.value) if mx[i] > 0}
+
+    def set_launch_config(self, shapes: dict):
+        """Sets CTAs per SM by kernel name (others kept)."""
+        order = list(self._all_kernel_names())
+        arr = (C.c_int32 * len(order))(*[int(shapes.get(k, 0)) for k in order])
+        check(self._lib.dsmc_set_launch_config(self._h, arr, len(order)),
+              "dsmc_set_launch_config")
+
+    def autotune(self, steps_per_trial: int = 3) -> dict:
+        """Times the candidate shapes of each tunable kernel on real steps of
+        this run (it advances) and keeps the fastest; returns the shapes."""
+        check(self._lib.dsmc_autotune(self._h, int(steps_per_trial)), "dsmc_autotune")
+        return self.launch_config()
+
+    def _all_kernel_names(self):
+        names = (C.c_char_p * 32)()
+        n = C.c_int()
+        check(self._lib.dsmc_get_launch_config(self._h, None, None, 32, C.byref(n), names),
+              "dsmc_get_launch_config")
+        return [names[i].decode() for i in range(n.value)]
 
     # -- profiling ------------------------------------------------------------
     def set_profiling(self, on: bool):

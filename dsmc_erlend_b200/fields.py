@@ -1,0 +1,103 @@
+"""Macroscopic fields from the sampled moments, and field distances.
+
+The moments are the reference's CELL layout (include/Cell.h:4-10, 17 doubles
+per cell).  The conversion follows Printing (src/Sampling.cpp:36-268):
+n = W CountNP / SampleStep / DV, u = CountV / CountNP, T = m (<vv> - u u) / k
+with T the mean of its three diagonal components.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+K_BOLTZMANN = 1.380662e-23
+
+
+def macroscopic(cells: np.ndarray, weight: float, dv: float, molecule_mass: float,
+                sample_step: int) -> dict:
+    """n, ux, uy, T and the sample count of every cell from summed moments."""
+    cells = np.asarray(cells, dtype=np.float64)
+    npc = cells[:, 0]
+    n = weight * npc / max(sample_step, 1) / dv
+    with np.errstate(invalid="ignore", divide="ignore"):
+        u = cells[:, 1:4] / npc[:, None]
+        vv = cells[:, [4, 8, 12]] / npc[:, None]
+        t = molecule_mass * (vv - u * u) / K_BOLTZMANN
+    return {"n": n, "ux": u[:, 0], "uy": u[:, 1], "t": t.mean(axis=1), "count": npc}
+
+
+def wall_cells(p) -> np.ndarray:
+    """Cells whose centre lies within one cell of the box (x-major)."""
+    dx = (p.x2 - p.x1) / p.nx
+    dy = (p.y2 - p.y1) / p.ny
+    k, l = np.meshgrid(np.arange(p.nx), np.arange(p.ny), indexing="ij")
+    xc = p.x1 + (k.ravel() + 0.5) * dx
+    yc = p.y1 + (l.ravel() + 0.5) * dy
+    return (np.abs(xc - p.box_x) < p.box_width / 2 + dx) & \
+           (np.abs(yc - p.box_y) < p.box_height / 2 + dy)
+
+
+def weighted_errors(a: dict, b: dict, p, u_free: float) -> dict:
+    """Relative L2 errors of field a against field b outside the wall cells,
+    each cell weighted by b's sample count: the statistically natural norm
+    for a short sampling window, where a cell's noise falls as one over the
+    root of its samples.  Velocities are normalised by the freestream speed,
+    n and T by their own weighted norms."""
+    ok = ~wall_cells(p) & (a["count"] > 0) & (b["count"] > 0)
+    for k in ("ux", "uy", "t"):
+        ok &= np.isfinite(a[k]) & np.isfinite(b[k])
+    w = np.where(ok, b["count"], 0.0)
+    out = {}
+    for k in ("n", "t"):
+        d = np.nan_to_num(a[k] - b[k])
+        out[k] = np.sqrt((w * d * d).sum() / max((w * np.nan_to_num(b[k]) ** 2).sum(), 1e-300))
+    for k in ("ux", "uy"):
+        d = np.nan_to_num(a[k] - b[k])
+        out[k] = np.sqrt((w * d * d).sum() / max(w.sum(), 1e-300)) / u_free
+    return out
+
+
+def field_errors(a: dict, b: dict, p, u_free: float) -> dict:
+    """Relative L2 errors of field a against field b outside the wall cells.
+
+    n is compared over every such cell both fields sampled.  Velocity and
+    temperature are moments per sampled particle, undefined where almost
+    nothing is sampled (the near-vacuum wake behind the box, where even
+    independent runs of the reference differ by O(100%)); ux, uy and T leave
+    out cells whose sample count in b is below 5% of b's median.  Velocities
+    are normalised by the freestream speed, n by ||n_b||, T by ||T_b||."""
+    sampled = ~wall_cells(p) & (a["count"] > 0) & (b["count"] > 0)
+    dense = sampled & (b["count"] >= 0.05 * np.median(b["count"][b["count"] > 0]))
+    out = {"n": np.linalg.norm(a["n"][sampled] - b["n"][sampled]) /
+                np.linalg.norm(b["n"][sampled]),
+           "t": np.linalg.norm(a["t"][dense] - b["t"][dense]) / np.linalg.norm(b["t"][dense])}
+    for key in ("ux", "uy"):
+        out[key] = np.linalg.norm(a[key][dense] - b[key][dense]) / \
+            (u_free * np.sqrt(max(int(dense.sum()), 1)))
+    return out
+
+
+def warm_input(f: dict) -> np.ndarray:
+    """The (n, ux, uy, T) array per cell that dsmc_init_warm takes; cells
+    without samples are left empty (n = 0)."""
+    ok = np.isfinite(f["ux"]) & np.isfinite(f["uy"]) & np.isfinite(f["t"]) & (f["count"] > 0)
+    out = np.zeros((len(f["n"]), 4), dtype=np.float64)
+    out[ok, 0] = f["n"][ok]
+    out[ok, 1] = f["ux"][ok]
+    out[ok, 2] = f["uy"][ok]
+    out[ok, 3] = np.maximum(f["t"][ok], 0.0)
+    return out
+
+
+def coarsen(f: dict, nx: int, ny: int, b: int) -> dict:
+    """Field on blocks of b x b cells (nx, ny multiples of b): n averaged,
+    velocity and temperature weighted by the sample counts."""
+    def blocks(a):
+        return a.reshape(nx // b, b, ny // b, b)
+
+    cnt = blocks(np.nan_to_num(f["count"])).sum(axis=(1, 3))
+    out = {"n": blocks(f["n"]).mean(axis=(1, 3)).ravel(), "count": cnt.ravel()}
+    w = blocks(np.nan_to_num(f["count"]))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        for k in ("ux", "uy", "t"):
+            out[k] = ((blocks(np.nan_to_num(f[k])) * w).sum(axis=(1, 3)) / cnt).ravel()
+    return out

@@ -1,0 +1,134 @@
+"""Surrogate pipeline: DSMC ensemble data on the GPU -> surrogate training ->
+hold-out error -> warm versus cold time to a 2% field on the warm-start case.
+
+    python -m dsmc_erlend_b200.sgpipeline --cases 1024 --epochs 40 --out DIR
+
+Writes DIR/report.json (data, training, hold-out errors, time to field) and
+DIR/surrogate_weights.npz.  Every DSMC run and every network step runs on the
+GPU through this package's kernels.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import setup
+from .abi import warm_start_case
+from .sgdata import case_input, generate, prediction_field, surrogate_cases
+from .surrogate import Surrogate, predict, relative_errors, train
+from .timetofield import coarse_prediction, reference_field, time_to_field
+
+
+def time_to_field_study(p, predictors: dict, ref_replicas: int, transient: int,
+                        ref_steps: int, cold_starts, warm_starts, check_every: int) -> dict:
+    """Best cold and best warm time to a 2% field over the given sampling
+    starts, against a reference field of `ref_replicas` replicas.
+    `predictors` maps a name to (predicted field, seconds the prediction
+    took); a warm run's time includes its prediction's."""
+    t0 = time.perf_counter()
+    ref = reference_field(p, ref_replicas, transient=transient, steps=ref_steps)
+    out = {"reference_seconds": time.perf_counter() - t0, "cold": []}
+
+    def best(runs):
+        ok = [r for r in runs if r["converged"]]
+        return min(ok, key=lambda r: r["seconds"]) if ok else None
+
+    for fs in cold_starts:
+        out["cold"].append(time_to_field(p, ref, "cold", first_sampling_step=fs,
+                                         check_every=check_every, max_steps=40000))
+    bc = best(out["cold"])
+    out["best_cold"] = bc
+    for name, (predicted, pred_s) in predictors.items():
+        runs = []
+        for fs in warm_starts:
+            r = time_to_field(p, ref, "warm", predicted=predicted, first_sampling_step=fs,
+                              check_every=check_every, max_steps=40000)
+            r["prediction_seconds"] = pred_s
+            r["seconds"] += pred_s
+            runs.append(r)
+        bw = best(runs)
+        out["warm_" + name] = {"runs": runs, "best": bw,
+                               "warm_over_cold": (bw["seconds"] / bc["seconds"])
+                               if bc and bw else None}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cases", type=int, default=1024)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--holdout", type=float, default=0.1)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=4096)
+    ap.add_argument("--chunk", type=int, default=128)
+    ap.add_argument("--no-ttf", action="store_true", help="skip the time-to-field study")
+    ap.add_argument("--out", default="surrogate_out")
+    args = ap.parse_args()
+    out = Path(args.out)
+    out.mkdir(parents=True, exist_ok=True)
+    report = {"args": vars(args)}
+
+    cases = surrogate_cases(args.cases, args.seed, steps=args.steps)
+    t0 = time.perf_counter()
+    x, t, m, ps = generate(cases, chunk=args.chunk, verbose=True)
+    gen_s = time.perf_counter() - t0
+    report["data"] = {"cases": len(cases), "seconds": gen_s, "particle_steps": ps,
+                      "particle_steps_per_s": ps / gen_s}
+    print(json.dumps(report["data"]), flush=True)
+
+    n_hold = max(1, int(round(args.holdout * len(cases))))
+    tr, ho = slice(0, len(cases) - n_hold), slice(len(cases) - n_hold, len(cases))
+    t0 = time.perf_counter()
+    net, hist = train(x[tr], t[tr], m[tr], epochs=args.epochs, batch=args.batch, lr=args.lr,
+                      log=lambda s: print(s, flush=True))
+    report["training"] = {"seconds": time.perf_counter() - t0,
+                          "history": [list(h) for h in hist],
+                          "tflops_last_epoch": hist[-1][3] if hist else None,
+                          "flops_per_step": net.flops_per_step()}
+    pred_tr = predict(net, x[tr][:n_hold])
+    pred_ho = predict(net, x[ho])
+    report["train_errors"] = relative_errors(pred_tr, t[tr][:n_hold], m[tr][:n_hold])
+    report["holdout_errors"] = relative_errors(pred_ho, t[ho], m[ho])
+    # The trivial predictor: the freestream everywhere.
+    free = np.zeros_like(t[ho])
+    for i in range(len(free)):
+        p = cases[len(cases) - n_hold + i]
+        d = setup(p)
+        free[i, ..., 0] = 1.0
+        free[i, ..., 1] = d.ux_free / d.u_free
+        free[i, ..., 2] = d.uy_free / d.u_free
+        free[i, ..., 3] = 1.0
+    report["freestream_errors"] = relative_errors(free, t[ho], m[ho])
+    print(json.dumps({k: report[k] for k in ("train_errors", "holdout_errors",
+                                             "freestream_errors")}), flush=True)
+    np.savez_compressed(out / "surrogate_weights.npz", **net.state_dict())
+
+    if not args.no_ttf:
+        p = warm_start_case(seed=1)
+        d = setup(p)
+        t0 = time.perf_counter()
+        one = Surrogate(1, seed=0)
+        one.load_state_dict(net.state_dict())
+        pred = predict(one, case_input(p)[None])[0]
+        predicted = prediction_field(p, d, pred)
+        sg_s = time.perf_counter() - t0
+        coarse, coarse_s = coarse_prediction(p)
+        report["time_to_field"] = time_to_field_study(
+            p, {"surrogate": (predicted, sg_s), "coarse": (coarse, coarse_s)},
+            ref_replicas=8, transient=6000, ref_steps=8000,
+            cold_starts=(2000, 4000, 6000, 8000), warm_starts=(500, 1000, 2000, 3000),
+            check_every=250)
+        tt = report["time_to_field"]
+        print(json.dumps({k: tt[k]["warm_over_cold"] for k in tt if k.startswith("warm_")}),
+              flush=True)
+    (out / "report.json").write_text(json.dumps(report, indent=1, default=float))
+
+
+if __name__ == "__main__":
+    main()

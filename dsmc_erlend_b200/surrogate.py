@@ -1,0 +1,340 @@
+"""The field surrogate: a BF16 convolutional encoder-decoder that maps a case
+to its sampled field, trained on DSMC ensembles, whose predictions seed the
+warm start (dsmc_init_warm).  The reference has no counterpart.
+
+Every layer runs through the C ABI of include/dsmc_surrogate.h (CUDA kernels
+in csrc/surrogate.cu: implicit-GEMM 3x3 convolutions on the tensor cores,
+their input and weight gradients, pooling, upsampling, the masked loss and
+Adam).  torch provides device memory only.
+
+Canvas: the domain [X1, X2] x [Y1, Y2] on RES x RES cells (x-major like the
+solver's fields).  Inputs (IN_CH channels, padded to 32): box mask, x and y
+of the cell centre, Mach / 8, cos and sin of the angle, log10(n) - 17, the
+wall model as three indicators, the CLL coefficients, box width and height /
+6.  Outputs (4 of 32 channels): n / NFree, ux / UFree, uy / UFree,
+T / TFree.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+
+RES = 128
+CH = 32
+OUT_CH = 4
+IN_CH = 14
+
+# (name, source, resampling before the conv, cin, cout, relu, skip added after)
+LAYERS = [
+    ("e1", "x", None, 32, 32, True, None),
+    ("e2", "e1", "pool", 32, 64, True, None),
+    ("e3", "e2", "pool", 64, 128, True, None),
+    ("b", "e3", "pool", 128, 128, True, None),
+    ("d3", "b", "up", 128, 128, True, "e3"),
+    ("d2", "d3", "up", 128, 64, True, "e2"),
+    ("d1", "d2", "up", 64, 32, True, "e1"),
+    ("out", "d1", None, 32, 32, False, None),
+]
+
+_LIB = Path(__file__).resolve().parent / "lib" / "libdsmc_surrogate.so"
+_lib = None
+
+_P = C.c_void_p
+_SIGS = {
+    "dsmc_sg_conv_fwd": [_P, _P, _P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                         C.c_int, _P],
+    "dsmc_sg_conv_dgrad": [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "dsmc_sg_conv_wgrad": [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "dsmc_sg_relu_bwd": [_P, _P, C.c_int64, _P],
+    "dsmc_sg_pool_fwd": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "dsmc_sg_pool_bwd": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "dsmc_sg_up_fwd": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "dsmc_sg_up_bwd": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "dsmc_sg_add": [_P, _P, C.c_int64, _P],
+    "dsmc_sg_mse": [_P, _P, _P, _P, _P, C.c_int64, C.c_int, C.c_int, _P],
+    "dsmc_sg_adam": [_P, _P, _P, _P, _P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float,
+                     C.c_int, _P],
+    "dsmc_sg_to_bf16": [_P, _P, C.c_int64, _P],
+}
+
+
+def lib():
+    """The surrogate kernel library; fails loudly when it is not built."""
+    global _lib
+    if _lib is None:
+        if not _LIB.exists():
+            raise RuntimeError(f"{_LIB} is not built: python -m dsmc_erlend_b200.build")
+        _lib = C.CDLL(os.fspath(_LIB))
+        for name, args in _SIGS.items():
+            fn = getattr(_lib, name)
+            fn.restype = C.c_int
+            fn.argtypes = args
+    return _lib
+
+
+def _ok(status: int, what: str):
+    if status != 0:
+        raise RuntimeError(f"{what}: status {status}")
+
+
+def ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+class Surrogate:
+    """Weights (FP32 masters, BF16 copies, Adam moments) and the activation
+    and gradient buffers of one batch size, on the current CUDA device."""
+
+    def __init__(self, batch: int, res: int = RES, seed: int = 0, stream=None):
+        import torch
+
+        self.torch = torch
+        self.n, self.res = batch, res
+        self.stream = stream
+        g = torch.Generator().manual_seed(seed)
+        dev = torch.device("cuda")
+        self.w32, self.wb, self.b32, self.m, self.v, self.gw, self.gb = {}, {}, {}, {}, {}, {}, {}
+        for name, _, _, cin, cout, _, _ in LAYERS:
+            std = math.sqrt(2.0 / (9 * cin))  # He initialisation
+            w = torch.randn(cout, 3, 3, cin, generator=g) * std
+            self.w32[name] = w.to(dev)
+            self.wb[name] = w.to(torch.bfloat16).to(dev)
+            self.b32[name] = torch.zeros(cout, device=dev)
+            self.gw[name] = torch.zeros_like(self.w32[name])
+            self.gb[name] = torch.zeros_like(self.b32[name])
+            for d in (self.m, self.v):
+                d[name + ".w"] = torch.zeros_like(self.w32[name])
+                d[name + ".b"] = torch.zeros_like(self.b32[name])
+        self.t = 0
+        self.w_rot = torch.empty(9 * 128 * 128, dtype=torch.bfloat16, device=dev)
+        self.shape = {"x": (res, CH)}
+        for name, src, op, cin, cout, _, _ in LAYERS:
+            r = self.shape[src][0]
+            r = r // 2 if op == "pool" else (r * 2 if op == "up" else r)
+            self.shape[name] = (r, cout)
+        bf = torch.bfloat16
+
+        def buf(r, c, dtype=bf):
+            return torch.empty(batch, r, r, c, dtype=dtype, device=dev)
+
+        self.a_in, self.relu_out, self.y = {}, {}, {}
+        for name, src, op, cin, cout, relu, skip in LAYERS:
+            r = self.shape[name][0]
+            self.a_in[name] = buf(r, cin) if op else None
+            self.relu_out[name] = buf(r, cout)
+            self.y[name] = buf(r, cout) if skip else self.relu_out[name]
+        self.out32 = buf(res, CH, torch.float32)
+        self.dy = {k: buf(*self.shape[k]) for k in self.shape}
+        self.scratch = {k: buf(*self.shape[k]) for k in self.shape}
+        self.da_in = {name: buf(self.shape[name][0], cin)
+                      for name, _, op, cin, _, _, _ in LAYERS}
+        self.loss = torch.zeros(2, device=dev)
+
+    @property
+    def _s(self):
+        return None if self.stream is None else C.c_void_p(self.stream)
+
+    def act(self, name):
+        return self.y[name]
+
+    # -- forward --------------------------------------------------------------
+    def forward(self, x) -> "torch.Tensor":
+        """x: (n, res, res, 32) bf16 -> (n, res, res, 32) fp32 (channels 0..3
+        are the prediction)."""
+        L, s, n = lib(), self._s, self.n
+        acts = {"x": x}
+        for name, src, op, cin, cout, relu, skip in LAYERS:
+            a = acts[src]
+            r = self.shape[name][0]
+            if op == "pool":
+                _ok(L.dsmc_sg_pool_fwd(ptr(a), ptr(self.a_in[name]), n, 2 * r, 2 * r, cin, s),
+                    "pool")
+                a = self.a_in[name]
+            elif op == "up":
+                _ok(L.dsmc_sg_up_fwd(ptr(a), ptr(self.a_in[name]), n, r // 2, r // 2, cin, s),
+                    "up")
+                a = self.a_in[name]
+            last = name == LAYERS[-1][0]
+            _ok(L.dsmc_sg_conv_fwd(ptr(a), ptr(self.wb[name]), ptr(self.b32[name]), None,
+                                   ptr(self.relu_out[name]), ptr(self.out32) if last else None,
+                                   n, r, r, cin, cout, int(relu), s), f"conv {name}")
+            if skip:
+                self.y[name].copy_(self.relu_out[name])
+                _ok(L.dsmc_sg_add(ptr(self.y[name]), ptr(acts[skip]), self.y[name].numel(), s),
+                    "skip")
+            acts[name] = self.y[name]
+        self._acts = acts
+        return self.out32
+
+    # -- backward -------------------------------------------------------------
+    def backward(self, dout):
+        """Weight and bias gradients (FP32, in gw / gb) for the output
+        gradient dout (bf16, same shape as the output)."""
+        L, s, n = lib(), self._s, self.n
+        acts = self._acts
+        for g in list(self.gw.values()) + list(self.gb.values()):
+            g.zero_()
+        last = LAYERS[-1][0]
+        for k in self.dy:
+            if k != last:
+                self.dy[k].zero_()
+        self.dy[last].copy_(dout)
+        for name, src, op, cin, cout, relu, skip in reversed(LAYERS):
+            r = self.shape[name][0]
+            dy = self.dy[name]
+            if skip:
+                _ok(L.dsmc_sg_add(ptr(self.dy[skip]), ptr(dy), dy.numel(), s), "skip grad")
+            if relu:
+                _ok(L.dsmc_sg_relu_bwd(ptr(dy), ptr(self.relu_out[name]), dy.numel(), s), "relu")
+            a = self.a_in[name] if op else acts[src]
+            _ok(L.dsmc_sg_conv_wgrad(ptr(dy), ptr(a), ptr(self.gw[name]), ptr(self.gb[name]),
+                                     n, r, r, cin, cout, s), f"wgrad {name}")
+            if src == "x":
+                continue
+            da = self.da_in[name]
+            _ok(L.dsmc_sg_conv_dgrad(ptr(dy), ptr(self.wb[name]), ptr(self.w_rot), ptr(da),
+                                     n, r, r, cin, cout, s), f"dgrad {name}")
+            tgt = self.scratch[src]
+            if op == "pool":
+                _ok(L.dsmc_sg_pool_bwd(ptr(da), ptr(tgt), n, 2 * r, 2 * r, cin, s), "pool bwd")
+            elif op == "up":
+                _ok(L.dsmc_sg_up_bwd(ptr(da), ptr(tgt), n, r // 2, r // 2, cin, s), "up bwd")
+            else:
+                tgt = da
+            _ok(L.dsmc_sg_add(ptr(self.dy[src]), ptr(tgt), tgt.numel(), s), "grad add")
+
+    def loss_and_grad(self, target, mask):
+        """Masked MSE of the last forward against target (n, res, res, 4)
+        fp32 with mask (n, res, res) fp32; returns the loss tensor [1] and
+        fills the output gradient."""
+        L = lib()
+        dout = self.scratch[LAYERS[-1][0]]
+        _ok(L.dsmc_sg_mse(ptr(self.out32), ptr(target), ptr(mask), ptr(dout), ptr(self.loss),
+                          self.n * self.res * self.res, CH, OUT_CH, self._s), "mse")
+        return self.loss[:1], dout
+
+    def adam_step(self, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999,
+                  eps: float = 1e-8):
+        L, s = lib(), self._s
+        self.t += 1
+        for name in self.w32:
+            _ok(L.dsmc_sg_adam(ptr(self.w32[name]), ptr(self.wb[name]), ptr(self.gw[name]),
+                               ptr(self.m[name + ".w"]), ptr(self.v[name + ".w"]),
+                               self.w32[name].numel(), lr, beta1, beta2, eps, self.t, s), "adam w")
+            _ok(L.dsmc_sg_adam(ptr(self.b32[name]), None, ptr(self.gb[name]),
+                               ptr(self.m[name + ".b"]), ptr(self.v[name + ".b"]),
+                               self.b32[name].numel(), lr, beta1, beta2, eps, self.t, s), "adam b")
+
+    def train_step(self, x, target, mask, lr: float = 1e-3):
+        self.forward(x)
+        loss, dout = self.loss_and_grad(target, mask)
+        self.backward(dout)
+        self.adam_step(lr)
+        return loss
+
+    def flops_per_step(self) -> float:
+        """Tensor-core FLOPs of one train step: forward 2 Cin Cout 9 H W per
+        sample and layer, backward twice that (dgrad and wgrad; the first
+        layer has no dgrad)."""
+        f = 0.0
+        for name, src, op, cin, cout, _, _ in LAYERS:
+            r = self.shape[name][0]
+            one = 2.0 * cin * cout * 9 * r * r * self.n
+            f += one * (2 if src == "x" else 3)
+        return f
+
+    def state_dict(self) -> dict:
+        out = {}
+        for name in self.w32:
+            out[name + ".w"] = self.w32[name].cpu().numpy()
+            out[name + ".b"] = self.b32[name].cpu().numpy()
+        return out
+
+    def load_state_dict(self, sd: dict):
+        torch = self.torch
+        for name in self.w32:
+            self.w32[name].copy_(torch.from_numpy(np.asarray(sd[name + ".w"], np.float32)))
+            self.b32[name].copy_(torch.from_numpy(np.asarray(sd[name + ".b"], np.float32)))
+            self.wb[name].copy_(self.w32[name].to(torch.bfloat16))
+
+
+# -- training ---------------------------------------------------------------------
+
+def relative_errors(pred: np.ndarray, target: np.ndarray, mask: np.ndarray) -> dict:
+    """Relative L2 error per output channel over the masked canvas cells:
+    ||pred - target|| / ||target|| for n and T, ||pred - target|| / sqrt(cells)
+    for the velocities (already in units of the freestream speed)."""
+    m = mask.astype(bool)
+    out = {}
+    for i, k in enumerate(("n", "ux", "uy", "t")):
+        d = (pred[..., i] - target[..., i])[m]
+        if k in ("n", "t"):
+            out[k] = float(np.linalg.norm(d) / max(np.linalg.norm(target[..., i][m]), 1e-30))
+        else:
+            out[k] = float(np.linalg.norm(d) / np.sqrt(max(m.sum(), 1)))
+    return out
+
+
+def train(x: np.ndarray, target: np.ndarray, mask: np.ndarray, epochs: int = 40,
+          batch: int = 32, lr: float = 2e-3, seed: int = 0, log=None) -> tuple:
+    """Trains a Surrogate on (N, RES, RES, CH) inputs, (N, RES, RES, 4)
+    targets and (N, RES, RES) masks with Adam (cosine learning-rate decay).
+    Returns the network and a history of (epoch, mean loss, step ms, TFLOP/s)."""
+    import torch
+
+    n = x.shape[0]
+    net = Surrogate(batch, res=x.shape[1], seed=seed)
+    dx = torch.from_numpy(x).to(torch.bfloat16).cuda()
+    dt = torch.from_numpy(target.astype(np.float32)).cuda()
+    dm = torch.from_numpy(mask.astype(np.float32)).cuda()
+    bx = torch.empty((batch,) + dx.shape[1:], dtype=torch.bfloat16, device="cuda")
+    bt = torch.empty((batch,) + dt.shape[1:], dtype=torch.float32, device="cuda")
+    bm = torch.empty((batch,) + dm.shape[1:], dtype=torch.float32, device="cuda")
+    rng = np.random.default_rng(seed)
+    steps_per_epoch = n // batch
+    total = epochs * steps_per_epoch
+    history = []
+    step = 0
+    for ep in range(epochs):
+        order = torch.from_numpy(rng.permutation(n)).cuda()
+        losses = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for s in range(steps_per_epoch):
+            idx = order[s * batch:(s + 1) * batch]
+            torch.index_select(dx, 0, idx, out=bx)
+            torch.index_select(dt, 0, idx, out=bt)
+            torch.index_select(dm, 0, idx, out=bm)
+            cur = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(total, 1)))
+            losses.append(net.train_step(bx, bt, bm, lr=cur).clone())
+            step += 1
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / max(steps_per_epoch, 1)
+        mean = float(torch.stack(losses).mean().item()) if losses else float("nan")
+        tf = net.flops_per_step() / (ms * 1e-3) / 1e12
+        history.append((ep, mean, ms, tf))
+        if log:
+            log(f"epoch {ep} loss {mean:.4e} {ms:.2f} ms/step {tf:.1f} TFLOP/s")
+    return net, history
+
+
+def predict(net: Surrogate, x: np.ndarray) -> np.ndarray:
+    """Predictions (N, RES, RES, 4) for inputs (N, RES, RES, CH) with a
+    trained network (its weights copied into a network of this batch)."""
+    import torch
+
+    out = []
+    b = net.n
+    for i in range(0, x.shape[0], b):
+        part = x[i:i + b]
+        pad = b - part.shape[0]
+        if pad:
+            part = np.concatenate([part, np.zeros((pad,) + part.shape[1:], part.dtype)])
+        y = net.forward(torch.from_numpy(part).to(torch.bfloat16).cuda())
+        out.append(y[: b - pad, ..., :OUT_CH].cpu().numpy())
+    return np.concatenate(out)

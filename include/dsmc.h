@@ -128,7 +128,30 @@ typedef struct dsmc_counters {
     double time;                  /* Time                                  */
     double sample_time;           /* SampleTime                            */
     double drag_sampling_time;    /* DragSamplingTime                      */
+    /* The impacts of the moves made while DragSamplingTime runs (steps after
+     * FirstSamplingStep): the window the mean drag force is taken over.  The
+     * reference's totals above count every step.                         */
+    int64_t drag_collision_count_window;
+    double drag_impulse_window;
 } dsmc_counters;
+
+/* Drag diagnostics of a run (Simulation.cpp:210-237, code the reference
+ * keeps commented out): mean force = impulse / DragSamplingTime and
+ * Cd = mean force / (0.5 NFree MoleculeMass UFree^2 BoxHeight DZ).        */
+typedef struct dsmc_drag {
+    double sampling_time;    /* DragSamplingTime, s                          */
+    double rho_free;         /* NFree * MoleculeMass, kg/m^3                 */
+    double area_ref;         /* BoxHeight * DZ, m^2                          */
+    /* The reference's expression: DragImpulseTotal over all steps divided by
+     * the sampling time.                                                  */
+    double mean_force_total; /* N                                            */
+    double cd_total;
+    int64_t box_collisions;  /* DragCollisionCount                           */
+    /* The same over the sampling window only (the physical mean force).    */
+    double mean_force;       /* N                                            */
+    double cd;
+    int64_t box_collisions_window;
+} dsmc_drag;
 
 /* Moments of one cell, laid out exactly as the reference's CELL
  * (include/Cell.h:4-10), 17 doubles.                                       */
@@ -157,6 +180,11 @@ const char *dsmc_wall_model_name(int wall_model);
 
 const char *dsmc_status_string(int status);
 
+/* Fills `out` from the counters of one case.  DSMC_ERR_STATE when no
+ * sampling time has elapsed yet (the reference would divide by zero).      */
+int dsmc_drag_report(const dsmc_params *p, const dsmc_derived *d, const dsmc_counters *c,
+                     dsmc_drag *out);
+
 /* Printing() (Sampling.cpp:36-268): writes <dir>/<wall>/DSMC2D_Field.plt and
  * .json from a gathered field of nx*ny cells in x-major order (k*ny + l),
  * exactly in the reference format.  `sample_step` is SampleStep. */
@@ -174,8 +202,22 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
 int dsmc_ctx_destroy(dsmc_ctx *ctx);
 
 /* InitialConditions() (Initialization.cpp:290-313) for every case, followed
- * by the cell sort that leaves particles ordered by cell. */
+ * by the cell sort that leaves particles ordered by cell.  Clears the device
+ * error word of a previous run (and so does dsmc_init_warm). */
 int dsmc_init_cold(dsmc_ctx *ctx);
+
+/* Warm start (no counterpart in the reference): instead of the uniform
+ * freestream of InitialConditions, every case is filled from the local
+ * Maxwellian of a given field, e.g. a surrogate's prediction or the
+ * converged field of a neighbouring case.  `host_field` holds 4 doubles per
+ * cell, cells x-major (k*ny + l) and cases one after another: number
+ * density n [1/m^3], velocity ux, uy [m/s], temperature T [K].  A cell gets
+ * floor(n DV / W) + Bernoulli(rest) particles, uniform in the cell, with
+ * velocity (ux, uy, 0) plus Gaussians of variance k T / m (each cell's own
+ * random stream); those inside the box are dropped.  Counters and moments
+ * start from zero as after InitialConditions.  DSMC_ERR_CAPACITY when a
+ * case's particles exceed its capacity. */
+int dsmc_init_warm(dsmc_ctx *ctx, const double *host_field);
 
 /* Runs n_steps complete time steps (Simulation.cpp:138-199) for every case:
  * move, boundary conditions, indexing, collisions, sampling.  Launched as
@@ -234,6 +276,35 @@ int dsmc_upload_particles(dsmc_ctx *ctx, int case_index, const double *x, const 
                           const double *vx, const double *vy, const double *vz, int64_t n);
 /* Cell start offsets (nx*ny + 1 entries) of the last sort. */
 int dsmc_get_cell_starts(dsmc_ctx *ctx, int case_index, int32_t *host_out);
+
+/* Checkpoint of every case of an idle context (between steps) in one file:
+ * the run counters, the particles in slot order and the sampled moments.
+ * The reference has none (its RunSimulation cannot resume).  Loading it
+ * into a context created with the same parameters (NStep aside), cases and
+ * precision resumes the run: the next steps are bit-identical to the uninterrupted
+ * run's (the random streams are keyed by the step), except the order of the
+ * atomic drag-impulse sums.  DSMC_ERR_ARGUMENT for a file that is not a
+ * checkpoint of such a context; DSMC_ERR_STATE in the middle of a step.    */
+int dsmc_checkpoint_save(dsmc_ctx *ctx, const char *path);
+int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path);
+
+/* Launch shapes (no counterpart in the reference): the CTAs per SM of the
+ * step's kernels whose grids are tunable, in the order and with the names
+ * of dsmc_get_kernel_times; max_ctas_per_sm is what fits on an SM (0 for a
+ * kernel with a fixed grid).  Every kernel gives the same results for any
+ * shape, so tuning never changes a run's particles or moments. */
+int dsmc_get_launch_config(dsmc_ctx *ctx, int32_t *ctas_per_sm, int32_t *max_ctas_per_sm,
+                           int max_kernels, int *n_kernels, const char **names_out);
+/* Sets the shapes of the first n kernels (entries <= 0 are kept; values are
+ * capped at the maximum); the step's CUDA graphs are rebuilt at the next
+ * dsmc_step. */
+int dsmc_set_launch_config(dsmc_ctx *ctx, const int32_t *ctas_per_sm, int n);
+/* Autotuner: for each tunable kernel in turn, times steps_per_trial steps
+ * (CUDA events around the kernel) for each candidate shape (the maximum,
+ * its half and quarter, 1, 2, 4, 8, 16 CTAs per SM) and keeps the fastest.
+ * The trial steps are real steps of the run (it advances); re-initialise
+ * afterwards for a run from step 0 with the tuned shapes. */
+int dsmc_autotune(dsmc_ctx *ctx, int steps_per_trial);
 
 /* Per-kernel device time of the stages, for profiling.  When enabled,
  * dsmc_step brackets every kernel with CUDA events; dsmc_get_kernel_times

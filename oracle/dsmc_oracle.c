@@ -34,6 +34,8 @@ struct dsmc_oracle {
     int sampling_mode;
     double time, sample_time, drag_impulse, drag_sampling_time;
     int64_t drag_count, last_nc, total_nc, particle_steps;
+    double drag_impulse_window; /* impacts of moves after FirstSamplingStep */
+    int64_t drag_count_window;
     double box_lo[2], box_hi[2];
     double local[4]; /* LocalX1 LocalY1 LocalX2 LocalY2 (MPIManager.cpp:216-229) */
     dsmc_stream rng;
@@ -282,6 +284,10 @@ static int move_one(dsmc_oracle *o, int64_t i)
     o->vz[i] = v[2];
     o->drag_impulse += o->d.weight * o->d.molecule_mass * (vx_in - v[0]);
     o->drag_count++;
+    if (o->step > o->p.first_sampling_step) {
+        o->drag_impulse_window += o->d.weight * o->d.molecule_mass * (vx_in - v[0]);
+        o->drag_count_window++;
+    }
     const double remaining = dt * (1.0 - t_hit);
     const double eps = 1e-12;
     o->x[i] = x_hit + remaining * v[0] + eps * nx;
@@ -651,6 +657,8 @@ int dsmc_oracle_get_counters(dsmc_oracle *o, dsmc_counters *c)
     c->time = o->time;
     c->sample_time = o->sample_time;
     c->drag_sampling_time = o->drag_sampling_time;
+    c->drag_collision_count_window = o->drag_count_window;
+    c->drag_impulse_window = o->drag_impulse_window;
     return DSMC_OK;
 }
 

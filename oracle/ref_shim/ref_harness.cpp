@@ -306,6 +306,9 @@ int dsmc_ref_get_counters(dsmc_counters *c)
     c->time = Time;
     c->sample_time = SampleTime;
     c->drag_sampling_time = DragSamplingTime;
+    // The reference keeps no per-window drag counters.
+    c->drag_collision_count_window = -1;
+    c->drag_impulse_window = -1.0;
     return DSMC_OK;
 }
 

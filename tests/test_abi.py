@@ -21,9 +21,10 @@ ROOT = Path(__file__).resolve().parent.parent
 GOLDEN = ROOT / "tests" / "golden"
 
 
-def declared_functions() -> set[str]:
+def declared_functions(headers=None) -> set[str]:
     names = set()
-    for h in (ROOT / "include").glob("*.h"):
+    for h in headers or [h for h in (ROOT / "include").glob("*.h")
+                         if h.name != "dsmc_surrogate.h"]:
         text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
         text = re.sub(r"//[^\n]*", "", text)
         for m in re.finditer(r"\b(dsmc_\w+)\s*\(", text):
@@ -40,6 +41,16 @@ def test_library_exports_every_declared_entry_point(engine_lib):
     missing = [n for n in sorted(declared) if not hasattr(engine_lib, n)]
     assert not missing, f"not exported: {missing}"
     assert set(_lib.SIGNATURES) <= declared
+
+
+def test_surrogate_library_exports_its_header():
+    from dsmc_erlend_b200 import surrogate
+
+    declared = declared_functions([ROOT / "include" / "dsmc_surrogate.h"])
+    assert "dsmc_sg_conv_fwd" in declared
+    lib = surrogate.lib()
+    assert not [n for n in sorted(declared) if not hasattr(lib, n)]
+    assert set(surrogate._SIGS) == declared
 
 
 def test_defaults_match_reference_settings(engine_lib):
@@ -108,3 +119,41 @@ def test_printing_is_byte_identical_to_reference(engine_lib, tmp_path, wall):
         got = (tmp_path / wall / f).read_bytes()
         want = (GOLDEN / f"printing_{wall}_{f}").read_bytes()
         assert got == want, f
+
+
+def test_drag_report_arithmetic(engine_lib):
+    """dsmc_drag_report: the drag block of Simulation.cpp:210-237 (mean force
+    over DragSamplingTime, Cd on BoxHeight * DZ) for both impulse totals."""
+    from dsmc_erlend_b200.engine import drag_report
+    from dsmc_erlend_b200.abi import reference_case
+
+    p = reference_case()
+    d = setup(p)
+    c = dict(np=0, step=40, sample_step=10, collisions_last_step=0, collisions_total=0,
+             drag_collision_count=120, particle_steps=0, drag_impulse_total=3.0e-18, time=0.0,
+             sample_time=0.0, drag_sampling_time=2.0e-4, drag_collision_count_window=70,
+             drag_impulse_window=1.5e-18)
+    r = drag_report(p, d, c)
+    rho = p.n_free * d.molecule_mass
+    q = 0.5 * rho * d.u_free ** 2 * (p.box_height * p.dz)
+    assert r["rho_free"] == rho and r["area_ref"] == p.box_height * p.dz
+    assert r["mean_force_total"] == pytest.approx(3.0e-18 / 2.0e-4, rel=1e-15)
+    assert r["cd_total"] == pytest.approx(3.0e-18 / 2.0e-4 / q, rel=1e-15)
+    assert r["cd"] == pytest.approx(1.5e-18 / 2.0e-4 / q, rel=1e-15)
+    assert r["box_collisions"] == 120 and r["box_collisions_window"] == 70
+    c["drag_sampling_time"] = 0.0
+    with pytest.raises(RuntimeError):
+        drag_report(p, d, c)
+
+
+def test_cli_lists_run_controls_and_rejects_bad_periods(engine_lib):
+    import subprocess
+
+    exe = Path(__file__).resolve().parents[1] / "dsmc_erlend_b200" / "lib" / "dsmc"
+    r = subprocess.run([str(exe), "--help"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0
+    for flag in ("--print-period", "--checkpoint", "--checkpoint-period", "--restart", "--drag"):
+        assert flag in r.stdout
+    for bad in (["--print-period", "0"], ["--checkpoint-period", "2.5"], ["--restart"]):
+        r = subprocess.run([str(exe), *bad], capture_output=True, text=True, timeout=60)
+        assert r.returncode == 2, bad

@@ -35,7 +35,9 @@ def test_ensemble_cases_equal_single_runs(cuda, engine_lib, precision):
         assert np.array_equal(ens.cell_starts(i), solo.cell_starts())
         assert np.array_equal(ens.fields(i), solo.fields())
         ca, cb = ens.counters(i), solo.counters()
-        ca.pop("drag_impulse_total"), cb.pop("drag_impulse_total")  # atomic sum order
+        for k in ("drag_impulse_total", "drag_impulse_window"):  # atomic sum order
+            x, y = ca.pop(k), cb.pop(k)
+            assert abs(x - y) <= 1e-12 * max(abs(y), 1e-300), (i, k)
         assert ca == cb, i
         solo.close()
     ens.close()
@@ -58,3 +60,28 @@ def test_ensemble_generator_ranges():
     walls = {p.wall_model for p in cases}
     assert walls == {0, 1, 2}
     assert len({p.seed for p in cases}) == 256
+
+
+def test_autotuned_launch_shapes_keep_results(cuda, engine_lib):
+    """The autotuner changes grid shapes only: a run with the tuned shapes is
+    bit-identical to a run with the default ones."""
+    cases = ensemble_cases(n=6, seed=31, precision=FP32, grid_range=(32, 96))
+    tuned = Engine(cases)
+    tuned.InitialConditions()
+    shapes = tuned.autotune(steps_per_trial=2)
+    assert shapes and all(1 <= v <= mx for v, mx in shapes.values())
+    tuned.InitialConditions()
+    tuned.step(15)
+    plain = Engine(cases)
+    plain.set_launch_config({k: 1 for k in shapes})  # the smallest grids
+    small = plain.launch_config()
+    assert all(v == 1 for v, _ in small.values())
+    plain.InitialConditions()
+    plain.step(15)
+    for i in range(len(cases)):
+        a, b = tuned.particles(i), plain.particles(i)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (i, k)
+        assert np.array_equal(tuned.fields(i), plain.fields(i))
+    tuned.close()
+    plain.close()

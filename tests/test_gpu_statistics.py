@@ -18,6 +18,7 @@ import pytest
 from dsmc_erlend_b200 import Engine, setup
 from dsmc_erlend_b200.abi import FP32, FP64, WALL_SPECULAR, default_params, reference_case
 from dsmc_erlend_b200.ensemble import replicas
+from dsmc_erlend_b200.fields import field_errors
 
 pytestmark = pytest.mark.gpu
 
@@ -37,36 +38,6 @@ def merged_fields(eng: Engine, n_cases: int):
         vv = m[:, [4, 8, 12]] / npc[:, None]
         t = d.molecule_mass * (vv - u * u) / K_B
     return {"n": n, "ux": u[:, 0], "uy": u[:, 1], "t": t.mean(axis=1), "count": npc}
-
-
-def field_errors(a: dict, b: dict, p, u_free: float) -> dict:
-    """Relative L2 errors of field a against field b over the cells outside
-    the wall cells (centre within one cell of the box).
-
-    n is compared over every such cell both runs sampled.  Velocity and
-    temperature are moments per sampled particle, undefined where almost
-    nothing is sampled: the near-vacuum wake right behind the box (about half
-    a percent of the cells here) holds tens of samples in a whole run, and
-    there even independent runs of the reference itself differ by O(100%).
-    ux, uy and T therefore leave out cells whose sample count in b is below
-    5% of b's median.  Velocities are normalised by the freestream speed,
-    n by ||n_b||, T by ||T_b||."""
-    dx = (p.x2 - p.x1) / p.nx
-    dy = (p.y2 - p.y1) / p.ny
-    k, l = np.meshgrid(np.arange(p.nx), np.arange(p.ny), indexing="ij")
-    xc = p.x1 + (k.ravel() + 0.5) * dx
-    yc = p.y1 + (l.ravel() + 0.5) * dy
-    wall = (np.abs(xc - p.box_x) < p.box_width / 2 + dx) & \
-           (np.abs(yc - p.box_y) < p.box_height / 2 + dy)
-    sampled = ~wall & (a["count"] > 0) & (b["count"] > 0)
-    dense = sampled & (b["count"] >= 0.05 * np.median(b["count"][b["count"] > 0]))
-    out = {"n": np.linalg.norm(a["n"][sampled] - b["n"][sampled]) /
-                np.linalg.norm(b["n"][sampled]),
-           "t": np.linalg.norm(a["t"][dense] - b["t"][dense]) / np.linalg.norm(b["t"][dense])}
-    for key in ("ux", "uy"):
-        out[key] = np.linalg.norm(a[key][dense] - b[key][dense]) / \
-            (u_free * np.sqrt(dense.sum()))
-    return out
 
 
 def test_equilibrium_collision_rate(cuda, engine_lib):

@@ -1,0 +1,202 @@
+"""The surrogate's CUDA kernels (csrc/surrogate.cu, through the C ABI of
+include/dsmc_surrogate.h) against the NumPy FP64 restatement in
+oracle/surrogate_ref.py, on small shapes.
+
+Inputs are bf16-representable, so the references see the kernels' exact
+operands.  Tolerances: FP32 results (forward with an FP32 output, weight and
+bias gradients) to 1e-4 relative to the result's scale (FP32 accumulation of
+at most a few thousand terms); bf16 results to 2^-7 relative (one bf16
+rounding) plus the same accumulation allowance.  The whole network, with the
+restatement rounding to bf16 where the kernels store bf16: output to 1% and
+weight gradients to 3% of each tensor's scale (the FP32 accumulation order
+still differs, and a value near a rounding boundary or a ReLU's zero can
+land on the other side), and one Adam step matches its formula to 1e-5
+(FP32).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import surrogate_ref as ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16).cuda()
+
+
+def _np(t):
+    return t.float().cpu().numpy().astype(np.float64)
+
+
+def _rand(rng, *shape, scale=1.0):
+    return rng.standard_normal(shape) * scale
+
+
+def _close(got, want, rtol, what):
+    scale = max(np.abs(want).max(), 1e-30)
+    err = np.abs(got - want).max() / scale
+    assert err <= rtol, f"{what}: max error {err:.3e} of scale {scale:.3e}"
+
+
+@pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 12, 20, 64, 96),
+                                            (3, 16, 16, 128, 64)])
+def test_conv_forward(cuda, n, h, w, cin, cout):
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    rng = np.random.default_rng(n * 100 + cin)
+    x = _bf16(torch, _rand(rng, n, h, w, cin))
+    wt = _bf16(torch, _rand(rng, cout, 3, 3, cin, scale=0.1))
+    b = torch.from_numpy(rng.standard_normal(cout).astype(np.float32)).cuda()
+    res = _bf16(torch, _rand(rng, n, h, w, cout))
+    y = torch.empty(n, h, w, cout, dtype=torch.bfloat16, device="cuda")
+    y32 = torch.empty(n, h, w, cout, dtype=torch.float32, device="cuda")
+    assert lib().dsmc_sg_conv_fwd(ptr(x), ptr(wt), ptr(b), None, None, ptr(y32), n, h, w, cin,
+                                  cout, 0, None) == 0
+    torch.cuda.synchronize()
+    want = ref.conv3x3(_np(x), _np(wt), b.cpu().numpy())
+    _close(_np(y32), want, 1e-4, "forward fp32")
+    assert lib().dsmc_sg_conv_fwd(ptr(x), ptr(wt), ptr(b), ptr(res), ptr(y), None, n, h, w, cin,
+                                  cout, 1, None) == 0
+    torch.cuda.synchronize()
+    _close(_np(y), np.maximum(want, 0.0) + _np(res), 2 ** -7 + 1e-4, "forward relu + res bf16")
+
+
+@pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 10, 6, 64, 32)])
+def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    rng = np.random.default_rng(7 + cin)
+    x = _bf16(torch, _rand(rng, n, h, w, cin))
+    wt = _bf16(torch, _rand(rng, cout, 3, 3, cin, scale=0.1))
+    dy = _bf16(torch, _rand(rng, n, h, w, cout))
+    w_rot = torch.empty(9 * cin * cout, dtype=torch.bfloat16, device="cuda")
+    dx = torch.empty(n, h, w, cin, dtype=torch.bfloat16, device="cuda")
+    dw = torch.zeros(cout, 3, 3, cin, dtype=torch.float32, device="cuda")
+    db = torch.zeros(cout, dtype=torch.float32, device="cuda")
+    L = lib()
+    assert L.dsmc_sg_conv_dgrad(ptr(dy), ptr(wt), ptr(w_rot), ptr(dx), n, h, w, cin, cout,
+                                None) == 0
+    assert L.dsmc_sg_conv_wgrad(ptr(dy), ptr(x), ptr(dw), ptr(db), n, h, w, cin, cout, None) == 0
+    torch.cuda.synchronize()
+    _close(_np(dx), ref.conv3x3_dgrad(_np(dy), _np(wt)), 2 ** -7 + 1e-4, "dgrad")
+    _close(_np(dw), ref.conv3x3_wgrad(_np(dy), _np(x)), 1e-4, "wgrad")
+    _close(_np(db), _np(dy).sum(axis=(0, 1, 2)), 1e-4, "bias grad")
+
+
+def test_wgrad_large_pixel_count_splits(cuda):
+    # Enough pixels for several pixel splits, and accumulation into dw.
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    rng = np.random.default_rng(3)
+    n, h, w, cin, cout = 4, 64, 64, 32, 64
+    x = _bf16(torch, _rand(rng, n, h, w, cin))
+    dy = _bf16(torch, _rand(rng, n, h, w, cout, scale=0.05))
+    dw = torch.ones(cout, 3, 3, cin, dtype=torch.float32, device="cuda")
+    assert lib().dsmc_sg_conv_wgrad(ptr(dy), ptr(x), ptr(dw), None, n, h, w, cin, cout,
+                                    None) == 0
+    torch.cuda.synchronize()
+    _close(_np(dw) - 1.0, ref.conv3x3_wgrad(_np(dy), _np(x)), 1e-4, "wgrad split")
+
+
+def test_resampling_and_loss_kernels(cuda):
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    L = lib()
+    rng = np.random.default_rng(11)
+    n, h, w, c = 2, 8, 12, 32
+    x = _bf16(torch, _rand(rng, n, h, w, c))
+    p = torch.empty(n, h // 2, w // 2, c, dtype=torch.bfloat16, device="cuda")
+    u = torch.empty(n, 2 * h, 2 * w, c, dtype=torch.bfloat16, device="cuda")
+    assert L.dsmc_sg_pool_fwd(ptr(x), ptr(p), n, h, w, c, None) == 0
+    assert L.dsmc_sg_up_fwd(ptr(x), ptr(u), n, h, w, c, None) == 0
+    pb = torch.empty_like(x)
+    ub = torch.empty_like(x)
+    assert L.dsmc_sg_pool_bwd(ptr(p), ptr(pb), n, h, w, c, None) == 0
+    assert L.dsmc_sg_up_bwd(ptr(u), ptr(ub), n, h, w, c, None) == 0
+    torch.cuda.synchronize()
+    _close(_np(p), ref.pool2(_np(x)), 2 ** -8, "pool")
+    assert np.array_equal(_np(u), ref.up2(_np(x)))
+    _close(_np(pb), ref.pool2_bwd(_np(p)), 2 ** -8, "pool bwd")
+    _close(_np(ub), ref.up2_bwd(_np(u)), 2 ** -7, "up bwd")
+    # ReLU gradient and add.
+    y = _bf16(torch, _rand(rng, n, h, w, c))
+    g = _bf16(torch, _rand(rng, n, h, w, c))
+    g0 = _np(g)
+    assert L.dsmc_sg_relu_bwd(ptr(g), ptr(y), g.numel(), None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(_np(g), g0 * (_np(y) > 0))
+    # Masked MSE.
+    out = torch.from_numpy(rng.standard_normal((n, h, w, c)).astype(np.float32)).cuda()
+    tgt = torch.from_numpy(rng.standard_normal((n, h, w, 4)).astype(np.float32)).cuda()
+    mask = torch.from_numpy((rng.random((n, h, w)) > 0.3).astype(np.float32)).cuda()
+    dy = torch.empty(n, h, w, c, dtype=torch.bfloat16, device="cuda")
+    loss = torch.zeros(2, device="cuda")
+    assert L.dsmc_sg_mse(ptr(out), ptr(tgt), ptr(mask), ptr(dy), ptr(loss), n * h * w, c, 4,
+                         None) == 0
+    torch.cuda.synchronize()
+    lw, gw = ref.mse(out.cpu().numpy().astype(np.float64), tgt.cpu().numpy(),
+                     mask.cpu().numpy(), 4)
+    assert abs(loss[0].item() - lw) <= 1e-5 * lw
+    _close(_np(dy), gw, 2 ** -8, "mse grad")
+
+
+def test_adam_step(cuda):
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    rng = np.random.default_rng(5)
+    w = rng.standard_normal(1000).astype(np.float32)
+    g = rng.standard_normal(1000).astype(np.float32)
+    m = rng.standard_normal(1000).astype(np.float32) * 0.1
+    v = rng.random(1000).astype(np.float32) * 0.1
+    tw, tg, tm, tv = (torch.from_numpy(a.copy()).cuda() for a in (w, g, m, v))
+    wb = torch.empty(1000, dtype=torch.bfloat16, device="cuda")
+    assert lib().dsmc_sg_adam(ptr(tw), ptr(wb), ptr(tg), ptr(tm), ptr(tv), 1000, 1e-3, 0.9,
+                              0.999, 1e-8, 3, None) == 0
+    torch.cuda.synchronize()
+    # The kernel's constants are the float32 roundings of 0.9 and 0.999.
+    b1, b2 = np.float32(0.9), np.float32(0.999)
+    m1 = b1 * m + (np.float32(1) - b1) * g
+    v1 = b2 * v + (np.float32(1) - b2) * g * g
+    w1 = w - 1e-3 * (m1 / (1 - b1 ** 3)) / (np.sqrt(v1 / (1 - b2 ** 3)) + 1e-8)
+    assert np.allclose(tw.cpu().numpy(), w1, rtol=1e-5, atol=1e-7)
+    # FP32 with contraction on the GPU: within a few ulp of the moments' terms.
+    assert np.allclose(tm.cpu().numpy(), m1, rtol=1e-5, atol=1e-7)
+    assert np.allclose(tv.cpu().numpy(), v1, rtol=1e-5, atol=1e-9)
+    assert np.allclose(wb.float().cpu().numpy(), w1, rtol=2 ** -7)
+
+
+def test_network_gradients_match_restatement(cuda):
+    from dsmc_erlend_b200.surrogate import LAYERS, Surrogate
+
+    torch = cuda
+    n, res = 2, 32
+    net = Surrogate(n, res=res, seed=4)
+    rng = np.random.default_rng(9)
+    # Nonzero biases, so every ReLU sees both signs.
+    for name in net.b32:
+        net.b32[name].copy_(torch.from_numpy(rng.standard_normal(net.b32[name].numel())
+                                             .astype(np.float32) * 0.1))
+    x = _bf16(torch, _rand(rng, n, res, res, 32))
+    out = net.forward(x)
+    torch.cuda.synchronize()
+    params = {}
+    for name in net.w32:
+        params[name + ".w"] = net.wb[name].float().cpu().numpy().astype(np.float64)
+        params[name + ".b"] = net.b32[name].cpu().numpy().astype(np.float64)
+    acts = ref.network_forward(params, _np(x), LAYERS)
+    _close(out.cpu().numpy(), acts[LAYERS[-1][0]], 0.01, "network output")
+    dout = _bf16(torch, _rand(rng, n, res, res, 32, scale=1e-2))
+    net.backward(dout)
+    torch.cuda.synchronize()
+    grads = ref.network_backward(params, acts, _np(dout), LAYERS)
+    for name in net.w32:
+        _close(net.gw[name].cpu().numpy(), grads[name + ".w"], 0.03, f"grad {name}.w")
+        _close(net.gb[name].cpu().numpy(), grads[name + ".b"], 0.03, f"grad {name}.b")
