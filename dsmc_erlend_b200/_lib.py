@@ -31,6 +31,7 @@ SIGNATURES = {
     "dsmc_ctx_destroy": (C.c_int, [C.c_void_p]),
     "dsmc_init_cold": (C.c_int, [C.c_void_p]),
     "dsmc_init_warm": (C.c_int, [C.c_void_p, _D]),
+    "dsmc_init_warm_tensor": (C.c_int, [C.c_void_p, _D]),
     "dsmc_step": (C.c_int, [C.c_void_p, C.c_int]),
     "dsmc_stage_move": (C.c_int, [C.c_void_p]),
     "dsmc_stage_boundary": (C.c_int, [C.c_void_p]),

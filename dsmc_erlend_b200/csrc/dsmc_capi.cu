@@ -676,16 +676,17 @@ __device__ __forceinline__ void warm_position(const CaseDev &c, int cl, dsmc_str
     y = clamp_into<T>(Store<T>::rn(c.y1 + (m + uniform(r)) * c.dy), c.y1, c.y2);
 }
 
-// Survivors per cell into cnt[global cell].
+// Survivors per cell into cnt[global cell].  `stride` doubles per cell.
 template <class T>
-__global__ void k_warm_count(const CaseDev *cases, int ncase, const double *field, int32_t *cnt)
+__global__ void k_warm_count(const CaseDev *cases, int ncase, const double *field, int stride,
+                             int32_t *cnt)
 {
     int64_t f0 = 0;
     for (int ci = 0; ci < ncase; ++ci) {
         const CaseDev &c = cases[ci];
         for (int cl = blockIdx.x * blockDim.x + threadIdx.x; cl < c.ncell;
              cl += gridDim.x * blockDim.x) {
-            const double *f = field + 4 * (f0 + cl);
+            const double *f = field + stride * (f0 + cl);
             const int nc = warm_candidates(c, f, cl);
             dsmc_stream r;
             open_stream(r, c, DSMC_RNG_WARM, 0, static_cast<uint32_t>(cl));
@@ -738,9 +739,13 @@ __global__ void __launch_bounds__(SCAN_THREADS)
 }
 
 // Writes the survivors of every cell from its offset, in cell order.
+// With stride 4 the velocity is (ux, uy, 0) plus isotropic Gaussians of
+// variance k T / m; with stride 7 the field gives the temperature tensor
+// (Txx, Tyy, Tzz, Txy) and the Gaussians are correlated through its
+// Cholesky factor (the xz and yz entries vanish in this 2-D flow).
 template <class T>
 __global__ void k_warm_fill(const CaseDev *cases, const CaseState *st, int ncase,
-                            const double *field, const int32_t *off, Slots<T> p)
+                            const double *field, int stride, const int32_t *off, Slots<T> p)
 {
     int64_t f0 = 0;
     for (int ci = 0; ci < ncase; ++ci) {
@@ -748,12 +753,20 @@ __global__ void k_warm_fill(const CaseDev *cases, const CaseState *st, int ncase
         const bool fits = st[ci].n_old > 0;
         for (int cl = blockIdx.x * blockDim.x + threadIdx.x; fits && cl < c.ncell;
              cl += gridDim.x * blockDim.x) {
-            const double *f = field + 4 * (f0 + cl);
+            const double *f = field + stride * (f0 + cl);
             const int nc = warm_candidates(c, f, cl);
             if (nc == 0)
                 continue;
             const double ux = f[1], uy = f[2];
             const double var = K_BOLTZMANN * fmax(f[3], 0.0) / c.mass;
+            double l11 = 0.0, l21 = 0.0, l22 = 0.0, l33 = 0.0;
+            if (stride == 7) {
+                const double kb = K_BOLTZMANN / c.mass;
+                l11 = sqrt(fmax(kb * f[3], 0.0));
+                l21 = l11 > 0.0 ? kb * f[6] / l11 : 0.0;
+                l22 = sqrt(fmax(kb * f[4] - l21 * l21, 0.0));
+                l33 = sqrt(fmax(kb * f[5], 0.0));
+            }
             dsmc_stream r, rv;
             open_stream(r, c, DSMC_RNG_WARM, 0, static_cast<uint32_t>(cl));
             open_stream(rv, c, DSMC_RNG_WARM, 1, static_cast<uint32_t>(cl));
@@ -762,9 +775,19 @@ __global__ void k_warm_fill(const CaseDev *cases, const CaseState *st, int ncase
             for (int j = 0; j < nc; ++j) {
                 T x, y;
                 warm_position<T>(c, cl, r, x, y);
-                const double vx = frand_gaussian(rv, ux, var);
-                const double vy = frand_gaussian(rv, uy, var);
-                const double vz = frand_gaussian(rv, 0.0, var);
+                double vx, vy, vz;
+                if (stride == 7) {
+                    const double z1 = frand_gaussian(rv, 0.0, 1.0);
+                    const double z2 = frand_gaussian(rv, 0.0, 1.0);
+                    const double z3 = frand_gaussian(rv, 0.0, 1.0);
+                    vx = ux + l11 * z1;
+                    vy = uy + l21 * z1 + l22 * z2;
+                    vz = l33 * z3;
+                } else {
+                    vx = frand_gaussian(rv, ux, var);
+                    vy = frand_gaussian(rv, uy, var);
+                    vz = frand_gaussian(rv, 0.0, var);
+                }
                 if (inside_box(c, static_cast<double>(x), static_cast<double>(y)))
                     continue;
                 p.x[g] = x;
@@ -779,14 +802,15 @@ __global__ void k_warm_fill(const CaseDev *cases, const CaseState *st, int ncase
     }
 }
 
-template <class T> int warm_fill(dsmc_ctx *c, const double *dfield, int32_t *cnt, int32_t *off)
+template <class T>
+int warm_fill(dsmc_ctx *c, const double *dfield, int stride, int32_t *cnt, int32_t *off)
 {
     const int grid = 4 * c->sms;
-    k_warm_count<T><<<grid, 256, 0, c->stream>>>(c->d_cases, c->ncase, dfield, cnt);
+    k_warm_count<T><<<grid, 256, 0, c->stream>>>(c->d_cases, c->ncase, dfield, stride, cnt);
     k_warm_scan<<<c->ncase, SCAN_THREADS, 0, c->stream>>>(c->d_cases, c->d_state, cnt, off,
                                                            c->d_err);
-    k_warm_fill<T><<<grid, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->ncase, dfield, off,
-                                                slots<T>(c, c->cur));
+    k_warm_fill<T><<<grid, 256, 0, c->stream>>>(c->d_cases, c->d_state, c->ncase, dfield, stride,
+                                                off, slots<T>(c, c->cur));
     CK(cudaGetLastError());
     return resort_all<T>(c);
 }
@@ -1120,7 +1144,9 @@ int dsmc_init_cold(dsmc_ctx *c)
     return DSMC_OK;
 }
 
-int dsmc_init_warm(dsmc_ctx *c, const double *host_field)
+namespace {
+
+int init_warm(dsmc_ctx *c, const double *host_field, int stride)
 {
     if (c == nullptr || host_field == nullptr)
         return DSMC_ERR_ARGUMENT;
@@ -1132,14 +1158,14 @@ int dsmc_init_warm(dsmc_ctx *c, const double *host_field)
     CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
     double *dfield = nullptr;
     int32_t *tmp = nullptr;
-    CK(cudaMallocAsync(reinterpret_cast<void **>(&dfield), sizeof(double) * 4 * cells, c->stream));
+    const size_t bytes = sizeof(double) * stride * cells;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&dfield), bytes, c->stream));
     CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(int32_t) * 2 * c->total_cells,
                        c->stream));
-    CK(cudaMemcpyAsync(dfield, host_field, sizeof(double) * 4 * cells, cudaMemcpyHostToDevice,
-                       c->stream));
-    const int s = c->precision == DSMC_FP32 ? warm_fill<float>(c, dfield, tmp, tmp + c->total_cells)
-                                            : warm_fill<double>(c, dfield, tmp,
-                                                                tmp + c->total_cells);
+    CK(cudaMemcpyAsync(dfield, host_field, bytes, cudaMemcpyHostToDevice, c->stream));
+    const int s = c->precision == DSMC_FP32
+                      ? warm_fill<float>(c, dfield, stride, tmp, tmp + c->total_cells)
+                      : warm_fill<double>(c, dfield, stride, tmp, tmp + c->total_cells);
     CK(cudaFreeAsync(dfield, c->stream));
     CK(cudaFreeAsync(tmp, c->stream));
     if (s)
@@ -1148,6 +1174,15 @@ int dsmc_init_warm(dsmc_ctx *c, const double *host_field)
     c->initialized = true;
     c->stage = 0;
     return device_error(c);
+}
+
+} // namespace
+
+int dsmc_init_warm(dsmc_ctx *c, const double *host_field) { return init_warm(c, host_field, 4); }
+
+int dsmc_init_warm_tensor(dsmc_ctx *c, const double *host_field)
+{
+    return init_warm(c, host_field, 7);
 }
 
 int dsmc_step(dsmc_ctx *c, int n_steps)

@@ -701,8 +701,11 @@ __global__ void __launch_bounds__(TILE_THREADS)
             }
             T xs = Store<T>::rn(x), ys = Store<T>::rn(y);
             if (init_mode) {
-                xs = clamp_into<T>(xs, b[0], b[2]);
-                ys = clamp_into<T>(ys, b[1], b[3]);
+                // The fill box ends at LocalX2 = X1 + NX DX, which can exceed
+                // X2 by an ulp; a float rounded up to X2 itself would then
+                // index cell NX.  Keep FP32 positions below both.
+                xs = clamp_into<T>(xs, b[0], fmin(b[2], c.x2));
+                ys = clamp_into<T>(ys, b[1], fmin(b[3], c.y2));
             }
             const int64_t q = s.n_old + j;
             const int64_t g = c.pbase + q;

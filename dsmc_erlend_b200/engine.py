@@ -97,12 +97,17 @@ class Engine:
 
     def init_warm(self, field: np.ndarray):
         """Fills every case from the local Maxwellian of `field`: (n, ux, uy,
-        T) per cell, cells x-major, cases one after another (dsmc_init_warm)."""
+        T) per cell, cells x-major, cases one after another (dsmc_init_warm),
+        or (n, ux, uy, Txx, Tyy, Tzz, Txy) (dsmc_init_warm_tensor)."""
         f = np.ascontiguousarray(field, dtype=np.float64)
         need = sum(p.nx * p.ny for p in self.params)
-        if f.shape != (need, 4):
-            raise ValueError(f"field must have shape ({need}, 4), not {f.shape}")
-        check(self._lib.dsmc_init_warm(self._h, f.ctypes.data_as(_D)), "dsmc_init_warm")
+        if f.shape not in ((need, 4), (need, 7)):
+            raise ValueError(f"field must have shape ({need}, 4) or ({need}, 7), not {f.shape}")
+        if f.shape[1] == 7:  # n, ux, uy, Txx, Tyy, Tzz, Txy: dsmc_init_warm_tensor
+            check(self._lib.dsmc_init_warm_tensor(self._h, f.ctypes.data_as(_D)),
+                  "dsmc_init_warm_tensor")
+        else:
+            check(self._lib.dsmc_init_warm(self._h, f.ctypes.data_as(_D)), "dsmc_init_warm")
 
     def step(self, n: int = 1):
         check(self._lib.dsmc_step(self._h, int(n)), "dsmc_step")

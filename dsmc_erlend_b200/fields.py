@@ -22,7 +22,9 @@ def macroscopic(cells: np.ndarray, weight: float, dv: float, molecule_mass: floa
         u = cells[:, 1:4] / npc[:, None]
         vv = cells[:, [4, 8, 12]] / npc[:, None]
         t = molecule_mass * (vv - u * u) / K_BOLTZMANN
-    return {"n": n, "ux": u[:, 0], "uy": u[:, 1], "t": t.mean(axis=1), "count": npc}
+        txy = molecule_mass * (cells[:, 5] / npc - u[:, 0] * u[:, 1]) / K_BOLTZMANN
+    return {"n": n, "ux": u[:, 0], "uy": u[:, 1], "t": t.mean(axis=1), "count": npc,
+            "txx": t[:, 0], "tyy": t[:, 1], "tzz": t[:, 2], "txy": txy}
 
 
 def wall_cells(p) -> np.ndarray:
@@ -76,15 +78,20 @@ def field_errors(a: dict, b: dict, p, u_free: float) -> dict:
     return out
 
 
-def warm_input(f: dict) -> np.ndarray:
-    """The (n, ux, uy, T) array per cell that dsmc_init_warm takes; cells
-    without samples are left empty (n = 0)."""
+def warm_input(f: dict, tensor: bool = False) -> np.ndarray:
+    """The (n, ux, uy, T) array per cell that dsmc_init_warm takes, or with
+    tensor the (n, ux, uy, Txx, Tyy, Tzz, Txy) one of dsmc_init_warm_tensor;
+    cells without samples are left empty (n = 0)."""
     ok = np.isfinite(f["ux"]) & np.isfinite(f["uy"]) & np.isfinite(f["t"]) & (f["count"] > 0)
-    out = np.zeros((len(f["n"]), 4), dtype=np.float64)
+    keys = ("txx", "tyy", "tzz", "txy") if tensor else ("t",)
+    for k in keys:
+        ok &= np.isfinite(f[k])
+    out = np.zeros((len(f["n"]), 3 + len(keys)), dtype=np.float64)
     out[ok, 0] = f["n"][ok]
     out[ok, 1] = f["ux"][ok]
     out[ok, 2] = f["uy"][ok]
-    out[ok, 3] = np.maximum(f["t"][ok], 0.0)
+    for i, k in enumerate(keys):
+        out[ok, 3 + i] = f[k][ok] if k == "txy" else np.maximum(f[k][ok], 0.0)
     return out
 
 

@@ -90,16 +90,23 @@ def _bilinear(src: np.ndarray, p, tx: int, ty: int) -> np.ndarray:
             (1 - wx) * wy * src[i0, j1] + wx * wy * src[i1, j1])
 
 
+def t_scale(p) -> float:
+    """The temperature unit of the surrogate: the freestream's stagnation
+    temperature TFree (1 + (gamma - 1) / 2 Ma^2), gamma = 5/3, so that the
+    targets of every Mach number are of order one."""
+    return p.t_free * (1.0 + p.ma_free ** 2 / 3.0)
+
+
 def field_target(p, d, f: dict, res: int = RES):
-    """A sampled field on the canvas, normalised by the freestream: (res,
-    res, OUT_CH) targets n / NFree, ux / UFree, uy / UFree, T / TFree, and
-    the (res, res) mask of canvas cells that are outside the box and whose
-    neighbourhood was sampled."""
+    """A sampled field on the canvas, normalised: (res, res, OUT_CH) targets
+    n / NFree, ux / UFree, uy / UFree, T / t_scale, and the (res, res) mask
+    of canvas cells that are outside the box and whose neighbourhood was
+    sampled."""
     nx, ny = p.nx, p.ny
     valid = (f["count"] > 0) & np.isfinite(f["ux"]) & np.isfinite(f["t"])
     free = {"n": p.n_free, "ux": d.ux_free, "uy": d.uy_free, "t": p.t_free}
     out = np.zeros((res, res, OUT_CH), dtype=np.float32)
-    scale = {"n": p.n_free, "ux": d.u_free, "uy": d.u_free, "t": p.t_free}
+    scale = {"n": p.n_free, "ux": d.u_free, "uy": d.u_free, "t": t_scale(p)}
     for i, k in enumerate(("n", "ux", "uy", "t")):
         v = np.where(valid, f[k], free[k] if k != "n" else 0.0).reshape(nx, ny)
         out[..., i] = _bilinear(v, p, res, res) / scale[k]
@@ -113,7 +120,7 @@ def prediction_field(p, d, pred: np.ndarray) -> dict:
     field dict dsmc_init_warm's input is made from (count 1 outside the
     box, n = 0 inside it)."""
     back = {}
-    scale = {"n": p.n_free, "ux": d.u_free, "uy": d.u_free, "t": p.t_free}
+    scale = {"n": p.n_free, "ux": d.u_free, "uy": d.u_free, "t": t_scale(p)}
     for i, k in enumerate(("n", "ux", "uy", "t")):
         back[k] = (_bilinear(pred[..., i].astype(np.float64), p, p.nx, p.ny) * scale[k]).ravel()
     back["n"] = np.maximum(back["n"], 0.0)

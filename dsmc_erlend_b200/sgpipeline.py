@@ -18,7 +18,7 @@ import numpy as np
 
 from . import setup
 from .abi import warm_start_case
-from .sgdata import case_input, generate, prediction_field, surrogate_cases
+from .sgdata import case_input, generate, prediction_field, surrogate_cases, t_scale
 from .surrogate import Surrogate, predict, relative_errors, train
 from .timetofield import coarse_prediction, reference_field, time_to_field
 
@@ -64,7 +64,7 @@ def main():
     ap.add_argument("--holdout", type=float, default=0.1)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=4096)
     ap.add_argument("--chunk", type=int, default=128)
     ap.add_argument("--no-ttf", action="store_true", help="skip the time-to-field study")
@@ -103,7 +103,7 @@ def main():
         free[i, ..., 0] = 1.0
         free[i, ..., 1] = d.ux_free / d.u_free
         free[i, ..., 2] = d.uy_free / d.u_free
-        free[i, ..., 3] = 1.0
+        free[i, ..., 3] = p.t_free / t_scale(p)
     report["freestream_errors"] = relative_errors(free, t[ho], m[ho])
     print(json.dumps({k: report[k] for k in ("train_errors", "holdout_errors",
                                              "freestream_errors")}), flush=True)

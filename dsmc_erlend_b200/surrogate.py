@@ -12,7 +12,7 @@ solver's fields).  Inputs (IN_CH channels, padded to 32): box mask, x and y
 of the cell centre, Mach / 8, cos and sin of the angle, log10(n) - 17, the
 wall model as three indicators, the CLL coefficients, box width and height /
 6.  Outputs (4 of 32 channels): n / NFree, ux / UFree, uy / UFree,
-T / TFree.
+T / (TFree (1 + Ma^2 / 3)) (the stagnation temperature, gamma = 5/3).
 """
 from __future__ import annotations
 

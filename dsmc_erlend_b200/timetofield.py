@@ -44,7 +44,7 @@ def reference_field(p, replicas_n: int, transient: int, steps: int, seed: int = 
 
 def time_to_field(p, ref: dict, start: str, predicted: dict | None = None,
                   first_sampling_step: int = 0, tol: float = 0.02, check_every: int = 250,
-                  max_steps: int = 200000) -> dict:
+                  max_steps: int = 200000, tensor: bool = False) -> dict:
     """Runs one case from `start` ("cold" or "warm") with sampling after
     `first_sampling_step`, checking the sampled field every `check_every`
     steps; returns the steps and the wall time of the run itself (start and
@@ -55,7 +55,7 @@ def time_to_field(p, ref: dict, start: str, predicted: dict | None = None,
     eng = Engine(q)
     t0 = time.perf_counter()
     if start == "warm":
-        eng.init_warm(warm_input(predicted))
+        eng.init_warm(warm_input(predicted, tensor=tensor))
     else:
         eng.InitialConditions()
     eng.synchronize()

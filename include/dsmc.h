@@ -218,6 +218,11 @@ int dsmc_init_cold(dsmc_ctx *ctx);
  * start from zero as after InitialConditions.  DSMC_ERR_CAPACITY when a
  * case's particles exceed its capacity. */
 int dsmc_init_warm(dsmc_ctx *ctx, const double *host_field);
+/* The same from 7 doubles per cell: n, ux, uy and the temperature tensor
+ * Txx, Tyy, Tzz, Txy [K] (m <(v - u)(v - u)> / k, as Printing's Tx, Ty and
+ * the moments give it): the velocities are Gaussians with that covariance,
+ * which keeps the anisotropy of shock layers and wakes. */
+int dsmc_init_warm_tensor(dsmc_ctx *ctx, const double *host_field);
 
 /* Runs n_steps complete time steps (Simulation.cpp:138-199) for every case:
  * move, boundary conditions, indexing, collisions, sampling.  Launched as
