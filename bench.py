@@ -51,8 +51,10 @@ CELL_BYTES = {"k_sample": 2 * 13 * 8 + 4}
 
 # DRAM bytes per particle (read + write) of each kernel from one ncu capture
 # of the same kernels on the 640x640 case (8.1e6 particles, FP32), scaled by
-# the particles of a launch.
-NCU_TRAFFIC_PER_PARTICLE = {}
+# the particles of a launch (profiles/*_640_case_ncu.md).  Below the
+# algorithmic bytes because part of the written state is still in the 126 MB
+# L2 when the kernel ends.
+NCU_TRAFFIC_PER_PARTICLE = {"k_scatter": 37.4, "k_move": 22.2, "k_sample": 19.7}
 
 
 def peaks():

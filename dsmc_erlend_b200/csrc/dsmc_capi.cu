@@ -201,7 +201,7 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_DEAD_SCAN);
-        k_dead_scan<<<c->ncase, SCAN_THREADS, 0, c->stream>>>(c->d_state, c->tile_dead,
+        k_dead_scan<<<c->ncase, SCAN_THREADS, SCAN_SMEM, c->stream>>>(c->d_state, c->tile_dead,
                                                               c->tile_dprefix, c->itile_dead,
                                                               c->itile_dprefix);
     }
@@ -238,7 +238,7 @@ template <class T> int enqueue_index(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_TILE_SCAN);
-        k_tile_scan<<<c->ncase, SCAN_THREADS, 0, c->stream>>>(c->d_state, c->tile_in,
+        k_tile_scan<<<c->ncase, SCAN_THREADS, SCAN_SMEM, c->stream>>>(c->d_state, c->tile_in,
                                                               c->tile_prefix);
     }
     {
@@ -511,6 +511,10 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
     occ(KID_SAMPLE, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_collide_select, 256, 0));
     occ(KID_COLLIDE_SELECT, b);
+    CK(cudaFuncSetAttribute(k_dead_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(SCAN_SMEM)));
+    CK(cudaFuncSetAttribute(k_tile_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(SCAN_SMEM)));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_olist, 256, 0));
     occ(KID_OLIST, b);
     c->ctas[KID_OLIST] = std::min(4, c->ctas_max[KID_OLIST]);

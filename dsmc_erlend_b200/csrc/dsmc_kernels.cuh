@@ -757,6 +757,54 @@ __global__ void __launch_bounds__(TILE_THREADS)
 // Threads of the one-CTA-per-case tile scans (k_dead_scan, k_tile_scan).
 constexpr int SCAN_THREADS = 1024;
 
+// Exclusive prefix (starting at carry) of n per-tile counts by one CTA of
+// SCAN_THREADS threads; returns carry plus the total.  Chunks of
+// SCAN_THREADS * SCAN_PER counts go through shared memory: loaded and stored
+// coalesced (thread t takes elements k * SCAN_THREADS + t), scanned as
+// SCAN_PER consecutive elements per thread; rows padded to SCAN_PER + 1 words
+// so that both access patterns are free of bank conflicts.  `buf` holds
+// SCAN_THREADS * (SCAN_PER + 1) words (dynamic shared memory).
+constexpr int SCAN_PER = 32;
+constexpr size_t SCAN_SMEM = sizeof(int32_t) * SCAN_THREADS * (SCAN_PER + 1);
+__device__ __forceinline__ int32_t cta_scan_counts(const int32_t *__restrict__ in,
+                                                   int32_t *__restrict__ out, int n,
+                                                   int32_t carry, int32_t *buf)
+{
+    constexpr int CHUNK = SCAN_THREADS * SCAN_PER;
+    auto at = [](int j) { return (j >> 5) * (SCAN_PER + 1) + (j & 31); };
+    for (int b = 0; b < n; b += CHUNK) {
+#pragma unroll 8
+        for (int k = 0; k < SCAN_PER; ++k) {
+            const int j = k * SCAN_THREADS + threadIdx.x;
+            buf[at(j)] = b + j < n ? in[b + j] : 0;
+        }
+        __syncthreads();
+        int32_t *row = buf + threadIdx.x * (SCAN_PER + 1);
+        int sum = 0;
+#pragma unroll
+        for (int m = 0; m < SCAN_PER; ++m)
+            sum += row[m];
+        int tot;
+        int run = carry + block_exclusive<int, SCAN_THREADS>(sum, tot);
+#pragma unroll
+        for (int m = 0; m < SCAN_PER; ++m) {
+            const int v = row[m];
+            row[m] = run;
+            run += v;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int k = 0; k < SCAN_PER; ++k) {
+            const int j = k * SCAN_THREADS + threadIdx.x;
+            if (b + j < n)
+                out[b + j] = buf[at(j)];
+        }
+        carry += tot;
+        __syncthreads();
+    }
+    return carry;
+}
+
 // k_dead_scan: per case (one CTA each), exclusive prefix of the removed-slot
 // counts of its move tiles, then of its inject tiles, in slot order; sets
 // dead_old and dead_total.
@@ -765,39 +813,18 @@ __global__ void __launch_bounds__(SCAN_THREADS)
     k_dead_scan(CaseState *st, const int32_t *tile_dead, int32_t *tile_dprefix,
                 const int32_t *itile_dead, int32_t *itile_dprefix)
 {
-    constexpr int PER = 8;
+    extern __shared__ int32_t scan_buf[];
     CaseState &s = st[blockIdx.x];
-    int32_t carry = 0;
-    for (int part = 0; part < 2; ++part) {
-        const int n = part == 0 ? s.n_move_tiles : s.n_inject_tiles;
-        const int t0 = part == 0 ? s.move_tile0 : s.inject_tile0;
-        const int32_t *in = (part == 0 ? tile_dead : itile_dead) + t0;
-        int32_t *out = (part == 0 ? tile_dprefix : itile_dprefix) + t0;
-        for (int b = 0; b < n; b += SCAN_THREADS * PER) {
-            const int i0 = b + threadIdx.x * PER;
-            int v[PER];
-            int sum = 0;
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                v[k] = i0 + k < n ? in[i0 + k] : 0;
-                sum += v[k];
-            }
-            int tot;
-            int run = carry + block_exclusive<int, SCAN_THREADS>(sum, tot);
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                if (i0 + k < n)
-                    out[i0 + k] = run;
-                run += v[k];
-            }
-            carry += tot;
-        }
-        if (threadIdx.x == 0) {
-            if (part == 0)
-                s.dead_old = carry;
-            else
-                s.dead_total = carry;
-        }
+    // The injected slots follow the old ones: their ranks continue the count.
+    const int32_t dead_old = cta_scan_counts(tile_dead + s.move_tile0,
+                                             tile_dprefix + s.move_tile0, s.n_move_tiles, 0,
+                                             scan_buf);
+    const int32_t dead_total = cta_scan_counts(itile_dead + s.inject_tile0,
+                                               itile_dprefix + s.inject_tile0,
+                                               s.n_inject_tiles, dead_old, scan_buf);
+    if (threadIdx.x == 0) {
+        s.dead_old = dead_old;
+        s.dead_total = dead_total;
     }
 }
 
@@ -854,24 +881,33 @@ __global__ void __launch_bounds__(TILE_THREADS)
 __global__ void k_plan2(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
                         const int32_t *hole_pos, int32_t *tmp, int ncase)
 {
-    for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
+    // One warp per case: a 33-way search (32 probes a round) for the number
+    // of removed slots below K (the holes); the list is in slot order.
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    for (int i = threadIdx.x >> 5; i < ncase; i += nwarps) {
         CaseState &s = st[i];
         const int64_t keep = s.n_total - s.dead_total; // dead_total: k_dead_scan
-        s.n_keep = keep;
-        // Holes are the removed slots below K; the list is in slot order.
         const int32_t *hp = hole_pos + cases[i].pbase;
-        int64_t lo = 0, hi = s.dead_total;
+        int64_t lo = 0, hi = s.dead_total; // first index with hp >= keep is in [lo, hi]
         while (lo < hi) {
-            const int64_t mid = (lo + hi) >> 1;
-            if (hp[mid] < keep)
-                lo = mid + 1;
-            else
-                hi = mid;
+            const int64_t span = hi - lo;
+            const int64_t idx = lo + ((lane + 1) * span) / 33; // < hi
+            const bool below = hp[idx] < keep;
+            const unsigned bl = __ballot_sync(0xffffffffu, below);
+            const int j = __popc(bl); // probes 0..j-1 are below (monotone)
+            const int64_t lo_n = j > 0 ? __shfl_sync(0xffffffffu, idx, j - 1) + 1 : lo;
+            const int64_t hi_n = j < 32 ? __shfl_sync(0xffffffffu, idx, j < 32 ? j : 31) : hi;
+            lo = lo_n;
+            hi = hi_n;
         }
-        s.n_holes = lo;
-        s.n_tail_tiles = static_cast<int32_t>((s.n_total - keep + TILE - 1) / TILE);
-        tmp[i] = s.n_tail_tiles;
-        tmp[ncase + i] = static_cast<int32_t>((keep + TILE - 1) / TILE);
+        if (lane == 0) {
+            s.n_keep = keep;
+            s.n_holes = lo;
+            s.n_tail_tiles = static_cast<int32_t>((s.n_total - keep + TILE - 1) / TILE);
+            tmp[i] = s.n_tail_tiles;
+            tmp[ncase + i] = static_cast<int32_t>((keep + TILE - 1) / TILE);
+        }
     }
     __syncthreads();
     case_scan(tt.tail0, tmp, ncase);
@@ -1037,31 +1073,10 @@ __global__ void __launch_bounds__(TILE_THREADS)
 __global__ void __launch_bounds__(SCAN_THREADS)
     k_tile_scan(const CaseState *st, const int32_t *tile_in, int32_t *tile_prefix)
 {
-    constexpr int PER = 8; // consecutive tiles per thread
+    extern __shared__ int32_t scan_buf[];
     const CaseState &s = st[blockIdx.x];
-    const int n = s.n_move_tiles;
-    const int32_t *in = tile_in + s.move_tile0;
-    int32_t *out = tile_prefix + s.move_tile0;
-    int32_t carry = 0;
-    for (int b = 0; b < n; b += SCAN_THREADS * PER) {
-        const int i0 = b + threadIdx.x * PER;
-        int v[PER];
-        int sum = 0;
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            v[k] = i0 + k < n ? in[i0 + k] : 0;
-            sum += v[k];
-        }
-        int tot;
-        int run = carry + block_exclusive<int, SCAN_THREADS>(sum, tot);
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            if (i0 + k < n)
-                out[i0 + k] = run;
-            run += v[k];
-        }
-        carry += tot;
-    }
+    cta_scan_counts(tile_in + s.move_tile0, tile_prefix + s.move_tile0, s.n_move_tiles, 0,
+                    scan_buf);
 }
 
 // ---------------------------------------------------------------------------
