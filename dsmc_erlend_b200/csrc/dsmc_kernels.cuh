@@ -405,14 +405,39 @@ static_assert(TILE_VEC * MOVE_WARPS == 32, "one warp scans the (iteration, warp)
 template <class T> struct MoveStage {
     T v[4][TILE]; // x, y, vx, vy
 };
-template <class T> __host__ __device__ constexpr int move_stages() { return sizeof(T) == 4 ? 3 : 2; }
+// Pipeline depths (build-time settings, -DDSMC_MOVE_STAGES=... etc.; the
+// defaults were chosen by measurement on B200).
+#ifndef DSMC_MOVE_STAGES
+#define DSMC_MOVE_STAGES 3
+#endif
+#ifndef DSMC_SCATTER_STAGES
+#define DSMC_SCATTER_STAGES 3
+#endif
+#ifndef DSMC_SAMPLE_STAGES
+#define DSMC_SAMPLE_STAGES 2
+#endif
+#ifndef DSMC_SAMPLE_UNROLL // unroll of k_sample's per-cell loop
+#define DSMC_SAMPLE_UNROLL 4
+#endif
+#ifndef DSMC_MOVE_MIN_BLOCKS // CTAs per SM k_move is compiled for (register budget)
+#define DSMC_MOVE_MIN_BLOCKS 4
+#endif
+// Two stages at least: a stage's flags and tile are rewritten by thread 0 after
+// the tile's barrier and read by the others one full iteration later, which
+// another barrier separates only when the next tile uses another stage.
+static_assert(DSMC_MOVE_STAGES >= 2 && DSMC_SCATTER_STAGES >= 2 && DSMC_SAMPLE_STAGES >= 2,
+              "the bulk-copy pipelines need two or more stages");
+template <class T> __host__ __device__ constexpr int move_stages()
+{
+    return sizeof(T) == 4 ? DSMC_MOVE_STAGES : 2;
+}
 template <class T> __host__ __device__ constexpr size_t move_smem()
 {
     return sizeof(MoveStage<T>) * move_stages<T>();
 }
 
 template <class T>
-__global__ void __launch_bounds__(TILE_THREADS, 4)
+__global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
     k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
            Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
            int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf,
@@ -1192,7 +1217,10 @@ template <class T> struct ScatterStage {
     uint32_t key[TILE];
     T v[5][TILE];
 };
-template <class T> __host__ __device__ constexpr int scatter_stages() { return sizeof(T) == 4 ? 3 : 2; }
+template <class T> __host__ __device__ constexpr int scatter_stages()
+{
+    return sizeof(T) == 4 ? DSMC_SCATTER_STAGES : 2;
+}
 template <class T> __host__ __device__ constexpr size_t scatter_smem()
 {
     return sizeof(ScatterStage<T>) * scatter_stages<T>();
@@ -1458,7 +1486,8 @@ __global__ void __launch_bounds__(128)
 // next blocks are in flight while the threads accumulate the current one.  A
 // block whose range exceeds a stage is read from global memory directly.
 // ---------------------------------------------------------------------------
-constexpr int SAMPLE_STAGES = 2;
+constexpr int SAMPLE_STAGES = DSMC_SAMPLE_STAGES;
+constexpr int SAMPLE_UNROLL = DSMC_SAMPLE_UNROLL;
 template <class T> __host__ __device__ constexpr int sample_pcl() { return 12288 / sizeof(T); }
 template <class T> struct SampleStage {
     T v[3][sample_pcl<T>() + 16 / sizeof(T)];
@@ -1552,6 +1581,10 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
                 vz = stage[sidx].v[2] + off;
             }
             if (mine && n > 0 && ok) {
+                // Unrolled so that the loads and products of the next
+                // particles overlap the adds of this one (the sums keep
+                // their order: only the adds into a[] chain).
+#pragma unroll SAMPLE_UNROLL
                 for (int i = 0; i < n; ++i) {
                     const double v0 = vx[i], v1 = vy[i], v2 = vz[i];
                     a[ACC_NP] += 1.0;

@@ -74,6 +74,33 @@ __device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const 
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
+// Eight bf16 (16 bytes) as floats.
+struct V8 {
+    float v[8];
+};
+__device__ __forceinline__ V8 ld8(const bf16 *p)
+{
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+    V8 r;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float2 f = __bfloat1622float2(h[i]);
+        r.v[2 * i] = f.x;
+        r.v[2 * i + 1] = f.y;
+    }
+    return r;
+}
+__device__ __forceinline__ void st8(bf16 *p, const V8 &r)
+{
+    uint4 u;
+    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        h[i] = __floats2bfloat162_rn(r.v[2 * i], r.v[2 * i + 1]);
+    *reinterpret_cast<uint4 *>(p) = u;
+}
+
 // ---------------------------------------------------------------------------
 // Forward (and dgrad): CTA tile 128 pixels x 64 output channels, k-tiles of
 // 32 input channels of one tap; 8 warps as 4 (pixels) x 2 (channels), each
@@ -314,105 +341,148 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// db[c] += sum over pixels of dy[pixel][c]: 256 threads = 8 pixel lanes x
-// 32 channels, a grid-stride over pixel chunks.
+// db[c] += sum over pixels of dy[pixel][c]: each thread sums one 8-channel
+// group over a strided set of pixels, the CTA reduces in shared memory and
+// adds with one atomic per channel.
 __global__ void k_bias_grad(const bf16 *__restrict__ dy, float *__restrict__ db, int M, int C)
 {
-    const int c = blockIdx.y * 32 + (threadIdx.x & 31);
-    const int lane_p = threadIdx.x >> 5;
-    float s = 0.0f;
-    if (c < C)
-        for (int p = blockIdx.x * 8 + lane_p; p < M; p += gridDim.x * 8)
-            s += __bfloat162float(dy[static_cast<int64_t>(p) * C + c]);
-    __shared__ float part[8][32];
-    part[lane_p][threadIdx.x & 31] = s;
+    const int c8 = C / 8;                 // channel groups (4..16)
+    const int lanes = blockDim.x / c8;    // pixel lanes of the CTA
+    const int g = threadIdx.x % c8, lp = threadIdx.x / c8;
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (lp < lanes)
+        for (int p = blockIdx.x * lanes + lp; p < M; p += gridDim.x * lanes) {
+            const V8 v = ld8(dy + static_cast<int64_t>(p) * C + 8 * g);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                s[k] += v.v[k];
+        }
+    __shared__ float part[256][9];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        part[threadIdx.x][k] = s[k];
     __syncthreads();
-    if (threadIdx.x < 32 && c < C) {
+    if (threadIdx.x < C) {
+        const int gg = threadIdx.x / 8, k = threadIdx.x % 8;
         float t = 0.0f;
-        for (int i = 0; i < 8; ++i)
-            t += part[i][threadIdx.x];
-        atomicAdd(db + c, t);
+        for (int l = 0; l < lanes; ++l)
+            t += part[l * c8 + gg][k];
+        atomicAdd(db + threadIdx.x, t);
     }
 }
 
 // ---------------------------------------------------------------------------
-// Elementwise kernels.
+// Elementwise kernels.  Channel counts are multiples of 32, so every kernel
+// moves 8 bf16 (16 bytes) per thread and step, never across a pixel.
 // ---------------------------------------------------------------------------
-__global__ void k_relu_bwd(bf16 *dy, const bf16 *y, int64_t n)
-{
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+// Grid-stride over n8 = count / 8 vectors.
+#define FOR_V8(n8)                                                                         \
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < (n8); \
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-        if (!(__bfloat162float(y[i]) > 0.0f))
-            dy[i] = __float2bfloat16(0.0f);
+
+__global__ void k_relu_bwd(bf16 *dy, const bf16 *y, int64_t n8)
+{
+    FOR_V8(n8)
+    {
+        V8 g = ld8(dy + 8 * i);
+        const V8 a = ld8(y + 8 * i);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            g.v[k] = a.v[k] > 0.0f ? g.v[k] : 0.0f;
+        st8(dy + 8 * i, g);
+    }
 }
 
+__global__ void k_add(bf16 *a, const bf16 *b, int64_t n8)
+{
+    FOR_V8(n8)
+    {
+        V8 x = ld8(a + 8 * i);
+        const V8 y = ld8(b + 8 * i);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            x.v[k] += y.v[k];
+        st8(a + 8 * i, x);
+    }
+}
+
+// Output vector i of (n, h/2, w/2, c): c8 = c / 8 vectors per pixel.
 __global__ void k_pool_fwd(const bf16 *x, bf16 *y, int N, int H, int W, int C)
 {
-    const int Ho = H / 2, Wo = W / 2;
-    const int64_t total = static_cast<int64_t>(N) * Ho * Wo * C;
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const int64_t pix = i / C;
+    const int c8 = C / 8, Ho = H / 2, Wo = W / 2;
+    const int64_t n8 = static_cast<int64_t>(N) * Ho * Wo * c8;
+    FOR_V8(n8)
+    {
+        const int cv = static_cast<int>(i % c8);
+        const int64_t pix = i / c8;
         const int wo = static_cast<int>(pix % Wo), ho = static_cast<int>((pix / Wo) % Ho);
         const int64_t n = pix / (static_cast<int64_t>(Wo) * Ho);
-        const int64_t b = ((n * H + 2 * ho) * W + 2 * wo) * C + c;
-        const float s = __bfloat162float(x[b]) + __bfloat162float(x[b + C]) +
-                        __bfloat162float(x[b + static_cast<int64_t>(W) * C]) +
-                        __bfloat162float(x[b + static_cast<int64_t>(W) * C + C]);
-        y[i] = __float2bfloat16(0.25f * s);
+        const bf16 *b = x + ((n * H + 2 * ho) * W + 2 * wo) * C + 8 * cv;
+        const int64_t row = static_cast<int64_t>(W) * C;
+        const V8 a = ld8(b), bb = ld8(b + C), cc = ld8(b + row), dd = ld8(b + row + C);
+        V8 r;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            r.v[k] = 0.25f * (a.v[k] + bb.v[k] + cc.v[k] + dd.v[k]);
+        st8(y + 8 * i, r);
     }
 }
 
+// Input-gradient vector i of (n, h, w, c).
 __global__ void k_pool_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
 {
-    const int64_t total = static_cast<int64_t>(N) * H * W * C;
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const int64_t pix = i / C;
+    const int c8 = C / 8;
+    const int64_t n8 = static_cast<int64_t>(N) * H * W * c8;
+    FOR_V8(n8)
+    {
+        const int cv = static_cast<int>(i % c8);
+        const int64_t pix = i / c8;
         const int w = static_cast<int>(pix % W), h = static_cast<int>((pix / W) % H);
         const int64_t n = pix / (static_cast<int64_t>(W) * H);
-        const int64_t o = ((n * (H / 2) + h / 2) * (W / 2) + w / 2) * C + c;
-        dx[i] = __float2bfloat16(0.25f * __bfloat162float(dy[o]));
+        V8 g = ld8(dy + ((n * (H / 2) + h / 2) * (W / 2) + w / 2) * C + 8 * cv);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            g.v[k] *= 0.25f;
+        st8(dx + 8 * i, g);
     }
 }
 
-// (n, h, w, c) -> (n, 2h, 2w, c), nearest.
+// (n, h, w, c) -> (n, 2h, 2w, c), nearest: output vector i.
 __global__ void k_up_fwd(const bf16 *x, bf16 *y, int N, int H, int W, int C)
 {
-    const int64_t total = static_cast<int64_t>(N) * 4 * H * W * C;
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const int64_t pix = i / C;
+    const int c8 = C / 8;
+    const int64_t n8 = static_cast<int64_t>(N) * 4 * H * W * c8;
+    FOR_V8(n8)
+    {
+        const int cv = static_cast<int>(i % c8);
+        const int64_t pix = i / c8;
         const int w2 = static_cast<int>(pix % (2 * W)), h2 = static_cast<int>((pix / (2 * W)) % (2 * H));
         const int64_t n = pix / (4 * static_cast<int64_t>(W) * H);
-        y[i] = x[((n * H + h2 / 2) * W + w2 / 2) * C + c];
+        *reinterpret_cast<uint4 *>(y + 8 * i) = *reinterpret_cast<const uint4 *>(
+            x + ((n * H + h2 / 2) * W + w2 / 2) * C + 8 * cv);
     }
 }
 
+// Input-gradient vector i of (n, h, w, c) from dy of (n, 2h, 2w, c).
 __global__ void k_up_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
 {
-    const int64_t total = static_cast<int64_t>(N) * H * W * C;
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int c = static_cast<int>(i % C);
-        const int64_t pix = i / C;
+    const int c8 = C / 8;
+    const int64_t n8 = static_cast<int64_t>(N) * H * W * c8;
+    FOR_V8(n8)
+    {
+        const int cv = static_cast<int>(i % c8);
+        const int64_t pix = i / c8;
         const int w = static_cast<int>(pix % W), h = static_cast<int>((pix / W) % H);
         const int64_t n = pix / (static_cast<int64_t>(W) * H);
-        const int64_t b = ((n * 2 * H + 2 * h) * (2 * W) + 2 * w) * C + c;
+        const bf16 *b = dy + ((n * 2 * H + 2 * h) * (2 * W) + 2 * w) * C + 8 * cv;
         const int64_t row = 2 * static_cast<int64_t>(W) * C;
-        dx[i] = __float2bfloat16(__bfloat162float(dy[b]) + __bfloat162float(dy[b + C]) +
-                                 __bfloat162float(dy[b + row]) + __bfloat162float(dy[b + row + C]));
+        const V8 a = ld8(b), bb = ld8(b + C), cc = ld8(b + row), dd = ld8(b + row + C);
+        V8 r;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            r.v[k] = a.v[k] + bb.v[k] + cc.v[k] + dd.v[k];
+        st8(dx + 8 * i, r);
     }
-}
-
-__global__ void k_add(bf16 *a, const bf16 *b, int64_t n)
-{
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-        a[i] = __float2bfloat16(__bfloat162float(a[i]) + __bfloat162float(b[i]));
 }
 
 __global__ void k_mask_sum(const float *mask, int64_t n, float *sum)
@@ -519,7 +589,7 @@ int dsmc_sg_conv_dgrad(const uint16_t *dy, const uint16_t *w, uint16_t *w_rot, u
 int dsmc_sg_conv_wgrad(const uint16_t *dy, const uint16_t *x, float *dw, float *db, int n, int h,
                        int w_, int cin, int cout, void *stream)
 {
-    if (!dy || !x || !dw || !conv_shape_ok(n, h, w_, cin, cout))
+    if (!dy || !x || !dw || !conv_shape_ok(n, h, w_, cin, cout) || (db && cout > 256))
         return ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int M = n * h * w_;
@@ -536,8 +606,7 @@ int dsmc_sg_conv_wgrad(const uint16_t *dy, const uint16_t *x, float *dw, float *
                                       reinterpret_cast<const bf16 *>(x), dw, n, h, w_, cin, cout,
                                       per);
     if (db) {
-        dim3 gb(256, (cout + 31) / 32);
-        k_bias_grad<<<gb, 256, 0, s>>>(reinterpret_cast<const bf16 *>(dy), db, M, cout);
+        k_bias_grad<<<512, 256, 0, s>>>(reinterpret_cast<const bf16 *>(dy), db, M, cout);
     }
     return status();
 }
@@ -546,43 +615,45 @@ int dsmc_sg_relu_bwd(uint16_t *dy, const uint16_t *y, int64_t count, void *strea
 {
     if (!dy || !y || count < 0)
         return ERR_ARG;
-    k_relu_bwd<<<grid_for(count), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<bf16 *>(dy), reinterpret_cast<const bf16 *>(y), count);
+    if (count % 8)
+        return ERR_ARG;
+    k_relu_bwd<<<grid_for(count / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<bf16 *>(dy), reinterpret_cast<const bf16 *>(y), count / 8);
     return status();
 }
 
 int dsmc_sg_pool_fwd(const uint16_t *x, uint16_t *y, int n, int h, int w_, int c, void *stream)
 {
-    if (!x || !y || n <= 0 || h <= 0 || w_ <= 0 || c <= 0 || h % 2 || w_ % 2)
+    if (!x || !y || n <= 0 || h <= 0 || w_ <= 0 || c <= 0 || h % 2 || w_ % 2 || c % 8)
         return ERR_ARG;
-    k_pool_fwd<<<grid_for(int64_t(n) * h * w_ * c / 4), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    k_pool_fwd<<<grid_for(int64_t(n) * h * w_ * c / 32), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         reinterpret_cast<const bf16 *>(x), reinterpret_cast<bf16 *>(y), n, h, w_, c);
     return status();
 }
 
 int dsmc_sg_pool_bwd(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c, void *stream)
 {
-    if (!dy || !dx || n <= 0 || h <= 0 || w_ <= 0 || c <= 0 || h % 2 || w_ % 2)
+    if (!dy || !dx || n <= 0 || h <= 0 || w_ <= 0 || c <= 0 || h % 2 || w_ % 2 || c % 8)
         return ERR_ARG;
-    k_pool_bwd<<<grid_for(int64_t(n) * h * w_ * c), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    k_pool_bwd<<<grid_for(int64_t(n) * h * w_ * c / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         reinterpret_cast<const bf16 *>(dy), reinterpret_cast<bf16 *>(dx), n, h, w_, c);
     return status();
 }
 
 int dsmc_sg_up_fwd(const uint16_t *x, uint16_t *y, int n, int h, int w_, int c, void *stream)
 {
-    if (!x || !y || n <= 0 || h <= 0 || w_ <= 0 || c <= 0)
+    if (!x || !y || n <= 0 || h <= 0 || w_ <= 0 || c <= 0 || c % 8)
         return ERR_ARG;
-    k_up_fwd<<<grid_for(int64_t(n) * 4 * h * w_ * c), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    k_up_fwd<<<grid_for(int64_t(n) * 4 * h * w_ * c / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         reinterpret_cast<const bf16 *>(x), reinterpret_cast<bf16 *>(y), n, h, w_, c);
     return status();
 }
 
 int dsmc_sg_up_bwd(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c, void *stream)
 {
-    if (!dy || !dx || n <= 0 || h <= 0 || w_ <= 0 || c <= 0)
+    if (!dy || !dx || n <= 0 || h <= 0 || w_ <= 0 || c <= 0 || c % 8)
         return ERR_ARG;
-    k_up_bwd<<<grid_for(int64_t(n) * h * w_ * c), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    k_up_bwd<<<grid_for(int64_t(n) * h * w_ * c / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         reinterpret_cast<const bf16 *>(dy), reinterpret_cast<bf16 *>(dx), n, h, w_, c);
     return status();
 }
@@ -591,8 +662,10 @@ int dsmc_sg_add(uint16_t *a, const uint16_t *b, int64_t count, void *stream)
 {
     if (!a || !b || count < 0)
         return ERR_ARG;
-    k_add<<<grid_for(count), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<bf16 *>(a), reinterpret_cast<const bf16 *>(b), count);
+    if (count % 8)
+        return ERR_ARG;
+    k_add<<<grid_for(count / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<bf16 *>(a), reinterpret_cast<const bf16 *>(b), count / 8);
     return status();
 }
 

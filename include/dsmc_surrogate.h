@@ -33,7 +33,8 @@ int dsmc_sg_conv_dgrad(const uint16_t *dy, const uint16_t *w, uint16_t *w_rot, u
                        int n, int h, int w_, int cin, int cout, void *stream);
 
 /* dw += sum over pixels of dy (x) shifted x, FP32 [Cout][3][3][Cin];
- * db += sum over pixels of dy (db may be NULL).  Accumulates: clear first. */
+ * db += sum over pixels of dy (db may be NULL; cout <= 256 with db).
+ * Accumulates: clear first. */
 int dsmc_sg_conv_wgrad(const uint16_t *dy, const uint16_t *x, float *dw, float *db, int n,
                        int h, int w_, int cin, int cout, void *stream);
 
