@@ -255,7 +255,7 @@ template <class T> int enqueue_index(dsmc_ctx *c)
     }
     {
         Span sp(c, KID_SCATTER);
-        k_scatter<T><<<grid(c, KID_SCATTER), TILE_THREADS, scatter_smem<T>(), c->stream>>>(
+        k_scatter<T><<<grid(c, KID_SCATTER), SC_THREADS, scatter_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->tt, slots<T>(c, side), slots<T>(c, side ^ 1), c->key,
             c->cells, c->tile_prefix, c->ncase, c->d_err);
     }
@@ -501,7 +501,7 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
     occ(KID_HOLES, b);
     CK(cudaFuncSetAttribute(k_scatter<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(scatter_smem<T>())));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, TILE_THREADS,
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, SC_THREADS,
                                                      scatter_smem<T>()));
     occ(KID_SCATTER, b);
     CK(cudaFuncSetAttribute(k_sample<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -1208,15 +1208,25 @@ __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *s
 // Tiles are staged whole in shared memory by bulk asynchronous copies, SCATTER
 // stages deep: while the warps place tile i, the copies of the next tiles of
 // this CTA are in flight, so the kernel keeps HBM busy without holding the
-// loads in registers.  Iteration k of thread t takes slot k * TILE_THREADS + t
-// of the tile, so the 32 lanes of a warp store 32 consecutive destinations
-// when they share a cell.  One barrier per tile: it publishes the in-range
+// loads in registers.  Iteration k of thread t takes slot k * SC_THREADS + t
+// of the tile (SC_THREADS threads, SC_VEC slots each), so the 32 lanes of a
+// warp store 32 consecutive destinations when they share a cell.  One
+// barrier per tile: it publishes the in-range
 // counts of the (iteration, warp) chunks and frees the stage for its refill.
 // ---------------------------------------------------------------------------
 template <class T> struct ScatterStage {
     uint32_t key[TILE];
     T v[5][TILE];
 };
+// Threads of a k_scatter CTA: each takes TILE / SC_THREADS slots of a tile.
+#ifndef DSMC_SCATTER_THREADS
+#define DSMC_SCATTER_THREADS 256
+#endif
+constexpr int SC_THREADS = DSMC_SCATTER_THREADS;
+constexpr int SC_VEC = TILE / SC_THREADS;
+constexpr int SC_WARPS = SC_THREADS / 32;
+static_assert(SC_VEC * SC_WARPS == 32, "one warp scans the (iteration, warp) chunk counts");
+
 template <class T> __host__ __device__ constexpr int scatter_stages()
 {
     return sizeof(T) == 4 ? DSMC_SCATTER_STAGES : 2;
@@ -1227,7 +1237,7 @@ template <class T> __host__ __device__ constexpr size_t scatter_smem()
 }
 
 template <class T>
-__global__ void __launch_bounds__(TILE_THREADS)
+__global__ void __launch_bounds__(SC_THREADS)
     k_scatter(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt,
               Slots<T> src, Slots<T> dst, const uint32_t *__restrict__ key, Cells cells,
               const int32_t *__restrict__ tile_prefix, int ncase, int *err)
@@ -1278,12 +1288,12 @@ __global__ void __launch_bounds__(TILE_THREADS)
         const int64_t keep = s.n_keep;
         const ScatterStage<T> &sg = stage[sidx];
         const int64_t tile0 = static_cast<int64_t>(local_tile) * TILE;
-        uint32_t keys[TILE_VEC];
-        T x[TILE_VEC], y[TILE_VEC], vx[TILE_VEC], vy[TILE_VEC], vz[TILE_VEC];
-        unsigned bin[TILE_VEC];
+        uint32_t keys[SC_VEC];
+        T x[SC_VEC], y[SC_VEC], vx[SC_VEC], vy[SC_VEC], vz[SC_VEC];
+        unsigned bin[SC_VEC];
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            const int e = k * TILE_THREADS + threadIdx.x;
+        for (int k = 0; k < SC_VEC; ++k) {
+            const int e = k * SC_THREADS + threadIdx.x;
             keys[k] = (ok && tile0 + e < keep) ? sg.key[e] : KEY_DEAD;
             x[k] = sg.v[0][e];
             y[k] = sg.v[1][e];
@@ -1292,7 +1302,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
             vz[k] = sg.v[4][e];
             bin[k] = __ballot_sync(0xffffffffu, (keys[k] & KEY_IN) != 0);
             if (lane == 0)
-                s_cnt[it & 1][k * MOVE_WARPS + warp] = __popc(bin[k]);
+                s_cnt[it & 1][k * SC_WARPS + warp] = __popc(bin[k]);
         }
         // Every thread has copied its part of the stage into registers.
         if (__syncthreads_or(!ok)) {
@@ -1320,10 +1330,10 @@ __global__ void __launch_bounds__(TILE_THREADS)
         const int cexcl = cinc - cnt;
         const int tile_total = __shfl_sync(0xffffffffu, cinc, 31);
         const int64_t base = tile_total > 0 ? tile_prefix[s.move_tile0 + local_tile] : 0;
-        int64_t fin[TILE_VEC];
+        int64_t fin[SC_VEC];
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            const int pre = __shfl_sync(0xffffffffu, cexcl, k * MOVE_WARPS + warp);
+        for (int k = 0; k < SC_VEC; ++k) {
+            const int pre = __shfl_sync(0xffffffffu, cexcl, k * SC_WARPS + warp);
             if (keys[k] & KEY_DEAD)
                 fin[k] = -1;
             else if (keys[k] & KEY_IN)
@@ -1333,7 +1343,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
                 fin[k] = keys[k];
         }
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
+        for (int k = 0; k < SC_VEC; ++k) {
             if (keys[k] & KEY_DEAD)
                 continue;
             if (fin[k] < 0 || fin[k] >= keep) {
