@@ -414,7 +414,7 @@ template <class T> struct MoveStage {
 #define DSMC_SCATTER_STAGES 3
 #endif
 #ifndef DSMC_SAMPLE_STAGES
-#define DSMC_SAMPLE_STAGES 2
+#define DSMC_SAMPLE_STAGES 1
 #endif
 #ifndef DSMC_SAMPLE_UNROLL // unroll of k_sample's per-cell loop
 #define DSMC_SAMPLE_UNROLL 4
@@ -422,11 +422,12 @@ template <class T> struct MoveStage {
 #ifndef DSMC_MOVE_MIN_BLOCKS // CTAs per SM k_move is compiled for (register budget)
 #define DSMC_MOVE_MIN_BLOCKS 4
 #endif
-// Two stages at least: a stage's flags and tile are rewritten by thread 0 after
-// the tile's barrier and read by the others one full iteration later, which
-// another barrier separates only when the next tile uses another stage.
-static_assert(DSMC_MOVE_STAGES >= 2 && DSMC_SCATTER_STAGES >= 2 && DSMC_SAMPLE_STAGES >= 2,
-              "the bulk-copy pipelines need two or more stages");
+// k_move and k_scatter need two stages at least: a stage's tile is rewritten
+// by thread 0 after the tile's barrier and read by the others one full
+// iteration later, which another barrier separates only when the next tile
+// uses another stage.  k_sample adds that barrier when it runs one stage.
+static_assert(DSMC_MOVE_STAGES >= 2 && DSMC_SCATTER_STAGES >= 2 && DSMC_SAMPLE_STAGES >= 1,
+              "the tile pipelines need two or more stages");
 template <class T> __host__ __device__ constexpr int move_stages()
 {
     return sizeof(T) == 4 ? DSMC_MOVE_STAGES : 2;
@@ -1491,10 +1492,10 @@ __global__ void __launch_bounds__(128)
 // k_sample: Sampling's accumulation (Sampling.cpp:14-31) in the reference's
 // order: one thread per cell walks its particles sequentially, so every FP64
 // sum is bit-identical to the reference's.  The velocities of a block of
-// COLLIDE_CELLS cells are one contiguous slot range; bulk asynchronous copies
-// stage it in shared memory, SAMPLE_STAGES blocks ahead, so the loads of the
-// next blocks are in flight while the threads accumulate the current one.  A
-// block whose range exceeds a stage is read from global memory directly.
+// COLLIDE_CELLS cells are one contiguous slot range, staged in shared memory
+// by bulk asynchronous copies (SAMPLE_STAGES per CTA; with one stage, which
+// measured fastest, more CTAs fit on an SM and overlap each other's copies).
+// A block whose range exceeds a stage is read from global memory directly.
 // ---------------------------------------------------------------------------
 constexpr int SAMPLE_STAGES = DSMC_SAMPLE_STAGES;
 constexpr int SAMPLE_UNROLL = DSMC_SAMPLE_UNROLL;
@@ -1634,6 +1635,8 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
             if (bn < nblocks)
                 issue(bn, sidx);
         }
+        if (S == 1) // the next block reads this stage's flags: publish them first
+            __syncthreads();
     }
 }
 
