@@ -1508,6 +1508,47 @@ template <class T> __host__ __device__ constexpr size_t sample_smem()
     return sizeof(SampleStage<T>) * SAMPLE_STAGES;
 }
 
+// One particle's terms of the moment sums, in Sampling.cpp:24-30's order.
+// FP64 velocities: products rounded, then added.
+__device__ __forceinline__ void sample_add(double a[ACC_NC], double v0, double v1, double v2)
+{
+    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
+    a[ACC_V0] += v0;
+    a[ACC_V1] += v1;
+    a[ACC_V2] += v2;
+    a[ACC_V2V0] += vv * v0;
+    a[ACC_V2V1] += vv * v1;
+    a[ACC_V2V2] += vv * v2;
+    a[ACC_VV00] += v0 * v0;
+    a[ACC_VV01] += v0 * v1;
+    a[ACC_VV02] += v0 * v2;
+    a[ACC_VV11] += v1 * v1;
+    a[ACC_VV12] += v1 * v2;
+    a[ACC_VV22] += v2 * v2;
+}
+// FP32 velocities: the product of two floats is exact in FP64 (24 + 24
+// significand bits), so s + u * v rounds once either way and a fused
+// multiply-add gives the same bits as the separate product and sum, with one
+// FP64 operation instead of two.  vv * v is not exact and keeps its rounding.
+__device__ __forceinline__ void sample_add(double a[ACC_NC], float f0, float f1, float f2)
+{
+    const double v0 = f0, v1 = f1, v2 = f2;
+    const double p00 = v0 * v0;
+    const double vv = __fma_rn(v2, v2, __fma_rn(v1, v1, p00));
+    a[ACC_V0] += v0;
+    a[ACC_V1] += v1;
+    a[ACC_V2] += v2;
+    a[ACC_V2V0] += vv * v0;
+    a[ACC_V2V1] += vv * v1;
+    a[ACC_V2V2] += vv * v2;
+    a[ACC_VV00] += p00;
+    a[ACC_VV01] = __fma_rn(v0, v1, a[ACC_VV01]);
+    a[ACC_VV02] = __fma_rn(v0, v2, a[ACC_VV02]);
+    a[ACC_VV11] = __fma_rn(v1, v1, a[ACC_VV11]);
+    a[ACC_VV12] = __fma_rn(v1, v2, a[ACC_VV12]);
+    a[ACC_VV22] = __fma_rn(v2, v2, a[ACC_VV22]);
+}
+
 template <class T>
 __global__ void __launch_bounds__(COLLIDE_CELLS)
     k_sample(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt, Slots<T> p,
@@ -1592,27 +1633,14 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
                 vz = stage[sidx].v[2] + off;
             }
             if (mine && n > 0 && ok) {
+                // The count is a sum of n ones: exact, so one add of n.
+                a[ACC_NP] += static_cast<double>(n);
                 // Unrolled so that the loads and products of the next
                 // particles overlap the adds of this one (the sums keep
                 // their order: only the adds into a[] chain).
 #pragma unroll SAMPLE_UNROLL
-                for (int i = 0; i < n; ++i) {
-                    const double v0 = vx[i], v1 = vy[i], v2 = vz[i];
-                    a[ACC_NP] += 1.0;
-                    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
-                    a[ACC_V0] += v0;
-                    a[ACC_V1] += v1;
-                    a[ACC_V2] += v2;
-                    a[ACC_V2V0] += vv * v0;
-                    a[ACC_V2V1] += vv * v1;
-                    a[ACC_V2V2] += vv * v2;
-                    a[ACC_VV00] += v0 * v0;
-                    a[ACC_VV01] += v0 * v1;
-                    a[ACC_VV02] += v0 * v2;
-                    a[ACC_VV11] += v1 * v1;
-                    a[ACC_VV12] += v1 * v2;
-                    a[ACC_VV22] += v2 * v2;
-                }
+                for (int i = 0; i < n; ++i)
+                    sample_add(a, vx[i], vy[i], vz[i]);
 #pragma unroll
                 for (int m = 0; m < ACC_NC; ++m)
                     cells.acc[m * cells.acc_stride + cg] = a[m];
