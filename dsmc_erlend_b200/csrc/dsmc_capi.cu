@@ -53,6 +53,11 @@ struct dsmc_ctx {
     int sms = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // The step graph's second branch: kernels that depend on neither
+    // neighbour on the main stream run there (captured only, see `par`).
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t branch_ev[6] = {nullptr};
+    bool par = false; // true while the full step is captured into a graph
     int ncase = 0;
     int precision = DSMC_FP64;
     std::vector<dsmc_params> params;
@@ -163,6 +168,49 @@ int clear_step_scratch(dsmc_ctx *c)
     return DSMC_OK;
 }
 
+// Branch points of the step graph.  Captured into the graph (never run
+// eagerly), the side stream holds kernels whose inputs and outputs are
+// disjoint from those of the main-stream kernels they overlap:
+//   k_inject         || k_move, k_move_near   (slots [n_old, n_total) against
+//                       [0, n_old); commutative cell counters; the
+//                       out-of-range list is ordered by slot later)
+//   k_tile_scan      || k_cell_scan, k_olist, k_cell_fix (tile counts only)
+//   k_collide_select || k_olist, k_cell_fix, k_scatter (the new cell starts,
+//                       final after k_cell_scan; no particle data)
+enum { EV_PLAN, EV_INJECT, EV_TAIL, EV_TILE_SCAN, EV_CELL_SCAN, EV_SELECT };
+
+// `to` waits for what `from` has enqueued so far (event `ev`).
+int branch(dsmc_ctx *c, int ev, cudaStream_t from, cudaStream_t to)
+{
+    CK(cudaEventRecord(c->branch_ev[ev], from));
+    CK(cudaStreamWaitEvent(to, c->branch_ev[ev], 0));
+    return DSMC_OK;
+}
+
+template <class T> void launch_inject(dsmc_ctx *c, cudaStream_t stream)
+{
+    Span sp(c, KID_INJECT);
+    k_inject<T><<<grid(c, KID_INJECT), TILE_THREADS, 0, stream>>>(
+        c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
+        c->itile_dead, c->obuf, c->ncase, c->d_err);
+}
+
+void launch_tile_scan(dsmc_ctx *c, cudaStream_t stream)
+{
+    Span sp(c, KID_TILE_SCAN);
+    k_tile_scan<<<c->ncase, SCAN_THREADS, SCAN_SMEM, stream>>>(c->d_state, c->tile_in,
+                                                            c->tile_prefix);
+}
+
+// `side`: the buffer that holds the sorted particles of this step.
+void launch_collide_select(dsmc_ctx *c, int side, cudaStream_t stream)
+{
+    Span sp(c, KID_COLLIDE_SELECT);
+    k_collide_select<<<grid(c, KID_COLLIDE_SELECT), 256, 0, stream>>>(
+        c->d_cases, c->d_state, c->d_scratch, c->tt, c->cells, side, c->coll_list,
+        c->total_cells, c->ncase);
+}
+
 // MoveParticles: plan + move.
 template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
 {
@@ -173,6 +221,12 @@ template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
         Span sp(c, KID_PLAN);
         k_plan<<<1, 1024, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch, c->tt, c->d_tmp,
                                           c->ncase, init_mode, c->d_err);
+    }
+    if (!init_mode && c->par) {
+        if ((s = branch(c, EV_PLAN, c->stream, c->side_stream)))
+            return s;
+        launch_inject<T>(c, c->side_stream);
+        CK(cudaEventRecord(c->branch_ev[EV_INJECT], c->side_stream));
     }
     if (!init_mode) {
         Span sp(c, KID_MOVE);
@@ -193,12 +247,10 @@ template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
 // BoundaryConditions: inflow strips, then the swap-with-last removal.
 template <class T> int enqueue_boundary(dsmc_ctx *c)
 {
-    {
-        Span sp(c, KID_INJECT);
-        k_inject<T><<<grid(c, KID_INJECT), TILE_THREADS, 0, c->stream>>>(
-            c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
-            c->itile_dead, c->obuf, c->ncase, c->d_err);
-    }
+    if (c->par) // launched on the side stream by enqueue_move
+        CK(cudaStreamWaitEvent(c->stream, c->branch_ev[EV_INJECT], 0));
+    else
+        launch_inject<T>(c, c->stream);
     {
         Span sp(c, KID_DEAD_SCAN);
         k_dead_scan<<<c->ncase, SCAN_THREADS, SCAN_SMEM, c->stream>>>(c->d_state, c->tile_dead,
@@ -230,16 +282,26 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
 template <class T> int enqueue_index(dsmc_ctx *c)
 {
     const int side = c->cur;
+    int s;
+    if (c->par) {
+        if ((s = branch(c, EV_TAIL, c->stream, c->side_stream)))
+            return s;
+        launch_tile_scan(c, c->side_stream);
+        CK(cudaEventRecord(c->branch_ev[EV_TILE_SCAN], c->side_stream));
+    }
     {
         Span sp(c, KID_CELL_SCAN);
         k_cell_scan<<<grid(c, KID_CELL_SCAN), TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_scratch, c->tt, c->cells, side ^ 1, lb_chain(c, 3), c->ncase,
             c->d_err);
     }
-    {
-        Span sp(c, KID_TILE_SCAN);
-        k_tile_scan<<<c->ncase, SCAN_THREADS, SCAN_SMEM, c->stream>>>(c->d_state, c->tile_in,
-                                                              c->tile_prefix);
+    if (c->par) {
+        if ((s = branch(c, EV_CELL_SCAN, c->stream, c->side_stream)))
+            return s;
+        launch_collide_select(c, side ^ 1, c->side_stream);
+        CK(cudaEventRecord(c->branch_ev[EV_SELECT], c->side_stream));
+    } else {
+        launch_tile_scan(c, c->stream);
     }
     {
         Span sp(c, KID_OLIST);
@@ -253,6 +315,8 @@ template <class T> int enqueue_index(dsmc_ctx *c)
                                                              c->cells, side, c->key, c->olist,
                                                              c->total_cells, c->ncase, c->d_err);
     }
+    if (c->par)
+        CK(cudaStreamWaitEvent(c->stream, c->branch_ev[EV_TILE_SCAN], 0));
     {
         Span sp(c, KID_SCATTER);
         k_scatter<T><<<grid(c, KID_SCATTER), SC_THREADS, scatter_smem<T>(), c->stream>>>(
@@ -267,12 +331,10 @@ template <class T> int enqueue_index(dsmc_ctx *c)
 template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sample)
 {
     if (do_collide) {
-        {
-            Span sp(c, KID_COLLIDE_SELECT);
-            k_collide_select<<<grid(c, KID_COLLIDE_SELECT), 256, 0, c->stream>>>(
-                c->d_cases, c->d_state, c->d_scratch, c->tt, c->cells, c->cur, c->coll_list,
-                c->total_cells, c->ncase);
-        }
+        if (c->par) // launched on the side stream by enqueue_index
+            CK(cudaStreamWaitEvent(c->stream, c->branch_ev[EV_SELECT], 0));
+        else
+            launch_collide_select(c, c->cur, c->stream);
         {
             Span sp(c, KID_COLLIDE);
             k_collide_pairs<T><<<2 * c->sms, 128, 0, c->stream>>>(
@@ -320,12 +382,19 @@ int dispatch_step(dsmc_ctx *c)
 
 int build_graphs(dsmc_ctx *c)
 {
+    if (c->side_stream == nullptr) {
+        CK(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
+        for (auto &e : c->branch_ev)
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     for (int side = 0; side < 2; ++side) {
         const int saved = c->cur;
         c->cur = side;
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->par = true;
         const int s = dispatch_step(c);
+        c->par = false;
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         c->cur = saved;
         if (s)
@@ -529,6 +598,11 @@ void free_ctx(dsmc_ctx *c)
     for (auto &g : c->graph)
         if (g)
             cudaGraphExecDestroy(g);
+    for (auto e : c->branch_ev)
+        if (e)
+            cudaEventDestroy(e);
+    if (c->side_stream)
+        cudaStreamDestroy(c->side_stream);
     for (auto &t : c->timed) {
         cudaEventDestroy(t.a);
         cudaEventDestroy(t.b);
