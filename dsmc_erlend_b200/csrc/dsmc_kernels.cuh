@@ -60,6 +60,13 @@ struct Cells {
     int64_t acc_stride;  // elements per moment array
 };
 
+// The start offsets of buffer `side`.  A select, not an index: indexing the
+// kernel parameter with a run-time value would copy it to local memory.
+__device__ __forceinline__ int32_t *start_of(const Cells &c, int side)
+{
+    return side ? c.start[1] : c.start[0];
+}
+
 // Moments kept per cell.  The reference's CELL (include/Cell.h:4-10) holds
 // CountVV as a 3x3 tensor; it is symmetric and stored once here.
 enum : int {
@@ -799,11 +806,16 @@ __device__ __forceinline__ int32_t cta_scan_counts(const int32_t *__restrict__ i
     constexpr int CHUNK = SCAN_THREADS * SCAN_PER;
     auto at = [](int j) { return (j >> 5) * (SCAN_PER + 1) + (j & 31); };
     for (int b = 0; b < n; b += CHUNK) {
-#pragma unroll 8
+        // Every load of the chunk in flight at once, then the transpose.
+        int32_t v[SCAN_PER];
+#pragma unroll
         for (int k = 0; k < SCAN_PER; ++k) {
             const int j = k * SCAN_THREADS + threadIdx.x;
-            buf[at(j)] = b + j < n ? in[b + j] : 0;
+            v[k] = b + j < n ? in[b + j] : 0;
         }
+#pragma unroll
+        for (int k = 0; k < SCAN_PER; ++k)
+            buf[at(k * SCAN_THREADS + threadIdx.x)] = v[k];
         __syncthreads();
         int32_t *row = buf + threadIdx.x * (SCAN_PER + 1);
         int sum = 0;
@@ -1040,7 +1052,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
 {
     __shared__ int s_tile;
     __shared__ uint64_t s_excl;
-    int32_t *start = cells.start[new_side];
+    int32_t *start = start_of(cells, new_side);
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0)
@@ -1109,6 +1121,10 @@ __global__ void __launch_bounds__(SCAN_THREADS)
 // k_olist: buckets the particles that are not in range (changed cell, were
 // injected, or refilled a hole) into per-cell lists; order is fixed later.
 // ---------------------------------------------------------------------------
+// Each thread takes OLIST_BATCH entries at a time, one phase of dependent
+// accesses (list entry, key, counter, list slot) for all of them before the
+// next, so that their memory latencies overlap.
+constexpr int OLIST_BATCH = 4;
 __global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
                         const StepScratch *sc, const uint32_t *__restrict__ obuf,
                         const uint32_t *__restrict__ key, Cells cells,
@@ -1116,30 +1132,49 @@ __global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
                         int ncase, int *err)
 {
     const uint32_t n = sc->obuf_count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += gridDim.x * blockDim.x) {
-        const uint32_t g = obuf[i];
-        int lo = 0, hi = ncase - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (pbases[mid] <= static_cast<int64_t>(g))
-                lo = mid;
-            else
-                hi = mid - 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n;
+         i0 += OLIST_BATCH * stride) {
+        uint32_t g[OLIST_BATCH], kw[OLIST_BATCH];
+        int64_t q[OLIST_BATCH];
+        int32_t cg[OLIST_BATCH], j[OLIST_BATCH];
+        int ci[OLIST_BATCH];
+#pragma unroll
+        for (int k = 0; k < OLIST_BATCH; ++k) {
+            const uint32_t i = i0 + k * stride;
+            g[k] = i < n ? obuf[i] : 0u;
+            kw[k] = i < n ? key[g[k]] : KEY_DEAD;
         }
-        const int64_t q = static_cast<int64_t>(g) - pbases[lo];
-        if (q >= st[lo].n_keep)
-            continue; // a tail slot that moved into a hole; listed there
-        const uint32_t k = key[g];
-        if (k & (KEY_DEAD | KEY_IN))
-            continue;
-        const int32_t cg = static_cast<int32_t>(k & KEY_CELL);
-        const int32_t j = atomicAdd(cells.o_fill + cg, 1);
-        if (j >= cells.n_o[cg]) {
-            report_error(err, DSMC_ERR_STATE); // counts and list disagree
-            continue;
+#pragma unroll
+        for (int k = 0; k < OLIST_BATCH; ++k) {
+            int lo = 0, hi = ncase - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (pbases[mid] <= static_cast<int64_t>(g[k]))
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            ci[k] = lo;
+            q[k] = static_cast<int64_t>(g[k]) - pbases[lo];
+            // Not listed: removed, in range, or a tail slot that moved into
+            // a hole (listed there).
+            const bool listed = !(kw[k] & (KEY_DEAD | KEY_IN)) && q[k] < st[lo].n_keep;
+            cg[k] = listed ? static_cast<int32_t>(kw[k] & KEY_CELL) : -1;
         }
-        olist[pbases[lo] + cells.ostart[cg] + j] = static_cast<int32_t>(q);
+#pragma unroll
+        for (int k = 0; k < OLIST_BATCH; ++k)
+            j[k] = cg[k] >= 0 ? atomicAdd(cells.o_fill + cg[k], 1) : 0;
+#pragma unroll
+        for (int k = 0; k < OLIST_BATCH; ++k) {
+            if (cg[k] < 0)
+                continue;
+            if (j[k] >= cells.n_o[cg[k]]) {
+                report_error(err, DSMC_ERR_STATE); // counts and list disagree
+                continue;
+            }
+            olist[pbases[ci[k]] + cells.ostart[cg[k]] + j[k]] = static_cast<int32_t>(q[k]);
+        }
     }
 }
 
@@ -1148,12 +1183,32 @@ __global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
 // those particles its final slot (written into its key word, bit 31 clear),
 // and computes the base offset of the cell's in-range particles.
 // ---------------------------------------------------------------------------
+// The j-th particle, in slot order, of a cell's out-of-range list (old slot
+// q) gets its final slot: after the cell's `ni` in-range particles when it
+// lies above the cell's old slot range [o_lo, o_hi).  Returns 1 when it lies
+// below that range.
+__device__ __forceinline__ int fix_place(int32_t q, int j, int32_t start, int32_t ni,
+                                         int32_t o_lo, int32_t o_hi, int64_t keep,
+                                         uint32_t *key, int64_t pbase, int *err)
+{
+    const int64_t fin = start + j + (q >= o_hi ? ni : 0);
+    if (q < 0 || q >= keep || fin < 0 || fin >= keep)
+        report_error(err, DSMC_ERR_STATE); // counts and list disagree
+    else
+        key[pbase + q] = static_cast<uint32_t>(fin);
+    return q < o_lo ? 1 : 0;
+}
+
+// Lists of up to FIX_REG entries (nearly all: a few particles enter a cell
+// per step) are sorted in registers; longer ones in place.
+constexpr int FIX_REG = 8;
+
 __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *st,
                            TileTables tt, Cells cells, int old_side, uint32_t *__restrict__ key,
                            int32_t *__restrict__ olist, int total_cells, int ncase, int *err)
 {
-    const int32_t *os = cells.start[old_side];
-    const int32_t *ns = cells.start[old_side ^ 1];
+    const int32_t *os = start_of(cells, old_side);
+    const int32_t *ns = start_of(cells, old_side ^ 1);
     for (int cg = blockIdx.x * blockDim.x + threadIdx.x; cg < total_cells;
          cg += gridDim.x * blockDim.x) {
         const int ci = case_of(tt.cellbase, ncase, cg);
@@ -1161,40 +1216,56 @@ __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *s
         const int cl = cg - c.cbase;
         if (cl >= c.ncell)
             continue;
+        // Every per-cell word first, so that their loads overlap.
         const int32_t n = cells.n_o[cg];
+        const int32_t ost = cells.ostart[cg];
+        const int32_t fin_cell = cells.fin[cg];
+        const int32_t nend = ns[cg + 1];
         const int32_t ni = cells.n_in[cg];
         const int32_t start = ns[cg];
         const int32_t o_lo = os[cg], o_hi = os[cg + 1];
         int32_t lo = 0;
         if (n > 0) {
-            int32_t *seg = olist + c.pbase + cells.ostart[cg];
-            // Insertion sort by slot: lists are a few entries long.
-            for (int a = 1; a < n; ++a) {
-                const int32_t v = seg[a];
-                int b = a - 1;
-                while (b >= 0 && seg[b] > v) {
-                    seg[b + 1] = seg[b];
-                    --b;
-                }
-                seg[b + 1] = v;
-            }
+            int32_t *seg = olist + c.pbase + ost;
             const int64_t keep = st[ci].n_keep;
-            for (int j = 0; j < n; ++j) {
-                const int32_t q = seg[j];
-                if (q < o_lo)
-                    ++lo;
-                const int64_t fin = start + j + (q >= o_hi ? ni : 0);
-                if (q < 0 || q >= keep || fin < 0 || fin >= keep) {
-                    report_error(err, DSMC_ERR_STATE); // counts and list disagree
-                    continue;
+            if (n <= FIX_REG) {
+                int32_t v[FIX_REG];
+#pragma unroll
+                for (int a = 0; a < FIX_REG; ++a)
+                    v[a] = a < n ? seg[a] : INT32_MAX;
+                // Odd-even transposition sort: FIX_REG rounds sort FIX_REG
+                // values (slots are distinct; the padding sorts last).
+#pragma unroll
+                for (int r = 0; r < FIX_REG; ++r)
+#pragma unroll
+                    for (int a = r & 1; a + 1 < FIX_REG; a += 2) {
+                        const int32_t x = v[a], y = v[a + 1];
+                        v[a] = min(x, y);
+                        v[a + 1] = max(x, y);
+                    }
+#pragma unroll
+                for (int j = 0; j < FIX_REG; ++j)
+                    if (j < n)
+                        lo += fix_place(v[j], j, start, ni, o_lo, o_hi, keep, key, c.pbase, err);
+            } else {
+                // Insertion sort by slot, in place.
+                for (int a = 1; a < n; ++a) {
+                    const int32_t v = seg[a];
+                    int b = a - 1;
+                    while (b >= 0 && seg[b] > v) {
+                        seg[b + 1] = seg[b];
+                        --b;
+                    }
+                    seg[b + 1] = v;
                 }
-                key[c.pbase + q] = static_cast<uint32_t>(fin);
+                for (int j = 0; j < n; ++j)
+                    lo += fix_place(seg[j], j, start, ni, o_lo, o_hi, keep, key, c.pbase, err);
             }
         }
-        cells.base_in[cg] = start + lo - cells.fin[cg];
+        cells.base_in[cg] = start + lo - fin_cell;
         // The next step starts with every particle of the cell counted as
         // in range; k_move subtracts the ones that leave.
-        cells.n_in[cg] = ns[cg + 1] - start;
+        cells.n_in[cg] = nend - start;
         cells.n_o[cg] = 0;
         cells.o_fill[cg] = 0;
     }
@@ -1397,7 +1468,7 @@ __global__ void __launch_bounds__(256)
                      TileTables tt, Cells cells, int side, uint32_t *__restrict__ coll_list,
                      int total_cells, int ncase)
 {
-    const int32_t *start = cells.start[side];
+    const int32_t *start = start_of(cells, side);
     for (int base = blockIdx.x * blockDim.x; base < total_cells; base += gridDim.x * blockDim.x) {
         const int cg = base + threadIdx.x;
         bool listed = false;
@@ -1433,7 +1504,7 @@ __global__ void __launch_bounds__(128)
                     TileTables tt, Slots<T> p, Cells cells, int side,
                     const uint32_t *__restrict__ coll_list, int ncase)
 {
-    const int32_t *start = cells.start[side];
+    const int32_t *start = start_of(cells, side);
     const uint32_t count = sc->coll_count;
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
          w += gridDim.x * blockDim.x) {
@@ -1561,7 +1632,7 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
     __shared__ uint64_t bar[S];
     __shared__ int s_staged[S];
     __shared__ int64_t s_r0[S]; // first staged slot (rounded down to A)
-    const int32_t *start = cells.start[side];
+    const int32_t *start = start_of(cells, side);
     const int nblocks = tt.cblock0[ncase];
 
     // Thread 0 only: stages the velocities of block b in stage sidx when its
