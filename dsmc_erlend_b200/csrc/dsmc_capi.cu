@@ -66,6 +66,7 @@ struct dsmc_ctx {
     int64_t total_slots = 0;
     int total_cells = 0; // global cell ids, ncell + 1 per case
     int max_slot_tiles = 0;
+    int64_t max_case_tiles = 0; // most move + inject tiles of one case
     int total_cell_tiles = 0;
 
     CaseDev *d_cases = nullptr;
@@ -148,6 +149,13 @@ struct Span {
 
 int grid(const dsmc_ctx *c, int kid) { return std::max(1, c->ctas[kid]) * c->sms; }
 
+// Chunks of the tile-count scans: enough for the most tiles a case can have
+// (its slots, move and inject tiles rounded up separately).
+int scan_chunks(const dsmc_ctx *c)
+{
+    return static_cast<int>((c->max_case_tiles + SCAN_CHUNK - 1) / SCAN_CHUNK);
+}
+
 template <class T> Slots<T> slots(dsmc_ctx *c, int side)
 {
     Slots<T> s;
@@ -198,8 +206,8 @@ template <class T> void launch_inject(dsmc_ctx *c, cudaStream_t stream)
 void launch_tile_scan(dsmc_ctx *c, cudaStream_t stream)
 {
     Span sp(c, KID_TILE_SCAN);
-    k_tile_scan<<<c->ncase, SCAN_THREADS, SCAN_SMEM, stream>>>(c->d_state, c->tile_in,
-                                                            c->tile_prefix);
+    k_tile_scan<<<dim3(scan_chunks(c), c->ncase), SCAN_THREADS, 0, stream>>>(
+        c->d_state, c->tile_in, c->tile_prefix);
 }
 
 // `side`: the buffer that holds the sorted particles of this step.
@@ -253,9 +261,8 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
         launch_inject<T>(c, c->stream);
     {
         Span sp(c, KID_DEAD_SCAN);
-        k_dead_scan<<<c->ncase, SCAN_THREADS, SCAN_SMEM, c->stream>>>(c->d_state, c->tile_dead,
-                                                              c->tile_dprefix, c->itile_dead,
-                                                              c->itile_dprefix);
+        k_dead_scan<<<dim3(scan_chunks(c), c->ncase), SCAN_THREADS, 0, c->stream>>>(
+            c->d_state, c->tile_dead, c->tile_dprefix, c->itile_dead, c->itile_dprefix);
     }
     {
         Span sp(c, KID_HOLES);
@@ -580,10 +587,6 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
     occ(KID_SAMPLE, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_collide_select, 256, 0));
     occ(KID_COLLIDE_SELECT, b);
-    CK(cudaFuncSetAttribute(k_dead_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(SCAN_SMEM)));
-    CK(cudaFuncSetAttribute(k_tile_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(SCAN_SMEM)));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_olist, 256, 0));
     occ(KID_OLIST, b);
     c->ctas[KID_OLIST] = std::min(4, c->ctas_max[KID_OLIST]);
@@ -1019,8 +1022,8 @@ extern "C" {
 int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n_cases,
                     void *cuda_stream, dsmc_ctx **out)
 {
-    if (cases == nullptr || out == nullptr || n_cases < 1)
-        return DSMC_ERR_ARGUMENT;
+    if (cases == nullptr || out == nullptr || n_cases < 1 || n_cases > 65535)
+        return DSMC_ERR_ARGUMENT; // 65535: the cases are a grid dimension of the scans
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -1093,6 +1096,7 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
         cell_tiles += (cd.ncell + TILE - 1) / TILE;
         cblocks += (cd.ncell + COLLIDE_CELLS - 1) / COLLIDE_CELLS;
         max_tiles += static_cast<int>(cap / TILE) + 1;
+        c->max_case_tiles = std::max<int64_t>(c->max_case_tiles, cap / TILE + 2);
         c->hcases[i] = cd;
     }
     cellbase[n_cases] = cell;

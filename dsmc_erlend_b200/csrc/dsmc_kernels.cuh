@@ -8,10 +8,12 @@
 //   k_move      tiles    MoveParticles + the new cell of every slot, removal
 //                        flag, in-range flag, per-cell counts, hole list
 //   k_inject    tiles    GenerateNewParticles for the four strips, appended
+//   k_dead_scan chunks   prefix of removed-slot counts per tile
+//   k_holes     tiles    removed-slot list in slot order
 //   k_plan2     1 CTA    survivors K, hole count H, tail tiles
 //   k_tail      tiles    swap-with-last: alive tail slots refill the holes
 //   k_cell_scan tiles    per-cell offsets (stable counting sort)
-//   k_tile_scan 1 CTA/case  prefix of in-range counts per tile
+//   k_tile_scan chunks   prefix of in-range counts per tile
 //   k_olist     grid     lists of the particles that changed cell
 //   k_cell_fix  grid     orders those lists, places them, per-cell bases
 //   k_scatter   tiles    places every in-range particle
@@ -787,82 +789,101 @@ __global__ void __launch_bounds__(TILE_THREADS)
 }
 
 // ---------------------------------------------------------------------------
-// Threads of the one-CTA-per-case tile scans (k_dead_scan, k_tile_scan).
+// Threads of a CTA of the per-case scans (also k_warm_scan).
 constexpr int SCAN_THREADS = 1024;
 
-// Exclusive prefix (starting at carry) of n per-tile counts by one CTA of
-// SCAN_THREADS threads; returns carry plus the total.  Chunks of
-// SCAN_THREADS * SCAN_PER counts go through shared memory: loaded and stored
-// coalesced (thread t takes elements k * SCAN_THREADS + t), scanned as
-// SCAN_PER consecutive elements per thread; rows padded to SCAN_PER + 1 words
-// so that both access patterns are free of bank conflicts.  `buf` holds
-// SCAN_THREADS * (SCAN_PER + 1) words (dynamic shared memory).
-constexpr int SCAN_PER = 32;
-constexpr size_t SCAN_SMEM = sizeof(int32_t) * SCAN_THREADS * (SCAN_PER + 1);
-__device__ __forceinline__ int32_t cta_scan_counts(const int32_t *__restrict__ in,
-                                                   int32_t *__restrict__ out, int n,
-                                                   int32_t carry, int32_t *buf)
+// The tile-count scans (k_dead_scan, k_tile_scan): the exclusive prefix of a
+// case's sequence of per-tile counts, cut into chunks of SCAN_CHUNK counts,
+// one CTA each, all at once.  A CTA first sums every count before its chunk
+// (read directly: no CTA waits for another), then scans its chunk, SCAN_VEC
+// consecutive counts per thread.
+constexpr int SCAN_VEC = 4;
+constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_VEC;
+
+// Count i of the sequence a[0, na) followed by b.
+__device__ __forceinline__ int32_t seq_count(const int32_t *a, int na, const int32_t *b, int i)
 {
-    constexpr int CHUNK = SCAN_THREADS * SCAN_PER;
-    auto at = [](int j) { return (j >> 5) * (SCAN_PER + 1) + (j & 31); };
-    for (int b = 0; b < n; b += CHUNK) {
-        // Every load of the chunk in flight at once, then the transpose.
-        int32_t v[SCAN_PER];
-#pragma unroll
-        for (int k = 0; k < SCAN_PER; ++k) {
-            const int j = k * SCAN_THREADS + threadIdx.x;
-            v[k] = b + j < n ? in[b + j] : 0;
-        }
-#pragma unroll
-        for (int k = 0; k < SCAN_PER; ++k)
-            buf[at(k * SCAN_THREADS + threadIdx.x)] = v[k];
-        __syncthreads();
-        int32_t *row = buf + threadIdx.x * (SCAN_PER + 1);
-        int sum = 0;
-#pragma unroll
-        for (int m = 0; m < SCAN_PER; ++m)
-            sum += row[m];
-        int tot;
-        int run = carry + block_exclusive<int, SCAN_THREADS>(sum, tot);
-#pragma unroll
-        for (int m = 0; m < SCAN_PER; ++m) {
-            const int v = row[m];
-            row[m] = run;
-            run += v;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int k = 0; k < SCAN_PER; ++k) {
-            const int j = k * SCAN_THREADS + threadIdx.x;
-            if (b + j < n)
-                out[b + j] = buf[at(j)];
-        }
-        carry += tot;
-        __syncthreads();
-    }
-    return carry;
+    return i < na ? a[i] : b[i - na];
 }
 
-// k_dead_scan: per case (one CTA each), exclusive prefix of the removed-slot
-// counts of its move tiles, then of its inject tiles, in slot order; sets
-// dead_old and dead_total.
+// Sum of counts [0, c0) of the sequence, in every thread.
+__device__ __forceinline__ int32_t seq_before(const int32_t *a, int na, const int32_t *b, int c0)
+{
+    int32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0; // four loads in flight per round
+    int i = threadIdx.x;
+    for (; i + 3 * SCAN_THREADS < c0; i += 4 * SCAN_THREADS) {
+        s0 += seq_count(a, na, b, i);
+        s1 += seq_count(a, na, b, i + SCAN_THREADS);
+        s2 += seq_count(a, na, b, i + 2 * SCAN_THREADS);
+        s3 += seq_count(a, na, b, i + 3 * SCAN_THREADS);
+    }
+    for (; i < c0; i += SCAN_THREADS)
+        s0 += seq_count(a, na, b, i);
+    int32_t tot;
+    (void)block_exclusive<int32_t, SCAN_THREADS>(s0 + s1 + s2 + s3, tot);
+    return tot;
+}
+
+// Exclusive prefixes of chunk [c0, c0 + SCAN_CHUNK) of the sequence of
+// length n (from `carry`) into oa / ob; returns the prefix of each of this
+// thread's counts in pre[] and carry plus the chunk's total.
+__device__ __forceinline__ int32_t seq_chunk(const int32_t *a, int32_t *oa, int na,
+                                             const int32_t *b, int32_t *ob, int n, int c0,
+                                             int32_t carry, int32_t pre[SCAN_VEC])
+{
+    const int i0 = c0 + static_cast<int>(threadIdx.x) * SCAN_VEC;
+    int32_t v[SCAN_VEC];
+    int32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_VEC; ++k) {
+        v[k] = i0 + k < n ? seq_count(a, na, b, i0 + k) : 0;
+        sum += v[k];
+    }
+    int32_t tot;
+    int32_t run = carry + block_exclusive<int32_t, SCAN_THREADS>(sum, tot);
+#pragma unroll
+    for (int k = 0; k < SCAN_VEC; ++k) {
+        const int i = i0 + k;
+        pre[k] = run;
+        if (i < n) {
+            if (i < na)
+                oa[i] = run;
+            else
+                ob[i - na] = run;
+        }
+        run += v[k];
+    }
+    return carry + tot;
+}
+
+// k_dead_scan: grid (chunks, cases).  Exclusive prefix of the removed-slot
+// counts of a case's move tiles, then of its inject tiles (their ranks
+// continue the count, in slot order); sets dead_old and dead_total.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(SCAN_THREADS)
     k_dead_scan(CaseState *st, const int32_t *tile_dead, int32_t *tile_dprefix,
                 const int32_t *itile_dead, int32_t *itile_dprefix)
 {
-    extern __shared__ int32_t scan_buf[];
-    CaseState &s = st[blockIdx.x];
-    // The injected slots follow the old ones: their ranks continue the count.
-    const int32_t dead_old = cta_scan_counts(tile_dead + s.move_tile0,
-                                             tile_dprefix + s.move_tile0, s.n_move_tiles, 0,
-                                             scan_buf);
-    const int32_t dead_total = cta_scan_counts(itile_dead + s.inject_tile0,
-                                               itile_dprefix + s.inject_tile0,
-                                               s.n_inject_tiles, dead_old, scan_buf);
-    if (threadIdx.x == 0) {
-        s.dead_old = dead_old;
-        s.dead_total = dead_total;
+    CaseState &s = st[blockIdx.y];
+    const int na = s.n_move_tiles;
+    const int n = na + s.n_inject_tiles;
+    const int c0 = static_cast<int>(blockIdx.x) * SCAN_CHUNK;
+    if (c0 >= n)
+        return; // uniform over the CTA
+    const int32_t *a = tile_dead + s.move_tile0, *b = itile_dead + s.inject_tile0;
+    const int32_t carry = seq_before(a, na, b, c0);
+    int32_t pre[SCAN_VEC];
+    const int32_t total = seq_chunk(a, tile_dprefix + s.move_tile0, na, b,
+                                    itile_dprefix + s.inject_tile0, n, c0, carry, pre);
+    const int i0 = c0 + static_cast<int>(threadIdx.x) * SCAN_VEC;
+#pragma unroll
+    for (int k = 0; k < SCAN_VEC; ++k)
+        if (i0 + k == na && na < n) // the first inject tile: all move tiles before it
+            s.dead_old = pre[k];
+    if (c0 + SCAN_CHUNK >= n && threadIdx.x == 0) { // the last chunk
+        s.dead_total = total;
+        if (na == n)
+            s.dead_old = total;
     }
 }
 
@@ -1004,33 +1025,51 @@ __global__ void __launch_bounds__(TILE_THREADS)
         }
         __syncthreads();
         int64_t r = static_cast<int64_t>(s_excl) + alive_excl;
+        const int lane = threadIdx.x & 31;
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
-            if (keys[k] & KEY_DEAD)
-                continue;
-            const int64_t m = s.n_holes - 1 - r;
-            ++r;
-            if (m < 0) {
-                report_error(err, DSMC_ERR_STATE);
-                continue;
+            const bool alive = !(keys[k] & KEY_DEAD);
+            int64_t m = -1;
+            if (alive) {
+                m = s.n_holes - 1 - r;
+                ++r;
+                if (m < 0)
+                    report_error(err, DSMC_ERR_STATE);
             }
-            const int64_t h = hole_pos[c.pbase + m];
-            const int32_t hoc = hole_oc[c.pbase + m];
+            const bool go = alive && m >= 0;
+            int64_t h = 0;
+            int32_t hoc = NO_CELL;
+            if (go) {
+                h = hole_pos[c.pbase + m];
+                hoc = hole_oc[c.pbase + m];
+            }
             const int32_t cg = static_cast<int32_t>(keys[k] & KEY_CELL);
             const bool was_in = (keys[k] & KEY_IN) != 0;
-            const bool now_in = hoc == cg;
-            if (was_in)
-                atomicSub(cells.n_in + cg, 1);
-            else if (now_in)
-                atomicSub(cells.n_o + cg, 1);
-            if (now_in) {
-                atomicAdd(cells.n_in + cg, 1);
-                atomicAdd(tile_in + s.move_tile0 + static_cast<int>(h / TILE), 1);
-            } else {
-                if (was_in)
-                    atomicAdd(cells.n_o + cg, 1);
-                obuf[atomicAdd(&sc->obuf_count, 1u)] = static_cast<uint32_t>(c.pbase + h);
+            const bool now_in = go && hoc == cg;
+            const bool listed = go && !now_in;
+            // One increment of the list counter per warp.
+            const unsigned lm = __ballot_sync(0xffffffffu, listed);
+            uint32_t lbase = 0;
+            if (lm) {
+                const int lead = __ffs(lm) - 1;
+                if (lane == lead)
+                    lbase = atomicAdd(&sc->obuf_count, static_cast<uint32_t>(__popc(lm)));
+                lbase = __shfl_sync(0xffffffffu, lbase, lead);
             }
+            if (!go)
+                continue;
+            if (was_in && !now_in) {
+                atomicSub(cells.n_in + cg, 1);
+                atomicAdd(cells.n_o + cg, 1);
+            } else if (!was_in && now_in) {
+                atomicSub(cells.n_o + cg, 1);
+                atomicAdd(cells.n_in + cg, 1);
+            }
+            if (now_in)
+                atomicAdd(tile_in + s.move_tile0 + static_cast<int>(h / TILE), 1);
+            else
+                obuf[lbase + __popc(lm & ((1u << lane) - 1u))] =
+                    static_cast<uint32_t>(c.pbase + h);
             const int64_t gs = c.pbase + q0 + k, gd = c.pbase + h;
             p.x[gd] = p.x[gs];
             p.y[gd] = p.y[gs];
@@ -1051,7 +1090,6 @@ __global__ void __launch_bounds__(TILE_THREADS)
                 int new_side, uint64_t *lb, int ncase, int *err)
 {
     __shared__ int s_tile;
-    __shared__ uint64_t s_excl;
     int32_t *start = start_of(cells, new_side);
     for (;;) {
         __syncthreads();
@@ -1080,13 +1118,9 @@ __global__ void __launch_bounds__(TILE_THREADS)
         unsigned long long tot;
         const unsigned long long ex =
             block_exclusive<unsigned long long>(pack2(sa, sb), tot);
-        if (threadIdx.x < 32) {
-            const uint64_t excl = lookback_warp(lb, t, t - local_tile, tot, err);
-            if (threadIdx.x == 0)
-                s_excl = excl;
-        }
-        __syncthreads();
-        const uint64_t base = s_excl + ex;
+        // All tiles of a grid run in one wave: the whole CTA walks back.
+        const uint64_t base =
+            lookback_block<TILE_THREADS>(lb, t, t - local_tile, tot, err) + ex;
         uint32_t ra = pack2_a(base), rb = pack2_b(base);
 #pragma unroll
         for (int k = 0; k < TILE_VEC; ++k) {
@@ -1105,16 +1139,22 @@ __global__ void __launch_bounds__(TILE_THREADS)
 }
 
 // ---------------------------------------------------------------------------
-// k_tile_scan: per case (one CTA each), exclusive prefix of the in-range
-// counts of its move tiles, in place into tile_prefix.
+// k_tile_scan: grid (chunks, cases).  Exclusive prefix of the in-range
+// counts of a case's move tiles into tile_prefix.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(SCAN_THREADS)
     k_tile_scan(const CaseState *st, const int32_t *tile_in, int32_t *tile_prefix)
 {
-    extern __shared__ int32_t scan_buf[];
-    const CaseState &s = st[blockIdx.x];
-    cta_scan_counts(tile_in + s.move_tile0, tile_prefix + s.move_tile0, s.n_move_tiles, 0,
-                    scan_buf);
+    const CaseState &s = st[blockIdx.y];
+    const int n = s.n_move_tiles;
+    const int c0 = static_cast<int>(blockIdx.x) * SCAN_CHUNK;
+    if (c0 >= n)
+        return; // uniform over the CTA
+    const int32_t *a = tile_in + s.move_tile0;
+    const int32_t carry = seq_before(a, n, a, c0);
+    int32_t pre[SCAN_VEC];
+    (void)seq_chunk(a, tile_prefix + s.move_tile0, n, a, tile_prefix + s.move_tile0, n, c0,
+                    carry, pre);
 }
 
 // ---------------------------------------------------------------------------

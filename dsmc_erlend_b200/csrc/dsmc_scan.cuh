@@ -135,6 +135,77 @@ __device__ __forceinline__ uint64_t lookback_warp(uint64_t *status, int t, int c
     return excl;
 }
 
+// Block-wide form of lookback(): called by all NT threads of a CTA.  Each
+// poll reads the NT predecessors t-1 .. t-NT at once (one per thread), so a
+// chain whose tiles all run in one wave, and have published only their
+// aggregates, is crossed NT tiles per poll.  Same contract as lookback_warp.
+template <int NT>
+__device__ __forceinline__ uint64_t lookback_block(uint64_t *status, int t, int chain0,
+                                                   uint64_t agg, int *err)
+{
+    static_assert(NT % 32 == 0 && NT <= 1024, "block of whole warps");
+    constexpr int NW = NT / 32;
+    __shared__ uint64_t s_part[NW];
+    __shared__ int s_near[NW]; // lowest lane holding an inclusive prefix, 32 if none
+    volatile uint64_t *vs = status;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    if (t == chain0) {
+        if (threadIdx.x == 0) {
+            __threadfence();
+            vs[t] = LB_INC | agg;
+        }
+        return 0;
+    }
+    if (threadIdx.x == 0)
+        vs[t] = LB_AGG | agg;
+    __threadfence();
+    uint64_t excl = 0;
+    int base = t - 1;
+    uint32_t spins = 0;
+    for (;;) {
+        const int j = base - static_cast<int>(threadIdx.x);
+        uint64_t w = LB_INC; // value 0 before the chain
+        if (j >= chain0)
+            w = vs[j];
+        if (!__syncthreads_and((w & LB_FLAGS) != 0)) {
+            if (++spins > SPIN_LIMIT) { // uniform: every thread counts the same polls
+                if (threadIdx.x == 0) {
+                    report_error(err, DSMC_ERR_TIMEOUT);
+                    vs[t] = LB_INC | agg;
+                }
+                return 0;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        const unsigned inc = __ballot_sync(0xffffffffu, (w & LB_FLAGS) == LB_INC);
+        const int near = inc ? __ffs(inc) - 1 : 32;
+        const uint64_t part = warp_sum_u64(lane <= near ? (w & LB_VALUE) : 0ull);
+        if (lane == 0) {
+            s_part[warp] = part;
+            s_near[warp] = near;
+        }
+        __syncthreads();
+        // Windows nearer than the first one holding an inclusive prefix are
+        // summed whole; that one up to its prefix.
+        bool done = false;
+        for (int i = 0; i < NW && !done; ++i) {
+            excl += s_part[i];
+            done = s_near[i] < 32;
+        }
+        __syncthreads(); // s_part is rewritten by the next poll
+        if (done)
+            break;
+        base -= NT;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        vs[t] = LB_INC | (excl + agg);
+    }
+    return excl;
+}
+
 // Block-wide exclusive sum over NT threads; also returns the total.
 template <class V, int NT = TILE_THREADS>
 __device__ __forceinline__ V block_exclusive(V v, V &total)

@@ -193,8 +193,8 @@ int dsmc_write_field(const dsmc_params *p, const dsmc_derived *d, int64_t sample
 
 /* ---- context ------------------------------------------------------------ */
 
-/* Creates a context of n_cases independent cases on the current CUDA device.
- * `derived` may be NULL (computed by dsmc_setup) or an array of n_cases
+/* Creates a context of n_cases (1 to 65535) independent cases on the current
+ * CUDA device.  `derived` may be NULL (computed by dsmc_setup) or an array of n_cases
  * overrides.  `cuda_stream` is a cudaStream_t to launch on, or NULL for a
  * stream owned by the context. */
 int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n_cases,
