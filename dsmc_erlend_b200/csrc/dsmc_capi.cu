@@ -228,7 +228,7 @@ template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
     {
         Span sp(c, KID_PLAN);
         k_plan<<<1, 1024, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch, c->tt, c->d_tmp,
-                                          c->ncase, init_mode, c->d_err);
+                                          c->itile_dead, c->ncase, init_mode, c->d_err);
     }
     if (!init_mode && c->par) {
         if ((s = branch(c, EV_PLAN, c->stream, c->side_stream)))
@@ -1093,7 +1093,7 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
         cblock0[i] = cblocks;
         slot += cap;
         cell += cd.ncell + 1;
-        cell_tiles += (cd.ncell + TILE - 1) / TILE;
+        cell_tiles += (cd.ncell + CELL_TILE - 1) / CELL_TILE;
         cblocks += (cd.ncell + COLLIDE_CELLS - 1) / COLLIDE_CELLS;
         max_tiles += static_cast<int>(cap / TILE) + 1;
         c->max_case_tiles = std::max<int64_t>(c->max_case_tiles, cap / TILE + 2);

@@ -114,7 +114,7 @@ __device__ __forceinline__ void case_scan(int32_t *base, const int32_t *count_of
 // k_plan: start of a step (or of the cold start when init_mode is set).
 // ---------------------------------------------------------------------------
 __global__ void k_plan(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
-                       int32_t *tmp, int ncase, int init_mode, int *err)
+                       int32_t *tmp, int32_t *itile_dead, int ncase, int init_mode, int *err)
 {
     for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
         const CaseDev &c = cases[i];
@@ -186,6 +186,9 @@ __global__ void k_plan(const CaseDev *cases, CaseState *st, StepScratch *sc, Til
         sc->total_inject_tiles = tt.inject0[ncase];
         sc->init_mode = init_mode;
     }
+    // k_inject adds the removed slots of each quarter of an inject tile.
+    for (int i = threadIdx.x; i < tt.inject0[ncase]; i += blockDim.x)
+        itile_dead[i] = 0;
     for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
         st[i].move_tile0 = tt.move0[i];
         st[i].inject_tile0 = tt.inject0[i];
@@ -689,30 +692,31 @@ __global__ void __launch_bounds__(TILE_THREADS)
              Slots<T> p, uint32_t *__restrict__ key, Cells cells,
              int32_t *__restrict__ itile_dead, uint32_t *__restrict__ obuf, int ncase, int *err)
 {
-    __shared__ int s_tile;
+    __shared__ int s_unit;
     const int init_mode = sc->init_mode;
+    const int lane = threadIdx.x & 31;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0)
-            s_tile = static_cast<int>(atomicAdd(&sc->inject_ticket, 1u));
+            s_unit = static_cast<int>(atomicAdd(&sc->inject_ticket, 1u));
         __syncthreads();
-        const int t = s_tile;
-        if (t >= sc->total_inject_tiles)
+        // A unit is a quarter of an inject tile, one slot per thread, so the
+        // long per-particle chain (stream seek, five draws) runs once per
+        // thread.
+        const int u = s_unit;
+        if (u >= sc->total_inject_tiles * TILE_VEC)
             return;
+        const int t = u / TILE_VEC;
         const int ci = case_of(tt.inject0, ncase, t);
         const CaseDev &c = cases[ci];
         const CaseState &s = st[ci];
         const int64_t n_inj = s.inj_off[5];
         const int local_tile = t - tt.inject0[ci];
-        const int64_t j0 = static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
-        uint32_t keys[TILE_VEC];
+        const int64_t j = static_cast<int64_t>(local_tile) * TILE +
+                          (u % TILE_VEC) * TILE_THREADS + threadIdx.x;
+        uint32_t kw = KEY_DEAD | KEY_CELL;
         int n_dead = 0;
-#pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            keys[k] = KEY_DEAD | KEY_CELL;
-            const int64_t j = j0 + k;
-            if (j >= n_inj)
-                continue;
+        if (j < n_inj) {
             int strip = 0;
             while (strip < 4 && j >= s.inj_off[strip + 1])
                 ++strip;
@@ -752,39 +756,35 @@ __global__ void __launch_bounds__(TILE_THREADS)
             const double xd = static_cast<double>(xs), yd = static_cast<double>(ys);
             const bool dead = init_mode ? inside_box(c, xd, yd) : outside_domain(c, xd, yd);
             if (dead) {
-                n_dead++;
+                n_dead = 1;
             } else {
                 const int32_t nc = cell_of(c, xd, yd);
                 if (nc < 0) {
                     report_error(err, DSMC_ERR_EXCHANGE);
-                    n_dead++;
+                    n_dead = 1;
                 } else {
-                    keys[k] = static_cast<uint32_t>(c.cbase + nc);
+                    kw = static_cast<uint32_t>(c.cbase + nc);
                 }
             }
-            key[g] = keys[k];
+            key[g] = kw;
         }
-#pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            const bool alive = !(keys[k] & KEY_DEAD);
-            const int32_t cg = static_cast<int32_t>(keys[k] & KEY_CELL);
-            warp_aggregated_inc(cells.n_o, cg, alive);
-            const unsigned m = __ballot_sync(0xffffffffu, alive);
-            if (m) {
-                const int lane = threadIdx.x & 31;
-                uint32_t base = 0;
-                if (lane == __ffs(m) - 1)
-                    base = atomicAdd(&sc->obuf_count, static_cast<uint32_t>(__popc(m)));
-                base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-                if (alive)
-                    obuf[base + __popc(m & ((1u << lane) - 1u))] =
-                        static_cast<uint32_t>(c.pbase + s.n_old + j0 + k);
-            }
+        const bool alive = !(kw & KEY_DEAD);
+        const int32_t cg = static_cast<int32_t>(kw & KEY_CELL);
+        warp_aggregated_inc(cells.n_o, cg, alive);
+        const unsigned m = __ballot_sync(0xffffffffu, alive);
+        if (m) {
+            uint32_t base = 0;
+            if (lane == __ffs(m) - 1)
+                base = atomicAdd(&sc->obuf_count, static_cast<uint32_t>(__popc(m)));
+            base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+            if (alive)
+                obuf[base + __popc(m & ((1u << lane) - 1u))] =
+                    static_cast<uint32_t>(c.pbase + s.n_old + j);
         }
         int dead_total;
         (void)block_exclusive<int>(n_dead, dead_total);
-        if (threadIdx.x == 0)
-            itile_dead[t] = dead_total;
+        if (threadIdx.x == 0 && dead_total > 0)
+            atomicAdd(itile_dead + t, dead_total);
     }
 }
 
@@ -897,40 +897,54 @@ __global__ void __launch_bounds__(TILE_THREADS)
             const int32_t *tile_dprefix, const int32_t *itile_dead, const int32_t *itile_dprefix,
             int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc, int ncase)
 {
+    __shared__ int s_list[TILE_THREADS];
     const int n_move = sc->total_move_tiles;
     const int total = n_move + sc->total_inject_tiles;
-    for (int T = blockIdx.x; T < total; T += gridDim.x) {
-        const bool moved = T < n_move;
-        const int t = moved ? T : T - n_move;
-        const int count = moved ? tile_dead[t] : itile_dead[t];
-        if (count == 0)
-            continue; // uniform over the block
-        const int ci = case_of(moved ? tt.move0 : tt.inject0, ncase, t);
-        const CaseDev &c = cases[ci];
-        const CaseState &s = st[ci];
-        const int local_tile = t - (moved ? tt.move0[ci] : tt.inject0[ci]);
-        const int64_t first = moved ? 0 : s.n_old;
-        const int64_t end = moved ? s.n_old : s.n_total;
-        const int64_t q0 = first + static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
-        uint32_t keys[TILE_VEC];
-        int n_dead = 0;
+    for (int T0 = blockIdx.x; T0 < total; T0 += gridDim.x * TILE_THREADS) {
+        // The counts of this CTA's next TILE_THREADS tiles are read at once
+        // and the tiles with removed slots listed: most tiles have none.
+        const int Tm = T0 + static_cast<int>(threadIdx.x) * gridDim.x;
+        int cnt = 0;
+        if (Tm < total)
+            cnt = Tm < n_move ? tile_dead[Tm] : itile_dead[Tm - n_move];
+        int n_list;
+        const int pos = block_exclusive<int>(cnt > 0 ? 1 : 0, n_list);
+        if (cnt > 0)
+            s_list[pos] = Tm;
+        __syncthreads();
+        for (int li = 0; li < n_list; ++li) {
+            const int T = s_list[li];
+            const bool moved = T < n_move;
+            const int t = moved ? T : T - n_move;
+            const int ci = case_of(moved ? tt.move0 : tt.inject0, ncase, t);
+            const CaseDev &c = cases[ci];
+            const CaseState &s = st[ci];
+            const int local_tile = t - (moved ? tt.move0[ci] : tt.inject0[ci]);
+            const int64_t first = moved ? 0 : s.n_old;
+            const int64_t end = moved ? s.n_old : s.n_total;
+            const int64_t q0 =
+                first + static_cast<int64_t>(local_tile) * TILE + threadIdx.x * TILE_VEC;
+            uint32_t keys[TILE_VEC];
+            int n_dead = 0;
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            keys[k] = q0 + k < end ? key[c.pbase + q0 + k] : 0u;
-            n_dead += (keys[k] & KEY_DEAD) ? 1 : 0;
-        }
-        int tot;
-        int64_t rank = (moved ? tile_dprefix[t] : itile_dprefix[t]) +
-                       block_exclusive<int>(n_dead, tot);
+            for (int k = 0; k < TILE_VEC; ++k) {
+                keys[k] = q0 + k < end ? key[c.pbase + q0 + k] : 0u;
+                n_dead += (keys[k] & KEY_DEAD) ? 1 : 0;
+            }
+            int tot;
+            int64_t rank = (moved ? tile_dprefix[t] : itile_dprefix[t]) +
+                           block_exclusive<int>(n_dead, tot);
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
-            if (!(keys[k] & KEY_DEAD))
-                continue;
-            const uint32_t oc = keys[k] & KEY_CELL;
-            hole_pos[c.pbase + rank] = static_cast<int32_t>(q0 + k);
-            hole_oc[c.pbase + rank] = oc == KEY_CELL ? NO_CELL : static_cast<int32_t>(oc);
-            ++rank;
+            for (int k = 0; k < TILE_VEC; ++k) {
+                if (!(keys[k] & KEY_DEAD))
+                    continue;
+                const uint32_t oc = keys[k] & KEY_CELL;
+                hole_pos[c.pbase + rank] = static_cast<int32_t>(q0 + k);
+                hole_oc[c.pbase + rank] = oc == KEY_CELL ? NO_CELL : static_cast<int32_t>(oc);
+                ++rank;
+            }
         }
+        __syncthreads(); // s_list is rewritten by the next group
     }
 }
 
@@ -1085,6 +1099,12 @@ __global__ void __launch_bounds__(TILE_THREADS)
 // k_cell_scan: per case, exclusive sums over its cells of the in-range and
 // out-of-range counts (Fin, ostart) and the new cell starts.
 // ---------------------------------------------------------------------------
+// Cells per tile of k_cell_scan (CELL_VEC consecutive cells per thread).
+// Measured on B200: 4 (1024-cell tiles) against 16, which halves the tiles
+// in flight and doubled the kernel's time.
+constexpr int CELL_VEC = 4;
+constexpr int CELL_TILE = TILE_THREADS * CELL_VEC;
+
 __global__ void __launch_bounds__(TILE_THREADS)
     k_cell_scan(const CaseDev *__restrict__ cases, StepScratch *sc, TileTables tt, Cells cells,
                 int new_side, uint64_t *lb, int ncase, int *err)
@@ -1102,11 +1122,11 @@ __global__ void __launch_bounds__(TILE_THREADS)
         const int ci = case_of(tt.cell0, ncase, t);
         const CaseDev &c = cases[ci];
         const int local_tile = t - tt.cell0[ci];
-        const int c0 = local_tile * TILE + threadIdx.x * TILE_VEC;
-        uint32_t a[TILE_VEC], b[TILE_VEC];
+        const int c0 = local_tile * CELL_TILE + threadIdx.x * CELL_VEC;
+        uint32_t a[CELL_VEC], b[CELL_VEC];
         uint32_t sa = 0, sb = 0;
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
+        for (int k = 0; k < CELL_VEC; ++k) {
             a[k] = b[k] = 0;
             if (c0 + k < c.ncell) {
                 a[k] = static_cast<uint32_t>(cells.n_in[c.cbase + c0 + k]);
@@ -1123,7 +1143,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
             lookback_block<TILE_THREADS>(lb, t, t - local_tile, tot, err) + ex;
         uint32_t ra = pack2_a(base), rb = pack2_b(base);
 #pragma unroll
-        for (int k = 0; k < TILE_VEC; ++k) {
+        for (int k = 0; k < CELL_VEC; ++k) {
             const int cc = c0 + k;
             if (cc < c.ncell) {
                 cells.fin[c.cbase + cc] = static_cast<int32_t>(ra);
@@ -1202,6 +1222,14 @@ __global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
             const bool listed = !(kw[k] & (KEY_DEAD | KEY_IN)) && q[k] < st[lo].n_keep;
             cg[k] = listed ? static_cast<int32_t>(kw[k] & KEY_CELL) : -1;
         }
+        // The cell's count and list offset do not depend on the increment:
+        // loaded before it, so both latencies overlap.
+        int32_t no[OLIST_BATCH], os[OLIST_BATCH];
+#pragma unroll
+        for (int k = 0; k < OLIST_BATCH; ++k) {
+            no[k] = cg[k] >= 0 ? cells.n_o[cg[k]] : 0;
+            os[k] = cg[k] >= 0 ? cells.ostart[cg[k]] : 0;
+        }
 #pragma unroll
         for (int k = 0; k < OLIST_BATCH; ++k)
             j[k] = cg[k] >= 0 ? atomicAdd(cells.o_fill + cg[k], 1) : 0;
@@ -1209,11 +1237,11 @@ __global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
         for (int k = 0; k < OLIST_BATCH; ++k) {
             if (cg[k] < 0)
                 continue;
-            if (j[k] >= cells.n_o[cg[k]]) {
+            if (j[k] >= no[k]) {
                 report_error(err, DSMC_ERR_STATE); // counts and list disagree
                 continue;
             }
-            olist[pbases[ci[k]] + cells.ostart[cg[k]] + j[k]] = static_cast<int32_t>(q[k]);
+            olist[pbases[ci[k]] + os[k] + j[k]] = static_cast<int32_t>(q[k]);
         }
     }
 }
