@@ -339,7 +339,12 @@ __device__ __forceinline__ bool free_flight(const CaseDev &c, double x0, double 
 // FP32 slots: the end point is rounded from the FP64 sum as in the exact
 // body; the box, domain and cell tests run on floats (exact or conservative,
 // as their helpers state), with the FP64 estimate as a second chance for a
-// cell the float estimate leaves open.
+// cell the float estimate leaves open.  A certain float estimate also decides
+// the removal test: its floors are those of (x - X1) / DX and (y - Y1) / DY,
+// at least the window's margin (far above the ulps between X2 and X1 + NX DX)
+// away from an integer, so the position lies strictly inside the domain
+// exactly when that cell is in the grid.  Only an open estimate takes the
+// exact domain test.
 __device__ __forceinline__ bool free_flight(const CaseDev &c, float x0, float y0, float vx,
                                             float vy, float &xn, float &yn, int32_t &oc,
                                             bool &gone, int32_t &nc)
@@ -348,12 +353,15 @@ __device__ __forceinline__ bool free_flight(const CaseDev &c, float x0, float y0
     yn = __double2float_rn(static_cast<double>(y0) + c.dt * static_cast<double>(vy));
     const bool near = near_box_f(c, x0, y0, xn, yn);
     bool ok_o = cell_of_fast_f(c, x0, y0, oc);
-    gone = outside_domain_f(c, xn, yn);
-    bool ok_n = cell_of_fast_f(c, xn, yn, nc) | gone;
+    bool ok_n = cell_of_fast_f(c, xn, yn, nc);
+    gone = nc == NO_CELL;
     if (!ok_o)
         ok_o = cell_of_fast(c, static_cast<double>(x0), static_cast<double>(y0), oc);
-    if (!ok_n)
-        ok_n = cell_of_fast(c, static_cast<double>(xn), static_cast<double>(yn), nc);
+    if (!ok_n) {
+        gone = outside_domain_f(c, xn, yn);
+        nc = NO_CELL;
+        ok_n = gone || cell_of_fast(c, static_cast<double>(xn), static_cast<double>(yn), nc);
+    }
     return !near & ok_o & ok_n;
 }
 
@@ -463,9 +471,10 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
     MoveStage<T> *stage = reinterpret_cast<MoveStage<T> *>(smem_raw);
     __shared__ uint64_t bar[S];
     __shared__ CaseDev s_case; // constants of the current tile's case
-    __shared__ unsigned s_dead[NB][32], s_out[NB][32], s_in[NB][32]; // per (iteration, warp)
-    __shared__ unsigned s_opre[NB][32];                              // exclusive prefix of s_out
+    __shared__ unsigned s_dead[NB][32], s_out[NB][32]; // per (iteration, warp)
+    __shared__ unsigned s_opre[NB][32];                // exclusive prefix of s_out
     __shared__ uint32_t s_obase[NB];
+    __shared__ int s_nnear[NB]; // slots of the tile queued for k_move_near
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
@@ -501,6 +510,8 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
             if (blockIdx.x + i * gridDim.x < total)
                 issue(blockIdx.x + i * gridDim.x, i);
     }
+    if (threadIdx.x < NB)
+        s_nnear[threadIdx.x] = 0;
     __syncthreads();
 
     int cur_case = -1;
@@ -557,11 +568,9 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
             }
             const unsigned bd = __ballot_sync(0xffffffffu, m.dead);
             const unsigned bo = __ballot_sync(0xffffffffu, m.out);
-            const unsigned bi = __ballot_sync(0xffffffffu, m.in);
             if (lane == 0) {
                 s_dead[nb][k * MOVE_WARPS + warp] = bd;
                 s_out[nb][k * MOVE_WARPS + warp] = bo;
-                s_in[nb][k * MOVE_WARPS + warp] = bi;
             }
         }
         // Slots for the exact body go to k_move_near's queue as (tile, slot
@@ -569,6 +578,8 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
         const unsigned nq = __ballot_sync(0xffffffffu, near != 0);
         if (nq) {
             int n_mine = __popc(near);
+            if (n_mine)
+                atomicAdd(&s_nnear[nb], n_mine);
             int incl = n_mine;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -620,8 +631,12 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
             const unsigned out_tile = __shfl_sync(0xffffffffu, oi, 31);
             const unsigned dead_tile =
                 static_cast<unsigned>(warp_sum_u64(__popc(s_dead[nb][lane])));
-            const unsigned in_tile = static_cast<unsigned>(warp_sum_u64(__popc(s_in[nb][lane])));
             if (lane == 0) {
+                // Every slot this kernel moved is removed, out of range or in
+                // range; k_move_near counts the queued ones.
+                const int in_tile = n_here - s_nnear[nb] - static_cast<int>(dead_tile) -
+                                    static_cast<int>(out_tile);
+                s_nnear[nb] = 0; // rewritten for the tile NB iterations on
                 tile_in[t] = static_cast<int32_t>(in_tile);
                 tile_dead[t] = static_cast<int32_t>(dead_tile);
                 s_obase[nb] = out_tile ? atomicAdd(&sc->obuf_count, out_tile) : 0u;
