@@ -57,6 +57,10 @@ struct dsmc_ctx {
     // neighbour on the main stream run there (captured only, see `par`).
     cudaStream_t side_stream = nullptr;
     cudaEvent_t branch_ev[6] = {nullptr};
+    // Pinned chunks of the field read-back into pageable host memory
+    // (allocated by the first large read-back).
+    void *field_stage[2] = {nullptr, nullptr};
+    cudaEvent_t field_ev[2] = {nullptr, nullptr};
     bool par = false; // true while the full step is captured into a graph
     int ncase = 0;
     int precision = DSMC_FP64;
@@ -78,6 +82,7 @@ struct dsmc_ctx {
     int64_t *d_pbases = nullptr;
     TileTables tt{};
 
+    void *arena = nullptr; // the one device allocation all buffers below are carved from
     void *buf[2][5] = {{nullptr}};
     uint32_t *key = nullptr;
     Cells cells{};
@@ -148,6 +153,9 @@ struct Span {
 };
 
 int grid(const dsmc_ctx *c, int kid) { return std::max(1, c->ctas[kid]) * c->sms; }
+
+// Bytes per pinned chunk of the field read-back.
+constexpr size_t FIELD_CHUNK = size_t(8) << 20;
 
 // Chunks of the tile-count scans: enough for the most tiles a case can have
 // (its slots, move and inject tiles rounded up separately).
@@ -351,7 +359,7 @@ template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sampl
     }
     if (do_sample) {
         Span sp(c, KID_SAMPLE);
-        k_sample<T><<<grid(c, KID_SAMPLE), COLLIDE_CELLS, sample_smem<T>(), c->stream>>>(
+        k_sample<T><<<grid(c, KID_SAMPLE), SAMPLE_THREADS, sample_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, c->ncase,
             c->d_err);
     }
@@ -582,7 +590,7 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
     occ(KID_SCATTER, b);
     CK(cudaFuncSetAttribute(k_sample<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(sample_smem<T>())));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sample<T>, COLLIDE_CELLS,
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sample<T>, SAMPLE_THREADS,
                                                      sample_smem<T>()));
     occ(KID_SAMPLE, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_collide_select, 256, 0));
@@ -604,6 +612,12 @@ void free_ctx(dsmc_ctx *c)
     for (auto e : c->branch_ev)
         if (e)
             cudaEventDestroy(e);
+    for (auto e : c->field_ev)
+        if (e)
+            cudaEventDestroy(e);
+    for (void *h : c->field_stage)
+        if (h)
+            cudaFreeHost(h);
     if (c->side_stream)
         cudaStreamDestroy(c->side_stream);
     for (auto &t : c->timed) {
@@ -612,20 +626,8 @@ void free_ctx(dsmc_ctx *c)
     }
     for (auto e : c->event_pool)
         cudaEventDestroy(e);
-    void *ptrs[] = {c->d_cases, c->d_state, c->d_scratch, c->d_err, c->d_tables, c->d_tmp,
-                    c->d_pbases, c->key, c->cells.n_in, c->cells.n_o, c->cells.o_fill,
-                    c->cells.fin, c->cells.ostart, c->cells.base_in, c->cells.start[0],
-                    c->cells.start[1], c->cells.acc, c->tile_in, c->tile_prefix, c->tile_dead,
-                    c->tile_dprefix, c->itile_dead, c->itile_dprefix, c->lb,
-                    c->hole_pos, c->hole_oc, c->obuf, c->olist, c->coll_list,
-                    c->near_list};
-    for (void *p : ptrs)
-        if (p)
-            cudaFree(p);
-    for (auto &side : c->buf)
-        for (void *p : side)
-            if (p)
-                cudaFree(p);
+    if (c->arena) // every device buffer of the context lives in it
+        cudaFree(c->arena);
     if (c->own_stream && c->stream)
         cudaStreamDestroy(c->stream);
     delete c;
@@ -1113,8 +1115,14 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     }
 
     const size_t esz = c->precision == DSMC_FP32 ? sizeof(float) : sizeof(double);
+    // Every device buffer of the context is carved from one allocation (one
+    // cudaMalloc maps the whole range at once: creating and destroying a
+    // context of a few GB then takes about a millisecond instead of tens).
+    // Buffers start on 256-byte boundaries.
+    std::vector<std::pair<void **, size_t>> carve;
     auto alloc = [&](void **p, size_t bytes) -> bool {
-        return cudaMalloc(p, std::max<size_t>(bytes, 16)) == cudaSuccess;
+        carve.emplace_back(p, (std::max<size_t>(bytes, 16) + 255) & ~size_t(255));
+        return true;
     };
     bool ok = true;
     ok &= alloc(reinterpret_cast<void **>(&c->d_cases), sizeof(CaseDev) * n_cases);
@@ -1152,9 +1160,21 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     ok &= alloc(reinterpret_cast<void **>(&c->near_list), sizeof(uint32_t) * slot);
     ok &= alloc(reinterpret_cast<void **>(&c->olist), sizeof(int32_t) * slot);
     ok &= alloc(reinterpret_cast<void **>(&c->coll_list), sizeof(uint32_t) * cell);
+    size_t arena_bytes = 0;
+    for (const auto &b : carve)
+        arena_bytes += b.second;
+    ok &= cudaMalloc(&c->arena, arena_bytes) == cudaSuccess;
     if (!ok) {
+        c->arena = nullptr;
         free_ctx(c);
         return DSMC_ERR_CUDA;
+    }
+    {
+        char *at = static_cast<char *>(c->arena);
+        for (const auto &b : carve) {
+            *b.first = at;
+            at += b.second;
+        }
     }
     int32_t *t = c->d_tables;
     const int w = n_cases + 1;
@@ -1416,12 +1436,45 @@ int dsmc_get_fields(dsmc_ctx *c, int i, dsmc_cell *host_out)
     if (c == nullptr || host_out == nullptr || i < 0 || i >= c->ncase)
         return DSMC_ERR_ARGUMENT;
     const CaseDev &cd = c->hcases[i];
+    const size_t bytes = sizeof(double) * 17 * cd.ncell;
+    // A pinned destination is copied into directly; pageable memory, which
+    // the driver would copy through its own small bounce buffers, goes
+    // through two pinned chunks of the context instead, the device copy of
+    // one overlapping the host copy of the other.
+    cudaPointerAttributes pa{};
+    const bool pinned =
+        cudaPointerGetAttributes(&pa, host_out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError(); // an unregistered pointer is not an error to keep
+    const bool staged = !pinned && bytes > FIELD_CHUNK;
+    if (staged && c->field_stage[0] == nullptr) {
+        for (int k = 0; k < 2; ++k) {
+            CK(cudaMallocHost(&c->field_stage[k], FIELD_CHUNK));
+            CK(cudaEventCreateWithFlags(&c->field_ev[k], cudaEventDisableTiming));
+        }
+    }
     double *tmp = nullptr;
-    CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(double) * 17 * cd.ncell, c->stream));
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), bytes, c->stream));
     int s = dsmc_get_fields_device(c, i, tmp);
-    if (s == 0) {
-        CK(cudaMemcpyAsync(host_out, tmp, sizeof(double) * 17 * cd.ncell, cudaMemcpyDeviceToHost,
-                           c->stream));
+    if (s == 0 && !staged) {
+        CK(cudaMemcpyAsync(host_out, tmp, bytes, cudaMemcpyDeviceToHost, c->stream));
+    } else if (s == 0) {
+        const size_t n = (bytes + FIELD_CHUNK - 1) / FIELD_CHUNK;
+        auto span = [&](size_t k) { return std::min(FIELD_CHUNK, bytes - k * FIELD_CHUNK); };
+        auto issue = [&](size_t k) -> int {
+            CK(cudaMemcpyAsync(c->field_stage[k & 1], reinterpret_cast<char *>(tmp) + k * FIELD_CHUNK,
+                               span(k), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaEventRecord(c->field_ev[k & 1], c->stream));
+            return DSMC_OK;
+        };
+        for (size_t k = 0; k < n && k < 2 && s == 0; ++k)
+            s = issue(k);
+        for (size_t k = 0; k < n && s == 0; ++k) {
+            CK(cudaEventSynchronize(c->field_ev[k & 1]));
+            std::memcpy(reinterpret_cast<char *>(host_out) + k * FIELD_CHUNK, c->field_stage[k & 1],
+                        span(k));
+            if (k + 2 < n)
+                s = issue(k + 2);
+        }
     }
     CK(cudaFreeAsync(tmp, c->stream));
     CK(cudaStreamSynchronize(c->stream));

@@ -1644,16 +1644,35 @@ __global__ void __launch_bounds__(128)
 
 // ---------------------------------------------------------------------------
 // k_sample: Sampling's accumulation (Sampling.cpp:14-31) in the reference's
-// order: one thread per cell walks its particles sequentially, so every FP64
-// sum is bit-identical to the reference's.  The velocities of a block of
-// COLLIDE_CELLS cells are one contiguous slot range, staged in shared memory
+// order: each sum of a cell is made by one thread that walks the cell's
+// particles sequentially, so every FP64 sum is bit-identical to the
+// reference's.  The velocities of a block of SAMPLE_CELLS cells are one
+// contiguous slot range, staged in shared memory
 // by bulk asynchronous copies (SAMPLE_STAGES per CTA; with one stage, which
 // measured fastest, more CTAs fit on an SM and overlap each other's copies).
 // A block whose range exceeds a stage is read from global memory directly.
 // ---------------------------------------------------------------------------
 constexpr int SAMPLE_STAGES = DSMC_SAMPLE_STAGES;
 constexpr int SAMPLE_UNROLL = DSMC_SAMPLE_UNROLL;
-template <class T> __host__ __device__ constexpr int sample_pcl() { return 12288 / sizeof(T); }
+// Sample blocks of SAMPLE_CELLS cells (a half of a collision block), two
+// threads per cell: the warps of the first half of the CTA sum NP, V and
+// VV00 .. VV11 of their cells, those of the second half VV12, VV22 and V2V.
+// Every sum stays with one thread, in slot order; the split halves the chain
+// each thread walks.
+constexpr int SAMPLE_CELLS = 64;
+constexpr int SAMPLE_SUB = COLLIDE_CELLS / SAMPLE_CELLS; // sample blocks per collision block
+constexpr int SAMPLE_THREADS = 2 * SAMPLE_CELLS;
+static_assert(SAMPLE_CELLS % 32 == 0 && COLLIDE_CELLS % SAMPLE_CELLS == 0,
+              "whole warps per half, whole sample blocks per collision block");
+template <class T> __host__ __device__ constexpr int sample_pcl()
+{
+    return 12288 / sizeof(T) / SAMPLE_SUB;
+}
+// First cell (in its case) of sample block b of case ci.
+__device__ __forceinline__ int sample_cell0(const TileTables &tt, int ci, int b)
+{
+    return (b / SAMPLE_SUB - tt.cblock0[ci]) * COLLIDE_CELLS + (b % SAMPLE_SUB) * SAMPLE_CELLS;
+}
 template <class T> struct SampleStage {
     T v[3][sample_pcl<T>() + 16 / sizeof(T)];
 };
@@ -1662,21 +1681,26 @@ template <class T> __host__ __device__ constexpr size_t sample_smem()
     return sizeof(SampleStage<T>) * SAMPLE_STAGES;
 }
 
-// One particle's terms of the moment sums, in Sampling.cpp:24-30's order.
-// FP64 velocities: products rounded, then added.
-__device__ __forceinline__ void sample_add(double a[ACC_NC], double v0, double v1, double v2)
+// One particle's terms of the moment sums (Sampling.cpp:24-30), split into
+// the two halves of a cell's threads (add0: NP's partner sums V, VV00, VV01,
+// VV02, VV11; add1: V2V, VV12, VV22).  FP64 velocities: products rounded,
+// then added.
+__device__ __forceinline__ void sample_add0(double a[ACC_NC], double v0, double v1, double v2)
 {
-    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
     a[ACC_V0] += v0;
     a[ACC_V1] += v1;
     a[ACC_V2] += v2;
-    a[ACC_V2V0] += vv * v0;
-    a[ACC_V2V1] += vv * v1;
-    a[ACC_V2V2] += vv * v2;
     a[ACC_VV00] += v0 * v0;
     a[ACC_VV01] += v0 * v1;
     a[ACC_VV02] += v0 * v2;
     a[ACC_VV11] += v1 * v1;
+}
+__device__ __forceinline__ void sample_add1(double a[ACC_NC], double v0, double v1, double v2)
+{
+    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
+    a[ACC_V2V0] += vv * v0;
+    a[ACC_V2V1] += vv * v1;
+    a[ACC_V2V2] += vv * v2;
     a[ACC_VV12] += v1 * v2;
     a[ACC_VV22] += v2 * v2;
 }
@@ -1684,27 +1708,30 @@ __device__ __forceinline__ void sample_add(double a[ACC_NC], double v0, double v
 // significand bits), so s + u * v rounds once either way and a fused
 // multiply-add gives the same bits as the separate product and sum, with one
 // FP64 operation instead of two.  vv * v is not exact and keeps its rounding.
-__device__ __forceinline__ void sample_add(double a[ACC_NC], float f0, float f1, float f2)
+__device__ __forceinline__ void sample_add0(double a[ACC_NC], float f0, float f1, float f2)
 {
     const double v0 = f0, v1 = f1, v2 = f2;
-    const double p00 = v0 * v0;
-    const double vv = __fma_rn(v2, v2, __fma_rn(v1, v1, p00));
     a[ACC_V0] += v0;
     a[ACC_V1] += v1;
     a[ACC_V2] += v2;
-    a[ACC_V2V0] += vv * v0;
-    a[ACC_V2V1] += vv * v1;
-    a[ACC_V2V2] += vv * v2;
-    a[ACC_VV00] += p00;
+    a[ACC_VV00] += v0 * v0;
     a[ACC_VV01] = __fma_rn(v0, v1, a[ACC_VV01]);
     a[ACC_VV02] = __fma_rn(v0, v2, a[ACC_VV02]);
     a[ACC_VV11] = __fma_rn(v1, v1, a[ACC_VV11]);
+}
+__device__ __forceinline__ void sample_add1(double a[ACC_NC], float f0, float f1, float f2)
+{
+    const double v0 = f0, v1 = f1, v2 = f2;
+    const double vv = __fma_rn(v2, v2, __fma_rn(v1, v1, v0 * v0));
+    a[ACC_V2V0] += vv * v0;
+    a[ACC_V2V1] += vv * v1;
+    a[ACC_V2V2] += vv * v2;
     a[ACC_VV12] = __fma_rn(v1, v2, a[ACC_VV12]);
     a[ACC_VV22] = __fma_rn(v2, v2, a[ACC_VV22]);
 }
 
 template <class T>
-__global__ void __launch_bounds__(COLLIDE_CELLS)
+__global__ void __launch_bounds__(SAMPLE_THREADS)
     k_sample(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt, Slots<T> p,
              Cells cells, int side, int ncase, int *err)
 {
@@ -1716,18 +1743,20 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
     __shared__ int s_staged[S];
     __shared__ int64_t s_r0[S]; // first staged slot (rounded down to A)
     const int32_t *start = start_of(cells, side);
-    const int nblocks = tt.cblock0[ncase];
+    const int nblocks = tt.cblock0[ncase] * SAMPLE_SUB;
 
     // Thread 0 only: stages the velocities of block b in stage sidx when its
     // case samples this step and the range fits.
     auto issue = [&](int b, int sidx) {
         s_staged[sidx] = 0;
-        const int ci = case_of(tt.cblock0, ncase, b);
+        const int ci = case_of(tt.cblock0, ncase, b / SAMPLE_SUB);
         if (st[ci].sampling_mode != 1)
             return;
         const CaseDev &c = cases[ci];
-        const int cl0 = (b - tt.cblock0[ci]) * COLLIDE_CELLS;
-        const int cl1 = min(cl0 + COLLIDE_CELLS, c.ncell);
+        const int cl0 = sample_cell0(tt, ci, b);
+        if (cl0 >= c.ncell)
+            return;
+        const int cl1 = min(cl0 + SAMPLE_CELLS, c.ncell);
         const int64_t r0 = start[c.cbase + cl0] & ~static_cast<int64_t>(A - 1);
         const int64_t r1 = (start[c.cbase + cl1] + A - 1) & ~static_cast<int64_t>(A - 1);
         const int64_t n = r1 - r0;
@@ -1757,13 +1786,13 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
         if (b >= nblocks)
             return;
         const int sidx = it % S;
-        const int ci = case_of(tt.cblock0, ncase, b);
+        const int ci = case_of(tt.cblock0, ncase, b / SAMPLE_SUB);
         const bool staged = s_staged[sidx] != 0;
+        const int half = threadIdx.x / SAMPLE_CELLS; // uniform over a warp
         bool ok = true;
         if (st[ci].sampling_mode == 1) {
             const CaseDev &c = cases[ci];
-            const int cl0 = (b - tt.cblock0[ci]) * COLLIDE_CELLS;
-            const int cl = cl0 + threadIdx.x;
+            const int cl = sample_cell0(tt, ci, b) + static_cast<int>(threadIdx.x % SAMPLE_CELLS);
             const int cg = c.cbase + cl;
             const bool mine = cl < c.ncell;
             int64_t a0 = 0;
@@ -1774,7 +1803,8 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
                 n = static_cast<int>(start[cg + 1] - a0);
 #pragma unroll
                 for (int m = 0; m < ACC_NC; ++m)
-                    a[m] = cells.acc[m * cells.acc_stride + cg];
+                    if ((m <= ACC_VV11) == (half == 0))
+                        a[m] = cells.acc[m * cells.acc_stride + cg];
             }
             const T *vx = p.vx + c.pbase + a0, *vy = p.vy + c.pbase + a0,
                     *vz = p.vz + c.pbase + a0;
@@ -1787,17 +1817,26 @@ __global__ void __launch_bounds__(COLLIDE_CELLS)
                 vz = stage[sidx].v[2] + off;
             }
             if (mine && n > 0 && ok) {
-                // The count is a sum of n ones: exact, so one add of n.
-                a[ACC_NP] += static_cast<double>(n);
                 // Unrolled so that the loads and products of the next
                 // particles overlap the adds of this one (the sums keep
                 // their order: only the adds into a[] chain).
+                if (half == 0) {
+                    // The count is a sum of n ones: exact, so one add of n.
+                    a[ACC_NP] += static_cast<double>(n);
 #pragma unroll SAMPLE_UNROLL
-                for (int i = 0; i < n; ++i)
-                    sample_add(a, vx[i], vy[i], vz[i]);
+                    for (int i = 0; i < n; ++i)
+                        sample_add0(a, vx[i], vy[i], vz[i]);
 #pragma unroll
-                for (int m = 0; m < ACC_NC; ++m)
-                    cells.acc[m * cells.acc_stride + cg] = a[m];
+                    for (int m = 0; m <= ACC_VV11; ++m)
+                        cells.acc[m * cells.acc_stride + cg] = a[m];
+                } else {
+#pragma unroll SAMPLE_UNROLL
+                    for (int i = 0; i < n; ++i)
+                        sample_add1(a, vx[i], vy[i], vz[i]);
+#pragma unroll
+                    for (int m = ACC_VV12; m < ACC_NC; ++m)
+                        cells.acc[m * cells.acc_stride + cg] = a[m];
+                }
             }
         }
         // The stage is consumed: refill it with this CTA's block it + S.
