@@ -29,14 +29,14 @@ namespace {
     } while (0)
 
 enum KernelId {
-    KID_PLAN, KID_MOVE, KID_MOVE_NEAR, KID_INJECT, KID_DEAD_SCAN, KID_HOLES, KID_PLAN2, KID_TAIL,
+    KID_PLAN, KID_MOVE, KID_MOVE_NEAR, KID_INJECT, KID_DEAD_SCAN, KID_HOLES, KID_TAIL,
     KID_CELL_SCAN, KID_TILE_SCAN,
     KID_OLIST, KID_CELL_FIX, KID_SCATTER, KID_COLLIDE_SELECT, KID_COLLIDE, KID_SAMPLE,
     KID_FINISH, KID_COUNT
 };
 const char *kKernelNames[KID_COUNT] = {
     "k_plan",      "k_move",   "k_move_near",      "k_inject",         "k_dead_scan",     "k_holes",
-    "k_plan2",     "k_tail",
+    "k_tail",
     "k_cell_scan", "k_tile_scan", "k_olist",       "k_cell_fix",      "k_scatter",
     "k_collide_select", "k_collide_pairs", "k_sample", "k_finish"};
 
@@ -276,12 +276,7 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
         Span sp(c, KID_HOLES);
         k_holes<<<grid(c, KID_HOLES), TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, c->key, c->tile_dead, c->tile_dprefix,
-            c->itile_dead, c->itile_dprefix, c->hole_pos, c->hole_oc, c->ncase);
-    }
-    {
-        Span sp(c, KID_PLAN2);
-        k_plan2<<<1, 1024, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch, c->tt,
-                                           c->hole_pos, c->d_tmp, c->ncase);
+            c->itile_dead, c->itile_dprefix, c->hole_pos, c->hole_oc, c->d_tmp, c->ncase);
     }
     {
         Span sp(c, KID_TAIL);
@@ -343,7 +338,9 @@ template <class T> int enqueue_index(dsmc_ctx *c)
     return DSMC_OK;
 }
 
-template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sample)
+// `finish`: k_sample also ends the step (a full step; the staged calls end
+// it with k_finish).
+template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sample, int finish = 0)
 {
     if (do_collide) {
         if (c->par) // launched on the side stream by enqueue_index
@@ -361,7 +358,7 @@ template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sampl
         Span sp(c, KID_SAMPLE);
         k_sample<T><<<grid(c, KID_SAMPLE), SAMPLE_THREADS, sample_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, c->ncase,
-            c->d_err);
+            finish, c->d_err);
     }
     CK(cudaGetLastError());
     return DSMC_OK;
@@ -385,9 +382,7 @@ template <class T> int enqueue_step(dsmc_ctx *c)
         return s;
     if ((s = enqueue_index<T>(c)))
         return s;
-    if ((s = enqueue_collide<T>(c, 1, 1)))
-        return s;
-    return enqueue_finish(c, 0, 1, 1);
+    return enqueue_collide<T>(c, 1, 1, 1); // k_sample ends the step
 }
 
 int dispatch_step(dsmc_ctx *c)

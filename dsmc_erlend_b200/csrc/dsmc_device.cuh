@@ -101,6 +101,7 @@ struct StepScratch {
     uint32_t obuf_count;
     uint32_t near_count;  // slots queued by k_move for k_move_near
     uint32_t coll_count;  // cells listed by k_collide_select
+    uint32_t holes_done;  // CTAs of k_holes that have finished
     int32_t init_mode;
 };
 

@@ -9,8 +9,8 @@
 //                        flag, in-range flag, per-cell counts, hole list
 //   k_inject    tiles    GenerateNewParticles for the four strips, appended
 //   k_dead_scan chunks   prefix of removed-slot counts per tile
-//   k_holes     tiles    removed-slot list in slot order
-//   k_plan2     1 CTA    survivors K, hole count H, tail tiles
+//   k_holes     tiles    removed-slot list in slot order; its last CTA:
+//                        survivors K, hole count H, tail tiles
 //   k_tail      tiles    swap-with-last: alive tail slots refill the holes
 //   k_cell_scan tiles    per-cell offsets (stable counting sort)
 //   k_tile_scan chunks   prefix of in-range counts per tile
@@ -19,8 +19,9 @@
 //   k_scatter   tiles    places every in-range particle
 //   k_collide_select  cells  NTC pair counts, list of cells with candidates
 //   k_collide_pairs   list   NTC + VHS collisions of the listed cells
-//   k_sample    cells    moment sampling, one thread per cell
-//   k_finish    1 CTA    Step++, NP = K
+//   k_sample    cells    moment sampling, two threads per cell; in a full
+//                        step its first CTA also ends the step (Step++,
+//                        NP = K); the staged calls use k_finish for that
 //
 // Particle order contract (the reference's, made parallel):
 //   * at the start of a step slots [0, n_old) are sorted by cell, each cell
@@ -903,15 +904,64 @@ __global__ void __launch_bounds__(SCAN_THREADS)
 }
 
 // ---------------------------------------------------------------------------
+// Survivors, holes and the tail of every case, once the removed-slot list is
+// complete (run by the last CTA of k_holes).
+// ---------------------------------------------------------------------------
+__device__ void plan_tail(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
+                          const int32_t *hole_pos, int32_t *tmp, int ncase)
+{
+    // One warp per case: a 33-way search (32 probes a round) for the number
+    // of removed slots below K (the holes); the list is in slot order.  The
+    // list was written by other CTAs of this kernel: read through L2.
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    for (int i = threadIdx.x >> 5; i < ncase; i += nwarps) {
+        CaseState &s = st[i];
+        const int64_t keep = s.n_total - s.dead_total; // dead_total: k_dead_scan
+        const int32_t *hp = hole_pos + cases[i].pbase;
+        int64_t lo = 0, hi = s.dead_total; // first index with hp >= keep is in [lo, hi]
+        while (lo < hi) {
+            const int64_t span = hi - lo;
+            const int64_t idx = lo + ((lane + 1) * span) / 33; // < hi
+            const bool below = __ldcg(hp + idx) < keep;
+            const unsigned bl = __ballot_sync(0xffffffffu, below);
+            const int j = __popc(bl); // probes 0..j-1 are below (monotone)
+            const int64_t lo_n = j > 0 ? __shfl_sync(0xffffffffu, idx, j - 1) + 1 : lo;
+            const int64_t hi_n = j < 32 ? __shfl_sync(0xffffffffu, idx, j < 32 ? j : 31) : hi;
+            lo = lo_n;
+            hi = hi_n;
+        }
+        if (lane == 0) {
+            s.n_keep = keep;
+            s.n_holes = lo;
+            s.n_tail_tiles = static_cast<int32_t>((s.n_total - keep + TILE - 1) / TILE);
+            tmp[i] = s.n_tail_tiles;
+            tmp[ncase + i] = static_cast<int32_t>((keep + TILE - 1) / TILE);
+        }
+    }
+    __syncthreads();
+    case_scan(tt.tail0, tmp, ncase);
+    __syncthreads();
+    case_scan(tt.scatter0, tmp + ncase, ncase);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        sc->total_tail_tiles = tt.tail0[ncase];
+    for (int i = threadIdx.x; i < ncase; i += blockDim.x)
+        st[i].tail_tile0 = tt.tail0[i];
+}
+
+// ---------------------------------------------------------------------------
 // k_holes: the removed-slot list in slot order (hole_pos, and the old cell of
 // each removed slot in hole_oc), from the tiles that have removed slots.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(TILE_THREADS)
-    k_holes(const CaseDev *__restrict__ cases, const CaseState *st, const StepScratch *sc,
-            TileTables tt, const uint32_t *__restrict__ key, const int32_t *tile_dead,
+    k_holes(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+            const uint32_t *__restrict__ key, const int32_t *tile_dead,
             const int32_t *tile_dprefix, const int32_t *itile_dead, const int32_t *itile_dprefix,
-            int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc, int ncase)
+            int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc, int32_t *tmp,
+            int ncase)
 {
+    __shared__ bool s_last;
     __shared__ int s_list[TILE_THREADS];
     const int n_move = sc->total_move_tiles;
     const int total = n_move + sc->total_inject_tiles;
@@ -961,51 +1011,16 @@ __global__ void __launch_bounds__(TILE_THREADS)
         }
         __syncthreads(); // s_list is rewritten by the next group
     }
-}
-
-// ---------------------------------------------------------------------------
-// k_plan2: survivors, holes and the tail of every case.
-// ---------------------------------------------------------------------------
-__global__ void k_plan2(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
-                        const int32_t *hole_pos, int32_t *tmp, int ncase)
-{
-    // One warp per case: a 33-way search (32 probes a round) for the number
-    // of removed slots below K (the holes); the list is in slot order.
-    const int lane = threadIdx.x & 31;
-    const int nwarps = blockDim.x >> 5;
-    for (int i = threadIdx.x >> 5; i < ncase; i += nwarps) {
-        CaseState &s = st[i];
-        const int64_t keep = s.n_total - s.dead_total; // dead_total: k_dead_scan
-        const int32_t *hp = hole_pos + cases[i].pbase;
-        int64_t lo = 0, hi = s.dead_total; // first index with hp >= keep is in [lo, hi]
-        while (lo < hi) {
-            const int64_t span = hi - lo;
-            const int64_t idx = lo + ((lane + 1) * span) / 33; // < hi
-            const bool below = hp[idx] < keep;
-            const unsigned bl = __ballot_sync(0xffffffffu, below);
-            const int j = __popc(bl); // probes 0..j-1 are below (monotone)
-            const int64_t lo_n = j > 0 ? __shfl_sync(0xffffffffu, idx, j - 1) + 1 : lo;
-            const int64_t hi_n = j < 32 ? __shfl_sync(0xffffffffu, idx, j < 32 ? j : 31) : hi;
-            lo = lo_n;
-            hi = hi_n;
-        }
-        if (lane == 0) {
-            s.n_keep = keep;
-            s.n_holes = lo;
-            s.n_tail_tiles = static_cast<int32_t>((s.n_total - keep + TILE - 1) / TILE);
-            tmp[i] = s.n_tail_tiles;
-            tmp[ncase + i] = static_cast<int32_t>((keep + TILE - 1) / TILE);
-        }
-    }
-    __syncthreads();
-    case_scan(tt.tail0, tmp, ncase);
-    __syncthreads();
-    case_scan(tt.scatter0, tmp + ncase, ncase);
+    // The last CTA to finish plans the tail: every hole is listed by then.
+    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0)
-        sc->total_tail_tiles = tt.tail0[ncase];
-    for (int i = threadIdx.x; i < ncase; i += blockDim.x)
-        st[i].tail_tile0 = tt.tail0[i];
+        s_last = atomicAdd(&sc->holes_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last)
+        return;
+    __threadfence();
+    plan_tail(cases, st, sc, tt, hole_pos, tmp, ncase);
 }
 
 // ---------------------------------------------------------------------------
@@ -1681,6 +1696,32 @@ template <class T> __host__ __device__ constexpr size_t sample_smem()
     return sizeof(SampleStage<T>) * SAMPLE_STAGES;
 }
 
+// End of the step (Simulation.cpp:160-161) and Sampling's counters
+// (Sampling.cpp:17-18) when the step sampled, by the threads of one CTA.
+// k_sample's first CTA runs it in a full step: nothing k_sample reads is
+// changed by it.
+__device__ __forceinline__ void finish_cases(const CaseDev *cases, CaseState *st, int ncase,
+                                             int init_mode, int did_sample, int end_step)
+{
+    for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
+        CaseState &s = st[i];
+        s.n_old = s.n_keep;
+        if (init_mode)
+            continue;
+        if (did_sample && s.sampling_mode == 1) {
+            s.sample_step++;
+            s.sample_time += cases[i].dt;
+        }
+        if (end_step) {
+            s.nc_last = s.nc_step;
+            s.nc_total += s.nc_step;
+            s.particle_steps += s.n_keep;
+            s.step++;
+            s.time += cases[i].dt;
+        }
+    }
+}
+
 // One particle's terms of the moment sums (Sampling.cpp:24-30), split into
 // the two halves of a cell's threads (add0: NP's partner sums V, VV00, VV01,
 // VV02, VV11; add1: V2V, VV12, VV22).  FP64 velocities: products rounded,
@@ -1732,9 +1773,11 @@ __device__ __forceinline__ void sample_add1(double a[ACC_NC], float f0, float f1
 
 template <class T>
 __global__ void __launch_bounds__(SAMPLE_THREADS)
-    k_sample(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt, Slots<T> p,
-             Cells cells, int side, int ncase, int *err)
+    k_sample(const CaseDev *__restrict__ cases, CaseState *st, TileTables tt, Slots<T> p,
+             Cells cells, int side, int ncase, int finish, int *err)
 {
+    if (finish && blockIdx.x == 0)
+        finish_cases(cases, st, ncase, 0, 1, 1);
     constexpr int S = SAMPLE_STAGES;
     constexpr int A = 16 / sizeof(T); // elements per 16 bytes
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1868,23 +1911,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS)
 __global__ void k_finish(const CaseDev *cases, CaseState *st, int ncase, int init_mode,
                          int did_sample, int end_step)
 {
-    for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
-        CaseState &s = st[i];
-        s.n_old = s.n_keep;
-        if (init_mode)
-            continue;
-        if (did_sample && s.sampling_mode == 1) {
-            s.sample_step++;
-            s.sample_time += cases[i].dt;
-        }
-        if (end_step) {
-            s.nc_last = s.nc_step;
-            s.nc_total += s.nc_step;
-            s.particle_steps += s.n_keep;
-            s.step++;
-            s.time += cases[i].dt;
-        }
-    }
+    finish_cases(cases, st, ncase, init_mode, did_sample, end_step);
 }
 
 } // namespace dsmc

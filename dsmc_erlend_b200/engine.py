@@ -140,10 +140,20 @@ class Engine:
         check(self._lib.dsmc_get_counters(self._h, case, C.byref(c)), "dsmc_get_counters")
         return c.as_dict()
 
-    def GatherGlobalField(self, case: int = 0) -> np.ndarray:
-        """Moments of every cell, shape (nx*ny, 17), CELL layout, x-major."""
+    def GatherGlobalField(self, case: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """Moments of every cell, shape (nx*ny, 17), CELL layout, x-major.
+
+        `out`, when given, receives them (float64, C-contiguous, that shape) and
+        is returned: a buffer kept across calls avoids touching fresh pages,
+        and a pinned one (page-locked, e.g. from torch's pin_memory) is copied
+        into directly by the device."""
         p = self.params[case]
-        out = np.empty((p.nx * p.ny, 17), dtype=np.float64)
+        shape = (p.nx * p.ny, 17)
+        if out is None:
+            out = np.empty(shape, dtype=np.float64)
+        elif (out.shape != shape or out.dtype != np.float64
+              or not out.flags["C_CONTIGUOUS"] or not out.flags["WRITEABLE"]):
+            raise ValueError(f"out must be a writeable C-contiguous float64 array of shape {shape}")
         check(self._lib.dsmc_get_fields(self._h, case, out.ctypes.data_as(C.c_void_p)),
               "dsmc_get_fields")
         return out
