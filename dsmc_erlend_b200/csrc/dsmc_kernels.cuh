@@ -438,7 +438,7 @@ template <class T> struct MoveStage {
 #define DSMC_SAMPLE_STAGES 1
 #endif
 #ifndef DSMC_SAMPLE_UNROLL // unroll of k_sample's per-cell loop
-#define DSMC_SAMPLE_UNROLL 4
+#define DSMC_SAMPLE_UNROLL 8
 #endif
 #ifndef DSMC_MOVE_MIN_BLOCKS // CTAs per SM k_move is compiled for (register budget)
 #define DSMC_MOVE_MIN_BLOCKS 4
@@ -1129,10 +1129,13 @@ __global__ void __launch_bounds__(TILE_THREADS)
 // k_cell_scan: per case, exclusive sums over its cells of the in-range and
 // out-of-range counts (Fin, ostart) and the new cell starts.
 // ---------------------------------------------------------------------------
-// Cells per tile of k_cell_scan (CELL_VEC consecutive cells per thread).
-// Measured on B200: 4 (1024-cell tiles) against 16, which halves the tiles
-// in flight and doubled the kernel's time.
-constexpr int CELL_VEC = 4;
+// Cells per tile of k_cell_scan: each warp takes 32 x CELL_VEC consecutive
+// cells as CELL_VEC rows of 32 (a row per load, so every load and store of a
+// warp is contiguous), scanned row by row with warp shuffles.
+#ifndef DSMC_CELL_VEC
+#define DSMC_CELL_VEC 4
+#endif
+constexpr int CELL_VEC = DSMC_CELL_VEC;
 constexpr int CELL_TILE = TILE_THREADS * CELL_VEC;
 
 __global__ void __launch_bounds__(TILE_THREADS)
@@ -1141,6 +1144,8 @@ __global__ void __launch_bounds__(TILE_THREADS)
 {
     __shared__ int s_tile;
     int32_t *start = start_of(cells, new_side);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0)
@@ -1152,38 +1157,49 @@ __global__ void __launch_bounds__(TILE_THREADS)
         const int ci = case_of(tt.cell0, ncase, t);
         const CaseDev &c = cases[ci];
         const int local_tile = t - tt.cell0[ci];
-        const int c0 = local_tile * CELL_TILE + threadIdx.x * CELL_VEC;
-        uint32_t a[CELL_VEC], b[CELL_VEC];
-        uint32_t sa = 0, sb = 0;
+        const int w0 = local_tile * CELL_TILE + warp * (32 * CELL_VEC); // warp's first cell
+        unsigned long long v[CELL_VEC]; // pack2(in-range, out-of-range) of row k's cell
+        unsigned long long mine = 0;
 #pragma unroll
         for (int k = 0; k < CELL_VEC; ++k) {
-            a[k] = b[k] = 0;
-            if (c0 + k < c.ncell) {
-                a[k] = static_cast<uint32_t>(cells.n_in[c.cbase + c0 + k]);
-                b[k] = static_cast<uint32_t>(cells.n_o[c.cbase + c0 + k]);
+            const int cc = w0 + k * 32 + lane;
+            uint32_t a = 0, b = 0;
+            if (cc < c.ncell) {
+                a = static_cast<uint32_t>(cells.n_in[c.cbase + cc]);
+                b = static_cast<uint32_t>(cells.n_o[c.cbase + cc]);
             }
-            sa += a[k];
-            sb += b[k];
+            v[k] = pack2(a, b);
+            mine += v[k];
         }
+        // Warps in cell order: the exclusive prefix of lane 0 of a warp is
+        // the sum of the warps before it.
         unsigned long long tot;
-        const unsigned long long ex =
-            block_exclusive<unsigned long long>(pack2(sa, sb), tot);
-        // All tiles of a grid run in one wave: the whole CTA walks back.
-        const uint64_t base =
-            lookback_block<TILE_THREADS>(lb, t, t - local_tile, tot, err) + ex;
-        uint32_t ra = pack2_a(base), rb = pack2_b(base);
+        const unsigned long long ex = block_exclusive<unsigned long long>(mine, tot);
+        const unsigned long long wex = __shfl_sync(0xffffffffu, ex, 0);
+        unsigned long long run =
+            lookback_block<TILE_THREADS>(lb, t, t - local_tile, tot, err) + wex;
 #pragma unroll
         for (int k = 0; k < CELL_VEC; ++k) {
-            const int cc = c0 + k;
+            unsigned long long inc = v[k];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long u = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o)
+                    inc += u;
+            }
+            const unsigned long long base = run + inc - v[k];
+            const int cc = w0 + k * 32 + lane;
+            const uint32_t ra = pack2_a(base), rb = pack2_b(base);
             if (cc < c.ncell) {
                 cells.fin[c.cbase + cc] = static_cast<int32_t>(ra);
                 cells.ostart[c.cbase + cc] = static_cast<int32_t>(rb);
                 start[c.cbase + cc] = static_cast<int32_t>(ra + rb);
             }
-            ra += a[k];
-            rb += b[k];
-            if (cc == c.ncell - 1)
-                start[c.cbase + c.ncell] = static_cast<int32_t>(ra + rb);
+            if (cc == c.ncell - 1) {
+                const unsigned long long end = base + v[k];
+                start[c.cbase + c.ncell] = static_cast<int32_t>(pack2_a(end) + pack2_b(end));
+            }
+            run += __shfl_sync(0xffffffffu, inc, 31);
         }
     }
 }
