@@ -1447,8 +1447,16 @@ int dsmc_get_fields(dsmc_ctx *c, int i, dsmc_cell *host_out)
             CK(cudaEventCreateWithFlags(&c->field_ev[k], cudaEventDisableTiming));
         }
     }
+    // The gathered cells go to the changed-cell list buffer when it is large
+    // enough and no staged step is in progress: it is rebuilt within every
+    // step, and this call is ordered on the context's stream between steps.
+    const bool in_scratch = c->stage == 0 &&
+                            bytes <= sizeof(uint32_t) * 2 * static_cast<size_t>(c->total_slots);
     double *tmp = nullptr;
-    CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), bytes, c->stream));
+    if (in_scratch)
+        tmp = reinterpret_cast<double *>(c->obuf);
+    else
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&tmp), bytes, c->stream));
     int s = dsmc_get_fields_device(c, i, tmp);
     if (s == 0 && !staged) {
         CK(cudaMemcpyAsync(host_out, tmp, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -1471,7 +1479,8 @@ int dsmc_get_fields(dsmc_ctx *c, int i, dsmc_cell *host_out)
                 s = issue(k + 2);
         }
     }
-    CK(cudaFreeAsync(tmp, c->stream));
+    if (!in_scratch)
+        CK(cudaFreeAsync(tmp, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return s;
 }
