@@ -54,7 +54,7 @@ CELL_BYTES = {"k_sample": 2 * 13 * 8 + 4}
 # the particles of a launch (profiles/*_640_case_ncu.md).  Below the
 # algorithmic bytes because part of the written state is still in the 126 MB
 # L2 when the kernel ends.
-NCU_TRAFFIC_PER_PARTICLE = {"k_scatter": 37.4, "k_move": 22.2, "k_sample": 19.7}
+NCU_TRAFFIC_PER_PARTICLE = {"k_scatter": 37.7, "k_move": 22.2, "k_sample": 19.4}
 
 
 def peaks():
