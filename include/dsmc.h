@@ -245,15 +245,19 @@ int dsmc_synchronize(dsmc_ctx *ctx);
 int dsmc_get_counters(dsmc_ctx *ctx, int case_index, dsmc_counters *out);
 
 /* Accumulated moments of one case, nx*ny cells x-major, as GatherGlobalField
- * (MPIManager.cpp:305-499) returns them. */
+ * (MPIManager.cpp:305-499) returns them.  The expanded moments are gathered
+ * on the device into the context's changed-cell list buffer (between steps,
+ * when it is large enough) or else a temporary stream-ordered allocation,
+ * then copied to host_out: directly when host_out is page-locked, otherwise
+ * through two pinned chunks of the context. */
 int dsmc_get_fields(dsmc_ctx *ctx, int case_index, dsmc_cell *host_out);
 /* dsmc_get_fields without any allocation.  No counterpart in the reference:
  * it exists for callers that cannot allocate device memory at read-out time,
  * for example a thread reading results while another thread captures a CUDA
  * graph in global capture mode (cudaMalloc then fails), an application whose
  * device memory is already reserved by its own pool, or a monitor that must
- * not stall the device (cudaFree synchronizes it).  dsmc_get_fields stages the
- * expanded moments in a temporary device buffer; this variant stages them in
+ * not stall the device (cudaFree synchronizes it).  dsmc_get_fields may stage
+ * the expanded moments in a temporary device buffer; this variant stages them in
  * one static device array of DSMC_FIELDS_NOALLOC_MAX_CELLS cells (8.9 MB,
  * held by every GPU that loads the library until the process exits).
  *   - A case with more cells returns DSMC_ERR_TOO_LARGE and touches nothing.
