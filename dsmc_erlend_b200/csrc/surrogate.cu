@@ -1,9 +1,11 @@
 // surrogate.cu - kernels of the BF16 convolutional field surrogate
 // (include/dsmc_surrogate.h).
 //
-// The 3x3 convolutions are implicit GEMMs on the tensor cores with
-// mma.sync.m16n8k16 (bf16 in, fp32 accumulate); tiles move global -> shared
-// with cp.async and shared -> registers with ldmatrix, in a 3-stage pipeline.
+// The 3x3 convolutions are implicit GEMMs on the tensor cores.  Forward and
+// dgrad run on the 5th-generation tensor cores (tcgen05.mma, operands in
+// shared memory, FP32 accumulator in tensor memory, read back with
+// tcgen05.ld); the weight gradient uses mma.sync.m16n8k16 with tiles moved
+// global -> shared by cp.async and shared -> registers by ldmatrix.
 //   forward  C[pixel][cout]       = sum_(tap, cin) X[pixel + tap][cin] W[cout][tap][cin]
 //   dgrad    the forward with the weights rotated by 180 degrees and the
 //            channel roles swapped (stride 1, padding 1: the transpose of a
@@ -14,12 +16,13 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "../../include/dsmc_surrogate.h"
 
 namespace {
 
-constexpr int OK = 0, ERR_ARG = 2, ERR_CUDA = 50;
+constexpr int OK = 0, ERR_ARG = 2, ERR_CUDA = 50, ERR_TIMEOUT = 60;
 
 using bf16 = __nv_bfloat16;
 
@@ -42,22 +45,10 @@ template <int N> __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-__device__ __forceinline__ void ldsm_x4(uint32_t r[4], const void *p)
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
 __device__ __forceinline__ void ldsm_x4_t(uint32_t r[4], const void *p)
 {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
-__device__ __forceinline__ void ldsm_x2(uint32_t r[2], const void *p)
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];"
-                 : "=r"(r[0]), "=r"(r[1])
                  : "r"(smem_u32(p)));
 }
 __device__ __forceinline__ void ldsm_x2_t(uint32_t r[2], const void *p)
@@ -102,129 +93,289 @@ __device__ __forceinline__ void st8(bf16 *p, const V8 &r)
 }
 
 // ---------------------------------------------------------------------------
-// Forward (and dgrad): CTA tile 128 pixels x 64 output channels, k-tiles of
-// 32 input channels of one tap; 8 warps as 4 (pixels) x 2 (channels), each
-// 32 x 32.  Shared rows are padded to 40 elements (80 bytes) so ldmatrix's
-// eight 16-byte rows fall on distinct banks.
+// Forward (and dgrad) on the 5th-generation tensor cores.
+//
+// CTA tile TBM = 128 pixels x BN output channels, warp-specialised: warps
+// 0-3 (128 threads) gather the operands and later run the epilogue (thread t
+// owns accumulator row t, i.e. tensor-memory lane t; warp w reads lanes
+// 32w .. 32w + 31); warp 4 allocates tensor memory and one of its threads
+// issues the MMAs.  The reduction index is k = tap * Cin + ci, cut into
+// chunks of TBK = 64; a chunk is gathered with cp.async (the implicit
+// im2col: 8 consecutive k of a pixel are 16 contiguous bytes of x, zeros
+// outside the image or beyond the 9 taps) into one of TST stages.  Each
+// gatherer waits for its own copies, fences them to the async proxy and
+// arrives on the stage's `full` barrier; the MMA thread waits on it, issues
+// the chunk's four tcgen05.mma (M 128, N BN, K 16) and commits them to the
+// stage's `empty` barrier, which the gatherers wait on before the refill.
+//
+// Shared operands are K-major with the 128-byte swizzle: a row's 64 k (128
+// bytes) fill one 128-byte line, 8-row groups are 1024-byte atoms, and the
+// 16-byte piece j of row r sits at piece j ^ (r % 8) of its line:
+//   (r / 8) * 1024 + (r % 8) * 128 + ((j ^ (r % 8)) * 16).
+// A warp's copies then cover whole global lines (8 lanes per row) and whole
+// shared lines (no bank conflict).  Descriptor: stride-byte offset 1024 (the
+// next 8 rows), leading-byte offset unused (16), layout SWIZZLE_128B; the
+// j-th K-16 step starts 32 j bytes into the atom.
 // ---------------------------------------------------------------------------
-constexpr int FBM = 128, FBN = 64, FBK = 32, FST = 3, FLD = FBK + 8;
+constexpr int TBM = 128, TBK = 64, TST = 4;
+constexpr int TC_THREADS = TBM + 32;
+constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;
 
-__global__ void __launch_bounds__(256)
-    k_conv_fwd(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
-               const float *__restrict__ bias, const bf16 *__restrict__ res, bf16 *__restrict__ y,
-               float *__restrict__ y32, int N, int H, int W, int Cin, int Cout, int relu)
+__device__ int g_tc_error; // a bounded wait of a tensor-core kernel gave up
+
+__device__ __forceinline__ void tc_mbar_init(uint64_t *bar, uint32_t count)
 {
-    __shared__ __align__(128) bf16 sA[FST][FBM][FLD];
-    __shared__ __align__(128) bf16 sB[FST][FBN][FLD];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp & 3, wn = warp >> 2;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool tc_mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    for (uint32_t spins = 0; spins < TC_SPIN_LIMIT; ++spins) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(smem_u32(bar)), "r"(parity)
+                     : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, version 1.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
+{
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (1ull << 16) | // LBO (unused)
+           (static_cast<uint64_t>(1024 >> 4) << 32) |                     // SBO: 8 rows
+           (1ull << 46) |                                                 // version
+           (2ull << 61);                                                  // SWIZZLE_128B
+}
+// Byte offset of 16-byte piece j of row r in a swizzled operand.
+__device__ __forceinline__ uint32_t sw128_off(int r, int j)
+{
+    return static_cast<uint32_t>((r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4));
+}
+// Instruction descriptor: bf16 A and B (K-major), FP32 accumulator, M x N.
+template <int BN> __host__ __device__ constexpr uint32_t umma_idesc()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
+           (static_cast<uint32_t>(TBM >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                 ::"r"(tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+                 : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Stages plus 1 KB to align the first to a swizzle atom.
+template <int BN> constexpr int tc_smem() { return TST * (TBM + BN) * TBK * 2 + 1024; }
+
+template <int BN>
+__global__ void __launch_bounds__(TC_THREADS)
+    k_conv_fwd_tc(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
+                  const float *__restrict__ bias, const bf16 *__restrict__ res,
+                  bf16 *__restrict__ y, float *__restrict__ y32, int N, int H, int W, int Cin,
+                  int Cout, int relu)
+{
+    static_assert(BN == 32 || BN == 64 || BN == 128, "tensor-memory columns: a power of 2");
+    constexpr uint32_t A_BYTES = TBM * TBK * 2, B_BYTES = BN * TBK * 2;
+    constexpr uint32_t STAGE = A_BYTES + B_BYTES;
+    extern __shared__ __align__(1024) unsigned char tc_smem_dyn[];
+    __shared__ uint64_t bar_full[TST], bar_empty[TST];
+    __shared__ uint64_t bar_done;
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5;
     const int M = N * H * W;
-    const int m0 = blockIdx.x * FBM, n0 = blockIdx.y * FBN;
-    const int cblocks = Cin / FBK;
-    const int KT = 9 * cblocks;
+    const int m0 = blockIdx.x * TBM, n0 = blockIdx.y * BN;
+    const int K = 9 * Cin;
+    const int KT = (K + TBK - 1) / TBK;
 
-    // The two A rows this thread copies, and its B row.
-    int an[2], ah[2], aw[2];
-    bool am[2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        const int m = m0 + (tid >> 2) + 64 * i;
-        am[i] = m < M;
-        const int mm = am[i] ? m : 0;
-        an[i] = mm / (H * W);
-        ah[i] = (mm / W) % H;
-        aw[i] = mm % W;
+    if (warp == 4) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&s_tmem)), "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    const int chunk = (tid & 3) * 8;
-    const int bco = n0 + (tid >> 2);
-
-    auto load = [&](int kt, int st) {
-        const int tap = kt / cblocks, cb = (kt % cblocks) * FBK;
-        const int kh = tap / 3, kw = tap % 3;
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int hh = ah[i] + kh - 1, ww = aw[i] + kw - 1;
-            const bool ok = am[i] && hh >= 0 && hh < H && ww >= 0 && ww < W;
-            const bf16 *src =
-                ok ? x + ((static_cast<int64_t>(an[i]) * H + hh) * W + ww) * Cin + cb + chunk : x;
-            cp_async16(&sA[st][(tid >> 2) + 64 * i][chunk], src, ok);
+    if (tid == 0) {
+        for (int i = 0; i < TST; ++i) {
+            tc_mbar_init(&bar_full[i], TBM); // every gatherer arrives
+            tc_mbar_init(&bar_empty[i], 1);  // one tcgen05.commit
         }
-        const bool okb = bco < Cout;
-        const bf16 *srcb = okb ? w + (static_cast<int64_t>(bco) * 9 + tap) * Cin + cb + chunk : w;
-        cp_async16(&sB[st][tid >> 2][chunk], srcb, okb);
-    };
-
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                acc[i][j][k] = 0.0f;
-
-#pragma unroll
-    for (int s = 0; s < FST - 1; ++s) {
-        if (s < KT)
-            load(s, s);
-        cp_async_commit();
+        tc_mbar_init(&bar_done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int kt = 0; kt < KT; ++kt) {
-        cp_async_wait<FST - 2>();
-        __syncthreads();
-        if (kt + FST - 1 < KT)
-            load(kt + FST - 1, (kt + FST - 1) % FST);
-        cp_async_commit();
-        const int st = kt % FST;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    bool ok = true;
+    // The swizzle acts on address bits: stages start on 1024-byte boundaries.
+    unsigned char *tc_smem_raw =
+        tc_smem_dyn + ((1024u - (smem_u32(tc_smem_dyn) & 1023u)) & 1023u);
+
+    if (warp < 4) {
+        // Gatherer: piece j = tid % 8 of rows tid / 8 + 16 i of A (i < 8)
+        // and of B (i < BN / 16).
+        const int j = tid & 7, r0 = tid >> 3;
+        int an[TBM / 16], ah[TBM / 16], aw[TBM / 16];
+        bool am[TBM / 16];
 #pragma unroll
-        for (int kk = 0; kk < FBK; kk += 16) {
-            uint32_t a[2][4], b[4][2];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-                ldsm_x4(a[mi], &sA[st][wm * 32 + mi * 16 + (lane & 15)][kk + (lane >> 4) * 8]);
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
-                ldsm_x2(b[ni], &sB[st][wn * 32 + ni * 8 + (lane & 7)][kk + ((lane >> 3) & 1) * 8]);
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni)
-                    mma_bf16(acc[mi][ni], a[mi], b[ni]);
+        for (int i = 0; i < TBM / 16; ++i) {
+            const int m = m0 + r0 + 16 * i;
+            am[i] = m < M;
+            const int mm = am[i] ? m : 0;
+            an[i] = mm / (H * W);
+            ah[i] = (mm / W) % H;
+            aw[i] = mm % W;
         }
-    }
-    cp_async_wait<0>();
-
-    const int g = lane >> 2, t = lane & 3;
+        auto load = [&](int kt, int st) {
+            unsigned char *sa = tc_smem_raw + st * STAGE;
+            unsigned char *sb = sa + A_BYTES;
+            const int k = kt * TBK + 8 * j;
+            const bool kin = k < K;
+            const int tap = kin ? k / Cin : 0, ci = k % Cin;
+            const int dh = tap / 3 - 1, dw = tap % 3 - 1;
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+            for (int i = 0; i < TBM / 16; ++i) {
+                const int hh = ah[i] + dh, ww = aw[i] + dw;
+                const bool v = am[i] && kin && hh >= 0 && hh < H && ww >= 0 && ww < W;
+                const bf16 *src =
+                    v ? x + ((static_cast<int64_t>(an[i]) * H + hh) * W + ww) * Cin + ci : x;
+                cp_async16(sa + sw128_off(r0 + 16 * i, j), src, v);
+            }
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int m = m0 + wm * 32 + mi * 16 + g + half * 8;
-            if (m >= M)
-                continue;
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni) {
-                const int co = n0 + wn * 32 + ni * 8 + 2 * t;
-                if (co >= Cout)
-                    continue;
-                float v0 = acc[mi][ni][2 * half] + (bias ? bias[co] : 0.0f);
-                float v1 = acc[mi][ni][2 * half + 1] + (bias ? bias[co + 1] : 0.0f);
-                if (relu) {
-                    v0 = fmaxf(v0, 0.0f);
-                    v1 = fmaxf(v1, 0.0f);
-                }
-                const int64_t o = static_cast<int64_t>(m) * Cout + co;
-                if (res) {
-                    const __nv_bfloat162 r = *reinterpret_cast<const __nv_bfloat162 *>(res + o);
-                    v0 += __bfloat162float(r.x);
-                    v1 += __bfloat162float(r.y);
-                }
-                if (y)
-                    *reinterpret_cast<__nv_bfloat162 *>(y + o) = __floats2bfloat162_rn(v0, v1);
-                if (y32)
-                    *reinterpret_cast<float2 *>(y32 + o) = make_float2(v0, v1);
+            for (int i = 0; i < BN / 16; ++i) {
+                const int row = r0 + 16 * i;
+                const int co = n0 + row;
+                const bool v = co < Cout && kin;
+                // w[co][tap][ci] is w[co][k]: k runs over taps and channels.
+                const bf16 *src = v ? w + static_cast<int64_t>(co) * K + k : w;
+                cp_async16(sb + sw128_off(row, j), src, v);
+            }
+        };
+        // Keep TST - 1 chunks in flight; a chunk's barrier gets this
+        // thread's arrival once its copies have landed.
+        auto publish = [&](int kt) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_mbar_arrive(&bar_full[kt % TST]);
+        };
+        for (int kt = 0; kt < KT; ++kt) {
+            const int st = kt % TST;
+            if (kt >= TST && ok)
+                ok = tc_mbar_wait(&bar_empty[st], static_cast<uint32_t>(((kt - TST) / TST) & 1));
+            if (ok)
+                load(kt, st);
+            cp_async_commit();
+            if (kt >= TST - 1) {
+                cp_async_wait<TST - 1>();
+                publish(kt - (TST - 1));
             }
         }
+        cp_async_wait<0>();
+        for (int kt = KT - (TST - 1) < 0 ? 0 : KT - (TST - 1); kt < KT; ++kt)
+            publish(kt);
+    } else if (tid == TBM) {
+        // MMA issuer.
+        for (int kt = 0; kt < KT; ++kt) {
+            const int st = kt % TST;
+            if (ok)
+                ok = tc_mbar_wait(&bar_full[st], static_cast<uint32_t>((kt / TST) & 1));
+            if (!ok)
+                break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(tc_smem_raw + st * STAGE), sb = sa + A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < TBK / 16; ++kk)
+                umma_bf16(tmem, umma_desc_sw128(sa + 32 * kk), umma_desc_sw128(sb + 32 * kk),
+                          umma_idesc<BN>(), (kt > 0 || kk > 0) ? 1u : 0u);
+            umma_commit(&bar_empty[st]);
+        }
+        umma_commit(&bar_done); // arrives once every MMA issued above is complete
+    }
+    // Epilogue: the gatherers, once every MMA is complete.
+    bool done = true;
+    if (warp < 4)
+        done = tc_mbar_wait(&bar_done, 0);
+    const bool ok_all = __syncthreads_and(ok && done);
+    if (!ok_all && tid == 0)
+        atomicExch(&g_tc_error, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok_all && warp < 4) {
+        const int m = m0 + tid;
+        const bool am = m < M;
+#pragma unroll
+        for (int c = 0; c < BN; c += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c),
+                      r);
+            const int co = n0 + c;
+            if (!am || co >= Cout)
+                continue;
+            float v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                v[i] = __uint_as_float(r[i]) + (bias ? bias[co + i] : 0.0f);
+                if (relu)
+                    v[i] = fmaxf(v[i], 0.0f);
+            }
+            const int64_t o = static_cast<int64_t>(m) * Cout + co;
+            if (res) {
+#pragma unroll
+                for (int h8 = 0; h8 < 2; ++h8) {
+                    const V8 rr = ld8(res + o + 8 * h8);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        v[8 * h8 + i] += rr.v[i];
+                }
+            }
+            if (y) {
+#pragma unroll
+                for (int h8 = 0; h8 < 2; ++h8) {
+                    V8 out;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        out.v[i] = v[8 * h8 + i];
+                    st8(y + o + 8 * h8, out);
+                }
+            }
+            if (y32) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    *reinterpret_cast<float4 *>(y32 + o + 4 * q) =
+                        make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 4)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN)
+                     : "memory");
 }
 
 // w_rot[ci][tap][co] = w[co][8 - tap][ci]: the weights of the dgrad conv.
@@ -549,6 +700,36 @@ int grid_for(int64_t n) { return static_cast<int>(n / 256 + 1 < 4096 ? n / 256 +
 
 int status() { return cudaGetLastError() == cudaSuccess ? OK : ERR_CUDA; }
 
+// The forward convolution on the tensor cores: the widest channel tile that
+// divides Cout (128, 64 or 32 columns of tensor memory).
+template <int BN>
+int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
+                float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
+{
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_fwd_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    tc_smem<BN>());
+    });
+    if (attr != cudaSuccess)
+        return ERR_CUDA;
+    const int M = n * h * w_;
+    dim3 grid((M + TBM - 1) / TBM, cout / BN);
+    k_conv_fwd_tc<BN><<<grid, TC_THREADS, tc_smem<BN>(), s>>>(x, w, bias, res, y, y32, n, h, w_,
+                                                             cin, cout, relu);
+    return status();
+}
+int conv_fwd_launch(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
+                    float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
+{
+    if (cout % 128 == 0)
+        return conv_fwd_tc<128>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, s);
+    if (cout % 64 == 0)
+        return conv_fwd_tc<64>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, s);
+    return conv_fwd_tc<32>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, s);
+}
+
 bool conv_shape_ok(int n, int h, int w, int cin, int cout)
 {
     return n > 0 && h > 0 && w > 0 && cin > 0 && cout > 0 && cin % 32 == 0 && cout % 32 == 0 &&
@@ -565,13 +746,25 @@ int dsmc_sg_conv_fwd(const uint16_t *x, const uint16_t *w, const float *bias, co
 {
     if (!x || !w || (!y && !y32) || !conv_shape_ok(n, h, w_, cin, cout))
         return ERR_ARG;
-    const int M = n * h * w_;
-    dim3 grid((M + FBM - 1) / FBM, (cout + FBN - 1) / FBN);
-    k_conv_fwd<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<const bf16 *>(x), reinterpret_cast<const bf16 *>(w), bias,
-        reinterpret_cast<const bf16 *>(res), reinterpret_cast<bf16 *>(y), y32, n, h, w_, cin,
-        cout, relu);
-    return status();
+    return conv_fwd_launch(reinterpret_cast<const bf16 *>(x), reinterpret_cast<const bf16 *>(w),
+                           bias, reinterpret_cast<const bf16 *>(res), reinterpret_cast<bf16 *>(y),
+                           y32, n, h, w_, cin, cout, relu, static_cast<cudaStream_t>(stream));
+}
+
+int dsmc_sg_check(void *stream)
+{
+    if (cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess)
+        return ERR_CUDA;
+    int flag = 0;
+    if (cudaMemcpyFromSymbol(&flag, g_tc_error, sizeof(int)) != cudaSuccess)
+        return ERR_CUDA;
+    if (flag) {
+        const int zero = 0;
+        if (cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int)) != cudaSuccess)
+            return ERR_CUDA;
+        return ERR_TIMEOUT;
+    }
+    return OK;
 }
 
 int dsmc_sg_conv_dgrad(const uint16_t *dy, const uint16_t *w, uint16_t *w_rot, uint16_t *dx,

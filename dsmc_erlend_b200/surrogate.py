@@ -59,6 +59,7 @@ _SIGS = {
     "dsmc_sg_adam": [_P, _P, _P, _P, _P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float,
                      C.c_int, _P],
     "dsmc_sg_to_bf16": [_P, _P, C.c_int64, _P],
+    "dsmc_sg_check": [_P],
 }
 
 

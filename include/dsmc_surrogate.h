@@ -7,7 +7,8 @@
  * Tensors are NHWC with channel counts that are multiples of 32; activations
  * and weights are bfloat16 (passed as uint16_t bit patterns), accumulation
  * and optimizer state FP32.  Convolutions are 3 x 3, stride 1, zero padding
- * 1; weights are [Cout][3][3][Cin].  Every function enqueues on `stream`
+ * 1; weights are [Cout][3][3][Cin]; forward and input gradient run on the
+ * tcgen05 tensor cores (accumulator in tensor memory).  Every function enqueues on `stream`
  * (a cudaStream_t, NULL for the default stream) and returns DSMC_OK (0),
  * DSMC_ERR_ARGUMENT (2) for shapes outside these rules, or DSMC_ERR_CUDA (50).
  */
@@ -68,6 +69,11 @@ int dsmc_sg_adam(float *w, uint16_t *w_bf16, const float *g, float *m, float *v,
 
 /* FP32 -> bf16 (round to nearest even). */
 int dsmc_sg_to_bf16(const float *x, uint16_t *y, int64_t count, void *stream);
+
+/* Synchronizes `stream`; returns 60 (a timeout) when a tensor-core kernel
+ * gave up one of its bounded waits since the last check (and forgets it),
+ * 50 on a CUDA error, else 0. */
+int dsmc_sg_check(void *stream);
 
 #ifdef __cplusplus
 }
