@@ -95,11 +95,12 @@ __device__ __forceinline__ void st8(bf16 *p, const V8 &r)
 // ---------------------------------------------------------------------------
 // Forward (and dgrad) on the 5th-generation tensor cores.
 //
-// CTA tile TBM = 128 pixels x BN output channels, warp-specialised: warps
-// 0-3 (128 threads) gather the operands and later run the epilogue (thread t
-// owns accumulator row t, i.e. tensor-memory lane t; warp w reads lanes
-// 32w .. 32w + 31); warp 4 allocates tensor memory and one of its threads
-// issues the MMAs.  The reduction index is k = tap * Cin + ci, cut into
+// Persistent CTAs over tiles of TBM = 128 pixels x BN output channels,
+// warp-specialised: warps 0-3 gather the operands, one thread of warp 4
+// issues the MMAs into one of two tensor-memory accumulators (warp 4 also
+// allocates them), and warps 5-8 run the epilogue of the previous tile from
+// the other accumulator (warp w reads tensor-memory lanes 32 (w % 4) ..,
+// thread lane l of it accumulator row 32 (w % 4) + l).  The reduction index is k = tap * Cin + ci, cut into
 // chunks of TBK = 64; a chunk is gathered with cp.async (the implicit
 // im2col: 8 consecutive k of a pixel are 16 contiguous bytes of x, zeros
 // outside the image or beyond the 9 taps) into one of TST stages.  Each
@@ -118,7 +119,7 @@ __device__ __forceinline__ void st8(bf16 *p, const V8 &r)
 // j-th K-16 step starts 32 j bytes into the atom.
 // ---------------------------------------------------------------------------
 constexpr int TBM = 128, TBK = 64, TST = 4;
-constexpr int TC_THREADS = TBM + 32;
+constexpr int TC_THREADS = TBM + 32 + TBM; // gatherers, MMA warp, epilogue
 constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;
 
 __device__ int g_tc_error; // a bounded wait of a tensor-core kernel gave up
@@ -207,17 +208,19 @@ __global__ void __launch_bounds__(TC_THREADS)
     constexpr uint32_t STAGE = A_BYTES + B_BYTES;
     extern __shared__ __align__(1024) unsigned char tc_smem_dyn[];
     __shared__ uint64_t bar_full[TST], bar_empty[TST];
+    __shared__ uint64_t bar_acc_full[2], bar_acc_empty[2];
     __shared__ uint64_t bar_done;
     __shared__ uint32_t s_tmem;
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int M = N * H * W;
-    const int m0 = blockIdx.x * TBM, n0 = blockIdx.y * BN;
     const int K = 9 * Cin;
     const int KT = (K + TBK - 1) / TBK;
+    const int ntiles_n = Cout / BN;
+    const int ntiles = ((M + TBM - 1) / TBM) * ntiles_n;
 
-    if (warp == 4) {
+    if (warp == 4) { // two accumulators: the epilogue of a tile overlaps the next
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     ::"r"(smem_u32(&s_tmem)), "r"(BN)
+                     ::"r"(smem_u32(&s_tmem)), "r"(2 * BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -225,6 +228,10 @@ __global__ void __launch_bounds__(TC_THREADS)
         for (int i = 0; i < TST; ++i) {
             tc_mbar_init(&bar_full[i], TBM); // every gatherer arrives
             tc_mbar_init(&bar_empty[i], 1);  // one tcgen05.commit
+        }
+        for (int i = 0; i < 2; ++i) {
+            tc_mbar_init(&bar_acc_full[i], 1);    // one tcgen05.commit
+            tc_mbar_init(&bar_acc_empty[i], TBM); // every epilogue thread arrives
         }
         tc_mbar_init(&bar_done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -240,141 +247,165 @@ __global__ void __launch_bounds__(TC_THREADS)
 
     if (warp < 4) {
         // Gatherer: piece j = tid % 8 of rows tid / 8 + 16 i of A (i < 8)
-        // and of B (i < BN / 16).
+        // and of B (i < BN / 16).  Chunks are counted across the CTA's tiles
+        // (g), so the stage ring runs on from one tile to the next.
         const int j = tid & 7, r0 = tid >> 3;
-        int an[TBM / 16], ah[TBM / 16], aw[TBM / 16];
-        bool am[TBM / 16];
-#pragma unroll
-        for (int i = 0; i < TBM / 16; ++i) {
-            const int m = m0 + r0 + 16 * i;
-            am[i] = m < M;
-            const int mm = am[i] ? m : 0;
-            an[i] = mm / (H * W);
-            ah[i] = (mm / W) % H;
-            aw[i] = mm % W;
-        }
-        auto load = [&](int kt, int st) {
-            unsigned char *sa = tc_smem_raw + st * STAGE;
-            unsigned char *sb = sa + A_BYTES;
-            const int k = kt * TBK + 8 * j;
-            const bool kin = k < K;
-            const int tap = kin ? k / Cin : 0, ci = k % Cin;
-            const int dh = tap / 3 - 1, dw = tap % 3 - 1;
+        int g = 0;
+        auto publish = [&](int gc) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_mbar_arrive(&bar_full[gc % TST]);
+        };
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const int m0 = (t / ntiles_n) * TBM, n0 = (t % ntiles_n) * BN;
+            int an[TBM / 16], ah[TBM / 16], aw[TBM / 16];
+            bool am[TBM / 16];
 #pragma unroll
             for (int i = 0; i < TBM / 16; ++i) {
-                const int hh = ah[i] + dh, ww = aw[i] + dw;
-                const bool v = am[i] && kin && hh >= 0 && hh < H && ww >= 0 && ww < W;
-                const bf16 *src =
-                    v ? x + ((static_cast<int64_t>(an[i]) * H + hh) * W + ww) * Cin + ci : x;
-                cp_async16(sa + sw128_off(r0 + 16 * i, j), src, v);
+                const int m = m0 + r0 + 16 * i;
+                am[i] = m < M;
+                const int mm = am[i] ? m : 0;
+                an[i] = mm / (H * W);
+                ah[i] = (mm / W) % H;
+                aw[i] = mm % W;
             }
+            for (int kc = 0; kc < KT; ++kc, ++g) {
+                const int st = g % TST;
+                if (g >= TST && ok)
+                    ok = tc_mbar_wait(&bar_empty[st],
+                                      static_cast<uint32_t>(((g - TST) / TST) & 1));
+                if (ok) {
+                    unsigned char *sa = tc_smem_raw + st * STAGE;
+                    unsigned char *sb = sa + A_BYTES;
+                    const int k = kc * TBK + 8 * j;
+                    const bool kin = k < K;
+                    const int tap = kin ? k / Cin : 0, ci = k % Cin;
+                    const int dh = tap / 3 - 1, dw = tap % 3 - 1;
 #pragma unroll
-            for (int i = 0; i < BN / 16; ++i) {
-                const int row = r0 + 16 * i;
-                const int co = n0 + row;
-                const bool v = co < Cout && kin;
-                // w[co][tap][ci] is w[co][k]: k runs over taps and channels.
-                const bf16 *src = v ? w + static_cast<int64_t>(co) * K + k : w;
-                cp_async16(sb + sw128_off(row, j), src, v);
-            }
-        };
-        // Keep TST - 1 chunks in flight; a chunk's barrier gets this
-        // thread's arrival once its copies have landed.
-        auto publish = [&](int kt) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            tc_mbar_arrive(&bar_full[kt % TST]);
-        };
-        for (int kt = 0; kt < KT; ++kt) {
-            const int st = kt % TST;
-            if (kt >= TST && ok)
-                ok = tc_mbar_wait(&bar_empty[st], static_cast<uint32_t>(((kt - TST) / TST) & 1));
-            if (ok)
-                load(kt, st);
-            cp_async_commit();
-            if (kt >= TST - 1) {
-                cp_async_wait<TST - 1>();
-                publish(kt - (TST - 1));
+                    for (int i = 0; i < TBM / 16; ++i) {
+                        const int hh = ah[i] + dh, ww = aw[i] + dw;
+                        const bool v = am[i] && kin && hh >= 0 && hh < H && ww >= 0 && ww < W;
+                        const bf16 *src =
+                            v ? x + ((static_cast<int64_t>(an[i]) * H + hh) * W + ww) * Cin + ci
+                              : x;
+                        cp_async16(sa + sw128_off(r0 + 16 * i, j), src, v);
+                    }
+#pragma unroll
+                    for (int i = 0; i < BN / 16; ++i) {
+                        const int row = r0 + 16 * i;
+                        const int co = n0 + row;
+                        const bool v = co < Cout && kin;
+                        // w[co][tap][ci] is w[co][k]: k runs over taps and channels.
+                        const bf16 *src = v ? w + static_cast<int64_t>(co) * K + k : w;
+                        cp_async16(sb + sw128_off(row, j), src, v);
+                    }
+                }
+                cp_async_commit();
+                // Keep TST - 1 chunks in flight; a chunk's barrier gets this
+                // thread's arrival once its copies have landed.
+                if (g >= TST - 1) {
+                    cp_async_wait<TST - 1>();
+                    publish(g - (TST - 1));
+                }
             }
         }
         cp_async_wait<0>();
-        for (int kt = KT - (TST - 1) < 0 ? 0 : KT - (TST - 1); kt < KT; ++kt)
-            publish(kt);
-    } else if (tid == TBM) {
-        // MMA issuer.
-        for (int kt = 0; kt < KT; ++kt) {
-            const int st = kt % TST;
-            if (ok)
-                ok = tc_mbar_wait(&bar_full[st], static_cast<uint32_t>((kt / TST) & 1));
-            if (!ok)
-                break;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(tc_smem_raw + st * STAGE), sb = sa + A_BYTES;
+        for (int gc = g - (TST - 1) < 0 ? 0 : g - (TST - 1); gc < g; ++gc)
+            publish(gc);
+    } else if (warp == 4) {
+        if (lane == 0) { // MMA issuer
+            int g = 0, i = 0;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
+                const int b = i & 1;
+                if (i >= 2)
+                    ok = tc_mbar_wait(&bar_acc_empty[b],
+                                      static_cast<uint32_t>(((i >> 1) - 1) & 1));
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int kc = 0; kc < KT && ok; ++kc, ++g) {
+                    const int st = g % TST;
+                    ok = tc_mbar_wait(&bar_full[st], static_cast<uint32_t>((g / TST) & 1));
+                    if (!ok)
+                        break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = smem_u32(tc_smem_raw + st * STAGE), sb = sa + A_BYTES;
 #pragma unroll
-            for (int kk = 0; kk < TBK / 16; ++kk)
-                umma_bf16(tmem, umma_desc_sw128(sa + 32 * kk), umma_desc_sw128(sb + 32 * kk),
-                          umma_idesc<BN>(), (kt > 0 || kk > 0) ? 1u : 0u);
-            umma_commit(&bar_empty[st]);
+                    for (int kk = 0; kk < TBK / 16; ++kk)
+                        umma_bf16(tmem + static_cast<uint32_t>(b * BN),
+                                  umma_desc_sw128(sa + 32 * kk), umma_desc_sw128(sb + 32 * kk),
+                                  umma_idesc<BN>(), (kc > 0 || kk > 0) ? 1u : 0u);
+                    umma_commit(&bar_empty[st]);
+                }
+                umma_commit(&bar_acc_full[b]);
+            }
+            umma_commit(&bar_done); // arrives once every MMA issued above is complete
         }
-        umma_commit(&bar_done); // arrives once every MMA issued above is complete
+    } else {
+        // Epilogue: warps 5-8; warp w reads tensor-memory lanes 32 (w % 4) ..
+        const int q = warp & 3;
+        const int row = 32 * q + lane;
+        int i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+            const int b = i & 1;
+            if (ok)
+                ok = tc_mbar_wait(&bar_acc_full[b], static_cast<uint32_t>((i >> 1) & 1));
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int m0 = (t / ntiles_n) * TBM, n0 = (t % ntiles_n) * BN;
+            const int m = m0 + row;
+            const bool am = m < M;
+#pragma unroll
+            for (int c = 0; c < BN; c += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) +
+                              static_cast<uint32_t>(b * BN + c),
+                          r);
+                const int co = n0 + c;
+                if (!ok || !am || co >= Cout)
+                    continue;
+                float v[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    v[e] = __uint_as_float(r[e]) + (bias ? bias[co + e] : 0.0f);
+                    if (relu)
+                        v[e] = fmaxf(v[e], 0.0f);
+                }
+                const int64_t o = static_cast<int64_t>(m) * Cout + co;
+                if (res) {
+#pragma unroll
+                    for (int h8 = 0; h8 < 2; ++h8) {
+                        const V8 rr = ld8(res + o + 8 * h8);
+#pragma unroll
+                        for (int e = 0; e < 8; ++e)
+                            v[8 * h8 + e] += rr.v[e];
+                    }
+                }
+                if (y) {
+#pragma unroll
+                    for (int h8 = 0; h8 < 2; ++h8) {
+                        V8 out;
+#pragma unroll
+                        for (int e = 0; e < 8; ++e)
+                            out.v[e] = v[8 * h8 + e];
+                        st8(y + o + 8 * h8, out);
+                    }
+                }
+                if (y32) {
+#pragma unroll
+                    for (int e4 = 0; e4 < 4; ++e4)
+                        *reinterpret_cast<float4 *>(y32 + o + 4 * e4) = make_float4(
+                            v[4 * e4], v[4 * e4 + 1], v[4 * e4 + 2], v[4 * e4 + 3]);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            tc_mbar_arrive(&bar_acc_empty[b]); // this buffer may be reused
+        }
     }
-    // Epilogue: the gatherers, once every MMA is complete.
-    bool done = true;
-    if (warp < 4)
-        done = tc_mbar_wait(&bar_done, 0);
-    const bool ok_all = __syncthreads_and(ok && done);
-    if (!ok_all && tid == 0)
+    // Every MMA is complete before the tensor memory is released.
+    const bool done = tc_mbar_wait(&bar_done, 0);
+    if (!__syncthreads_and(ok && done) && tid == 0)
         atomicExch(&g_tc_error, 1);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok_all && warp < 4) {
-        const int m = m0 + tid;
-        const bool am = m < M;
-#pragma unroll
-        for (int c = 0; c < BN; c += 16) {
-            uint32_t r[16];
-            tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c),
-                      r);
-            const int co = n0 + c;
-            if (!am || co >= Cout)
-                continue;
-            float v[16];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                v[i] = __uint_as_float(r[i]) + (bias ? bias[co + i] : 0.0f);
-                if (relu)
-                    v[i] = fmaxf(v[i], 0.0f);
-            }
-            const int64_t o = static_cast<int64_t>(m) * Cout + co;
-            if (res) {
-#pragma unroll
-                for (int h8 = 0; h8 < 2; ++h8) {
-                    const V8 rr = ld8(res + o + 8 * h8);
-#pragma unroll
-                    for (int i = 0; i < 8; ++i)
-                        v[8 * h8 + i] += rr.v[i];
-                }
-            }
-            if (y) {
-#pragma unroll
-                for (int h8 = 0; h8 < 2; ++h8) {
-                    V8 out;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i)
-                        out.v[i] = v[8 * h8 + i];
-                    st8(y + o + 8 * h8, out);
-                }
-            }
-            if (y32) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    *reinterpret_cast<float4 *>(y32 + o + 4 * q) =
-                        make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-            }
-        }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
     if (warp == 4)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(2 * BN)
                      : "memory");
 }
 
@@ -714,8 +745,19 @@ int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res
     });
     if (attr != cudaSuccess)
         return ERR_CUDA;
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return ERR_CUDA;
+    }
+    // Persistent: as many CTAs as fit (shared memory: one of 128 channels,
+    // two of fewer per SM), each taking tiles blockIdx.x + i * gridDim.x.
     const int M = n * h * w_;
-    dim3 grid((M + TBM - 1) / TBM, cout / BN);
+    const int64_t tiles = static_cast<int64_t>((M + TBM - 1) / TBM) * (cout / BN);
+    const int per_sm = BN == 128 ? 1 : 2;
+    const int grid = static_cast<int>(tiles < int64_t(sms) * per_sm ? tiles : int64_t(sms) * per_sm);
     k_conv_fwd_tc<BN><<<grid, TC_THREADS, tc_smem<BN>(), s>>>(x, w, bias, res, y, y32, n, h, w_,
                                                              cin, cout, relu);
     return status();
