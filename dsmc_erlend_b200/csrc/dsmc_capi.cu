@@ -230,13 +230,12 @@ void launch_collide_select(dsmc_ctx *c, int side, cudaStream_t stream)
 // MoveParticles: plan + move.
 template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
 {
-    int s = clear_step_scratch(c);
-    if (s)
-        return s;
+    int s; // k_plan clears the step's scratch and the cell scan's chain
     {
         Span sp(c, KID_PLAN);
         k_plan<<<1, 1024, 0, c->stream>>>(c->d_cases, c->d_state, c->d_scratch, c->tt, c->d_tmp,
-                                          c->itile_dead, c->ncase, init_mode, c->d_err);
+                                          c->itile_dead, lb_chain(c, 3), c->ncase, init_mode,
+                                          c->d_err);
     }
     if (!init_mode && c->par) {
         if ((s = branch(c, EV_PLAN, c->stream, c->side_stream)))
@@ -276,7 +275,8 @@ template <class T> int enqueue_boundary(dsmc_ctx *c)
         Span sp(c, KID_HOLES);
         k_holes<<<grid(c, KID_HOLES), TILE_THREADS, 0, c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, c->key, c->tile_dead, c->tile_dprefix,
-            c->itile_dead, c->itile_dprefix, c->hole_pos, c->hole_oc, c->d_tmp, c->ncase);
+            c->itile_dead, c->itile_dprefix, c->hole_pos, c->hole_oc, c->d_tmp, lb_chain(c, 2),
+            c->ncase);
     }
     {
         Span sp(c, KID_TAIL);

@@ -114,9 +114,21 @@ __device__ __forceinline__ void case_scan(int32_t *base, const int32_t *count_of
 // ---------------------------------------------------------------------------
 // k_plan: start of a step (or of the cold start when init_mode is set).
 // ---------------------------------------------------------------------------
+// It first clears the step's scratch counters and the look-back status
+// words of the cell scan (the first kernel of a step: nothing reads them
+// before), so the step needs no memset of its own.
 __global__ void k_plan(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
-                       int32_t *tmp, int32_t *itile_dead, int ncase, int init_mode, int *err)
+                       int32_t *tmp, int32_t *itile_dead, uint64_t *cell_chain, int ncase,
+                       int init_mode, int *err)
 {
+    {
+        uint32_t *words = reinterpret_cast<uint32_t *>(sc);
+        for (int i = threadIdx.x; i < static_cast<int>(sizeof(StepScratch) / 4); i += blockDim.x)
+            words[i] = 0u;
+        for (int i = threadIdx.x; i < tt.cell0[ncase]; i += blockDim.x)
+            cell_chain[i] = 0ull;
+        __syncthreads();
+    }
     for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
         const CaseDev &c = cases[i];
         CaseState &s = st[i];
@@ -908,7 +920,7 @@ __global__ void __launch_bounds__(SCAN_THREADS)
 // complete (run by the last CTA of k_holes).
 // ---------------------------------------------------------------------------
 __device__ void plan_tail(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
-                          const int32_t *hole_pos, int32_t *tmp, int ncase)
+                          const int32_t *hole_pos, int32_t *tmp, uint64_t *tail_chain, int ncase)
 {
     // One warp per case: a 33-way search (32 probes a round) for the number
     // of removed slots below K (the holes); the list is in slot order.  The
@@ -948,6 +960,9 @@ __device__ void plan_tail(const CaseDev *cases, CaseState *st, StepScratch *sc, 
         sc->total_tail_tiles = tt.tail0[ncase];
     for (int i = threadIdx.x; i < ncase; i += blockDim.x)
         st[i].tail_tile0 = tt.tail0[i];
+    // The look-back status words k_tail is about to use.
+    for (int i = threadIdx.x; i < tt.tail0[ncase]; i += blockDim.x)
+        tail_chain[i] = 0ull;
 }
 
 // ---------------------------------------------------------------------------
@@ -959,7 +974,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
             const uint32_t *__restrict__ key, const int32_t *tile_dead,
             const int32_t *tile_dprefix, const int32_t *itile_dead, const int32_t *itile_dprefix,
             int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc, int32_t *tmp,
-            int ncase)
+            uint64_t *tail_chain, int ncase)
 {
     __shared__ bool s_last;
     __shared__ int s_list[TILE_THREADS];
@@ -1020,7 +1035,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
     if (!s_last)
         return;
     __threadfence();
-    plan_tail(cases, st, sc, tt, hole_pos, tmp, ncase);
+    plan_tail(cases, st, sc, tt, hole_pos, tmp, tail_chain, ncase);
 }
 
 // ---------------------------------------------------------------------------
