@@ -67,7 +67,8 @@ def test_conv_forward(cuda, n, h, w, cin, cout):
     assert lib().dsmc_sg_check(None) == 0
 
 
-@pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 10, 6, 64, 32)])
+@pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 10, 6, 64, 32),
+                                            (2, 12, 9, 128, 128), (1, 7, 13, 64, 96)])
 def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
@@ -88,6 +89,7 @@ def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     _close(_np(dx), ref.conv3x3_dgrad(_np(dy), _np(wt)), 2 ** -7 + 1e-4, "dgrad")
     _close(_np(dw), ref.conv3x3_wgrad(_np(dy), _np(x)), 1e-4, "wgrad")
     _close(_np(db), _np(dy).sum(axis=(0, 1, 2)), 1e-4, "bias grad")
+    assert L.dsmc_sg_check(None) == 0
 
 
 def test_wgrad_large_pixel_count_splits(cuda):
@@ -104,6 +106,24 @@ def test_wgrad_large_pixel_count_splits(cuda):
                                     None) == 0
     torch.cuda.synchronize()
     _close(_np(dw) - 1.0, ref.conv3x3_wgrad(_np(dy), _np(x)), 1e-4, "wgrad split")
+
+
+def test_wgrad_wide_input_pixel_splits(cuda):
+    # Cin 128: several pixel splits, a ragged last split, and accumulation
+    # into dw.
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    rng = np.random.default_rng(5)
+    n, h, w, cin, cout = 3, 45, 37, 128, 64
+    x = _bf16(torch, _rand(rng, n, h, w, cin))
+    dy = _bf16(torch, _rand(rng, n, h, w, cout, scale=0.05))
+    dw = torch.ones(cout, 3, 3, cin, dtype=torch.float32, device="cuda")
+    assert lib().dsmc_sg_conv_wgrad(ptr(dy), ptr(x), ptr(dw), None, n, h, w, cin, cout,
+                                    None) == 0
+    torch.cuda.synchronize()
+    _close(_np(dw) - 1.0, ref.conv3x3_wgrad(_np(dy), _np(x)), 1e-4, "wgrad wide split")
+    assert lib().dsmc_sg_check(None) == 0
 
 
 def test_resampling_and_loss_kernels(cuda):
