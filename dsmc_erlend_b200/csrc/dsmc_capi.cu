@@ -96,6 +96,7 @@ struct dsmc_ctx {
     uint32_t *near_list = nullptr; // slots queued by k_move for k_move_near
     int32_t *olist = nullptr;
     uint32_t *coll_list = nullptr; // cells with candidate pairs, per step
+    dsmc_counters *d_counters = nullptr; // every case's counters at the end of the last full step
 
     int cur = 0;
     bool initialized = false;
@@ -358,7 +359,7 @@ template <class T> int enqueue_collide(dsmc_ctx *c, int do_collide, int do_sampl
         Span sp(c, KID_SAMPLE);
         k_sample<T><<<grid(c, KID_SAMPLE), SAMPLE_THREADS, sample_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->tt, slots<T>(c, c->cur), c->cells, c->cur, c->ncase,
-            finish, c->d_err);
+            finish, finish ? c->d_counters : nullptr, c->d_err);
     }
     CK(cudaGetLastError());
     return DSMC_OK;
@@ -1155,6 +1156,7 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     ok &= alloc(reinterpret_cast<void **>(&c->near_list), sizeof(uint32_t) * slot);
     ok &= alloc(reinterpret_cast<void **>(&c->olist), sizeof(int32_t) * slot);
     ok &= alloc(reinterpret_cast<void **>(&c->coll_list), sizeof(uint32_t) * cell);
+    ok &= alloc(reinterpret_cast<void **>(&c->d_counters), sizeof(dsmc_counters) * n_cases);
     size_t arena_bytes = 0;
     for (const auto &b : carve)
         arena_bytes += b.second;
@@ -1280,6 +1282,20 @@ int dsmc_init_warm(dsmc_ctx *c, const double *host_field) { return init_warm(c, 
 int dsmc_init_warm_tensor(dsmc_ctx *c, const double *host_field)
 {
     return init_warm(c, host_field, 7);
+}
+
+int dsmc_step_read(dsmc_ctx *c, int n_steps, dsmc_counters *host_out)
+{
+    if (c == nullptr || host_out == nullptr || n_steps < 0)
+        return DSMC_ERR_ARGUMENT;
+    for (int k = 0; k < n_steps; ++k) {
+        const int s = dsmc_step(c, 1);
+        if (s)
+            return s;
+        CK(cudaMemcpyAsync(host_out + static_cast<size_t>(k) * c->ncase, c->d_counters,
+                           sizeof(dsmc_counters) * c->ncase, cudaMemcpyDeviceToHost, c->stream));
+    }
+    return DSMC_OK;
 }
 
 int dsmc_step(dsmc_ctx *c, int n_steps)

@@ -1732,7 +1732,8 @@ template <class T> __host__ __device__ constexpr size_t sample_smem()
 // k_sample's first CTA runs it in a full step: nothing k_sample reads is
 // changed by it.
 __device__ __forceinline__ void finish_cases(const CaseDev *cases, CaseState *st, int ncase,
-                                             int init_mode, int did_sample, int end_step)
+                                             int init_mode, int did_sample, int end_step,
+                                             dsmc_counters *rec = nullptr)
 {
     for (int i = threadIdx.x; i < ncase; i += blockDim.x) {
         CaseState &s = st[i];
@@ -1749,6 +1750,22 @@ __device__ __forceinline__ void finish_cases(const CaseDev *cases, CaseState *st
             s.particle_steps += s.n_keep;
             s.step++;
             s.time += cases[i].dt;
+        }
+        if (rec) { // the counters of the ended step, as dsmc_get_counters gives them
+            dsmc_counters &r = rec[i];
+            r.np = s.n_old;
+            r.step = s.step;
+            r.sample_step = s.sample_step;
+            r.collisions_last_step = s.nc_last;
+            r.collisions_total = s.nc_total;
+            r.drag_collision_count = static_cast<int64_t>(s.drag_count);
+            r.particle_steps = s.particle_steps;
+            r.drag_impulse_total = s.drag_impulse;
+            r.time = s.time;
+            r.sample_time = s.sample_time;
+            r.drag_sampling_time = s.drag_time;
+            r.drag_collision_count_window = static_cast<int64_t>(s.drag_count_window);
+            r.drag_impulse_window = s.drag_impulse_window;
         }
     }
 }
@@ -1805,10 +1822,10 @@ __device__ __forceinline__ void sample_add1(double a[ACC_NC], float f0, float f1
 template <class T>
 __global__ void __launch_bounds__(SAMPLE_THREADS)
     k_sample(const CaseDev *__restrict__ cases, CaseState *st, TileTables tt, Slots<T> p,
-             Cells cells, int side, int ncase, int finish, int *err)
+             Cells cells, int side, int ncase, int finish, dsmc_counters *rec, int *err)
 {
     if (finish && blockIdx.x == 0)
-        finish_cases(cases, st, ncase, 0, 1, 1);
+        finish_cases(cases, st, ncase, 0, 1, 1, rec);
     constexpr int S = SAMPLE_STAGES;
     constexpr int A = 16 / sizeof(T); // elements per 16 bytes
     extern __shared__ __align__(128) unsigned char smem_raw[];

@@ -112,6 +112,14 @@ class Engine:
     def step(self, n: int = 1):
         check(self._lib.dsmc_step(self._h, int(n)), "dsmc_step")
 
+    def step_read(self, n: int, out_address: int):
+        """n steps; after step k the counters of every case are copied
+        asynchronously to the Counters array at out_address (n * n_cases
+        records, case-minor); complete after synchronize().  Give it
+        page-locked memory for the copies to overlap the steps."""
+        check(self._lib.dsmc_step_read(self._h, int(n), C.c_void_p(out_address)),
+              "dsmc_step_read")
+
     def MoveParticles(self):
         check(self._lib.dsmc_stage_move(self._h), "dsmc_stage_move")
 

@@ -230,6 +230,15 @@ int dsmc_init_warm_tensor(dsmc_ctx *ctx, const double *host_field);
  * reported by the next dsmc_synchronize(). */
 int dsmc_step(dsmc_ctx *ctx, int n_steps);
 
+/* dsmc_step with the counters of every step read back without stopping the
+ * device: after step k, the counters of case i (as dsmc_get_counters would
+ * return them then) are copied asynchronously into
+ * host_out[k * n_cases + i].  No counterpart in the reference (which prints
+ * its progress from the host); the values are complete once
+ * dsmc_synchronize() returns, and the copies overlap the steps only when
+ * host_out is page-locked. */
+int dsmc_step_read(dsmc_ctx *ctx, int n_steps, dsmc_counters *host_out);
+
 /* The stages of one step, for callers of the per-function surface.  They
  * must be called in this order; dsmc_stage_end_step advances Step. */
 int dsmc_stage_move(dsmc_ctx *ctx);      /* MoveParticles (Boundary.cpp:284-328) */

@@ -292,3 +292,40 @@ def test_field_readback_paths_agree(cuda, engine_lib):
     with pytest.raises(ValueError):
         g.GatherGlobalField(out=np.empty((10, 17)))
     g.close()
+
+
+def test_step_read_records_every_step(cuda, engine_lib):
+    """dsmc_step_read's records equal dsmc_get_counters read after each step
+    (the FP64 drag sums to rounding: their atomic additions have no fixed
+    order)."""
+    import ctypes as C
+
+    import torch
+
+    from dsmc_erlend_b200.abi import Counters
+
+    cases = [small_case(WALL_DIFFUSE, seed=31), small_case(WALL_SPECULAR, seed=32)]
+    n_steps = 6
+    a = Engine(cases)
+    b = Engine(cases)
+    a.InitialConditions()
+    b.InitialConditions()
+    ring = torch.zeros(n_steps * len(cases) * C.sizeof(Counters), dtype=torch.uint8,
+                       pin_memory=True)
+    a.step_read(n_steps, ring.data_ptr())
+    a.synchronize()
+    recs = (Counters * (n_steps * len(cases))).from_address(ring.data_ptr())
+    for k in range(n_steps):
+        b.step(1)
+        b.synchronize()
+        for i in range(len(cases)):
+            want = b.counters(i)
+            got = recs[k * len(cases) + i].as_dict()
+            for key, v in want.items():
+                if isinstance(v, float):
+                    assert got[key] == pytest.approx(v, rel=1e-12, abs=1e-300), (k, i, key)
+                else:
+                    assert got[key] == v, (k, i, key)
+    assert recs[-1].step == n_steps and recs[-1].particle_steps > 0
+    a.close()
+    b.close()
