@@ -103,7 +103,7 @@ __device__ __forceinline__ void st8(bf16 *p, const V8 &r)
 // thread lane l of it accumulator row 32 (w % 4) + l).  The reduction index is k = tap * Cin + ci, cut into
 // chunks of TBK = 64; a chunk is gathered with cp.async (the implicit
 // im2col: 8 consecutive k of a pixel are 16 contiguous bytes of x, zeros
-// outside the image or beyond the 9 taps) into one of TST stages.  Each
+// outside the image or beyond the 9 taps) into one of 2-3 stages.  Each
 // gatherer waits for its own copies, fences them to the async proxy and
 // arrives on the stage's `full` barrier; the MMA thread waits on it, issues
 // the chunk's four tcgen05.mma (M 128, N BN, K 16) and commits them to the
@@ -118,7 +118,11 @@ __device__ __forceinline__ void st8(bf16 *p, const V8 &r)
 // next 8 rows), leading-byte offset unused (16), layout SWIZZLE_128B; the
 // j-th K-16 step starts 32 j bytes into the atom.
 // ---------------------------------------------------------------------------
-constexpr int TBM = 128, TBK = 64, TST = 4;
+constexpr int TBM = 128, TBK = 64;
+// Stages per CTA and CTAs per SM (bounded by the 512 tensor-memory columns,
+// 2 BN a CTA): measured on B200, deeper stages lose to more CTAs.
+template <int BN> __host__ __device__ constexpr int tc_stages() { return BN == 64 ? 2 : 3; }
+template <int BN> constexpr int tc_ctas_per_sm() { return BN == 128 ? 2 : (BN == 64 ? 4 : 3); }
 constexpr int TC_THREADS = TBM + 32 + TBM; // gatherers, MMA warp, epilogue
 constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;
 
@@ -194,7 +198,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
 }
 
 // Stages plus 1 KB to align the first to a swizzle atom.
-template <int BN> constexpr int tc_smem() { return TST * (TBM + BN) * TBK * 2 + 1024; }
+template <int BN> constexpr int tc_smem() { return tc_stages<BN>() * (TBM + BN) * TBK * 2 + 1024; }
 
 template <int BN>
 __global__ void __launch_bounds__(TC_THREADS)
@@ -204,6 +208,7 @@ __global__ void __launch_bounds__(TC_THREADS)
                   int Cout, int relu)
 {
     static_assert(BN == 32 || BN == 64 || BN == 128, "tensor-memory columns: a power of 2");
+    constexpr int TST = tc_stages<BN>();
     constexpr uint32_t A_BYTES = TBM * TBK * 2, B_BYTES = BN * TBK * 2;
     constexpr uint32_t STAGE = A_BYTES + B_BYTES;
     extern __shared__ __align__(1024) unsigned char tc_smem_dyn[];
@@ -752,11 +757,11 @@ int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
             return ERR_CUDA;
     }
-    // Persistent: as many CTAs as fit (shared memory: one of 128 channels,
-    // two of fewer per SM), each taking tiles blockIdx.x + i * gridDim.x.
+    // Persistent: tc_ctas_per_sm CTAs per SM, each taking tiles
+    // blockIdx.x + i * gridDim.x.
     const int M = n * h * w_;
     const int64_t tiles = static_cast<int64_t>((M + TBM - 1) / TBM) * (cout / BN);
-    const int per_sm = BN == 128 ? 1 : 2;
+    const int per_sm = tc_ctas_per_sm<BN>();
     const int grid = static_cast<int>(tiles < int64_t(sms) * per_sm ? tiles : int64_t(sms) * per_sm);
     k_conv_fwd_tc<BN><<<grid, TC_THREADS, tc_smem<BN>(), s>>>(x, w, bias, res, y, y32, n, h, w_,
                                                              cin, cout, relu);
