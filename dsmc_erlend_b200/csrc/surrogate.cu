@@ -262,17 +262,18 @@ __global__ void __launch_bounds__(TC_THREADS)
         };
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
             const int m0 = (t / ntiles_n) * TBM, n0 = (t % ntiles_n) * BN;
-            int an[TBM / 16], ah[TBM / 16], aw[TBM / 16];
+            int ah[TBM / 16], aw[TBM / 16];
             bool am[TBM / 16];
 #pragma unroll
             for (int i = 0; i < TBM / 16; ++i) {
                 const int m = m0 + r0 + 16 * i;
                 am[i] = m < M;
                 const int mm = am[i] ? m : 0;
-                an[i] = mm / (H * W);
                 ah[i] = (mm / W) % H;
                 aw[i] = mm % W;
             }
+            // Element offset of row r0 in x; row r0 + 16 i is 16 i Cin on.
+            const int64_t arow = static_cast<int64_t>(m0 + r0) * Cin;
             for (int kc = 0; kc < KT; ++kc, ++g) {
                 const int st = g % TST;
                 if (g >= TST && ok)
@@ -285,13 +286,14 @@ __global__ void __launch_bounds__(TC_THREADS)
                     const bool kin = k < K;
                     const int tap = kin ? k / Cin : 0, ci = k % Cin;
                     const int dh = tap / 3 - 1, dw = tap % 3 - 1;
+                    // The tap's pixel is dh W + dw pixels from the row's own.
+                    const int64_t koff = arow + static_cast<int64_t>(dh * W + dw) * Cin + ci;
+                    const int64_t rstep = 16 * static_cast<int64_t>(Cin);
 #pragma unroll
                     for (int i = 0; i < TBM / 16; ++i) {
                         const int hh = ah[i] + dh, ww = aw[i] + dw;
                         const bool v = am[i] && kin && hh >= 0 && hh < H && ww >= 0 && ww < W;
-                        const bf16 *src =
-                            v ? x + ((static_cast<int64_t>(an[i]) * H + hh) * W + ww) * Cin + ci
-                              : x;
+                        const bf16 *src = v ? x + (koff + i * rstep) : x;
                         cp_async16(sa + sw128_off(r0 + 16 * i, j), src, v);
                     }
 #pragma unroll
@@ -414,6 +416,211 @@ __global__ void __launch_bounds__(TC_THREADS)
                      : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradient on the 5th-generation tensor cores (Cin 32, 64 or 128;
+// Cout up to 256).  A CTA takes a group of TAPS = 128 / Cin taps and a range
+// of pixels and accumulates
+//   D[(tap, ci)][co] = sum_p X[p + off(tap)][ci] dY[p][co]
+// in tensor memory (M 128 = taps x Cin, N = Cout rounded up to NB; K =
+// 64-pixel chunks), then adds D to dW with FP32 atomics, coalesced over the
+// input channels of a warp.  Both operands are MN-major (the pixel is the
+// reduction index; channels are contiguous in memory), 128-byte swizzled:
+// element (row m, pixel k) at
+//   (m / 64) * 1024 + (k / 8) * SBO + (k % 8) * 128 + (((m % 64) / 8) ^ (k % 8)) * 16,
+// SBO being the bytes of one 8-pixel group of all the rows; the descriptor's
+// leading-byte offset is the 1024 between 64-row atoms, and the j-th K-16
+// step starts 2 j groups in.  Rows of a tap past the ninth and columns past
+// Cout are zero-filled.  Gatherers, MMA thread and barriers as in the
+// forward kernel; 3 stages, 1-3 CTAs per SM by NB.
+// ---------------------------------------------------------------------------
+constexpr int WG_PIX = 64, WG_ST = 3;
+constexpr int WG_THREADS = 128 + 32;
+
+__device__ __forceinline__ uint64_t umma_desc_sw128_mn(uint32_t saddr, uint32_t sbo)
+{
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(1024 >> 4) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (2ull << 61);
+}
+// bf16 x bf16 -> FP32, both operands MN-major, M 128 x N.
+template <int N> __host__ __device__ constexpr uint32_t umma_idesc_mn()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+           (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
+}
+__device__ __forceinline__ uint32_t sw128_mn_off(int m, int k, uint32_t sbo)
+{
+    return static_cast<uint32_t>((m >> 6) * 1024) + static_cast<uint32_t>(k >> 3) * sbo +
+           static_cast<uint32_t>((k & 7) * 128 + ((((m & 63) >> 3) ^ (k & 7)) << 4));
+}
+template <int NB> __host__ __device__ constexpr int wg_stage() { return 128 * WG_PIX * 2 + NB * WG_PIX * 2; }
+template <int NB> constexpr int wg_smem() { return WG_ST * wg_stage<NB>() + 1024; }
+template <int NB> constexpr int wg_ctas_per_sm() { return NB == 64 ? 3 : (NB == 128 ? 2 : 1); }
+
+template <int CI, int NB>
+__global__ void __launch_bounds__(WG_THREADS)
+    k_conv_wgrad_tc(const bf16 *__restrict__ dy, const bf16 *__restrict__ x,
+                    float *__restrict__ dw, int N, int H, int W, int Cout, int per)
+{
+    static_assert(CI == 32 || CI == 64 || CI == 128, "taps x Cin fill the 128 rows");
+    static_assert(NB == 64 || NB == 128 || NB == 256, "whole 64-channel swizzle atoms");
+    constexpr int TAPS = 128 / CI;
+    constexpr uint32_t A_BYTES = 128 * WG_PIX * 2;
+    constexpr uint32_t STAGE = wg_stage<NB>();
+    constexpr uint32_t SBO_A = 2 * 1024, SBO_B = (NB / 64) * 1024;
+    extern __shared__ __align__(1024) unsigned char wg_smem_dyn[];
+    __shared__ uint64_t bar_full[WG_ST], bar_empty[WG_ST];
+    __shared__ uint64_t bar_done;
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int M = N * H * W;
+    const int tap0 = blockIdx.y * TAPS;
+    const int p_begin = blockIdx.x * per;
+    const int p_end = min(M, p_begin + per);
+    const int KT = p_end > p_begin ? (p_end - p_begin + WG_PIX - 1) / WG_PIX : 0;
+
+    if (warp == 4) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&s_tmem)), "r"(NB)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < WG_ST; ++i) {
+            tc_mbar_init(&bar_full[i], 128);
+            tc_mbar_init(&bar_empty[i], 1);
+        }
+        tc_mbar_init(&bar_done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    bool ok = true;
+    unsigned char *sm = wg_smem_dyn + ((1024u - (smem_u32(wg_smem_dyn) & 1023u)) & 1023u);
+
+    if (warp < 4) {
+        // The 16 pieces of 8 rows a thread gathers: row 8 j = (tap tl, input
+        // channels ci8 .. ci8 + 7), the same for every chunk.
+        const int j = tid & 15;
+        const int tap = tap0 + (8 * j) / CI, ci8 = (8 * j) % CI;
+        const bool tap_ok = tap < 9;
+        const int dh = tap / 3 - 1, dwx = tap % 3 - 1;
+        // Element offsets of the thread's first X and dY pieces in chunk 0;
+        // piece i is 8 i pixels on, a chunk 64 pixels.
+        const int64_t xoff0 =
+            (static_cast<int64_t>(p_begin) + (tid >> 4) + static_cast<int64_t>(dh) * W + dwx) * CI +
+            ci8;
+        constexpr int BJ = NB / 8; // 16-byte pieces of a dY row
+        const int jb = tid % BJ;
+        const bool col_ok = 8 * jb < Cout;
+        const int64_t yoff0 = static_cast<int64_t>(p_begin + tid / BJ) * Cout + 8 * jb;
+        const int64_t ystep = static_cast<int64_t>(128 / BJ) * Cout;
+        // Row and column of the thread's 8 pixels (tid / 16 + 8 i of each
+        // chunk), stepped by 64 pixels a chunk instead of divided out.
+        int hh[8], ww[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int p = p_begin + (tid >> 4) + 8 * i;
+            hh[i] = (p / W) % H;
+            ww[i] = p % W;
+        }
+        auto publish = [&](int kc) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_mbar_arrive(&bar_full[kc % WG_ST]);
+        };
+        for (int kc = 0; kc < KT; ++kc) {
+            const int st = kc % WG_ST;
+            if (kc >= WG_ST && ok)
+                ok = tc_mbar_wait(&bar_empty[st], static_cast<uint32_t>(((kc - WG_ST) / WG_ST) & 1));
+            if (ok) {
+                unsigned char *sa = sm + st * STAGE;
+                const int p0 = p_begin + kc * WG_PIX;
+                const int64_t xoff = xoff0 + static_cast<int64_t>(kc) * WG_PIX * CI;
+                const int64_t yoff = yoff0 + static_cast<int64_t>(kc) * WG_PIX * Cout;
+                // X at the taps: 64 pixels x 16 pieces of 8 rows.
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int pp = (tid >> 4) + 8 * i;
+                    const int h2 = hh[i] + dh, w2 = ww[i] + dwx;
+                    const bool v =
+                        tap_ok && p0 + pp < p_end && h2 >= 0 && h2 < H && w2 >= 0 && w2 < W;
+                    const bf16 *src = v ? x + (xoff + 8 * i * CI) : x;
+                    cp_async16(sa + sw128_mn_off(8 * j, pp, SBO_A), src, v);
+                }
+                // dY: 64 pixels x NB / 8 pieces of 8 output channels.
+#pragma unroll
+                for (int i = 0; i < BJ * WG_PIX / 128; ++i) {
+                    const int pp = tid / BJ + (128 / BJ) * i;
+                    const bool v = col_ok && p0 + pp < p_end;
+                    const bf16 *src = v ? dy + (yoff + i * ystep) : dy;
+                    cp_async16(sa + A_BYTES + sw128_mn_off(8 * jb, pp, SBO_B), src, v);
+                }
+            }
+            cp_async_commit();
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                ww[i] += WG_PIX;
+                while (ww[i] >= W) {
+                    ww[i] -= W;
+                    hh[i] = hh[i] + 1 == H ? 0 : hh[i] + 1;
+                }
+            }
+            if (kc >= WG_ST - 1) {
+                cp_async_wait<WG_ST - 1>();
+                publish(kc - (WG_ST - 1));
+            }
+        }
+        cp_async_wait<0>();
+        for (int kc = KT - (WG_ST - 1) < 0 ? 0 : KT - (WG_ST - 1); kc < KT; ++kc)
+            publish(kc);
+    } else if (tid == 128) {
+        for (int kc = 0; kc < KT && ok; ++kc) {
+            const int st = kc % WG_ST;
+            ok = tc_mbar_wait(&bar_full[st], static_cast<uint32_t>((kc / WG_ST) & 1));
+            if (!ok)
+                break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(sm + st * STAGE);
+#pragma unroll
+            for (int kk = 0; kk < WG_PIX / 16; ++kk)
+                umma_bf16(tmem, umma_desc_sw128_mn(sa + kk * 2 * SBO_A, SBO_A),
+                          umma_desc_sw128_mn(sa + A_BYTES + kk * 2 * SBO_B, SBO_B),
+                          umma_idesc_mn<NB>(), (kc > 0 || kk > 0) ? 1u : 0u);
+            umma_commit(&bar_empty[st]);
+        }
+        umma_commit(&bar_done);
+    }
+    const bool done = tc_mbar_wait(&bar_done, 0);
+    const bool ok_all = __syncthreads_and(ok && done);
+    if (!ok_all && tid == 0)
+        atomicExch(&g_tc_error, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok_all && warp < 4 && KT > 0) {
+        // Tensor-memory lane = row = (tap, input channel); columns = Cout.
+        const int tap = tap0 + tid / CI, ci = tid % CI;
+        const bool row_ok = tap < 9;
+        float *d = dw + static_cast<int64_t>(tap) * CI + ci;
+#pragma unroll 1
+        for (int c = 0; c < NB && c < Cout; c += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c),
+                      r);
+            if (!row_ok)
+                continue;
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+                if (c + e < Cout)
+                    atomicAdd(d + static_cast<int64_t>(c + e) * 9 * CI, __uint_as_float(r[e]));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 4)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NB)
+                     : "memory");
+}
+
 // w_rot[ci][tap][co] = w[co][8 - tap][ci]: the weights of the dgrad conv.
 __global__ void k_rotate(const bf16 *__restrict__ w, bf16 *__restrict__ w_rot, int Cin, int Cout)
 {
@@ -428,7 +635,9 @@ __global__ void k_rotate(const bf16 *__restrict__ w, bf16 *__restrict__ w_rot, i
 }
 
 // ---------------------------------------------------------------------------
-// wgrad: CTA tile 64 output channels x 32 input channels of one tap, k-tiles
+// wgrad for the shapes the tensor-core kernel does not take (Cin other than
+// 32, 64, 128, or Cout > 256): CTA tile 64 output channels x 32 input
+// channels of one tap, k-tiles
 // of 32 pixels; the pixels of the problem are split over gridDim.z.  Shared
 // tiles are stored pixel-major as they sit in memory and read transposed
 // with ldmatrix.trans.  8 warps as 4 (cout) x 2 (cin), each 16 x 16.
@@ -767,6 +976,51 @@ int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res
                                                              cin, cout, relu);
     return status();
 }
+// Weight gradient on the tensor cores: groups of 128 / Cin taps x splits of
+// the pixels.
+template <int CI, int NB>
+int wgrad_tc(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int cout,
+             cudaStream_t s)
+{
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_wgrad_tc<CI, NB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, wg_smem<NB>());
+    });
+    if (attr != cudaSuccess)
+        return ERR_CUDA;
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return ERR_CUDA;
+    }
+    constexpr int groups = (9 + 128 / CI - 1) / (128 / CI);
+    const int M = n * h * w_;
+    const int chunks = (M + WG_PIX - 1) / WG_PIX;
+    // One wave: whole splits per tap group that fit the resident CTAs.
+    int splits = sms * wg_ctas_per_sm<NB>() / groups;
+    splits = splits < 1 ? 1 : (splits < chunks ? splits : chunks);
+    const int per = ((chunks + splits - 1) / splits) * WG_PIX;
+    splits = (M + per - 1) / per;
+    k_conv_wgrad_tc<CI, NB><<<dim3(splits, groups), WG_THREADS, wg_smem<NB>(), s>>>(
+        dy, x, dw, n, h, w_, cout, per);
+    return status();
+}
+
+template <int CI>
+int wgrad_tc_n(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int cout,
+               cudaStream_t s)
+{
+    if (cout <= 64)
+        return wgrad_tc<CI, 64>(dy, x, dw, n, h, w_, cout, s);
+    if (cout <= 128)
+        return wgrad_tc<CI, 128>(dy, x, dw, n, h, w_, cout, s);
+    return wgrad_tc<CI, 256>(dy, x, dw, n, h, w_, cout, s);
+}
+
 int conv_fwd_launch(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
                     float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
 {
@@ -833,6 +1087,18 @@ int dsmc_sg_conv_wgrad(const uint16_t *dy, const uint16_t *x, float *dw, float *
         return ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int M = n * h * w_;
+    if ((cin == 32 || cin == 64 || cin == 128) && cout <= 256) {
+        const bf16 *dyb = reinterpret_cast<const bf16 *>(dy);
+        const bf16 *xb = reinterpret_cast<const bf16 *>(x);
+        const int st = cin == 128  ? wgrad_tc_n<128>(dyb, xb, dw, n, h, w_, cout, s)
+                       : cin == 64 ? wgrad_tc_n<64>(dyb, xb, dw, n, h, w_, cout, s)
+                                   : wgrad_tc_n<32>(dyb, xb, dw, n, h, w_, cout, s);
+        if (st != OK)
+            return st;
+        if (db)
+            k_bias_grad<<<512, 256, 0, s>>>(reinterpret_cast<const bf16 *>(dy), db, M, cout);
+        return status();
+    }
     const int tiles = ((cout + WBM - 1) / WBM) * 9 * (cin / WBN);
     // Enough pixel splits for ~4 CTAs per SM of a 148-SM part, at least
     // 512 pixels each.

@@ -7,8 +7,9 @@
  * Tensors are NHWC with channel counts that are multiples of 32; activations
  * and weights are bfloat16 (passed as uint16_t bit patterns), accumulation
  * and optimizer state FP32.  Convolutions are 3 x 3, stride 1, zero padding
- * 1; weights are [Cout][3][3][Cin]; forward and input gradient run on the
- * tcgen05 tensor cores (accumulator in tensor memory).  Every function enqueues on `stream`
+ * 1; weights are [Cout][3][3][Cin]; forward and input gradient, and the
+ * weight gradient for Cin 32, 64 or 128 and Cout <= 256, run on the tcgen05
+ * tensor cores (accumulator in tensor memory).  Every function enqueues on `stream`
  * (a cudaStream_t, NULL for the default stream) and returns DSMC_OK (0),
  * DSMC_ERR_ARGUMENT (2) for shapes outside these rules, or DSMC_ERR_CUDA (50).
  */

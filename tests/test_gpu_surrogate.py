@@ -68,7 +68,9 @@ def test_conv_forward(cuda, n, h, w, cin, cout):
 
 
 @pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 10, 6, 64, 32),
-                                            (2, 12, 9, 128, 128), (1, 7, 13, 64, 96)])
+                                            (2, 12, 9, 128, 128), (1, 7, 13, 64, 96),
+                                            (1, 9, 11, 96, 64), (1, 5, 9, 32, 160),
+                                            (1, 6, 10, 128, 256)])
 def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
@@ -92,13 +94,14 @@ def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     assert L.dsmc_sg_check(None) == 0
 
 
-def test_wgrad_large_pixel_count_splits(cuda):
+@pytest.mark.parametrize("cin,cout", [(32, 64), (64, 128), (128, 32)])
+def test_wgrad_large_pixel_count_splits(cuda, cin, cout):
     # Enough pixels for several pixel splits, and accumulation into dw.
     from dsmc_erlend_b200.surrogate import lib, ptr
 
     torch = cuda
     rng = np.random.default_rng(3)
-    n, h, w, cin, cout = 4, 64, 64, 32, 64
+    n, h, w = 4, 64, 64
     x = _bf16(torch, _rand(rng, n, h, w, cin))
     dy = _bf16(torch, _rand(rng, n, h, w, cout, scale=0.05))
     dw = torch.ones(cout, 3, 3, cin, dtype=torch.float32, device="cuda")
@@ -106,6 +109,7 @@ def test_wgrad_large_pixel_count_splits(cuda):
                                     None) == 0
     torch.cuda.synchronize()
     _close(_np(dw) - 1.0, ref.conv3x3_wgrad(_np(dy), _np(x)), 1e-4, "wgrad split")
+    assert lib().dsmc_sg_check(None) == 0
 
 
 def test_wgrad_wide_input_pixel_splits(cuda):
