@@ -68,7 +68,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         subprocess.run(cmd, check=True)
     main = CSRC / "main.cpp"
     if main.exists() and (force or _stale(CLI, [main, LIB])):
-        cmd = [nvcc(), *NVCC_FLAGS, "-o", str(CLI), str(main), "-L", str(LIB_DIR),
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-o", str(CLI), str(main), "-L", str(LIB_DIR),
                "-ldsmc_b200", "-Xlinker", "-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))

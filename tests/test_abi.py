@@ -157,3 +157,15 @@ def test_cli_lists_run_controls_and_rejects_bad_periods(engine_lib):
     for bad in (["--print-period", "0"], ["--checkpoint-period", "2.5"], ["--restart"]):
         r = subprocess.run([str(exe), *bad], capture_output=True, text=True, timeout=60)
         assert r.returncode == 2, bad
+
+
+def test_sgbench_covers_every_layer_shape():
+    # The surrogate benchmark times each distinct (resolution, Cin, Cout) of
+    # the network once.
+    from dsmc_erlend_b200 import sgbench
+    from dsmc_erlend_b200.surrogate import LAYERS, RES
+
+    shapes = sgbench._shapes(8)
+    assert shapes[0] == (8, RES, RES, LAYERS[0][3], LAYERS[0][4])
+    assert len(shapes) == len({s[1:] for s in shapes})
+    assert {(s[3], s[4]) for s in shapes} == {(l[3], l[4]) for l in LAYERS}
