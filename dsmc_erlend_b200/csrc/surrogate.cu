@@ -12,10 +12,13 @@
 //            3x3 convolution is a 3x3 convolution)
 //   wgrad    C[cout][(tap, cin)]  = sum_pixel dY[pixel][cout] X[pixel + tap][cin]
 //            (split over pixels, FP32 atomics into dW)
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 
 #include "../../include/dsmc_surrogate.h"
@@ -152,6 +155,40 @@ __device__ __forceinline__ bool tc_mbar_wait(uint64_t *bar, uint32_t parity)
     }
     return false;
 }
+// The next arrival on `bar` also expects `bytes` from bulk tensor copies.
+__device__ __forceinline__ void tc_mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// TMA tile loads (no multicast) completing on an mbarrier of this CTA.
+// Coordinates are elements, innermost first; boxes outside the tensor read
+// zeros.
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, int c3, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+                 "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+                 : "memory");
+}
+// Shared-memory matrix descriptor: K-major, 64-byte swizzle (rows of 32
+// bf16, 8-row atoms of 512 bytes), version 1.
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr)
+{
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (1ull << 16) |
+           (static_cast<uint64_t>(512 >> 4) << 32) | (1ull << 46) | (4ull << 61);
+}
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, version 1.
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
 {
@@ -200,14 +237,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
 // Stages plus 1 KB to align the first to a swizzle atom.
 template <int BN> constexpr int tc_smem() { return tc_stages<BN>() * (TBM + BN) * TBK * 2 + 1024; }
 
-template <int BN>
+// AMODE selects how the stages are filled: 0, the cp.async im2col gather
+// (any shape); 1 and 2, TMA tile loads by one thread, for shapes whose
+// 128-pixel tile is a BW x BH rectangle of one image: the input through a
+// 4-D map [N][H][W][Cin] whose box is read at the tap's offset (zeros
+// outside the image are the padding), the weights through a 2-D map
+// [Cout][9 Cin].  AMODE 1 (Cin a multiple of 64): one box of 64 channels per
+// chunk, 128-byte swizzle, as the gather lays it out.  AMODE 2 (Cin 32): a
+// chunk is two taps, two boxes of 32 channels in 64-byte-swizzled K-major
+// tiles of 8 KB each (a tenth tap reads a box wholly outside the image).
+template <int BN, int AMODE>
 __global__ void __launch_bounds__(TC_THREADS)
     k_conv_fwd_tc(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
                   const float *__restrict__ bias, const bf16 *__restrict__ res,
                   bf16 *__restrict__ y, float *__restrict__ y32, int N, int H, int W, int Cin,
-                  int Cout, int relu)
+                  int Cout, int relu, const __grid_constant__ CUtensorMap tmx,
+                  const __grid_constant__ CUtensorMap tmw, int BW, int BH)
 {
     static_assert(BN == 32 || BN == 64 || BN == 128, "tensor-memory columns: a power of 2");
+    static_assert(AMODE >= 0 && AMODE <= 2, "gather, TMA 128-byte or TMA 64-byte tiles");
     constexpr int TST = tc_stages<BN>();
     constexpr uint32_t A_BYTES = TBM * TBK * 2, B_BYTES = BN * TBK * 2;
     constexpr uint32_t STAGE = A_BYTES + B_BYTES;
@@ -231,7 +279,7 @@ __global__ void __launch_bounds__(TC_THREADS)
     }
     if (tid == 0) {
         for (int i = 0; i < TST; ++i) {
-            tc_mbar_init(&bar_full[i], TBM); // every gatherer arrives
+            tc_mbar_init(&bar_full[i], AMODE ? 1 : TBM); // the TMA thread or every gatherer
             tc_mbar_init(&bar_empty[i], 1);  // one tcgen05.commit
         }
         for (int i = 0; i < 2; ++i) {
@@ -250,7 +298,40 @@ __global__ void __launch_bounds__(TC_THREADS)
     unsigned char *tc_smem_raw =
         tc_smem_dyn + ((1024u - (smem_u32(tc_smem_dyn) & 1023u)) & 1023u);
 
-    if (warp < 4) {
+    if (AMODE && warp < 4) {
+        if (tid == 0) { // TMA producer: chunks in the order the MMA thread takes them
+            int g = 0;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                const int m0 = (t / ntiles_n) * TBM, n0 = (t % ntiles_n) * BN;
+                const int img = m0 / (H * W), rem = m0 % (H * W);
+                const int h0 = rem / W, w0 = rem % W;
+                for (int kc = 0; kc < KT; ++kc, ++g) {
+                    const int st = g % TST;
+                    if (g >= TST)
+                        ok = tc_mbar_wait(&bar_empty[st],
+                                          static_cast<uint32_t>(((g - TST) / TST) & 1));
+                    if (!ok)
+                        break;
+                    unsigned char *sa = tc_smem_raw + st * STAGE;
+                    tc_mbar_expect_tx(&bar_full[st], STAGE);
+                    if (AMODE == 1) {
+                        const int k = kc * TBK, tap = k / Cin;
+                        tma_load_4d(sa, &tmx, k % Cin, w0 + tap % 3 - 1, h0 + tap / 3 - 1, img,
+                                    &bar_full[st]);
+                    } else {
+#pragma unroll
+                        for (int half = 0; half < 2; ++half) {
+                            const int tap = 2 * kc + half;
+                            const int hh = tap < 9 ? h0 + tap / 3 - 1 : -BH - 1;
+                            tma_load_4d(sa + half * (A_BYTES / 2), &tmx, 0, w0 + tap % 3 - 1, hh,
+                                        img, &bar_full[st]);
+                        }
+                    }
+                    tma_load_2d(sa + A_BYTES, &tmw, kc * TBK, n0, &bar_full[st]);
+                }
+            }
+        }
+    } else if (warp < 4) {
         // Gatherer: piece j = tid % 8 of rows tid / 8 + 16 i of A (i < 8)
         // and of B (i < BN / 16).  Chunks are counted across the CTA's tiles
         // (g), so the stage ring runs on from one tile to the next.
@@ -335,10 +416,17 @@ __global__ void __launch_bounds__(TC_THREADS)
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t sa = smem_u32(tc_smem_raw + st * STAGE), sb = sa + A_BYTES;
 #pragma unroll
-                    for (int kk = 0; kk < TBK / 16; ++kk)
-                        umma_bf16(tmem + static_cast<uint32_t>(b * BN),
-                                  umma_desc_sw128(sa + 32 * kk), umma_desc_sw128(sb + 32 * kk),
-                                  umma_idesc<BN>(), (kc > 0 || kk > 0) ? 1u : 0u);
+                    for (int kk = 0; kk < TBK / 16; ++kk) {
+                        // AMODE 2: k 0-31 in the first 64-byte-swizzled
+                        // tile, 32-63 in the second.
+                        const uint64_t da =
+                            AMODE == 2
+                                ? umma_desc_sw64(sa + (kk >> 1) * (A_BYTES / 2) + 32 * (kk & 1))
+                                : umma_desc_sw128(sa + 32 * kk);
+                        umma_bf16(tmem + static_cast<uint32_t>(b * BN), da,
+                                  umma_desc_sw128(sb + 32 * kk), umma_idesc<BN>(),
+                                  (kc > 0 || kk > 0) ? 1u : 0u);
+                    }
                     umma_commit(&bar_empty[st]);
                 }
                 umma_commit(&bar_acc_full[b]);
@@ -947,15 +1035,61 @@ int status() { return cudaGetLastError() == cudaSuccess ? OK : ERR_CUDA; }
 
 // The forward convolution on the tensor cores: the widest channel tile that
 // divides Cout (128, 64 or 32 columns of tensor memory).
-template <int BN>
-int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
-                float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
+// cuTensorMapEncodeTiled from the driver, found once through the runtime.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// The TMA maps of one convolution: the input [N][H][W][Cin] read in boxes of
+// cb channels x bw x bh pixels, the weights [Cout][9 Cin] in boxes of 64 k x
+// bn rows.  False when the shape or the pointers do not suit them.
+bool conv_tma_maps(const bf16 *x, const bf16 *w, int n, int h, int w_, int cin, int cout, int bn,
+                   int cb, int bw, int bh, CUtensorMap *mx, CUtensorMap *mw)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(x) & 15u) || (reinterpret_cast<uintptr_t>(w) & 15u))
+        return false;
+    const cuuint64_t xd[4] = {cuuint64_t(cin), cuuint64_t(w_), cuuint64_t(h), cuuint64_t(n)};
+    const cuuint64_t xs[3] = {cuuint64_t(cin) * 2, cuuint64_t(w_) * cin * 2,
+                              cuuint64_t(h) * w_ * cin * 2};
+    const cuuint32_t xb[4] = {cuuint32_t(cb), cuuint32_t(bw), cuuint32_t(bh), 1};
+    const cuuint32_t one[4] = {1, 1, 1, 1};
+    if (enc(mx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(x), xd, xs, xb, one,
+            CU_TENSOR_MAP_INTERLEAVE_NONE,
+            cb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    const cuuint64_t wd[2] = {cuuint64_t(9) * cin, cuuint64_t(cout)};
+    const cuuint64_t ws[1] = {cuuint64_t(9) * cin * 2};
+    const cuuint32_t wb[2] = {cuuint32_t(TBK), cuuint32_t(bn)};
+    return enc(mw, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(w), wd, ws, wb, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN, int AMODE>
+int conv_fwd_tc_mode(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
+                     float *y32, int n, int h, int w_, int cin, int cout, int relu,
+                     const CUtensorMap &mx, const CUtensorMap &mw, int bw, int bh, cudaStream_t s)
 {
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_conv_fwd_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    tc_smem<BN>());
+        attr = cudaFuncSetAttribute(k_conv_fwd_tc<BN, AMODE>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<BN>());
     });
     if (attr != cudaSuccess)
         return ERR_CUDA;
@@ -972,9 +1106,32 @@ int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res
     const int64_t tiles = static_cast<int64_t>((M + TBM - 1) / TBM) * (cout / BN);
     const int per_sm = tc_ctas_per_sm<BN>();
     const int grid = static_cast<int>(tiles < int64_t(sms) * per_sm ? tiles : int64_t(sms) * per_sm);
-    k_conv_fwd_tc<BN><<<grid, TC_THREADS, tc_smem<BN>(), s>>>(x, w, bias, res, y, y32, n, h, w_,
-                                                             cin, cout, relu);
+    k_conv_fwd_tc<BN, AMODE><<<grid, TC_THREADS, tc_smem<BN>(), s>>>(
+        x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx, mw, bw, bh);
     return status();
+}
+
+// TMA tiles when every 128-pixel tile is a rectangle of one image (W a
+// divisor or a multiple of 128, H W a multiple of 128) and Cin is 32 or a
+// multiple of 64; the cp.async gather otherwise.
+template <int BN>
+int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
+                float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
+{
+    CUtensorMap mx, mw;
+    const bool rect = (w_ % TBM == 0 || TBM % w_ == 0) && (int64_t(h) * w_) % TBM == 0;
+    const int bw = w_ < TBM ? w_ : TBM, bh = TBM / bw;
+    if (rect && cin % 64 == 0 &&
+        conv_tma_maps(x, w, n, h, w_, cin, cout, BN, 64, bw, bh, &mx, &mw))
+        return conv_fwd_tc_mode<BN, 1>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx,
+                                       mw, bw, bh, s);
+    if (rect && cin == 32 && conv_tma_maps(x, w, n, h, w_, cin, cout, BN, 32, bw, bh, &mx, &mw))
+        return conv_fwd_tc_mode<BN, 2>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx,
+                                       mw, bw, bh, s);
+    memset(&mx, 0, sizeof(mx));
+    memset(&mw, 0, sizeof(mw));
+    return conv_fwd_tc_mode<BN, 0>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx, mw,
+                                   0, 0, s);
 }
 // Weight gradient on the tensor cores: groups of 128 / Cin taps x splits of
 // the pixels.

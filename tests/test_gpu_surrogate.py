@@ -41,8 +41,13 @@ def _close(got, want, rtol, what):
     assert err <= rtol, f"{what}: max error {err:.3e} of scale {scale:.3e}"
 
 
+# Shapes whose 128-pixel tiles are rectangles of one image take the TMA
+# loads (Cin 32: two 64-byte-swizzled taps a chunk; Cin a multiple of 64:
+# 128-byte-swizzled boxes); the others, and Cin 96, the cp.async gather.
 @pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 12, 20, 64, 96),
-                                            (3, 16, 16, 128, 64)])
+                                            (3, 16, 16, 128, 64), (2, 16, 8, 32, 32),
+                                            (1, 32, 32, 32, 64), (1, 4, 256, 64, 128),
+                                            (2, 8, 16, 96, 32), (1, 2, 128, 256, 32)])
 def test_conv_forward(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
@@ -70,7 +75,8 @@ def test_conv_forward(cuda, n, h, w, cin, cout):
 @pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 10, 6, 64, 32),
                                             (2, 12, 9, 128, 128), (1, 7, 13, 64, 96),
                                             (1, 9, 11, 96, 64), (1, 5, 9, 32, 160),
-                                            (1, 6, 10, 128, 256)])
+                                            (1, 6, 10, 128, 256), (2, 16, 16, 64, 32),
+                                            (1, 8, 32, 32, 128)])
 def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
