@@ -524,6 +524,17 @@ __global__ void __launch_bounds__(TC_THREADS)
 constexpr int WG_PIX = 64, WG_ST = 3;
 constexpr int WG_THREADS = 128 + 32;
 
+// MN-major descriptor with the given leading (between MN atoms) and stride
+// (between 8-deep K groups) byte offsets; layout 2 = 128-byte swizzle (64-wide
+// atoms), 4 = 64-byte swizzle (32-wide atoms).
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr, uint32_t lbo, uint32_t sbo,
+                                                 uint32_t layout)
+{
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) |
+           (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) |
+           (static_cast<uint64_t>(layout) << 61);
+}
 __device__ __forceinline__ uint64_t umma_desc_sw128_mn(uint32_t saddr, uint32_t sbo)
 {
     return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(1024 >> 4) << 16) |
@@ -544,10 +555,20 @@ template <int NB> __host__ __device__ constexpr int wg_stage() { return 128 * WG
 template <int NB> constexpr int wg_smem() { return WG_ST * wg_stage<NB>() + 1024; }
 template <int NB> constexpr int wg_ctas_per_sm() { return NB == 64 ? 3 : (NB == 128 ? 2 : 1); }
 
-template <int CI, int NB>
+// TMA: the stages are filled by one thread with tile loads for shapes whose
+// 64-pixel chunks are BW x BH rectangles of one image: per tap a box of
+// CB = min(Cin, 64) channels x 64 pixels from a 4-D map of X (zeros outside
+// the image; a tap past the ninth reads a box wholly outside), and NB / 64
+// boxes of 64 channels x 64 pixels from a 2-D map of dY [pixels][Cout]
+// (zeros past Cout).  A box is rows of pixels as they sit in memory, which
+// is the MN-major swizzled tile: atoms along M a box apart (LBO), 8-pixel
+// groups one atom row apart (SBO); 64-byte swizzle for Cin 32.
+template <int CI, int NB, bool TMA>
 __global__ void __launch_bounds__(WG_THREADS)
     k_conv_wgrad_tc(const bf16 *__restrict__ dy, const bf16 *__restrict__ x,
-                    float *__restrict__ dw, int N, int H, int W, int Cout, int per)
+                    float *__restrict__ dw, int N, int H, int W, int Cout, int per,
+                    const __grid_constant__ CUtensorMap tmx,
+                    const __grid_constant__ CUtensorMap tmy, int BW, int BH)
 {
     static_assert(CI == 32 || CI == 64 || CI == 128, "taps x Cin fill the 128 rows");
     static_assert(NB == 64 || NB == 128 || NB == 256, "whole 64-channel swizzle atoms");
@@ -574,7 +595,7 @@ __global__ void __launch_bounds__(WG_THREADS)
     }
     if (tid == 0) {
         for (int i = 0; i < WG_ST; ++i) {
-            tc_mbar_init(&bar_full[i], 128);
+            tc_mbar_init(&bar_full[i], TMA ? 1 : 128);
             tc_mbar_init(&bar_empty[i], 1);
         }
         tc_mbar_init(&bar_done, 1);
@@ -587,7 +608,36 @@ __global__ void __launch_bounds__(WG_THREADS)
     bool ok = true;
     unsigned char *sm = wg_smem_dyn + ((1024u - (smem_u32(wg_smem_dyn) & 1023u)) & 1023u);
 
-    if (warp < 4) {
+    constexpr int CB = CI < 64 ? CI : 64;                  // channels of an X box
+    constexpr uint32_t XBOX = CB * WG_PIX * 2, YBOX = 64 * WG_PIX * 2;
+    if (TMA && warp < 4) {
+        if (tid == 0) {
+            for (int kc = 0; kc < KT; ++kc) {
+                const int st = kc % WG_ST;
+                if (kc >= WG_ST)
+                    ok = tc_mbar_wait(&bar_empty[st],
+                                      static_cast<uint32_t>(((kc - WG_ST) / WG_ST) & 1));
+                if (!ok)
+                    break;
+                unsigned char *sa = sm + st * STAGE;
+                const int p0 = p_begin + kc * WG_PIX;
+                const int img = p0 / (H * W), rem = p0 % (H * W);
+                const int h0 = rem / W, w0 = rem % W;
+                tc_mbar_expect_tx(&bar_full[st], STAGE);
+#pragma unroll
+                for (int b = 0; b < 128 / CB; ++b) {
+                    // Box b: tap tap0 + b (Cin <= 64) or channels 64 b of tap0.
+                    const int tap = CI <= 64 ? tap0 + b : tap0;
+                    const int hh = tap < 9 ? h0 + tap / 3 - 1 : -BH - 1;
+                    tma_load_4d(sa + b * XBOX, &tmx, CI <= 64 ? 0 : 64 * b, w0 + tap % 3 - 1, hh,
+                                img, &bar_full[st]);
+                }
+#pragma unroll
+                for (int b = 0; b < NB / 64; ++b)
+                    tma_load_2d(sa + A_BYTES + b * YBOX, &tmy, 64 * b, p0, &bar_full[st]);
+            }
+        }
+    } else if (warp < 4) {
         // The 16 pieces of 8 rows a thread gathers: row 8 j = (tap tl, input
         // channels ci8 .. ci8 + 7), the same for every chunk.
         const int j = tid & 15;
@@ -671,10 +721,15 @@ __global__ void __launch_bounds__(WG_THREADS)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t sa = smem_u32(sm + st * STAGE);
 #pragma unroll
-            for (int kk = 0; kk < WG_PIX / 16; ++kk)
-                umma_bf16(tmem, umma_desc_sw128_mn(sa + kk * 2 * SBO_A, SBO_A),
-                          umma_desc_sw128_mn(sa + A_BYTES + kk * 2 * SBO_B, SBO_B),
-                          umma_idesc_mn<NB>(), (kc > 0 || kk > 0) ? 1u : 0u);
+            for (int kk = 0; kk < WG_PIX / 16; ++kk) {
+                // TMA boxes: 8-pixel groups of CB (X) or 64 (dY) channels.
+                const uint64_t da =
+                    TMA ? umma_desc_mn(sa + kk * 2 * (CB * 16), XBOX, CB * 16, CB == 64 ? 2 : 4)
+                        : umma_desc_sw128_mn(sa + kk * 2 * SBO_A, SBO_A);
+                const uint64_t db = TMA ? umma_desc_mn(sa + A_BYTES + kk * 2 * 1024, YBOX, 1024, 2)
+                                        : umma_desc_sw128_mn(sa + A_BYTES + kk * 2 * SBO_B, SBO_B);
+                umma_bf16(tmem, da, db, umma_idesc_mn<NB>(), (kc > 0 || kk > 0) ? 1u : 0u);
+            }
             umma_commit(&bar_empty[st]);
         }
         umma_commit(&bar_done);
@@ -1135,6 +1190,35 @@ int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res
 }
 // Weight gradient on the tensor cores: groups of 128 / Cin taps x splits of
 // the pixels.
+// The TMA maps of the weight gradient: X [N][H][W][Cin] in boxes of cb
+// channels x bw x bh pixels (128- or 64-byte swizzle), dY [pixels][Cout] in
+// boxes of 64 channels x 64 pixels.  False when they do not suit.
+bool wgrad_tma_maps(const bf16 *dy, const bf16 *x, int n, int h, int w_, int cin, int cout,
+                    int cb, int bw, int bh, CUtensorMap *mx, CUtensorMap *my)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(x) & 15u) || (reinterpret_cast<uintptr_t>(dy) & 15u))
+        return false;
+    const cuuint32_t one[4] = {1, 1, 1, 1};
+    const cuuint64_t xd[4] = {cuuint64_t(cin), cuuint64_t(w_), cuuint64_t(h), cuuint64_t(n)};
+    const cuuint64_t xs[3] = {cuuint64_t(cin) * 2, cuuint64_t(w_) * cin * 2,
+                              cuuint64_t(h) * w_ * cin * 2};
+    const cuuint32_t xb[4] = {cuuint32_t(cb), cuuint32_t(bw), cuuint32_t(bh), 1};
+    if (enc(mx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(x), xd, xs, xb, one,
+            CU_TENSOR_MAP_INTERLEAVE_NONE,
+            cb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    const cuuint64_t yd[2] = {cuuint64_t(cout), cuuint64_t(n) * h * w_};
+    const cuuint64_t ys[1] = {cuuint64_t(cout) * 2};
+    const cuuint32_t yb[2] = {64, cuuint32_t(WG_PIX)};
+    return enc(my, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(dy), yd, ys, yb, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int CI, int NB>
 int wgrad_tc(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int cout,
              cudaStream_t s)
@@ -1142,8 +1226,12 @@ int wgrad_tc(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_conv_wgrad_tc<CI, NB>,
+        attr = cudaFuncSetAttribute(k_conv_wgrad_tc<CI, NB, false>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, wg_smem<NB>());
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_conv_wgrad_tc<CI, NB, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        wg_smem<NB>());
     });
     if (attr != cudaSuccess)
         return ERR_CUDA;
@@ -1162,8 +1250,19 @@ int wgrad_tc(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int
     splits = splits < 1 ? 1 : (splits < chunks ? splits : chunks);
     const int per = ((chunks + splits - 1) / splits) * WG_PIX;
     splits = (M + per - 1) / per;
-    k_conv_wgrad_tc<CI, NB><<<dim3(splits, groups), WG_THREADS, wg_smem<NB>(), s>>>(
-        dy, x, dw, n, h, w_, cout, per);
+    // TMA when every 64-pixel chunk is a rectangle of one image.
+    CUtensorMap mx, my;
+    const bool rect = (w_ % WG_PIX == 0 || WG_PIX % w_ == 0) && (int64_t(h) * w_) % WG_PIX == 0;
+    const int bw = w_ < WG_PIX ? w_ : WG_PIX, bh = WG_PIX / bw;
+    if (rect && wgrad_tma_maps(dy, x, n, h, w_, CI, cout, CI < 64 ? CI : 64, bw, bh, &mx, &my)) {
+        k_conv_wgrad_tc<CI, NB, true><<<dim3(splits, groups), WG_THREADS, wg_smem<NB>(), s>>>(
+            dy, x, dw, n, h, w_, cout, per, mx, my, bw, bh);
+    } else {
+        memset(&mx, 0, sizeof(mx));
+        memset(&my, 0, sizeof(my));
+        k_conv_wgrad_tc<CI, NB, false><<<dim3(splits, groups), WG_THREADS, wg_smem<NB>(), s>>>(
+            dy, x, dw, n, h, w_, cout, per, mx, my, 0, 0);
+    }
     return status();
 }
 

@@ -76,7 +76,8 @@ def test_conv_forward(cuda, n, h, w, cin, cout):
                                             (2, 12, 9, 128, 128), (1, 7, 13, 64, 96),
                                             (1, 9, 11, 96, 64), (1, 5, 9, 32, 160),
                                             (1, 6, 10, 128, 256), (2, 16, 16, 64, 32),
-                                            (1, 8, 32, 32, 128)])
+                                            (1, 8, 32, 32, 128), (1, 8, 16, 128, 256),
+                                            (2, 4, 64, 32, 160)])
 def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
