@@ -1088,8 +1088,6 @@ int grid_for(int64_t n) { return static_cast<int>(n / 256 + 1 < 4096 ? n / 256 +
 
 int status() { return cudaGetLastError() == cudaSuccess ? OK : ERR_CUDA; }
 
-// The forward convolution on the tensor cores: the widest channel tile that
-// divides Cout (128, 64 or 32 columns of tensor memory).
 // cuTensorMapEncodeTiled from the driver, found once through the runtime.
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
@@ -1280,7 +1278,17 @@ int wgrad_tc_n(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, i
 int conv_fwd_launch(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
                     float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
 {
-    if (cout % 128 == 0)
+    // The widest channel tile that divides Cout and still gives every SM a
+    // tile; for small images (16x16 x 32 is 64 pixel tiles) 64 channels.
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return ERR_CUDA;
+    }
+    const int64_t mt = (int64_t(n) * h * w_ + TBM - 1) / TBM;
+    if (cout % 128 == 0 && mt * (cout / 128) >= sms)
         return conv_fwd_tc<128>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, s);
     if (cout % 64 == 0)
         return conv_fwd_tc<64>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, s);

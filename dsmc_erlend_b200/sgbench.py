@@ -8,9 +8,9 @@ step: each layer shape of the network at a batch size, forward
 
 Prints one JSON line: per shape and op, milliseconds per call and TFLOP/s
 (2 Cin Cout 9 H W N), and the training step's milliseconds and TFLOP/s.
-`--profile` runs the forward and the weight gradient of one shape twice each
-(forward, weight gradient, forward, weight gradient) with no timing, for a
-profiler to capture the second pair.
+`--profile` runs forward, input gradient and weight gradient of one shape
+twice each (in that order) with no timing, for a profiler to capture the
+second round.
 """
 from __future__ import annotations
 
@@ -72,8 +72,8 @@ def main():
     if args.profile:
         f = ops(*shapes[0])
         for _ in range(2):
-            S._ok(f["fwd"](), "conv fwd")
-            S._ok(f["wgrad"](), "conv wgrad")
+            for name in ("fwd", "dgrad", "wgrad"):
+                S._ok(f[name](), "conv " + name)
         torch.cuda.synchronize()
         S._ok(L.dsmc_sg_check(None), "tensor-core wait")
         print(json.dumps({"profile": args.shape or "x".join(map(str, shapes[0]))}))

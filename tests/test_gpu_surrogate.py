@@ -47,7 +47,8 @@ def _close(got, want, rtol, what):
 @pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 12, 20, 64, 96),
                                             (3, 16, 16, 128, 64), (2, 16, 8, 32, 32),
                                             (1, 32, 32, 32, 64), (1, 4, 256, 64, 128),
-                                            (2, 8, 16, 96, 32), (1, 2, 128, 256, 32)])
+                                            (2, 8, 16, 96, 32), (1, 2, 128, 256, 32),
+                                            (1, 160, 128, 64, 128), (1, 150, 130, 32, 128)])
 def test_conv_forward(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
