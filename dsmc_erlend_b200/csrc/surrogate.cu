@@ -1060,9 +1060,16 @@ __global__ void k_mse(const float *out, const float *tgt, const float *mask, con
         atomicAdd(loss, l);
 }
 
+// hp, when given, holds {lr, c1, c2} in device memory (a captured step
+// whose learning rate and bias corrections change from replay to replay).
 __global__ void k_adam(float *w, bf16 *wb, const float *g, float *m, float *v, int64_t n, float lr,
-                       float b1, float b2, float eps, float c1, float c2)
+                       float b1, float b2, float eps, float c1, float c2, const float *hp)
 {
+    if (hp) {
+        lr = hp[0];
+        c1 = hp[1];
+        c2 = hp[2];
+    }
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const float gi = g[i];
@@ -1462,7 +1469,20 @@ int dsmc_sg_adam(float *w, uint16_t *w_bf16, const float *g, float *m, float *v,
     const float c1 = 1.0f - powf(beta1, static_cast<float>(t));
     const float c2 = 1.0f - powf(beta2, static_cast<float>(t));
     k_adam<<<grid_for(count), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        w, reinterpret_cast<bf16 *>(w_bf16), g, m, v, count, lr, beta1, beta2, eps, c1, c2);
+        w, reinterpret_cast<bf16 *>(w_bf16), g, m, v, count, lr, beta1, beta2, eps, c1, c2,
+        nullptr);
+    return status();
+}
+
+int dsmc_sg_adam_dev(float *w, uint16_t *w_bf16, const float *g, float *m, float *v,
+                     int64_t count, const float *step, float beta1, float beta2, float eps,
+                     void *stream)
+{
+    if (!w || !g || !m || !v || !step || count < 0)
+        return ERR_ARG;
+    k_adam<<<grid_for(count), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        w, reinterpret_cast<bf16 *>(w_bf16), g, m, v, count, 0.0f, beta1, beta2, eps, 1.0f, 1.0f,
+        step);
     return status();
 }
 

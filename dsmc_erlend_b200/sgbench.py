@@ -7,7 +7,8 @@ step: each layer shape of the network at a batch size, forward
     python -m dsmc_erlend_b200.sgbench --shape 128x128:32:32 --profile
 
 Prints one JSON line: per shape and op, milliseconds per call and TFLOP/s
-(2 Cin Cout 9 H W N), and the training step's milliseconds and TFLOP/s.
+(2 Cin Cout 9 H W N), and the training step's milliseconds and TFLOP/s,
+eager and replayed as one CUDA graph.
 `--profile` runs forward, input gradient and weight gradient of one shape
 twice each (in that order) with no timing, for a profiler to capture the
 second round.
@@ -120,6 +121,20 @@ def main():
         ms = e0.elapsed_time(e1) / args.iters
         out["train_step"] = {"ms": round(ms, 4),
                              "tflops": round(net.flops_per_step() / ms / 1e9, 1)}
+        # The same step replayed as one CUDA graph on the network's stream.
+        st = torch.cuda.Stream()
+        gnet = S.Surrogate(args.batch, stream=st.cuda_stream)
+        for _ in range(3):
+            gnet.train_step_graph(x, tgt, mask)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(args.iters):
+            gnet.train_step_graph(x, tgt, mask)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.iters
+        out["train_step_graph"] = {"ms": round(ms, 4),
+                                   "tflops": round(gnet.flops_per_step() / ms / 1e9, 1)}
     print(json.dumps(out))
 
 

@@ -58,6 +58,8 @@ _SIGS = {
     "dsmc_sg_mse": [_P, _P, _P, _P, _P, C.c_int64, C.c_int, C.c_int, _P],
     "dsmc_sg_adam": [_P, _P, _P, _P, _P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float,
                      C.c_int, _P],
+    "dsmc_sg_adam_dev": [_P, _P, _P, _P, _P, C.c_int64, _P, C.c_float, C.c_float, C.c_float,
+                         _P],
     "dsmc_sg_to_bf16": [_P, _P, C.c_int64, _P],
     "dsmc_sg_check": [_P],
 }
@@ -237,6 +239,61 @@ class Surrogate:
         self.adam_step(lr)
         return loss
 
+    def train_step_graph(self, x, target, mask, lr: float = 1e-3, beta1: float = 0.9,
+                         beta2: float = 0.999, eps: float = 1e-8):
+        """train_step replayed as one CUDA graph on the network's stream
+        (which must be set): captured on the first call for these x / target
+        / mask buffers (refill them between steps), the learning rate and
+        Adam's bias corrections written to device memory before each replay.
+        Returns the loss tensor [1]."""
+        torch = self.torch
+        if self.stream is None:
+            raise RuntimeError("graph training needs the network's own CUDA stream")
+        s = torch.cuda.ExternalStream(self.stream)
+        key = (x.data_ptr(), target.data_ptr(), mask.data_ptr())
+        if getattr(self, "_graph_key", None) != key:
+            self._hp = torch.zeros(3, device="cuda")
+            # Pinned staging of the step's values, four in flight.
+            self._hp_ring = [torch.zeros(3).pin_memory() for _ in range(4)]
+            self._hp_ev = [None] * 4
+            with torch.cuda.stream(s):
+                # Kernel attributes are set on first use, outside the capture.
+                self.forward(x)
+                self.loss_and_grad(target, mask)
+            s.synchronize()
+            g = torch.cuda.CUDAGraph()
+            L = lib()
+            with torch.cuda.graph(g, stream=s):
+                self.forward(x)
+                _, dout = self.loss_and_grad(target, mask)
+                self.backward(dout)
+                for name in self.w32:
+                    _ok(L.dsmc_sg_adam_dev(ptr(self.w32[name]), ptr(self.wb[name]),
+                                           ptr(self.gw[name]), ptr(self.m[name + ".w"]),
+                                           ptr(self.v[name + ".w"]), self.w32[name].numel(),
+                                           ptr(self._hp), beta1, beta2, eps, self._s), "adam w")
+                    _ok(L.dsmc_sg_adam_dev(ptr(self.b32[name]), None, ptr(self.gb[name]),
+                                           ptr(self.m[name + ".b"]), ptr(self.v[name + ".b"]),
+                                           self.b32[name].numel(), ptr(self._hp), beta1, beta2,
+                                           eps, self._s), "adam b")
+            self._graph, self._graph_key = g, key
+        self.t += 1
+        # The bias corrections as dsmc_sg_adam forms them (FP32 powf).
+        t32 = np.float32(self.t)
+        c1 = np.float32(1.0) - np.power(np.float32(beta1), t32)
+        c2 = np.float32(1.0) - np.power(np.float32(beta2), t32)
+        i = self.t % 4
+        if self._hp_ev[i] is not None:
+            self._hp_ev[i].synchronize()  # its last copy has been read
+        self._hp_ring[i].copy_(torch.tensor([lr, float(c1), float(c2)], dtype=torch.float32))
+        with torch.cuda.stream(s):
+            self._hp.copy_(self._hp_ring[i], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s)
+            self._hp_ev[i] = ev
+            self._graph.replay()
+        return self.loss[:1]
+
     def flops_per_step(self) -> float:
         """Tensor-core FLOPs of one train step: forward 2 Cin Cout 9 H W per
         sample and layer, backward twice that (dgrad and wgrad; the first
@@ -288,7 +345,9 @@ def train(x: np.ndarray, target: np.ndarray, mask: np.ndarray, epochs: int = 40,
     import torch
 
     n = x.shape[0]
-    net = Surrogate(batch, res=x.shape[1], seed=seed)
+    # One stream for the batch gathers and the graph-replayed steps.
+    st = torch.cuda.Stream()
+    net = Surrogate(batch, res=x.shape[1], seed=seed, stream=st.cuda_stream)
     dx = torch.from_numpy(x).to(torch.bfloat16).cuda()
     dt = torch.from_numpy(target.astype(np.float32)).cuda()
     dm = torch.from_numpy(mask.astype(np.float32)).cuda()
@@ -302,18 +361,22 @@ def train(x: np.ndarray, target: np.ndarray, mask: np.ndarray, epochs: int = 40,
     step = 0
     for ep in range(epochs):
         order = torch.from_numpy(rng.permutation(n)).cuda()
+        torch.cuda.current_stream().synchronize()
         losses = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        e0.record(st)
         for s in range(steps_per_epoch):
-            idx = order[s * batch:(s + 1) * batch]
-            torch.index_select(dx, 0, idx, out=bx)
-            torch.index_select(dt, 0, idx, out=bt)
-            torch.index_select(dm, 0, idx, out=bm)
             cur = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(total, 1)))
-            losses.append(net.train_step(bx, bt, bm, lr=cur).clone())
+            with torch.cuda.stream(st):
+                idx = order[s * batch:(s + 1) * batch]
+                torch.index_select(dx, 0, idx, out=bx)
+                torch.index_select(dt, 0, idx, out=bt)
+                torch.index_select(dm, 0, idx, out=bm)
+            loss = net.train_step_graph(bx, bt, bm, lr=cur)
+            with torch.cuda.stream(st):
+                losses.append(loss.clone())
             step += 1
-        e1.record()
+        e1.record(st)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / max(steps_per_epoch, 1)
         mean = float(torch.stack(losses).mean().item()) if losses else float("nan")
@@ -321,6 +384,10 @@ def train(x: np.ndarray, target: np.ndarray, mask: np.ndarray, epochs: int = 40,
         history.append((ep, mean, ms, tf))
         if log:
             log(f"epoch {ep} loss {mean:.4e} {ms:.2f} ms/step {tf:.1f} TFLOP/s")
+    # Hand the network back on the default stream (predictions read their
+    # outputs there).
+    st.synchronize()
+    net.stream = None
     return net, history
 
 

@@ -68,6 +68,14 @@ int dsmc_sg_mse(const float *out, const float *target, const float *mask, uint16
 int dsmc_sg_adam(float *w, uint16_t *w_bf16, const float *g, float *m, float *v, int64_t count,
                  float lr, float beta1, float beta2, float eps, int t, void *stream);
 
+/* The same step with the learning rate and the bias corrections read from
+ * device memory when the kernel runs: step = {lr, 1 - beta1^t, 1 - beta2^t}
+ * (FP32), so that a step captured in a CUDA graph can be replayed with the
+ * values of each step. */
+int dsmc_sg_adam_dev(float *w, uint16_t *w_bf16, const float *g, float *m, float *v,
+                     int64_t count, const float *step, float beta1, float beta2, float eps,
+                     void *stream);
+
 /* FP32 -> bf16 (round to nearest even). */
 int dsmc_sg_to_bf16(const float *x, uint16_t *y, int64_t count, void *stream);
 

@@ -289,3 +289,33 @@ def test_trained_surrogate_beats_freestream_and_shortens_transient(cuda, engine_
         errs[start] = weighted_errors(merged_field(e, 1), ref, p, d.u_free)
         e.close()
     assert errs["warm"]["n"] < errs["cold"]["n"], errs
+
+
+def test_graph_train_step_matches_eager(cuda):
+    # The captured step (device-side learning rate and bias corrections)
+    # gives the weights of the eager step, with a changing learning rate.
+    from dsmc_erlend_b200.surrogate import Surrogate, lib
+
+    torch = cuda
+    res = 32
+    rng = np.random.default_rng(11)
+    x = torch.from_numpy(rng.standard_normal((2, res, res, 32)).astype(np.float32))
+    x = x.to(torch.bfloat16).cuda()
+    tgt = torch.from_numpy(rng.standard_normal((2, res, res, 4)).astype(np.float32)).cuda()
+    mask = torch.ones(2, res, res, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    eager = Surrogate(2, res=res, seed=3, stream=s1.cuda_stream)
+    graph = Surrogate(2, res=res, seed=3, stream=s2.cuda_stream)
+    lrs = [1e-3, 5e-4, 2e-4]
+    with torch.cuda.stream(s1):
+        for lr in lrs:
+            eager.train_step(x, tgt, mask, lr=lr)
+    for lr in lrs:
+        graph.train_step_graph(x, tgt, mask, lr=lr)
+    torch.cuda.synchronize()
+    for name in eager.w32:
+        a, b = eager.w32[name].cpu().numpy(), graph.w32[name].cpu().numpy()
+        assert np.allclose(a, b, rtol=1e-5, atol=1e-7), name
+        assert np.array_equal(eager.wb[name].float().cpu().numpy(),
+                              graph.wb[name].float().cpu().numpy()) or np.allclose(a, b)
+    assert lib().dsmc_sg_check(None) == 0
