@@ -67,6 +67,20 @@ SIGNATURES = {
                                     C.c_void_p]),
     "dsmc_k_scatter": (C.c_int, [_P, _DV, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "dsmc_k_inject": (C.c_int, [_P, _DV, _D, C.c_double, C.c_double, C.c_double, C.c_double,
+                                C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int64,
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                _I64, C.c_void_p]),
+    "dsmc_k_collide": (C.c_int, [_P, _DV, C.c_double, C.c_int32, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                 C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dsmc_k_elastic": (C.c_int, [_P, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                 C.c_uint32, C.c_void_p, C.c_void_p]),
+    "dsmc_append_particles_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    "dsmc_remove_inside_box": (C.c_int, [C.c_void_p, C.c_int]),
+    "dsmc_collide_list": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int32, _I32, C.c_uint32,
+                                    C.c_uint32, C.c_uint32, _I32]),
 }
 
 _lib = None

@@ -13,6 +13,7 @@
 
 #include "../../include/dsmc.h"
 #include "dsmc_kernels.cuh"
+#include "dsmc_units.cuh"
 
 using namespace dsmc;
 
@@ -1938,6 +1939,161 @@ int dsmc_autotune(dsmc_ctx *c, int steps_per_trial)
     return device_error(c);
 }
 
+} // extern "C"
+
+namespace {
+
+// Removes, in the reference's swap-with-last order, the slots of [q0, n) of
+// case i that `pred` selects (slots below q0 all survive) and sets the case's
+// particle count; the caller re-sorts.  Temporary buffers come from the
+// stream-ordered allocator (these edits run between steps, rarely).
+template <class T> int edit_case(dsmc_ctx *c, int i, int64_t q0, int64_t n, int pred)
+{
+    const int64_t m = n - q0;
+    if (m <= 0)
+        return DSMC_OK;
+    const int64_t ntile = (m + TILE - 1) / TILE;
+    int32_t *tiles = nullptr;
+    int64_t *alive = nullptr, *holes = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&tiles), sizeof(int32_t) * ntile, c->stream));
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&alive), sizeof(int64_t), c->stream));
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&holes), sizeof(int64_t) * m, c->stream));
+    const Slots<T> p = slots<T>(c, c->cur);
+    const int g = static_cast<int>(std::min<int64_t>(ntile, 4 * c->sms));
+    k_edit_count<T><<<g, TILE_THREADS, 0, c->stream>>>(c->d_cases, i, p, q0, n, pred, tiles);
+    k_edit_scan<<<1, 1024, 0, c->stream>>>(tiles, ntile, alive);
+    k_edit_holes<T><<<g, TILE_THREADS, 0, c->stream>>>(c->d_cases, i, p, q0, n, pred, tiles,
+                                                        alive, holes);
+    k_edit_fill<T><<<g, TILE_THREADS, 0, c->stream>>>(c->d_cases, i, p, q0, n, pred, tiles, alive,
+                                                       holes, c->d_err);
+    k_edit_commit<<<1, 1, 0, c->stream>>>(c->d_state, i, q0, alive);
+    CK(cudaGetLastError());
+    CK(cudaFreeAsync(tiles, c->stream));
+    CK(cudaFreeAsync(alive, c->stream));
+    CK(cudaFreeAsync(holes, c->stream));
+    return DSMC_OK;
+}
+
+// Appends n FP64 particles (device arrays) to case i, drops those outside the
+// domain as BoundaryConditions would, and re-sorts.
+template <class T>
+int append_case(dsmc_ctx *c, int i, int64_t n_old, const double *x, const double *y,
+                const double *vx, const double *vy, const double *vz, int64_t n)
+{
+    if (n > 0) {
+        const int g = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256)));
+        k_upload_case<T><<<g, 256, 0, c->stream>>>(x, y, vx, vy, vz, n, slots<T>(c, c->cur),
+                                                    c->hcases[i].pbase + n_old);
+        CK(cudaGetLastError());
+    }
+    int s = edit_case<T>(c, i, n_old, n_old + n, EDIT_OUTSIDE_DOMAIN);
+    return s ? s : resort_all<T>(c);
+}
+
+template <class T> int remove_inside_case(dsmc_ctx *c, int i, int64_t n_old)
+{
+    int s = edit_case<T>(c, i, 0, n_old, EDIT_INSIDE_BOX);
+    return s ? s : resort_all<T>(c);
+}
+
+template <class T>
+int collide_list_case(dsmc_ctx *c, const CaseDev &cd, const int32_t *d_buf, uint32_t kind,
+                      uint32_t step, int32_t *d_nc)
+{
+    // d_buf: start[2], entity, then the list.
+    k_unit_collide<T><<<1, 32, 0, c->stream>>>(cd, 1, d_buf, d_buf + 3, slots<T>(c, c->cur),
+                                               cd.pbase, kind, step,
+                                               reinterpret_cast<const uint32_t *>(d_buf + 2),
+                                               d_nc);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int dsmc_append_particles_device(dsmc_ctx *c, int i, const double *x, const double *y,
+                                 const double *vx, const double *vy, const double *vz, int64_t n)
+{
+    if (c == nullptr || i < 0 || i >= c->ncase || n < 0 ||
+        (n > 0 && (!x || !y || !vx || !vy || !vz)))
+        return DSMC_ERR_ARGUMENT;
+    if (!c->initialized || c->stage != 0)
+        return DSMC_ERR_STATE;
+    std::vector<CaseState> st;
+    int s = read_state(c, st);
+    if (s)
+        return s;
+    if (st[i].n_old + n > c->hcases[i].cap)
+        return DSMC_ERR_CAPACITY;
+    s = c->precision == DSMC_FP32
+            ? append_case<float>(c, i, st[i].n_old, x, y, vx, vy, vz, n)
+            : append_case<double>(c, i, st[i].n_old, x, y, vx, vy, vz, n);
+    if (s)
+        return s;
+    CK(cudaStreamSynchronize(c->stream));
+    return device_error(c);
+}
+
+int dsmc_remove_inside_box(dsmc_ctx *c, int i)
+{
+    if (c == nullptr || i < 0 || i >= c->ncase)
+        return DSMC_ERR_ARGUMENT;
+    if (!c->initialized || c->stage != 0)
+        return DSMC_ERR_STATE;
+    std::vector<CaseState> st;
+    int s = read_state(c, st);
+    if (s)
+        return s;
+    s = c->precision == DSMC_FP32 ? remove_inside_case<float>(c, i, st[i].n_old)
+                                  : remove_inside_case<double>(c, i, st[i].n_old);
+    if (s)
+        return s;
+    CK(cudaStreamSynchronize(c->stream));
+    return device_error(c);
+}
+
+int dsmc_collide_list(dsmc_ctx *c, int i, double cell_volume, int32_t n, const int32_t *ipc,
+                      uint32_t kind, uint32_t step, uint32_t entity, int32_t *n_collisions)
+{
+    if (c == nullptr || i < 0 || i >= c->ncase || n < 0 || (n > 0 && ipc == nullptr) ||
+        n_collisions == nullptr || !(cell_volume > 0.0))
+        return DSMC_ERR_ARGUMENT;
+    if (!c->initialized || (c->stage != 0 && c->stage < 3))
+        return DSMC_ERR_STATE; // slots are a sorted population only between steps or after Indexing
+    std::vector<CaseState> st;
+    int s = read_state(c, st);
+    if (s)
+        return s;
+    const int64_t np = c->stage >= 2 ? st[i].n_keep : st[i].n_old;
+    for (int32_t k = 0; k < n; ++k)
+        if (ipc[k] < 0 || ipc[k] >= np)
+            return DSMC_ERR_ARGUMENT;
+    std::vector<int32_t> buf(3 + static_cast<size_t>(n));
+    buf[0] = 0;
+    buf[1] = n;
+    buf[2] = static_cast<int32_t>(entity);
+    std::copy(ipc, ipc + n, buf.begin() + 3);
+    CaseDev cd = c->hcases[i];
+    cd.dv = cell_volume; // BinaryCollisionsInCell's CellVolume argument
+    int32_t *d = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&d), sizeof(int32_t) * (buf.size() + 1),
+                       c->stream));
+    CK(cudaMemcpyAsync(d, buf.data(), sizeof(int32_t) * buf.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+    s = c->precision == DSMC_FP32 ? collide_list_case<float>(c, cd, d, kind, step, d + buf.size())
+                                  : collide_list_case<double>(c, cd, d, kind, step, d + buf.size());
+    if (s)
+        return s;
+    int32_t nc = 0;
+    CK(cudaMemcpyAsync(&nc, d + buf.size(), sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaFreeAsync(d, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *n_collisions = nc;
+    return device_error(c);
+}
+
 int dsmc_k_intersect(const dsmc_params *p, int64_t n, const double *x, const double *y,
                      const double *dx, const double *dy, int32_t *hit, double *t_hit, double *nx,
                      double *ny, void *cuda_stream)
@@ -1994,6 +2150,96 @@ int dsmc_k_scatter(const dsmc_params *p, const dsmc_derived *d, int64_t n, doubl
     const int grid = static_cast<int>(std::min<int64_t>(4096, (n + 255) / 256));
     k_unit_scatter<<<grid, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(c, n, v, nx, ny, kind,
                                                                              step, entity);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+
+int dsmc_k_inject(const dsmc_params *p, const dsmc_derived *d, const double *rect, double n_gas,
+                  double ux_gas, double uy_gas, double t_gas, int move_flag, uint32_t kind,
+                  uint32_t step, uint32_t entity, int64_t capacity, double *x, double *y,
+                  double *vx, double *vy, double *vz, int64_t *n_out, void *cuda_stream)
+{
+    if (p == nullptr || rect == nullptr || n_out == nullptr || capacity < 0)
+        return DSMC_ERR_ARGUMENT;
+    dsmc_derived dd;
+    const int s = dsmc_setup(p, &dd);
+    if (s)
+        return s;
+    if (d != nullptr)
+        dd = *d;
+    const CaseDev c = make_case(*p, dd);
+    // Boundary.cpp:62-63 and :53
+    const double v = (rect[2] - rect[0]) * (rect[3] - rect[1]) * p->dz;
+    const double navg = n_gas * v / dd.weight;
+    const double rt = K_BOLTZMANN * t_gas / dd.molecule_mass;
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    int32_t *cnt = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&cnt), 2 * sizeof(int32_t), st));
+    k_unit_inject_count<<<1, 1, 0, st>>>(c, navg, kind, step, entity, cnt);
+    int32_t h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *n_out = h[0];
+    int status = DSMC_OK;
+    if (h[0] > capacity) {
+        status = DSMC_ERR_CAPACITY;
+    } else if (h[0] > 0) {
+        if (!x || !y || !vx || !vy || !vz) {
+            status = DSMC_ERR_ARGUMENT;
+        } else {
+            const int g = static_cast<int>(std::min<int64_t>(4096, (h[0] + 255) / 256));
+            k_unit_inject_fill<<<g, 256, 0, st>>>(c, make_double4(rect[0], rect[1], rect[2], rect[3]),
+                                                  ux_gas, uy_gas, rt, move_flag, kind, step,
+                                                  entity, cnt, x, y, vx, vy, vz);
+            CK(cudaGetLastError());
+        }
+    }
+    CK(cudaFreeAsync(cnt, st));
+    return status;
+}
+
+int dsmc_k_collide(const dsmc_params *p, const dsmc_derived *d, double cell_volume,
+                   int32_t n_lists, const int32_t *list_start, const int32_t *ipc, double *vx,
+                   double *vy, double *vz, uint32_t kind, uint32_t step, const uint32_t *entity,
+                   int32_t *n_collisions, void *cuda_stream)
+{
+    if (p == nullptr || n_lists < 0 || !(cell_volume > 0.0) ||
+        (n_lists > 0 && (list_start == nullptr || !vx || !vy || !vz)))
+        return DSMC_ERR_ARGUMENT;
+    dsmc_derived dd;
+    const int s = dsmc_setup(p, &dd);
+    if (s)
+        return s;
+    if (d != nullptr)
+        dd = *d;
+    if (n_lists == 0)
+        return DSMC_OK;
+    CaseDev c = make_case(*p, dd);
+    c.dv = cell_volume; // BinaryCollisionsInCell's CellVolume argument
+    Slots<double> sl{nullptr, nullptr, vx, vy, vz};
+    const int g = static_cast<int>(std::min<int32_t>(4096, (n_lists + 127) / 128));
+    k_unit_collide<double><<<g, 128, 0, static_cast<cudaStream_t>(cuda_stream)>>>(
+        c, n_lists, list_start, ipc, sl, 0, kind, step, entity, n_collisions);
+    CK(cudaGetLastError());
+    return DSMC_OK;
+}
+
+int dsmc_k_elastic(const dsmc_params *p, int64_t n, double *v1, double *v2, const double *cr,
+                   uint32_t kind, uint32_t step, const uint32_t *entity, void *cuda_stream)
+{
+    if (p == nullptr || n < 0 || (n > 0 && (!v1 || !v2 || !cr)))
+        return DSMC_ERR_ARGUMENT;
+    dsmc_derived dd;
+    const int s = dsmc_setup(p, &dd);
+    if (s)
+        return s;
+    if (n == 0)
+        return DSMC_OK;
+    const CaseDev c = make_case(*p, dd);
+    const int g = static_cast<int>(std::min<int64_t>(4096, (n + 255) / 256));
+    k_unit_elastic<<<g, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(c, n, v1, v2, cr, kind,
+                                                                          step, entity);
     CK(cudaGetLastError());
     return DSMC_OK;
 }

@@ -155,6 +155,36 @@ __device__ __forceinline__ int irand_poisson(dsmc_stream &s, double e, int *draw
     return i - 1;
 }
 
+// The particle count of GenerateNewParticles (Boundary.cpp:62-71) for a mean
+// of navg: floor plus a Bernoulli draw above 20, a Poisson draw otherwise;
+// *draws receives the uniforms it used (the particles' draws follow them).
+__device__ __forceinline__ int inflow_count(dsmc_stream &r, double navg, int *draws)
+{
+    if (navg > 20.0) {
+        int n = static_cast<int>(navg);
+        if (uniform(r) < navg - n)
+            n++;
+        *draws = 1;
+        return n;
+    }
+    return irand_poisson(r, navg, draws);
+}
+
+// One particle of GenerateNewParticles (Boundary.cpp:85-90): a uniform
+// position in the rectangle rect = (x1, y1, x2, y2) (v2rand_uniform_rect,
+// :44-47), then a Maxwellian velocity around (ux, uy, 0) of variance rt =
+// k T / m per component (vrand_MB, :52-57).  Eight draws.
+__device__ __forceinline__ void new_particle(dsmc_stream &r, const double *rect, double ux,
+                                             double uy, double rt, double &x, double &y,
+                                             double &vx, double &vy, double &vz)
+{
+    x = rect[0] + (rect[2] - rect[0]) * uniform(r);
+    y = rect[1] + (rect[3] - rect[1]) * uniform(r);
+    vx = frand_gaussian(r, ux, rt);
+    vy = frand_gaussian(r, uy, rt);
+    vz = frand_gaussian(r, 0.0, rt);
+}
+
 // SampleGaussianPair, Boundary.cpp:27-41
 __device__ __forceinline__ void gaussian_pair(dsmc_stream &s, double variance, double &first,
                                               double &second)

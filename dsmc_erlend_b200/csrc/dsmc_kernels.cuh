@@ -156,16 +156,8 @@ __global__ void k_plan(const CaseDev *cases, CaseState *st, StepScratch *sc, Til
                 open_stream(r, c, DSMC_RNG_INIT, 0, 0);
             else
                 open_stream(r, c, DSMC_RNG_INJECT, s.step, static_cast<uint32_t>(k));
-            const double navg = c.strip_navg[k];
-            int n, draws;
-            if (navg > 20.0) {
-                n = static_cast<int>(navg);
-                if (uniform(r) < navg - n)
-                    n++;
-                draws = 1;
-            } else {
-                n = irand_poisson(r, navg, &draws);
-            }
+            int draws;
+            const int n = inflow_count(r, c.strip_navg[k], &draws);
             s.inj_count[k] = n;
             s.inj_c0[k] = draws;
             total += n;
@@ -756,12 +748,8 @@ __global__ void __launch_bounds__(TILE_THREADS)
                 open_stream(r, c, DSMC_RNG_INJECT, s.step, static_cast<uint32_t>(strip));
             dsmc_stream_seek(&r, static_cast<uint64_t>(s.inj_c0[strip]) + 8ull * js);
             const double *b = c.strip[strip];
-            // v2rand_uniform_rect (Boundary.cpp:44-47) and vrand_MB (:52-57).
-            double x = b[0] + (b[2] - b[0]) * uniform(r);
-            double y = b[1] + (b[3] - b[1]) * uniform(r);
-            const double vx = frand_gaussian(r, c.ux_free, c.rt_free);
-            const double vy = frand_gaussian(r, c.uy_free, c.rt_free);
-            const double vz = frand_gaussian(r, 0.0, c.rt_free);
+            double x, y, vx, vy, vz;
+            new_particle(r, b, c.ux_free, c.uy_free, c.rt_free, x, y, vx, vy, vz);
             if (!init_mode) {
                 x += c.dt * vx;
                 y += c.dt * vy;
@@ -1592,6 +1580,83 @@ __device__ __forceinline__ int ntc_pairs(const CaseDev &c, int n, dsmc_stream &r
     return (uniform(r) < frac) ? nn + 1 : nn;
 }
 
+// ElasticCollision (Collision.cpp:7-19) of velocities vi, vj with relative
+// speed cr, drawing v3rand_isotropic (rng/IsotropicVectorRNG.cxx:11-19) from
+// r; the new velocities replace vi and vj.
+__device__ __forceinline__ void elastic_collision(dsmc_stream &r, double vi[3], double vj[3],
+                                                  double cr)
+{
+    const double cos_t = 1.0 - 2.0 * uniform(r);
+    const double sin_t = sqrt(1.0 - cos_t * cos_t);
+    const double e = 2.0 * PI_D * uniform(r);
+    const double nv[3] = {cos_t, sin_t * cos(e), sin_t * sin(e)};
+    const double half = cr * 0.5;
+    const double vc0 = 0.5 * (vj[0] + vi[0]), vc1 = 0.5 * (vj[1] + vi[1]),
+                 vc2 = 0.5 * (vj[2] + vi[2]);
+    const double d0 = half * nv[0], d1 = half * nv[1], d2 = half * nv[2];
+    vi[0] = vc0 + d0;
+    vi[1] = vc1 + d1;
+    vi[2] = vc2 + d2;
+    vj[0] = vc0 - d0;
+    vj[1] = vc1 - d1;
+    vj[2] = vc2 - d2;
+}
+
+// The particles of one cell's list IPC: entry i is slot base + i, or
+// base + ipc[i] when a list is given.  Velocities are read as doubles and
+// stored rounded to the state's precision.
+template <class T> struct SlotRun {
+    Slots<T> p;
+    int64_t base;
+    const int32_t *ipc;
+    __device__ __forceinline__ int64_t at(int i) const { return base + (ipc ? ipc[i] : i); }
+    __device__ __forceinline__ void load(int i, double v[3]) const
+    {
+        const int64_t g = at(i);
+        v[0] = static_cast<double>(p.vx[g]);
+        v[1] = static_cast<double>(p.vy[g]);
+        v[2] = static_cast<double>(p.vz[g]);
+    }
+    __device__ __forceinline__ void store(int i, const double v[3]) const
+    {
+        const int64_t g = at(i);
+        p.vx[g] = Store<T>::rn(v[0]);
+        p.vy[g] = Store<T>::rn(v[1]);
+        p.vz[g] = Store<T>::rn(v[2]);
+    }
+};
+
+// The candidate loop of BinaryCollisionsInCell (Collision.cpp:29-42): nn
+// candidate pairs of the cell's n particles drawn from r (which continues
+// after the pair-count draw), VHS acceptance, elastic collision of the
+// accepted ones.  Returns the number of collisions.
+template <class Run>
+__device__ __forceinline__ int ntc_candidates(const CaseDev &c, int n, int nn, dsmc_stream &r,
+                                              const Run &run)
+{
+    int ncc = 0;
+    for (int kk = 0; kk < nn; ++kk) {
+        const int i = irand_uniform(r, n);
+        int j;
+        do {
+            j = irand_uniform(r, n);
+        } while (j == i);
+        double vi[3], vj[3];
+        run.load(i, vi);
+        run.load(j, vj);
+        const double vr0 = vj[0] - vi[0], vr1 = vj[1] - vi[1], vr2 = vj[2] - vi[2];
+        const double cr = sqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
+        const double sigma = c.sigma_ref * pow(c.cr_ref / cr, c.omega);
+        if (uniform(r) < sigma * cr / c.sc_max) {
+            elastic_collision(r, vi, vj, cr);
+            run.store(i, vi);
+            run.store(j, vj);
+            ncc++;
+        }
+    }
+    return ncc;
+}
+
 __global__ void __launch_bounds__(256)
     k_collide_select(const CaseDev *__restrict__ cases, const CaseState *st, StepScratch *sc,
                      TileTables tt, Cells cells, int side, uint32_t *__restrict__ coll_list,
@@ -1647,38 +1712,8 @@ __global__ void __launch_bounds__(128)
         dsmc_stream r;
         open_stream(r, c, DSMC_RNG_COLLIDE, s.step, static_cast<uint32_t>(cl));
         const int nn = ntc_pairs(c, n, r); // draw 0 again: the same value
-        int ncc = 0;
-        for (int kk = 0; kk < nn; ++kk) {
-            const int i = irand_uniform(r, n);
-            int j;
-            do {
-                j = irand_uniform(r, n);
-            } while (j == i);
-            const double vi0 = p.vx[a0 + i], vi1 = p.vy[a0 + i], vi2 = p.vz[a0 + i];
-            const double vj0 = p.vx[a0 + j], vj1 = p.vy[a0 + j], vj2 = p.vz[a0 + j];
-            const double vr0 = vj0 - vi0, vr1 = vj1 - vi1, vr2 = vj2 - vi2;
-            const double cr = sqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
-            const double sigma = c.sigma_ref * pow(c.cr_ref / cr, c.omega);
-            if (uniform(r) < sigma * cr / c.sc_max) {
-                // ElasticCollision, Collision.cpp:7-19, with v3rand_isotropic
-                // (rng/IsotropicVectorRNG.cxx:11-19).
-                const double cos_t = 1.0 - 2.0 * uniform(r);
-                const double sin_t = sqrt(1.0 - cos_t * cos_t);
-                const double e = 2.0 * PI_D * uniform(r);
-                const double nv[3] = {cos_t, sin_t * cos(e), sin_t * sin(e)};
-                const double half = cr * 0.5;
-                const double vc0 = 0.5 * (vj0 + vi0), vc1 = 0.5 * (vj1 + vi1),
-                             vc2 = 0.5 * (vj2 + vi2);
-                const double d0 = half * nv[0], d1 = half * nv[1], d2 = half * nv[2];
-                p.vx[a0 + i] = Store<T>::rn(vc0 + d0);
-                p.vy[a0 + i] = Store<T>::rn(vc1 + d1);
-                p.vz[a0 + i] = Store<T>::rn(vc2 + d2);
-                p.vx[a0 + j] = Store<T>::rn(vc0 - d0);
-                p.vy[a0 + j] = Store<T>::rn(vc1 - d1);
-                p.vz[a0 + j] = Store<T>::rn(vc2 - d2);
-                ncc++;
-            }
-        }
+        SlotRun<T> run{p, a0, nullptr};
+        const int ncc = ntc_candidates(c, n, nn, r, run);
         if (ncc > 0) {
             if (s.sampling_mode == 1) // CollideParticles, Collision.cpp:53
                 cells.acc[ACC_NC * cells.acc_stride + cg] += ncc;

@@ -9,6 +9,7 @@
 #include <filesystem>
 #include <fstream>
 #include <iomanip>
+#include <limits>
 #include <string>
 
 #include "../../include/dsmc.h"
@@ -22,6 +23,76 @@ bool cll_valid(double an, double at)
 {
     return std::isfinite(an) && an >= 0.0 && an <= 1.0 && std::isfinite(at) && at >= 0.0 &&
            at <= 1.0;
+}
+
+// The Gamma function of x > 0 with the reference's arithmetic
+// (src/Initialization.cpp:111-207), so that CrRef and the free-stream mean
+// free time and path come out with the same bits.  The method is the
+// published one that code follows:
+//   * x < 0.001: 1/Gamma(x) = x (1 + g x) + O(x^3), g = Euler's constant;
+//   * 0.001 <= x < 12: W. J. Cody's rational approximation of Gamma on
+//     (1, 2) (SPECFUN, Gamma(1 + z) = 1 + z P(z) / Q(z), the degree-8
+//     numerator and denominator of Cody's published table, evaluated by
+//     Horner's rule), then Gamma(x) = Gamma(x + 1) / x below 1 and the
+//     recurrence Gamma(x + 1) = x Gamma(x) above 2;
+//   * x >= 12: Stirling's series for log Gamma (Abramowitz and Stegun 6.1.41)
+//     with the first eight Bernoulli terms, infinity beyond 171.624.
+// Every operation is in the same order as there (this file is compiled
+// without contraction into fused multiply-adds).
+double gamma_ref(double x)
+{
+    constexpr double euler_gamma = 0.577215664901532860606512090;
+    if (x < 0.001)
+        return 1.0 / (x * (1.0 + euler_gamma * x));
+    if (x < 12.0) {
+        static const double num_coef[8] = {
+            -1.71618513886549492533811E+0, 2.47656508055759199108314E+1,
+            -3.79804256470945635097577E+2, 6.29331155312818442661052E+2,
+            8.66966202790413211295064E+2,  -3.14512729688483675254357E+4,
+            -3.61444134186911729807069E+4, 6.64561438202405440627855E+4};
+        static const double den_coef[8] = {
+            -3.08402300119738975254353E+1, 3.15350626979604161529144E+2,
+            -1.01515636749021914166146E+3, -3.10777167157231109440444E+3,
+            2.25381184209801510330112E+4,  4.75584627752788110767815E+3,
+            -1.34659959864969306392456E+5, -1.15132259675553483497211E+5};
+        const bool below_one = x < 1.0;
+        int shift = 0; // recurrence steps from (1, 2) back up to x
+        double y = x;
+        if (below_one) {
+            y += 1.0;
+        } else {
+            shift = static_cast<int>(std::floor(y)) - 1;
+            y -= shift;
+        }
+        const double z = y - 1;
+        double num = 0.0, den = 1.0;
+        for (int i = 0; i < 8; ++i) {
+            num = (num + num_coef[i]) * z;
+            den = den * z + den_coef[i];
+        }
+        double g = num / den + 1.0;
+        if (below_one) {
+            g /= (y - 1.0);
+        } else {
+            for (int i = 0; i < shift; ++i)
+                g *= y++;
+        }
+        return g;
+    }
+    if (x > 171.624)
+        return std::numeric_limits<double>::max() * 2.0;
+    static const double bern[8] = {1.0 / 12.0,   -1.0 / 360.0,      1.0 / 1260.0,
+                                   -1.0 / 1680.0, 1.0 / 1188.0,      -691.0 / 360360.0,
+                                   1.0 / 156.0,  -3617.0 / 122400.0};
+    const double z = 1.0 / (x * x);
+    double sum = bern[7];
+    for (int i = 6; i >= 0; --i) {
+        sum *= z;
+        sum += bern[i];
+    }
+    const double series = sum / x;
+    constexpr double half_log_2pi = 0.91893853320467274178032973640562;
+    return std::exp((x - 0.5) * std::log(x) - x + half_log_2pi + series);
 }
 } // namespace
 
@@ -66,8 +137,8 @@ void dsmc_default_params(dsmc_params *p)
     p->precision = DSMC_FP64;
 }
 
-// Setup(), src/Initialization.cpp:210-265.  The reference's private Gamma
-// (:111-207) is replaced by std::tgamma; CrRef then agrees to about an ulp.
+// Setup(), src/Initialization.cpp:210-265, with the reference's Gamma
+// (gamma_ref above): every derived constant has the reference's bits.
 int dsmc_setup(const dsmc_params *p, dsmc_derived *d)
 {
     if (p == nullptr || d == nullptr)
@@ -94,10 +165,10 @@ int dsmc_setup(const dsmc_params *p, dsmc_derived *d)
     d->sigma_ref = PI_D * p->d_ref * p->d_ref;
     d->omega = 2.0 * p->viscosity_index - 1.0;
     d->cr_ref = std::sqrt(4.0 * k * p->t_ref / m) /
-                std::pow(std::tgamma(2.5 - p->viscosity_index), 1.0 / d->omega);
+                std::pow(gamma_ref(2.5 - p->viscosity_index), 1.0 / d->omega);
     const double q = 1.0 - d->omega;
     const double mean_rel = std::pow(4.0 * k * p->t_free / m, q / 2.0) *
-                            std::tgamma((q + 3.0) / 2.0) / std::tgamma(1.5);
+                            gamma_ref((q + 3.0) / 2.0) / gamma_ref(1.5);
     const double rate = d->sigma_ref * std::pow(d->cr_ref, d->omega) * mean_rel;
     d->mft_free = 1.0 / (p->n_free * rate);
     const double mean_speed = std::sqrt(8.0 * k * p->t_free / (PI_D * m));

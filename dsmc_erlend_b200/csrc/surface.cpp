@@ -176,6 +176,7 @@ Scratch &scratch()
 } // namespace
 
 dsmc_ctx *dsmc::Context() { return g_ctx; }
+const dsmc_params &dsmc::Parameters() { return g_params; }
 
 // WallModelName, src/Boundary.cpp:15-24
 const char *WallModelName()
@@ -436,6 +437,117 @@ double brng()
     return dsmc_stream_uniform(&g_user);
 }
 
+// ---- single routines of the reference headers -----------------------------------
+namespace {
+// The population edits need the step's sort done: between steps they run
+// at once; after Indexing the open step is ended first; between
+// MoveParticles and Indexing the particles are mid-step and the call fails.
+void settle_population(const char *what)
+{
+    dsmc_ctx *c = ctx();
+    (void)c;
+    if (g_step_open) {
+        const int s = dsmc_stage_end_step(g_ctx);
+        if (s == DSMC_ERR_STATE)
+            fail(s, (std::string(what) + " between MoveParticles() and Indexing()").c_str());
+        check(s, what);
+        g_step_open = false;
+    }
+}
+
+// Device buffers of the generated particles, grown as needed.
+struct InjectBuffers {
+    double *d = nullptr;
+    int64_t cap = 0;
+    void reserve(int64_t n)
+    {
+        if (n <= cap)
+            return;
+        if (d != nullptr)
+            cudaFree(d);
+        d = nullptr;
+        cap = 0;
+        if (cudaMalloc(&d, sizeof(double) * 5 * static_cast<size_t>(n)) != cudaSuccess)
+            fail(DSMC_ERR_CUDA, "GenerateNewParticles buffers");
+        cap = n;
+    }
+};
+} // namespace
+
+// GenerateNewParticles, src/Boundary.cpp:60-92: the particles are drawn on
+// the device from the user stream, then join the population (those outside
+// the domain are dropped as BoundaryConditions would drop them) and are
+// sorted by cell as the next Indexing orders them.
+void GenerateNewParticles(double x1, double y1, double x2, double y2, double Ngas,
+                          double Ugasx, double Ugasy, double Tgas, int MoveFlag)
+{
+    settle_population("GenerateNewParticles");
+    static InjectBuffers buf;
+    const double rect[4] = {x1, y1, x2, y2};
+    const uint32_t step = g_user_calls++;
+    const double navg = Ngas * ((x2 - x1) * (y2 - y1) * DZ) / Weight;
+    buf.reserve(std::max<int64_t>(64, static_cast<int64_t>(navg + 10.0 * std::sqrt(navg)) + 64));
+    int64_t n = 0;
+    for (int attempt = 0;; ++attempt) {
+        const int64_t cap = buf.cap;
+        double *d = buf.d;
+        const int s = dsmc_k_inject(&g_params, &g_derived, rect, Ngas, Ugasx, Ugasy, Tgas,
+                                    MoveFlag, DSMC_RNG_USER, step, 0, cap, d, d + cap,
+                                    d + 2 * cap, d + 3 * cap, d + 4 * cap, &n, nullptr);
+        if (s == DSMC_ERR_CAPACITY && attempt == 0) { // the same draws again, more room
+            buf.reserve(n);
+            continue;
+        }
+        check(s, "GenerateNewParticles");
+        break;
+    }
+    const int64_t cap = buf.cap;
+    check(dsmc_append_particles_device(ctx(), 0, buf.d, buf.d + cap, buf.d + 2 * cap,
+                                       buf.d + 3 * cap, buf.d + 4 * cap, n),
+          "GenerateNewParticles");
+    pull_counters();
+}
+
+// RemoveParticlesInsideBox, src/Geometry.cpp:231-247
+void RemoveParticlesInsideBox()
+{
+    settle_population("RemoveParticlesInsideBox");
+    check(dsmc_remove_inside_box(ctx(), 0), "RemoveParticlesInsideBox");
+    pull_counters();
+}
+
+// ElasticCollision, src/Collision.cpp:7-19 (on the device, user stream)
+void ElasticCollision(double *V1, double *V2, double Cr)
+{
+    dsmc_params p = params_from_globals();
+    Scratch &s = scratch();
+    const double in[7] = {V1[0], V1[1], V1[2], V2[0], V2[1], V2[2], Cr};
+    if (cudaMemcpy(s.d, in, sizeof in, cudaMemcpyHostToDevice) != cudaSuccess)
+        fail(DSMC_ERR_CUDA, "ElasticCollision");
+    check(dsmc_k_elastic(&p, 1, s.d, s.d + 3, s.d + 6, DSMC_RNG_USER, g_user_calls++, nullptr,
+                         nullptr),
+          "ElasticCollision");
+    double out[6];
+    if (cudaMemcpy(out, s.d, sizeof out, cudaMemcpyDeviceToHost) != cudaSuccess)
+        fail(DSMC_ERR_CUDA, "ElasticCollision");
+    std::copy(out, out + 3, V1);
+    std::copy(out + 3, out + 6, V2);
+}
+
+// BinaryCollisionsInCell, src/Collision.cpp:21-44: IPC holds slot indices of
+// the current cell-sorted population (slot i is the i-th particle of
+// dsmc_download_particles); the pairs are drawn from the user stream.
+int BinaryCollisionsInCell(double CellVolume, int NPC, int *IPC)
+{
+    if (NPC < 2)
+        return 0;
+    int32_t nc = 0;
+    check(dsmc_collide_list(ctx(), 0, CellVolume, NPC, IPC, DSMC_RNG_USER, g_user_calls++, 0,
+                            &nc),
+          "BinaryCollisionsInCell");
+    return nc;
+}
+
 // ---- RunSimulation, src/Simulation.cpp:18-247 --------------------------------
 namespace {
 enum class ArgumentResult { Run, Help, Error };
@@ -502,7 +614,11 @@ ArgumentResult ParseArguments(int argc, char **argv)
             return ArgumentResult::Error;
         }
         if (++i == argc) {
-            std::cerr << option << " requires a value.\n";
+            // The angle flags keep the reference's message (Simulation.cpp:44).
+            if (option == "--angle-of-attack" || option == "--aoa")
+                std::cerr << option << " requires an angle in degrees.\n";
+            else
+                std::cerr << option << " requires a value.\n";
             return ArgumentResult::Error;
         }
         const std::string value = argv[i];

@@ -295,6 +295,32 @@ int dsmc_upload_particles(dsmc_ctx *ctx, int case_index, const double *x, const 
 /* Cell start offsets (nx*ny + 1 entries) of the last sort. */
 int dsmc_get_cell_starts(dsmc_ctx *ctx, int case_index, int32_t *host_out);
 
+/* Population edits between steps (ctx idle: after InitialConditions or a
+ * completed step; DSMC_ERR_STATE otherwise), for the reference-named
+ * GenerateNewParticles and RemoveParticlesInsideBox of callers that build
+ * their own inflow or initial state.  Both remove with the reference's
+ * swap-with-last loop and then re-sort by cell, as the reference's next
+ * Indexing would order the particles; NP changes accordingly.
+ *
+ * GenerateNewParticles' particles (Boundary.cpp:60-92) joining the case:
+ * n FP64 particles in device arrays are appended after its NP particles;
+ * those outside [X1, X2] x [Y1, Y2] are removed as BoundaryConditions'
+ * removal (Boundary.cpp:181-202) would remove them.  DSMC_ERR_CAPACITY when
+ * NP + n exceeds the case's slots. */
+int dsmc_append_particles_device(dsmc_ctx *ctx, int case_index, const double *x,
+                                 const double *y, const double *vx, const double *vy,
+                                 const double *vz, int64_t n);
+/* RemoveParticlesInsideBox (Geometry.cpp:231-247). */
+int dsmc_remove_inside_box(dsmc_ctx *ctx, int case_index);
+/* BinaryCollisionsInCell(CellVolume, NPC, IPC) (Collision.cpp:21-44) on the
+ * particles of case case_index at slots ipc[0, n) (host array of slot
+ * indices into the current cell-sorted population, as dsmc_download_particles
+ * orders it); draws from stream (kind, step, entity).  Valid between steps
+ * and after the step's Indexing; *n_collisions receives NC. */
+int dsmc_collide_list(dsmc_ctx *ctx, int case_index, double cell_volume, int32_t n,
+                      const int32_t *ipc, uint32_t kind, uint32_t step, uint32_t entity,
+                      int32_t *n_collisions);
+
 /* Checkpoint of every case of an idle context (between steps) in one file:
  * the run counters, the particles in slot order and the sampled moments.
  * The reference has none (its RunSimulation cannot resume).  Loading it
@@ -350,6 +376,40 @@ int dsmc_k_inside_box(const dsmc_params *p, int64_t n, const double *x, const do
 int dsmc_k_scatter(const dsmc_params *p, const dsmc_derived *d, int64_t n, double *v,
                    const double *nx, const double *ny, uint32_t kind, uint32_t step,
                    const uint32_t *entity, void *cuda_stream);
+
+/* GenerateNewParticles(X1, Y1, X2, Y2, Ngas, Ugasx, Ugasy, Tgas, MoveFlag)
+ * (Boundary.cpp:60-92) on the rectangle rect = {X1, Y1, X2, Y2} (host
+ * array), drawing from stream (kind, step, entity): the count (floor plus a
+ * Bernoulli draw when the mean Ngas V / Weight exceeds 20, else a Poisson
+ * draw), then per particle a uniform position and a Maxwellian velocity
+ * around (Ugasx, Ugasy, 0) at Tgas, pre-moved by Dt when move_flag is 1.
+ * The count is returned in *n_out (host; the call waits for it on the
+ * stream); the particles are written to the device arrays x .. vz, which
+ * hold `capacity` elements: DSMC_ERR_CAPACITY (nothing written) when the
+ * count exceeds it.  d, when given, replaces the derived constants (Weight,
+ * MoleculeMass, Dt come from p otherwise). */
+int dsmc_k_inject(const dsmc_params *p, const dsmc_derived *d, const double *rect, double n_gas,
+                  double ux_gas, double uy_gas, double t_gas, int move_flag, uint32_t kind,
+                  uint32_t step, uint32_t entity, int64_t capacity, double *x, double *y,
+                  double *vx, double *vy, double *vz, int64_t *n_out, void *cuda_stream);
+
+/* BinaryCollisionsInCell(CellVolume, NPC, IPC) (Collision.cpp:21-44) for
+ * n_lists independent lists: list l is IPC = ipc[list_start[l],
+ * list_start[l + 1]) (indices into vx, vy, vz), or the particles
+ * list_start[l] .. list_start[l + 1] - 1 themselves when ipc is NULL; it
+ * draws from stream (kind, step, entity[l]) (entity NULL: l) and its NC is
+ * written to n_collisions[l] (may be NULL).  Lists must not share particles.
+ * All pointers are device pointers. */
+int dsmc_k_collide(const dsmc_params *p, const dsmc_derived *d, double cell_volume,
+                   int32_t n_lists, const int32_t *list_start, const int32_t *ipc, double *vx,
+                   double *vy, double *vz, uint32_t kind, uint32_t step, const uint32_t *entity,
+                   int32_t *n_collisions, void *cuda_stream);
+
+/* ElasticCollision(V1, V2, Cr) (Collision.cpp:7-19) per pair i: v1, v2 are
+ * 3*n doubles updated in place, cr[i] the relative speed; pair i draws from
+ * stream (kind, step, entity[i]) (entity NULL: i). */
+int dsmc_k_elastic(const dsmc_params *p, int64_t n, double *v1, double *v2, const double *cr,
+                   uint32_t kind, uint32_t step, const uint32_t *entity, void *cuda_stream);
 
 #ifdef __cplusplus
 }

@@ -34,6 +34,12 @@ void CLLScattering(double *v, double m, double wallTemperature, double Nx, doubl
                    double normalAccommodation, double tangentialAccommodation);
 void MoveParticles();
 void BoundaryConditions();
+// Particles joining the case (Boundary.cpp:60-92).  Between steps or after
+// Indexing(): drawn on the device from the user stream, those outside
+// [X1, X2] x [Y1, Y2] dropped as BoundaryConditions() drops them, the rest
+// sorted by cell with the population (NP grows).
+void GenerateNewParticles(double X1, double Y1, double X2, double Y2, double Ngas, double Ugasx,
+                          double Ugasy, double Tgas, int MoveFlag);
 
 // include/Geometry.h
 extern double X1, X2;
@@ -47,6 +53,9 @@ extern double DV;
 void SetupGeometry();
 void Indexing();
 bool InsideBox(double x, double y);
+// Geometry.cpp:231-247, with the swap-with-last order; between steps or
+// after Indexing(), then the population is sorted by cell again.
+void RemoveParticlesInsideBox();
 bool IntersectBox(double x, double y, double dx, double dy, double &tHit, double &normalX,
                   double &normalY);
 
@@ -55,6 +64,12 @@ void Setup();
 void InitialConditions();
 
 // include/Collision.h
+// Collision.cpp:7-19, drawing from the user stream.
+void ElasticCollision(double *V1, double *V2, double Cr);
+// Collision.cpp:21-44 on the particles whose slots IPC lists (indices into
+// the cell-sorted population, as dsmc_download_particles orders it), drawing
+// from the user stream; returns NC.
+int BinaryCollisionsInCell(double CellVolume, int NPC, int *IPC);
 int CollideParticles();
 
 // include/Sampling.h
@@ -128,7 +143,9 @@ class Error : public std::runtime_error {
 extern int Precision;            // DSMC_FP64 (default) or DSMC_FP32
 extern std::string ResultsDirectory; // Printing() writes <dir>/<wall>/ ("results")
 
-// The device context behind the surface (null before Setup()).
+// The device context behind the surface (null before Setup()), and the
+// parameters the last Setup() gave it.
 dsmc_ctx *Context();
+const dsmc_params &Parameters();
 
 } // namespace dsmc

@@ -100,6 +100,13 @@ class OracleEngine(_Base):
             L.dsmc_oracle_inside_box.argtypes = [C.c_void_p, C.c_double, C.c_double]
             L.dsmc_oracle_scatter.argtypes = [C.c_void_p, _D, C.c_double, C.c_double,
                                               C.c_uint32, C.c_uint32, C.c_uint32]
+            L.dsmc_oracle_generate.argtypes = [C.c_void_p, _D] + [C.c_double] * 4 + \
+                [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32]
+            L.dsmc_oracle_collide_list.argtypes = [C.c_void_p, C.c_double, C.c_int, _I32,
+                                                   C.c_uint32, C.c_uint32, C.c_uint32,
+                                                   C.POINTER(C.c_int)]
+            L.dsmc_oracle_elastic.argtypes = [C.c_void_p, _D, _D, C.c_double, C.c_uint32,
+                                              C.c_uint32, C.c_uint32]
             cls._lib = L
         return cls._lib
 
@@ -162,6 +169,30 @@ class OracleEngine(_Base):
         s = self.lib().dsmc_oracle_scatter(C.c_void_p(self.h), _dptr(vv), nx, ny, kind, step,
                                            entity)
         return s, vv
+
+    def generate(self, rect, n_gas, ux, uy, t_gas, move_flag, kind, step, entity) -> int:
+        r = np.ascontiguousarray(rect, dtype=np.float64)
+        return self.lib().dsmc_oracle_generate(C.c_void_p(self.h), _dptr(r), n_gas, ux, uy,
+                                               t_gas, move_flag, kind, step, entity)
+
+    def collide_list(self, cell_volume, ipc, kind, step, entity) -> int:
+        ids = np.ascontiguousarray(ipc, dtype=np.int32)
+        nc = C.c_int()
+        self._call("collide_list", C.c_double(cell_volume), len(ids), ids.ctypes.data_as(_I32),
+                   kind, step, entity, C.byref(nc))
+        return nc.value
+
+    def elastic(self, v1, v2, cr, kind, step, entity):
+        a = np.ascontiguousarray(v1, dtype=np.float64).copy()
+        b = np.ascontiguousarray(v2, dtype=np.float64).copy()
+        self._call("elastic", _dptr(a), _dptr(b), C.c_double(cr), kind, step, entity)
+        return a, b
+
+    def remove_inside_box(self):
+        self._call("remove_inside_box")
+
+    def remove_outside_domain(self):
+        self._call("remove_outside_domain")
 
 
 class RefEngine(_Base):
@@ -252,6 +283,33 @@ class RefEngine(_Base):
         vv = np.ascontiguousarray(v, dtype=np.float64).copy()
         s = self.lib().dsmc_ref_cll(_dptr(vv), m, tw, nx, ny, an, at)
         return s, vv
+
+    def generate(self, rect, n_gas, ux, uy, t_gas, move_flag, kind, step, entity) -> int:
+        r = np.ascontiguousarray(rect, dtype=np.float64)
+        L = self.lib()
+        L.dsmc_ref_generate.argtypes = [_D] + [C.c_double] * 4 + [C.c_int] + [C.c_uint32] * 3
+        return L.dsmc_ref_generate(_dptr(r), n_gas, ux, uy, t_gas, move_flag, kind, step, entity)
+
+    def collide_list(self, cell_volume, ipc, kind, step, entity) -> int:
+        ids = np.ascontiguousarray(ipc, dtype=np.int32)
+        nc = C.c_int()
+        L = self.lib()
+        L.dsmc_ref_collide_list.argtypes = [C.c_double, C.c_int, _I32] + [C.c_uint32] * 3 + \
+            [C.POINTER(C.c_int)]
+        self._call("collide_list", cell_volume, len(ids), ids.ctypes.data_as(_I32), kind, step,
+                   entity, C.byref(nc))
+        return nc.value
+
+    def elastic(self, v1, v2, cr, kind, step, entity):
+        a = np.ascontiguousarray(v1, dtype=np.float64).copy()
+        b = np.ascontiguousarray(v2, dtype=np.float64).copy()
+        L = self.lib()
+        L.dsmc_ref_elastic.argtypes = [_D, _D, C.c_double] + [C.c_uint32] * 3
+        self._call("elastic", _dptr(a), _dptr(b), cr, kind, step, entity)
+        return a, b
+
+    def remove_inside_box(self):
+        self._call("remove_inside_box")
 
     def write_field(self, directory: str | os.PathLike):
         self._call("write_field", str(directory).encode())

@@ -8,6 +8,7 @@
  */
 #include "dsmc_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -297,10 +298,11 @@ static int move_one(dsmc_oracle *o, int64_t i)
 
 /* GenerateNewParticles, src/Boundary.cpp:60-92, with v2rand_uniform_rect
  * (:44-47) inlined.  Draws come from the stream selected by the caller. */
-static int generate(dsmc_oracle *o, double gx1, double gy1, double gx2, double gy2, int move_flag)
+static int generate_gas(dsmc_oracle *o, double gx1, double gy1, double gx2, double gy2,
+                        double n_gas, double ux_gas, double uy_gas, double t_gas, int move_flag)
 {
     const double v = (gx2 - gx1) * (gy2 - gy1) * o->p.dz;
-    const double n_avg = o->p.n_free * v / o->d.weight;
+    const double n_avg = n_gas * v / o->d.weight;
     int n_new;
     if (n_avg > 20.0) {
         n_new = (int)n_avg;
@@ -311,12 +313,12 @@ static int generate(dsmc_oracle *o, double gx1, double gy1, double gx2, double g
     }
     if (o->np + n_new > o->cap)
         return DSMC_ERR_CAPACITY;
-    const double u_gas[3] = {o->d.ux_free, o->d.uy_free, 0.0};
+    const double u_gas[3] = {ux_gas, uy_gas, 0.0};
     for (int64_t i = o->np; i < o->np + n_new; ++i) {
         o->x[i] = gx1 + (gx2 - gx1) * brng(o);
         o->y[i] = gy1 + (gy2 - gy1) * brng(o);
         double vel[3];
-        vrand_mb(o, vel, o->d.molecule_mass, u_gas, o->p.t_free);
+        vrand_mb(o, vel, o->d.molecule_mass, u_gas, t_gas);
         o->vx[i] = vel[0];
         o->vy[i] = vel[1];
         o->vz[i] = vel[2];
@@ -327,6 +329,13 @@ static int generate(dsmc_oracle *o, double gx1, double gy1, double gx2, double g
     }
     o->np += n_new;
     return DSMC_OK;
+}
+
+/* The freestream form that BoundaryConditions and InitialConditions use. */
+static int generate(dsmc_oracle *o, double gx1, double gy1, double gx2, double gy2, int move_flag)
+{
+    return generate_gas(o, gx1, gy1, gx2, gy2, o->p.n_free, o->d.ux_free, o->d.uy_free,
+                        o->p.t_free, move_flag);
 }
 
 int dsmc_oracle_stage_move(dsmc_oracle *o)
@@ -362,6 +371,13 @@ int dsmc_oracle_stage_boundary(dsmc_oracle *o)
         if (st != DSMC_OK)
             return st;
     }
+    return dsmc_oracle_remove_outside_domain(o);
+}
+
+/* The removal loop of BoundaryConditions, src/Boundary.cpp:181-202. */
+int dsmc_oracle_remove_outside_domain(dsmc_oracle *o)
+{
+    const dsmc_params *p = &o->p;
     for (int64_t i = 0; i < o->np;) {
         if (o->x[i] <= p->x1 || o->x[i] >= p->x2 || o->y[i] <= p->y1 || o->y[i] >= p->y2)
             swap_last(o, i);
@@ -414,31 +430,46 @@ int dsmc_oracle_stage_index(dsmc_oracle *o)
 }
 
 /* ElasticCollision, src/Collision.cpp:7-19 */
-static void elastic(dsmc_oracle *o, int64_t a, int64_t b, double cr)
+static void elastic_v(dsmc_oracle *o, double *v1, double *v2, double cr)
 {
     double n[3];
     v3rand_isotropic(o, n);
     cr *= 0.5;
-    const double vc[3] = {0.5 * (o->vx[b] + o->vx[a]), 0.5 * (o->vy[b] + o->vy[a]),
-                          0.5 * (o->vz[b] + o->vz[a])};
+    const double vc[3] = {0.5 * (v2[0] + v1[0]), 0.5 * (v2[1] + v1[1]), 0.5 * (v2[2] + v1[2])};
     const double vcr[3] = {cr * n[0], cr * n[1], cr * n[2]};
-    o->vx[a] = vc[0] + vcr[0];
-    o->vy[a] = vc[1] + vcr[1];
-    o->vz[a] = vc[2] + vcr[2];
-    o->vx[b] = vc[0] - vcr[0];
-    o->vy[b] = vc[1] - vcr[1];
-    o->vz[b] = vc[2] - vcr[2];
+    v1[0] = vc[0] + vcr[0];
+    v1[1] = vc[1] + vcr[1];
+    v1[2] = vc[2] + vcr[2];
+    v2[0] = vc[0] - vcr[0];
+    v2[1] = vc[1] - vcr[1];
+    v2[2] = vc[2] - vcr[2];
+}
+
+static void elastic(dsmc_oracle *o, int64_t a, int64_t b, double cr)
+{
+    double v1[3] = {o->vx[a], o->vy[a], o->vz[a]};
+    double v2[3] = {o->vx[b], o->vy[b], o->vz[b]};
+    elastic_v(o, v1, v2, cr);
+    o->vx[a] = v1[0];
+    o->vy[a] = v1[1];
+    o->vz[a] = v1[2];
+    o->vx[b] = v2[0];
+    o->vy[b] = v2[1];
+    o->vz[b] = v2[2];
 }
 
 /* BinaryCollisionsInCell, src/Collision.cpp:21-44: NTC with fixed SCMax and
- * VHS acceptance.  The cell's list is the contiguous run [start, start+n). */
-static int collide_cell(dsmc_oracle *o, int64_t start, int n)
+ * VHS acceptance.  The cell's list IPC is ids[0, n) when ids is given, else
+ * the contiguous run [start, start+n); cell_volume is the CellVolume
+ * argument (DV in CollideParticles). */
+static int collide_ids(dsmc_oracle *o, int64_t start, const int32_t *ids, int n,
+                       double cell_volume)
 {
     if (n < 2)
         return 0;
     const double sc_max = 9.0 * o->d.sigma_ref *
                           sqrt(K_BOLTZMANN * o->p.t_free / o->d.molecule_mass);
-    const double npair = 0.5 * n * (n - 1) * o->d.weight * sc_max * o->p.dt / o->d.dv;
+    const double npair = 0.5 * n * (n - 1) * o->d.weight * sc_max * o->p.dt / cell_volume;
     int nn = (int)npair;
     const double frac = npair - nn;
     nn = (brng(o) < frac) ? nn + 1 : nn;
@@ -449,8 +480,8 @@ static int collide_cell(dsmc_oracle *o, int64_t start, int n)
         do {
             j = irand_uniform(o, n);
         } while (j == i);
-        const int64_t a = start + i;
-        const int64_t b = start + j;
+        const int64_t a = ids ? ids[i] : start + i;
+        const int64_t b = ids ? ids[j] : start + j;
         const double vr[3] = {o->vx[b] - o->vx[a], o->vy[b] - o->vy[a], o->vz[b] - o->vz[a]};
         const double cr = sqrt(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
         const double sigma = o->d.sigma_ref * pow(o->d.cr_ref / cr, o->d.omega);
@@ -460,6 +491,11 @@ static int collide_cell(dsmc_oracle *o, int64_t start, int n)
         }
     }
     return nc;
+}
+
+static int collide_cell(dsmc_oracle *o, int64_t start, int n)
+{
+    return collide_ids(o, start, NULL, n, o->d.dv);
 }
 
 /* CollideParticles, src/Collision.cpp:45-56, one stream per cell. */
@@ -555,8 +591,65 @@ int dsmc_oracle_init_cold(dsmc_oracle *o)
 
 /* ---- setup -------------------------------------------------------------- */
 
-/* Setup, src/Initialization.cpp:210-265.  The reference's private Gamma
- * (:111-207) is replaced by the C library's tgamma. */
+/* Gamma(x), x > 0, src/Initialization.cpp:111-207: the reference's private
+ * routine, restated from the published method it follows.  Below 0.001 the
+ * two-term series of 1/Gamma; on [0.001, 12) W. J. Cody's rational
+ * approximation Gamma(1 + z) = 1 + z P(z) / Q(z) on (1, 2) (SPECFUN; the
+ * degree-8 coefficient table as published) with the recurrence outside
+ * (1, 2); from 12 Stirling's series, Abramowitz and Stegun 6.1.41.  The
+ * operation order is the reference's, so the result has its bits. */
+static double gamma_fn(double x)
+{
+    static const double P[8] = {-1.71618513886549492533811E+0, 2.47656508055759199108314E+1,
+                                -3.79804256470945635097577E+2, 6.29331155312818442661052E+2,
+                                8.66966202790413211295064E+2, -3.14512729688483675254357E+4,
+                                -3.61444134186911729807069E+4, 6.64561438202405440627855E+4};
+    static const double Q[8] = {-3.08402300119738975254353E+1, 3.15350626979604161529144E+2,
+                                -1.01515636749021914166146E+3, -3.10777167157231109440444E+3,
+                                2.25381184209801510330112E+4, 4.75584627752788110767815E+3,
+                                -1.34659959864969306392456E+5, -1.15132259675553483497211E+5};
+    static const double B[8] = {1.0 / 12.0, -1.0 / 360.0, 1.0 / 1260.0, -1.0 / 1680.0,
+                                1.0 / 1188.0, -691.0 / 360360.0, 1.0 / 156.0,
+                                -3617.0 / 122400.0};
+    if (x < 0.001)
+        return 1.0 / (x * (1.0 + 0.577215664901532860606512090 * x));
+    if (x < 12.0) {
+        double y = x, num = 0.0, den = 1.0, r;
+        int n = 0, i;
+        const int small = y < 1.0;
+        if (small)
+            y += 1.0;
+        else {
+            n = (int)floor(y) - 1;
+            y -= n;
+        }
+        for (i = 0; i < 8; ++i) {
+            num = (num + P[i]) * (y - 1);
+            den = den * (y - 1) + Q[i];
+        }
+        r = num / den + 1.0;
+        if (small)
+            r /= (y - 1.0);
+        else
+            for (i = 0; i < n; ++i)
+                r *= y++;
+        return r;
+    }
+    if (x > 171.624)
+        return DBL_MAX * 2.0;
+    {
+        const double z = 1.0 / (x * x);
+        double sum = B[7];
+        int i;
+        for (i = 6; i >= 0; --i) {
+            sum *= z;
+            sum += B[i];
+        }
+        return exp((x - 0.5) * log(x) - x + 0.91893853320467274178032973640562 + sum / x);
+    }
+}
+
+/* Setup, src/Initialization.cpp:210-265, with the reference's Gamma. */
 int dsmc_oracle_setup(const dsmc_params *p, dsmc_derived *d)
 {
     if (p->wall_model == DSMC_WALL_CLL && !cll_valid(p->cll_normal, p->cll_tangential))
@@ -577,10 +670,10 @@ int dsmc_oracle_setup(const dsmc_params *p, dsmc_derived *d)
     d->weight = d->dv * p->n_free / p->npc_free;
     d->sigma_ref = PI_D * p->d_ref * p->d_ref;
     d->omega = 2.0 * p->viscosity_index - 1.0;
-    d->cr_ref = sqrt(4.0 * k * p->t_ref / m) / pow(tgamma(2.5 - p->viscosity_index), 1.0 / d->omega);
+    d->cr_ref = sqrt(4.0 * k * p->t_ref / m) / pow(gamma_fn(2.5 - p->viscosity_index), 1.0 / d->omega);
     const double q = 1.0 - d->omega;
-    const double mean_rel = pow(4.0 * k * p->t_free / m, q / 2.0) * tgamma((q + 3.0) / 2.0) /
-                            tgamma(1.5);
+    const double mean_rel = pow(4.0 * k * p->t_free / m, q / 2.0) * gamma_fn((q + 3.0) / 2.0) /
+                            gamma_fn(1.5);
     const double rate_coeff = d->sigma_ref * pow(d->cr_ref, d->omega) * mean_rel;
     const double freq = p->n_free * rate_coeff;
     d->mft_free = 1.0 / freq;
@@ -736,4 +829,39 @@ int dsmc_oracle_scatter(dsmc_oracle *o, double *v, double nx, double ny, uint32_
 {
     select_stream(o, kind, step, entity);
     return wall_interaction(o, v, nx, ny);
+}
+
+/* ---- unit forms of single routines (parity of the ABI's unit kernels) -- */
+
+/* GenerateNewParticles(X1, Y1, X2, Y2, Ngas, Ugasx, Ugasy, Tgas, MoveFlag),
+ * src/Boundary.cpp:60-92, on stream (kind, step, entity); the particles are
+ * appended to the oracle's (unsorted) array. */
+int dsmc_oracle_generate(dsmc_oracle *o, const double *rect, double n_gas, double ux_gas,
+                         double uy_gas, double t_gas, int move_flag, uint32_t kind, uint32_t step,
+                         uint32_t entity)
+{
+    select_stream(o, kind, step, entity);
+    return generate_gas(o, rect[0], rect[1], rect[2], rect[3], n_gas, ux_gas, uy_gas, t_gas,
+                        move_flag);
+}
+
+/* BinaryCollisionsInCell(CellVolume, NPC, IPC), src/Collision.cpp:21-44, on
+ * stream (kind, step, entity) over the oracle's particles ipc[0, n); returns
+ * the number of collisions in *nc. */
+int dsmc_oracle_collide_list(dsmc_oracle *o, double cell_volume, int n, const int32_t *ipc,
+                             uint32_t kind, uint32_t step, uint32_t entity, int *nc)
+{
+    select_stream(o, kind, step, entity);
+    *nc = collide_ids(o, 0, ipc, n, cell_volume);
+    return DSMC_OK;
+}
+
+/* ElasticCollision(V1, V2, Cr), src/Collision.cpp:7-19, on stream
+ * (kind, step, entity). */
+int dsmc_oracle_elastic(dsmc_oracle *o, double *v1, double *v2, double cr, uint32_t kind,
+                        uint32_t step, uint32_t entity)
+{
+    select_stream(o, kind, step, entity);
+    elastic_v(o, v1, v2, cr);
+    return DSMC_OK;
 }

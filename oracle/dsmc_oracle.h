@@ -37,6 +37,7 @@ void dsmc_oracle_destroy(dsmc_oracle *o);
 
 int dsmc_oracle_init_cold(dsmc_oracle *o);
 int dsmc_oracle_remove_inside_box(dsmc_oracle *o);
+int dsmc_oracle_remove_outside_domain(dsmc_oracle *o);
 int dsmc_oracle_stage_move(dsmc_oracle *o);
 int dsmc_oracle_stage_boundary(dsmc_oracle *o);
 int dsmc_oracle_stage_index(dsmc_oracle *o);
@@ -62,6 +63,13 @@ int dsmc_oracle_intersect(dsmc_oracle *o, double x, double y, double dx, double 
                           double *nx, double *ny);
 int dsmc_oracle_inside_box(dsmc_oracle *o, double x, double y);
 int dsmc_oracle_scatter(dsmc_oracle *o, double *v, double nx, double ny, uint32_t kind,
+                        uint32_t step, uint32_t entity);
+int dsmc_oracle_generate(dsmc_oracle *o, const double *rect, double n_gas, double ux_gas,
+                         double uy_gas, double t_gas, int move_flag, uint32_t kind, uint32_t step,
+                         uint32_t entity);
+int dsmc_oracle_collide_list(dsmc_oracle *o, double cell_volume, int n, const int32_t *ipc,
+                             uint32_t kind, uint32_t step, uint32_t entity, int *nc);
+int dsmc_oracle_elastic(dsmc_oracle *o, double *v1, double *v2, double cr, uint32_t kind,
                         uint32_t step, uint32_t entity);
 
 #ifdef __cplusplus

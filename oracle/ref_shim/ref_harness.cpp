@@ -450,4 +450,45 @@ double dsmc_ref_gaussian(double e, double v) { return frand_Gaussian(e, v); }
 
 int dsmc_ref_poisson(double e) { return irand_Poisson(e); }
 
+// The reference's GenerateNewParticles (src/Boundary.cpp:60-92) on stream
+// (kind, step, entity): appends to P, NP grows.
+int dsmc_ref_generate(const double *rect, double n_gas, double ux, double uy, double t_gas,
+                      int move_flag, std::uint32_t kind, std::uint32_t step, std::uint32_t entity)
+{
+    return guarded([&] {
+        dsmc_ref_rng_select(kind, step, entity);
+        GenerateNewParticles(rect[0], rect[1], rect[2], rect[3], n_gas, ux, uy, t_gas, move_flag);
+    });
+}
+
+// The reference's BinaryCollisionsInCell (src/Collision.cpp:21-44) over P on
+// stream (kind, step, entity); the list is copied since the routine takes it
+// as int *.
+int dsmc_ref_collide_list(double cell_volume, int n, const int *ipc, std::uint32_t kind,
+                          std::uint32_t step, std::uint32_t entity, int *nc)
+{
+    return guarded([&] {
+        dsmc_ref_rng_select(kind, step, entity);
+        std::vector<int> ids(ipc, ipc + n);
+        *nc = BinaryCollisionsInCell(cell_volume, n, ids.data());
+    });
+}
+
+// The reference's ElasticCollision (src/Collision.cpp:7-19).
+int dsmc_ref_elastic(double *v1, double *v2, double cr, std::uint32_t kind, std::uint32_t step,
+                     std::uint32_t entity)
+{
+    return guarded([&] {
+        dsmc_ref_rng_select(kind, step, entity);
+        ElasticCollision(v1, v2, cr);
+    });
+}
+
+// The reference's RemoveParticlesInsideBox (src/Geometry.cpp:231-247) on P as
+// it stands (no sort).
+int dsmc_ref_remove_inside_box()
+{
+    return guarded([] { RemoveParticlesInsideBox(); });
+}
+
 } // extern "C"

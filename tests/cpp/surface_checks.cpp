@@ -1,10 +1,14 @@
 // Drives the engine only through the reference's C++ names
 // (include/dsmc_reference_api.h), as code written for the reference would:
 // geometry predicates, wall models, the CLL coefficient rule, the stage loop
-// of src/Simulation.cpp:138-199, the field gather and Printing().
+// of src/Simulation.cpp:138-199, the field gather and Printing(), and the
+// single routines GenerateNewParticles, RemoveParticlesInsideBox,
+// BinaryCollisionsInCell and ElasticCollision checked against the CPU oracle
+// (oracle/dsmc_oracle.h, test infrastructure) on the same streams.
 // Exit status 0 when every check holds.  Built and run by
 // tests/test_gpu_surface.py.
 #include <cmath>
+#include <cstring>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -12,7 +16,10 @@
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
+#include "dsmc_oracle.h"
+#include "dsmc_philox.h"
 #include "dsmc_reference_api.h"
 
 namespace {
@@ -23,6 +30,60 @@ void expect(bool ok, const char *what)
         std::cerr << "FAILED: " << what << '\n';
         ++failures;
     }
+}
+
+// Units in the last place between two doubles.
+long long ulps(double a, double b)
+{
+    long long ia, ib;
+    std::memcpy(&ia, &a, 8);
+    std::memcpy(&ib, &b, 8);
+    if (ia < 0)
+        ia = static_cast<long long>(0x8000000000000000ull) - ia;
+    if (ib < 0)
+        ib = static_cast<long long>(0x8000000000000000ull) - ib;
+    return ia > ib ? ia - ib : ib - ia;
+}
+
+struct State {
+    std::vector<double> a[5];
+    size_t size() const { return a[0].size(); }
+};
+
+State engine_state()
+{
+    State s;
+    dsmc_counters c;
+    dsmc_get_counters(dsmc::Context(), 0, &c);
+    for (auto &v : s.a)
+        v.resize(static_cast<size_t>(c.np));
+    int64_t n = 0;
+    dsmc_download_particles(dsmc::Context(), 0, s.a[0].data(), s.a[1].data(), s.a[2].data(),
+                            s.a[3].data(), s.a[4].data(), c.np, &n);
+    return s;
+}
+
+State oracle_state(dsmc_oracle *o)
+{
+    State s;
+    for (auto &v : s.a)
+        v.resize(static_cast<size_t>(dsmc_oracle_np(o)));
+    dsmc_oracle_get_particles(o, s.a[0].data(), s.a[1].data(), s.a[2].data(), s.a[3].data(),
+                              s.a[4].data());
+    return s;
+}
+
+// Positions within pos_ulp, velocities within vel_ulp (the transcendental
+// functions of the device and the host differ in their last bits).
+bool same_state(const State &g, const State &o, long long pos_ulp, long long vel_ulp)
+{
+    if (g.size() != o.size())
+        return false;
+    for (int k = 0; k < 5; ++k)
+        for (size_t i = 0; i < g.size(); ++i)
+            if (ulps(g.a[k][i], o.a[k][i]) > (k < 2 ? pos_ulp : vel_ulp))
+                return false;
+    return true;
 }
 } // namespace
 
@@ -117,6 +178,71 @@ int main(int argc, char **argv)
     std::getline(plt, header);
     expect(header == "VARIABLES = \"X\" \"Y\" \"N\" \"Ux\" \"Uy\" \"Tx\" \"Ty\" \"T\"",
            "field header");
+
+    // The single routines of the reference headers, against the oracle with
+    // the same streams: the user stream (kind 5) keyed by the seed, one step
+    // number per call, counted from SetSeed.
+    {
+        dsmc_oracle *o = dsmc_oracle_create(&dsmc::Parameters(), nullptr, 0);
+        State g0 = engine_state();
+        dsmc_oracle_set_particles_raw(o, g0.a[0].data(), g0.a[1].data(), g0.a[2].data(),
+                                      g0.a[3].data(), g0.a[4].data(),
+                                      static_cast<int64_t>(g0.size()));
+        SetSeed(7, 11); // the user-stream call counter starts again at 0
+        const double strip[4] = {X1 - 0.7, -6.0, X1 + 1.5, 6.0}; // partly outside the domain
+        GenerateNewParticles(strip[0], strip[1], strip[2], strip[3], 3 * NFree, UxFree, UyFree,
+                             400.0, 1);
+        dsmc_oracle_generate(o, strip, 3 * NFree, UxFree, UyFree, 400.0, 1, DSMC_RNG_USER, 0, 0);
+        dsmc_oracle_remove_outside_domain(o);
+        dsmc_oracle_stage_index(o);
+        const State g1 = engine_state(), o1 = oracle_state(o);
+        expect(g1.size() > g0.size() && static_cast<int64_t>(g1.size()) == NP,
+               "GenerateNewParticles adds particles");
+        expect(same_state(g1, o1, 1, 8), "GenerateNewParticles matches the oracle");
+
+        const double cover[4] = {BoxX - 2.0, BoxY - 3.0, BoxX + 2.0, BoxY + 3.0}; // the box
+        GenerateNewParticles(cover[0], cover[1], cover[2], cover[3], NFree, 0.0, 0.0, TFree, 0);
+        dsmc_oracle_generate(o, cover, NFree, 0.0, 0.0, TFree, 0, DSMC_RNG_USER, 1, 0);
+        dsmc_oracle_remove_outside_domain(o);
+        dsmc_oracle_stage_index(o);
+        const int with_box = NP;
+        RemoveParticlesInsideBox();
+        dsmc_oracle_remove_inside_box(o);
+        dsmc_oracle_stage_index(o);
+        expect(NP < with_box && NP == dsmc_oracle_np(o), "RemoveParticlesInsideBox count");
+        expect(same_state(engine_state(), oracle_state(o), 1, 8),
+               "RemoveParticlesInsideBox matches the oracle");
+
+        // The densest cell's list, collided in a volume small enough for many pairs.
+        std::vector<int32_t> starts(static_cast<size_t>(NX) * NY + 1);
+        dsmc_get_cell_starts(dsmc::Context(), 0, starts.data());
+        size_t best = 0;
+        for (size_t k = 0; k + 1 < starts.size(); ++k)
+            if (starts[k + 1] - starts[k] > starts[best + 1] - starts[best])
+                best = k;
+        std::vector<int> ipc;
+        for (int32_t q = starts[best + 1] - 1; q >= starts[best]; --q)
+            ipc.push_back(q);
+        const int nc = BinaryCollisionsInCell(DV * 1e-3, static_cast<int>(ipc.size()), ipc.data());
+        int onc = 0;
+        std::vector<int32_t> ids(ipc.begin(), ipc.end());
+        dsmc_oracle_collide_list(o, DV * 1e-3, static_cast<int>(ids.size()), ids.data(),
+                                 DSMC_RNG_USER, 2, 0, &onc);
+        expect(nc > 0 && nc == onc, "BinaryCollisionsInCell pairs");
+        expect(same_state(engine_state(), oracle_state(o), 1, 8),
+               "BinaryCollisionsInCell matches the oracle");
+
+        double v1[3] = {310.0, -45.0, 12.0}, v2[3] = {-150.0, 220.0, -80.0};
+        double w1[3] = {310.0, -45.0, 12.0}, w2[3] = {-150.0, 220.0, -80.0};
+        const double cr = std::sqrt(460.0 * 460.0 + 265.0 * 265.0 + 92.0 * 92.0);
+        ElasticCollision(v1, v2, cr);
+        dsmc_oracle_elastic(o, w1, w2, cr, DSMC_RNG_USER, 3, 0);
+        bool same = true;
+        for (int k = 0; k < 3; ++k)
+            same = same && ulps(v1[k], w1[k]) <= 8 && ulps(v2[k], w2[k]) <= 8;
+        expect(same, "ElasticCollision matches the oracle");
+        dsmc_oracle_destroy(o);
+    }
 
     // RunSimulation's argument handling.
     char prog[] = "dsmc", help[] = "--help", bad[] = "--bogus", aoa[] = "--aoa",

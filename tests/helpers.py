@@ -40,3 +40,27 @@ def assert_close(a: np.ndarray, b: np.ndarray, rtol: float, atol: float, what: s
 def assert_state_close(gpu: dict, ref: dict, what: str, rtol: float = 1e-11):
     for k, atol in (("x", 1e-9), ("y", 1e-9), ("vx", 1e-7), ("vy", 1e-7), ("vz", 1e-7)):
         assert_close(gpu[k], ref[k], rtol, atol, f"{what} {k}")
+
+
+def ulp_distance(a, b) -> np.ndarray:
+    """Distance in units in the last place between FP64 arrays: the number
+    of representable doubles between a and b (0 when bit-identical; +0 and
+    -0 are 0 apart)."""
+    def ordered(x):
+        i = np.ascontiguousarray(x, dtype=np.float64).view(np.int64)
+        return np.where(i < 0, np.int64(-0x8000000000000000) - i, i)
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    assert a.shape == b.shape, f"shape {a.shape} != {b.shape}"
+    return np.abs(ordered(a) - ordered(b))
+
+
+def assert_ulp(gpu, ref, max_ulp: int, what: str):
+    """Every element within max_ulp units in the last place (0: bit-exact)."""
+    u = ulp_distance(gpu, ref)
+    if u.size and u.max() > max_ulp:
+        i = int(np.argmax(u))
+        raise AssertionError(f"{what}: {int((u > max_ulp).sum())} of {u.size} beyond {max_ulp} ulp;"
+                             f" worst {int(u.max())} ulp at {i}: {np.ravel(gpu)[i]!r} vs "
+                             f"{np.ravel(ref)[i]!r}")
+    return int(u.max()) if u.size else 0

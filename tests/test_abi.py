@@ -15,7 +15,7 @@ from dsmc_erlend_b200 import _lib
 from dsmc_erlend_b200.abi import (WALL_CLL, WALL_DIFFUSE, WALL_SPECULAR, Derived, Params,
                                   default_params)
 from dsmc_erlend_b200.engine import setup, write_field
-from oracle.cpu import OracleEngine
+from oracle.cpu import OracleEngine, RefEngine, ref_available
 
 ROOT = Path(__file__).resolve().parent.parent
 GOLDEN = ROOT / "tests" / "golden"
@@ -69,6 +69,51 @@ def test_setup_matches_oracle(engine_lib, kw):
     s, od = OracleEngine.setup(p)
     assert s == 0
     assert d.as_dict() == od.as_dict()
+
+
+def test_setup_bits_equal_reference_golden(engine_lib):
+    """dsmc_setup restates the reference's Gamma (src/Initialization.cpp:111-207),
+    so every derived constant (CrRef, MFT, MFP, Kn included) has the bits the
+    reference's own Setup gave for the golden cases."""
+    import json
+    from pathlib import Path
+
+    g = json.loads((Path(__file__).resolve().parent / "golden" /
+                    "reference_steps.json").read_text())
+    for wall, case in g["cases"].items():
+        p = Params()
+        for k, v in case["params"].items():
+            setattr(p, k, v)
+        d = setup(p).as_dict()
+        for k, v in case["derived"].items():
+            assert d[k] == v, f"{wall}: {k} {d[k]!r} != {v!r}"
+
+
+SETUP_CASES = [
+    {},  # the reference's own settings
+    {"wall_model": WALL_SPECULAR, "n_step": 4000, "first_sampling_step": 2000},  # plain case
+    {"nx": 1000, "ny": 1000, "npc_free": 20.0, "attack_angle": 10.0, "dt": 1e-6,
+     "wall_model": WALL_DIFFUSE},  # the large single instance
+    {"nx": 512, "ny": 512, "ma_free": 6.0, "n_free": 3e17, "attack_angle": 15.0,
+     "cll_normal": 0.5, "cll_tangential": 0.9, "box_width": 3.0, "box_height": 5.0,
+     "npc_free": 30.0},  # warm-versus-cold case
+    {"viscosity_index": 0.5, "t_ref": 300.0, "d_ref": 3.6e-10, "molar_mass": 0.028},
+    {"viscosity_index": 1.0, "ma_free": 2.0, "attack_angle": -30.0},
+]
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built (make -C oracle ref)")
+@pytest.mark.parametrize("kw", SETUP_CASES)
+def test_setup_bits_equal_reference_setup(engine_lib, kw):
+    """Live: the reference's own Setup(), compiled here, against dsmc_setup
+    (grids above the reference's 200 x 200 capacity are cut to it)."""
+    p = default_params().copy(**kw)
+    p.nx, p.ny = min(p.nx, 200), min(p.ny, 200)
+    want = RefEngine(p).derived().as_dict()
+    got = setup(p).as_dict()
+    assert got == want
+    s, od = OracleEngine.setup(p)
+    assert s == 0 and od.as_dict() == want
 
 
 def test_setup_rejects_bad_cll(engine_lib):

@@ -126,9 +126,11 @@ def test_wall_scatter_matches_oracle(cuda, engine_lib, wall):
 
 
 def _pair(p, **kw):
-    d = setup(p)
-    g = Engine(p, derived=[d])
-    o = OracleEngine(p, d)
+    """The engine and the oracle, each with the constants of its own Setup
+    (both restate the reference's, Gamma included, bit for bit)."""
+    g = Engine(p)
+    o = OracleEngine(p)
+    assert g.derived[0].as_dict() == OracleEngine.setup(p)[1].as_dict()
     return g, o
 
 
@@ -229,7 +231,7 @@ def test_fp32_state_keeps_the_sort_invariant(cuda, engine_lib, wall):
 
     p = small_case(WALLS[wall], seed=61, precision=FP32, nx=64, ny=48, npc_free=12.0)
     d = setup(p)
-    g = Engine(p, derived=[d])
+    g = Engine(p)
     g.InitialConditions()
     for s in range(25):
         if s:

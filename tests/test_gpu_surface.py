@@ -14,10 +14,14 @@ pytestmark = pytest.mark.gpu
 
 def test_reference_style_program(cuda, engine_lib, tmp_path):
     exe = tmp_path / "surface_checks"
+    from oracle.cpu import build_oracle
+
+    olib = build_oracle().parent  # the checker: the C restatement of the reference
     subprocess.run(["g++", "-std=c++17", "-O1", "-I", str(ROOT / "include"),
-                    "-I", "/usr/local/cuda/include",
+                    "-I", str(ROOT / "oracle"), "-I", "/usr/local/cuda/include",
                     str(ROOT / "tests" / "cpp" / "surface_checks.cpp"), "-o", str(exe),
-                    "-L", str(LIB_DIR), "-ldsmc_b200", f"-Wl,-rpath,{LIB_DIR}"], check=True)
+                    "-L", str(LIB_DIR), "-ldsmc_b200", f"-Wl,-rpath,{LIB_DIR}",
+                    "-L", str(olib), "-ldsmc_oracle", f"-Wl,-rpath,{olib}"], check=True)
     r = subprocess.run([str(exe), str(tmp_path / "results")], capture_output=True, text=True,
                        timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
@@ -30,6 +34,8 @@ def test_command_line(cuda, engine_lib, tmp_path):
     assert r.returncode == 0 and "--angle-of-attack" in r.stdout
     r = subprocess.run([str(CLI), "--aoa", "abc"], capture_output=True, text=True)
     assert r.returncode == 2 and "Invalid angle" in r.stderr
+    r = subprocess.run([str(CLI), "--aoa"], capture_output=True, text=True)  # Simulation.cpp:44
+    assert r.returncode == 2 and r.stderr == "--aoa requires an angle in degrees.\n"
     r = subprocess.run([str(CLI), "--aoa", "10", "--wall", "diffuse", "--nx", "50", "--ny", "50",
                         "--steps", "300", "--first-sampling-step", "100", "--results",
                         str(tmp_path)], capture_output=True, text=True, timeout=600)

@@ -281,3 +281,77 @@ def test_gaussian_draw_order_of_reference_compiler():
     L.dsmc_ref_select_stream(7, 1, 2)
     u1, u2 = L.dsmc_ref_brng(), L.dsmc_ref_brng()
     assert g == math.sqrt(-2.0 * 1.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+
+# -- single routines of the reference headers, live ----------------------------
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built (make -C oracle ref)")
+@pytest.mark.parametrize("n_gas,move", [(1e17, 1), (3e15, 0), (2e18, 1)])
+def test_generate_matches_reference(n_gas, move):
+    """GenerateNewParticles(X1, Y1, X2, Y2, Ngas, Ugasx, Ugasy, Tgas, MoveFlag)
+    (src/Boundary.cpp:60-92) with non-freestream gas: same count, same bits."""
+    p = small_case(WALL_DIFFUSE, seed=41)
+    ref = RefEngine(p)
+    o = OracleEngine(p, ref.derived())
+    ref.set_particles({k: np.zeros(0) for k in ("x", "y", "vx", "vy", "vz")}, raw=True)
+    o.set_particles({k: np.zeros(0) for k in ("x", "y", "vx", "vy", "vz")}, raw=True)
+    rect = (-3.0, 1.0, 2.5, 4.0)
+    for e in range(3):
+        assert ref.generate(rect, n_gas, 410.0, -120.0, 350.0, move, 2, 9, e) == 0
+        assert o.generate(rect, n_gas, 410.0, -120.0, 350.0, move, 2, 9, e) == 0
+    pr, po = ref.particles(), o.particles()
+    assert len(pr["x"]) == len(po["x"]) > 0
+    for k in pr:
+        assert np.array_equal(pr[k], po[k]), k
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built (make -C oracle ref)")
+def test_collide_list_and_elastic_match_reference():
+    """BinaryCollisionsInCell(CellVolume, NPC, IPC) and ElasticCollision
+    (src/Collision.cpp:7-44) over arbitrary index lists: same pairs, bits."""
+    rng = np.random.default_rng(5)
+    p = small_case(WALL_SPECULAR, seed=2)
+    ref = RefEngine(p)
+    o = OracleEngine(p, ref.derived())
+    n = 400
+    st = {"x": rng.uniform(-10, 10, n), "y": rng.uniform(-10, 10, n),
+          "vx": rng.normal(0, 400, n), "vy": rng.normal(0, 400, n), "vz": rng.normal(0, 400, n)}
+    ref.set_particles(st, raw=True)
+    o.set_particles(st, raw=True)
+    total = 0
+    for e in range(40):
+        ipc = rng.permutation(n)[: rng.integers(2, 60)]
+        vol = 10 ** rng.uniform(-7, -3)  # small volumes: many candidate pairs
+        a = ref.collide_list(vol, ipc, 3, 17, e)
+        b = o.collide_list(vol, ipc, 3, 17, e)
+        assert a == b
+        total += a
+    assert total > 50
+    pr, po = ref.particles(), o.particles()
+    for k in pr:
+        assert np.array_equal(pr[k], po[k]), k
+    v1, v2 = rng.normal(0, 500, 3), rng.normal(0, 500, 3)
+    for e in range(20):
+        ra = ref.elastic(v1, v2, 731.5 + e, 5, 1, e)
+        oa = o.elastic(v1, v2, 731.5 + e, 5, 1, e)
+        assert np.array_equal(ra[0], oa[0]) and np.array_equal(ra[1], oa[1])
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built (make -C oracle ref)")
+def test_remove_inside_box_matches_reference():
+    """RemoveParticlesInsideBox (src/Geometry.cpp:231-247): swap-with-last order."""
+    rng = np.random.default_rng(9)
+    p = small_case(WALL_SPECULAR, seed=2)
+    ref = RefEngine(p)
+    o = OracleEngine(p, ref.derived())
+    n = 3000
+    st = {"x": rng.uniform(-6, 8, n), "y": rng.uniform(-4, 3, n),
+          "vx": rng.normal(0, 400, n), "vy": rng.normal(0, 400, n), "vz": rng.normal(0, 400, n)}
+    ref.set_particles(st, raw=True)
+    o.set_particles(st, raw=True)
+    ref.remove_inside_box()
+    o.remove_inside_box()
+    pr, po = ref.particles(), o.particles()
+    assert 0 < len(pr["x"]) < n
+    for k in pr:
+        assert np.array_equal(pr[k], po[k]), k
