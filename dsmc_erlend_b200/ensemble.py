@@ -52,9 +52,35 @@ def ensemble_cases(n: int = 256, seed: int = 2024, steps: int = 5000,
     return cases
 
 
+def shard(cases: list[Params], rank: int, world: int) -> list[tuple[int, Params]]:
+    """The cases rank `rank` of `world` runs: case i goes to rank i mod world,
+    so uneven cases spread evenly on average and every rank's share is known
+    without communication.  Returns (case index, parameters) pairs in case
+    order.  Cases are independent: the ranks exchange nothing while they run
+    (each case keeps its own Philox key, so its results do not depend on
+    which rank runs it or with which other cases)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of world {world}")
+    return [(i, p) for i, p in enumerate(cases) if i % world == rank]
+
+
+def gather_by_case(local: dict, group=None) -> dict:
+    """Merges {case index: result} dicts of every rank into one on every rank
+    (torch.distributed all_gather_object; for per-case summaries such as
+    counters or small fields, not for bulk data)."""
+    import torch.distributed as dist
+
+    parts = [None] * dist.get_world_size(group)
+    dist.all_gather_object(parts, local, group=group)
+    merged = {}
+    for part in parts:
+        merged.update(part)
+    return dict(sorted(merged.items()))
+
+
 def replicas(p: Params, n: int, seed: int = 1) -> list[Params]:
     """n copies of one case with distinct Philox keys (replica statistics)."""
     return [p.copy(seed=case_key(seed, i)) for i in range(n)]
 
 
-__all__ = ["ensemble_cases", "replicas", "case_key", "FP32", "FP64"]
+__all__ = ["ensemble_cases", "replicas", "case_key", "shard", "gather_by_case", "FP32", "FP64"]

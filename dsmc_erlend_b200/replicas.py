@@ -26,16 +26,20 @@ def reduce_replica_fields(fields: torch.Tensor, sample_step: int, group=None):
     return fields, int(ss.item())
 
 
-def engine_replica_reduce(engine, case: int = 0, group=None) -> int:
+def engine_replica_reduce(engine, case: int = 0, group=None, reduce=None) -> int:
     """All-reduces the moments of one case of a device Engine over NCCL and
     stores the merged moments back in the context.  Returns the merged
-    SampleStep."""
+    SampleStep.  `reduce(fields, sample_step) -> (fields, total)` replaces
+    the all-reduce (default reduce_replica_fields over `group`)."""
     p = engine.params[case]
     buf = torch.empty(p.nx * p.ny * 17, dtype=torch.float64, device="cuda")
     engine.fields_to_device(case, buf.data_ptr())
     torch.cuda.synchronize()
-    _, total = reduce_replica_fields(buf.view(-1, 17), engine.counters(case)["sample_step"],
-                                     group)
+    ss = engine.counters(case)["sample_step"]
+    if reduce is None:
+        _, total = reduce_replica_fields(buf.view(-1, 17), ss, group)
+    else:
+        _, total = reduce(buf.view(-1, 17), ss)
     engine.fields_from_device(case, buf.data_ptr(), total)
     torch.cuda.synchronize()
     return total

@@ -250,16 +250,23 @@ class Surrogate:
         if self.stream is None:
             raise RuntimeError("graph training needs the network's own CUDA stream")
         s = torch.cuda.ExternalStream(self.stream)
-        key = (x.data_ptr(), target.data_ptr(), mask.data_ptr())
+        # The Adam settings are kernel arguments inside the graph: new values
+        # capture a new graph.
+        key = (x.data_ptr(), target.data_ptr(), mask.data_ptr(), float(beta1), float(beta2),
+               float(eps))
         if getattr(self, "_graph_key", None) != key:
             self._hp = torch.zeros(3, device="cuda")
             # Pinned staging of the step's values, four in flight.
             self._hp_ring = [torch.zeros(3).pin_memory() for _ in range(4)]
             self._hp_ev = [None] * 4
             with torch.cuda.stream(s):
-                # Kernel attributes are set on first use, outside the capture.
+                # Kernel attributes, tensor maps and SM counts are set on
+                # first use: run every kernel of the step once outside the
+                # capture (the gradients are overwritten by the captured
+                # step, the weights are not touched).
                 self.forward(x)
-                self.loss_and_grad(target, mask)
+                _, dout = self.loss_and_grad(target, mask)
+                self.backward(dout)
             s.synchronize()
             g = torch.cuda.CUDAGraph()
             L = lib()

@@ -262,10 +262,9 @@ int dsmc_get_counters(dsmc_ctx *ctx, int case_index, dsmc_counters *out);
 int dsmc_get_fields(dsmc_ctx *ctx, int case_index, dsmc_cell *host_out);
 /* dsmc_get_fields without any allocation.  No counterpart in the reference:
  * it exists for callers that cannot allocate device memory at read-out time,
- * for example a thread reading results while another thread captures a CUDA
- * graph in global capture mode (cudaMalloc then fails), an application whose
- * device memory is already reserved by its own pool, or a monitor that must
- * not stall the device (cudaFree synchronizes it).  dsmc_get_fields may stage
+ * for example an application whose device memory is already reserved by its
+ * own pool, or a monitor that must not stall the device (cudaFree
+ * synchronizes it).  dsmc_get_fields may stage
  * the expanded moments in a temporary device buffer; this variant stages them in
  * one static device array of DSMC_FIELDS_NOALLOC_MAX_CELLS cells (8.9 MB,
  * held by every GPU that loads the library until the process exits).

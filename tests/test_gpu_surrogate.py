@@ -316,6 +316,9 @@ def test_graph_train_step_matches_eager(cuda):
     for name in eager.w32:
         a, b = eager.w32[name].cpu().numpy(), graph.w32[name].cpu().numpy()
         assert np.allclose(a, b, rtol=1e-5, atol=1e-7), name
-        assert np.array_equal(eager.wb[name].float().cpu().numpy(),
-                              graph.wb[name].float().cpu().numpy()) or np.allclose(a, b)
+        # The bf16 copies are the FP32 masters rounded: equal, or one bf16
+        # rounding apart where the masters differ in their last bits.
+        wa = eager.wb[name].float().cpu().numpy()
+        wg = graph.wb[name].float().cpu().numpy()
+        assert np.all(np.abs(wa - wg) <= 2.0 ** -8 * np.maximum(np.abs(wa), np.abs(wg))), name
     assert lib().dsmc_sg_check(None) == 0

@@ -19,8 +19,9 @@ import pytest
 from dsmc_erlend_b200.abi import Derived, Params
 from dsmc_erlend_b200.engine import write_field
 from oracle.cpu import OracleEngine
+from oracle.paths import REFERENCE_SOURCES
 
-REFERENCE = Path("/root/reference/postprocessing")
+REFERENCE = REFERENCE_SOURCES / "postprocessing"
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
 

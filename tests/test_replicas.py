@@ -70,3 +70,77 @@ def test_two_replicas_sum_over_gloo(tmp_path):
     assert total == s0 + s1
     np.testing.assert_array_equal(merged, f0 + f1)
     assert not np.array_equal(f0, f1)  # distinct keys, distinct replicas
+
+
+# -- ensemble sharding: case i on rank i mod N, no exchange while running --------
+
+def _ensemble():
+    from dsmc_erlend_b200.ensemble import FP64, ensemble_cases
+
+    cases = ensemble_cases(5, seed=77, steps=8, grid_range=(16, 28), precision=FP64)
+    for p in cases:
+        p.npc_free = min(p.npc_free, 6.0)
+        p.first_sampling_step = 2
+    return cases
+
+
+def _run_case(p):
+    from oracle.cpu import OracleEngine
+
+    o = OracleEngine(p)
+    assert o.init_cold() == 0
+    assert o.step(int(p.n_step)) == 0
+    return o.fields(), o.counters()
+
+
+def _shard_worker(rank, world, port, out):
+    import pickle
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+    import torch.distributed as dist
+
+    from dsmc_erlend_b200.ensemble import gather_by_case, shard
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mine = {i: _run_case(p) for i, p in shard(_ensemble(), rank, world)}
+        assert all(i % world == rank for i in mine)
+        merged = gather_by_case(mine)
+        if rank == 0:
+            with open(out, "wb") as fh:
+                pickle.dump(merged, fh)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_ensemble_equals_single_process(tmp_path):
+    """Two gloo ranks each run their share of an ensemble (the CPU oracle);
+    gathered, every case's moments and counters equal a single process's."""
+    import pickle
+
+    out = str(tmp_path / "merged.pkl")
+    mp.start_processes(_shard_worker, args=(2, _free_port(), out), nprocs=2, join=True,
+                       start_method="spawn")
+    with open(out, "rb") as fh:
+        merged = pickle.load(fh)
+    cases = _ensemble()
+    assert sorted(merged) == list(range(len(cases)))
+    for i, p in enumerate(cases):
+        f, c = _run_case(p)
+        np.testing.assert_array_equal(merged[i][0], f)
+        assert merged[i][1] == c
+
+
+def test_shard_assignment():
+    from dsmc_erlend_b200.ensemble import shard
+
+    cases = list(range(10))
+    parts = [shard(cases, r, 3) for r in range(3)]
+    assert [i for i, _ in parts[0]] == [0, 3, 6, 9]
+    assert sorted(i for part in parts for i, _ in part) == cases
+    with pytest.raises(ValueError):
+        shard(cases, 3, 3)

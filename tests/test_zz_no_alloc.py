@@ -1,6 +1,5 @@
 """dsmc_get_fields_noalloc: the field read-out for callers that cannot
-allocate device memory when they read results (a thread reading while
-another captures a CUDA graph in global mode, an application whose device
+allocate device memory when they read results (an application whose device
 memory is reserved by its own pool, a monitor that must not stall the device
 the way cudaFree does).  It stages the moments in one static device array
 instead of a temporary buffer.
