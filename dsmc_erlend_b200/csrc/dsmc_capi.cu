@@ -247,7 +247,7 @@ template <class T> int enqueue_move(dsmc_ctx *c, int init_mode)
     }
     if (!init_mode) {
         Span sp(c, KID_MOVE);
-        k_move<T><<<grid(c, KID_MOVE), MOVE_THREADS, 0, c->stream>>>(
+        k_move<T><<<grid(c, KID_MOVE), TILE_THREADS, move_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->d_scratch, c->tt, slots<T>(c, c->cur), c->key, c->cells,
             c->tile_in, c->tile_dead, c->obuf, c->near_list, c->ncase, c->d_err);
     }
@@ -331,7 +331,7 @@ template <class T> int enqueue_index(dsmc_ctx *c)
         CK(cudaStreamWaitEvent(c->stream, c->branch_ev[EV_TILE_SCAN], 0));
     {
         Span sp(c, KID_SCATTER);
-        k_scatter<T><<<grid(c, KID_SCATTER), SC_THREADS, 0, c->stream>>>(
+        k_scatter<T><<<grid(c, KID_SCATTER), SC_THREADS, scatter_smem<T>(), c->stream>>>(
             c->d_cases, c->d_state, c->tt, slots<T>(c, side), slots<T>(c, side ^ 1), c->key,
             c->cells, c->tile_prefix, c->ncase, c->d_err);
     }
@@ -567,7 +567,10 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
         c->ctas_max[kid] = std::max(1, occupancy);
         c->ctas[kid] = c->ctas_max[kid];
     };
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_move<T>, MOVE_THREADS, 0));
+    CK(cudaFuncSetAttribute(k_move<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(move_smem<T>())));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_move<T>, TILE_THREADS,
+                                                     move_smem<T>()));
     occ(KID_MOVE, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_inject<T>, TILE_THREADS, 0));
     occ(KID_INJECT, b);
@@ -577,7 +580,10 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
     occ(KID_CELL_SCAN, b);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_holes, TILE_THREADS, 0));
     occ(KID_HOLES, b);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, SC_THREADS, 0));
+    CK(cudaFuncSetAttribute(k_scatter<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(scatter_smem<T>())));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_scatter<T>, SC_THREADS,
+                                                     scatter_smem<T>()));
     occ(KID_SCATTER, b);
     CK(cudaFuncSetAttribute(k_sample<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(sample_smem<T>())));

@@ -284,13 +284,13 @@ struct MoveClass {
 // Removal (Boundary.cpp:183-188) and the new cell of a slot, given its old
 // cell `oc`, whether its new position lies outside the domain (`gone`) and
 // otherwise its new cell `nc` (NO_CELL outside the grid).
-__device__ __forceinline__ MoveClass classify_cells(int32_t cbase, int32_t oc, bool gone,
+__device__ __forceinline__ MoveClass classify_cells(const CaseDev &c, int32_t oc, bool gone,
                                                     int32_t nc, int *err)
 {
     MoveClass m;
     m.dead = m.out = m.in = false;
     m.key = KEY_DEAD;
-    m.ocg = oc < 0 ? NO_CELL : cbase + oc;
+    m.ocg = oc < 0 ? NO_CELL : c.cbase + oc;
     if (gone) {
         m.dead = true;
     } else if (nc < 0) {
@@ -299,10 +299,10 @@ __device__ __forceinline__ MoveClass classify_cells(int32_t cbase, int32_t oc, b
         report_error(err, DSMC_ERR_EXCHANGE);
         m.dead = true;
     } else if (nc == oc) {
-        m.key = static_cast<uint32_t>(cbase + nc) | KEY_IN;
+        m.key = static_cast<uint32_t>(c.cbase + nc) | KEY_IN;
         m.in = true;
     } else {
-        m.key = static_cast<uint32_t>(cbase + nc);
+        m.key = static_cast<uint32_t>(c.cbase + nc);
         m.out = true;
     }
     if (m.dead)
@@ -319,7 +319,7 @@ __device__ __forceinline__ MoveClass classify(const CaseDev &c, double x0, doubl
     const bool gone = outside_domain(c, static_cast<double>(xn), static_cast<double>(yn));
     const int32_t nc = gone ? NO_CELL
                             : cell_of(c, static_cast<double>(xn), static_cast<double>(yn));
-    return classify_cells(c.cbase, oc, gone, nc, err);
+    return classify_cells(c, oc, gone, nc, err);
 }
 
 // Free flight of one slot, without the impact test and with estimated cell
@@ -414,253 +414,248 @@ __device__ __forceinline__ MoveClass move_near_box(const CaseDev &c, int64_t ste
     return m;
 }
 
-// Pipeline depth of k_sample (build-time settings, -DDSMC_SAMPLE_STAGES=...;
-// the defaults were chosen by measurement on B200).
+// Slot mapping of a move tile: iteration k of thread t handles slot
+// tile + k * TILE_THREADS + t, so every load and store of a warp is one
+// contiguous 128-byte (FP32) access, and ranks in slot order come from warp
+// ballots: (iteration, warp) pairs are in slot order.
+constexpr int MOVE_WARPS = TILE_THREADS / 32;
+static_assert(TILE_VEC * MOVE_WARPS == 32, "one warp scans the (iteration, warp) counts");
+
+// Tiles are staged in shared memory by bulk asynchronous copies, MOVE
+// stages deep, so the loads of the next tiles of a CTA are in flight while it
+// moves the current one.  Tiles are dealt to CTAs statically (no tile waits on
+// another, so no ticket order is needed).  k_move moves every slot that
+// free_flight accepts and queues the other few for k_move_near, which runs
+// the exact body; both give the exact body's result for every slot.
+template <class T> struct MoveStage {
+    T v[4][TILE]; // x, y, vx, vy
+};
+// Pipeline depths (build-time settings, -DDSMC_MOVE_STAGES=... etc.; the
+// defaults were chosen by measurement on B200).
+#ifndef DSMC_MOVE_STAGES
+#define DSMC_MOVE_STAGES 3
+#endif
+#ifndef DSMC_SCATTER_STAGES
+#define DSMC_SCATTER_STAGES 3
+#endif
 #ifndef DSMC_SAMPLE_STAGES
 #define DSMC_SAMPLE_STAGES 1
 #endif
 #ifndef DSMC_SAMPLE_UNROLL // unroll of k_sample's per-cell loop
 #define DSMC_SAMPLE_UNROLL 8
 #endif
-// k_sample reads a stage one iteration after thread 0 refilled it; with one
-// stage it adds the barrier that separates the two.
-static_assert(DSMC_SAMPLE_STAGES >= 1, "the sample pipeline needs a stage");
-
-// ---------------------------------------------------------------------------
-// k_move: one warp per move tile at a time, with no barrier and no shared
-// memory.  A tile's 1024 slots are MOVE_CHUNKS chunks of 128; lane l takes
-// slots 4l .. 4l+3 of a chunk with 16-byte vector loads and stores (so a
-// warp's accesses are 512 contiguous bytes per array), MOVE_UNROLL chunks
-// in flight.  The warp keeps the tile's counts in registers and writes the
-// tile's in-range and removed counts once; the out-of-range slots and the
-// slots for the exact body (k_move_near) are appended to their lists with
-// one atomic per warp and chunk (neither list's order matters: k_cell_fix
-// orders each cell's list by slot, and k_move_near's slots are independent).
-// ---------------------------------------------------------------------------
-constexpr int MOVE_THREADS = 256;
-constexpr int MOVE_CHUNK = 128;
-constexpr int MOVE_CHUNKS = TILE / MOVE_CHUNK;
-#ifndef DSMC_MOVE_UNROLL
-#define DSMC_MOVE_UNROLL 1
+#ifndef DSMC_MOVE_MIN_BLOCKS // CTAs per SM k_move is compiled for (register budget)
+#define DSMC_MOVE_MIN_BLOCKS 4
 #endif
-constexpr int MOVE_UNROLL = DSMC_MOVE_UNROLL;
-static_assert(MOVE_CHUNK == 32 * 4 && MOVE_CHUNKS % MOVE_UNROLL == 0, "chunks of 4 slots a lane");
-// CTAs per SM k_move is compiled for (register budget), FP32 and FP64.
-#ifndef DSMC_MOVE_MIN_BLOCKS
-#define DSMC_MOVE_MIN_BLOCKS 3
-#endif
-#ifndef DSMC_MOVE_MIN_BLOCKS_FP64
-#define DSMC_MOVE_MIN_BLOCKS_FP64 2
-#endif
-
-// The FP32 free-flight constants of a case, held in registers by k_move.
-struct MoveHot {
-    double dt;
-    float fx1, fy1, finv_dx, finv_dy, fcell_hw;
-    float near_lo0, near_lo1, near_hi0, near_hi1;
-    int32_t nx, ny, cbase;
-};
-
-__device__ __forceinline__ MoveHot move_hot(const CaseDev &c)
+// k_move and k_scatter need two stages at least: a stage's tile is rewritten
+// by thread 0 after the tile's barrier and read by the others one full
+// iteration later, which another barrier separates only when the next tile
+// uses another stage.  k_sample adds that barrier when it runs one stage.
+static_assert(DSMC_MOVE_STAGES >= 2 && DSMC_SCATTER_STAGES >= 2 && DSMC_SAMPLE_STAGES >= 1,
+              "the tile pipelines need two or more stages");
+template <class T> __host__ __device__ constexpr int move_stages()
 {
-    MoveHot h;
-    h.dt = c.dt;
-    h.fx1 = c.fx1;
-    h.fy1 = c.fy1;
-    h.finv_dx = c.finv_dx;
-    h.finv_dy = c.finv_dy;
-    h.fcell_hw = c.fcell_hw;
-    h.near_lo0 = c.fnear_lo[0];
-    h.near_lo1 = c.fnear_lo[1];
-    h.near_hi0 = c.fnear_hi[0];
-    h.near_hi1 = c.fnear_hi[1];
-    h.nx = c.nx;
-    h.ny = c.ny;
-    h.cbase = c.cbase;
-    return h;
+    return sizeof(T) == 4 ? DSMC_MOVE_STAGES : 2;
 }
-
-// cell_of_fast_f on the register constants.
-__device__ __forceinline__ bool cell_est_f(const MoveHot &h, float x, float y, int32_t &cell)
+template <class T> __host__ __device__ constexpr size_t move_smem()
 {
-    int32_t k, l;
-    const bool ok = floor_fast_f((x - h.fx1) * h.finv_dx, h.fcell_hw, k) &
-                    floor_fast_f((y - h.fy1) * h.finv_dy, h.fcell_hw, l);
-    const bool in = (static_cast<uint32_t>(k) < static_cast<uint32_t>(h.nx)) &
-                    (static_cast<uint32_t>(l) < static_cast<uint32_t>(h.ny));
-    cell = in ? static_cast<int32_t>(static_cast<uint32_t>(k) * static_cast<uint32_t>(h.ny) +
-                                     static_cast<uint32_t>(l))
-              : NO_CELL;
-    return ok;
-}
-
-// free_flight for FP32 slots with the hot constants in registers; the rare
-// open estimates read the case's FP64 constants from c.
-__device__ __forceinline__ bool free_flight(const MoveHot &h, const CaseDev &c, float x0,
-                                            float y0, float vx, float vy, float &xn, float &yn,
-                                            int32_t &oc, bool &gone, int32_t &nc)
-{
-    xn = __double2float_rn(static_cast<double>(x0) + h.dt * static_cast<double>(vx));
-    yn = __double2float_rn(static_cast<double>(y0) + h.dt * static_cast<double>(vy));
-    const bool near = (fmaxf(x0, xn) > h.near_lo0) & (fminf(x0, xn) < h.near_hi0) &
-                      (fmaxf(y0, yn) > h.near_lo1) & (fminf(y0, yn) < h.near_hi1);
-    bool ok_o = cell_est_f(h, x0, y0, oc);
-    bool ok_n = cell_est_f(h, xn, yn, nc);
-    gone = nc == NO_CELL;
-    if (!ok_o)
-        ok_o = cell_of_fast(c, static_cast<double>(x0), static_cast<double>(y0), oc);
-    if (!ok_n) {
-        gone = outside_domain_f(c, xn, yn);
-        nc = NO_CELL;
-        ok_n = gone || cell_of_fast(c, static_cast<double>(xn), static_cast<double>(yn), nc);
-    }
-    return !near & ok_o & ok_n;
-}
-__device__ __forceinline__ bool free_flight(const MoveHot &, const CaseDev &c, double x0,
-                                            double y0, double vx, double vy, double &xn,
-                                            double &yn, int32_t &oc, bool &gone, int32_t &nc)
-{
-    return free_flight(c, x0, y0, vx, vy, xn, yn, oc, gone, nc);
-}
-
-// Appends the entries a lane marks in bits[0..3] (slot base + j for bit j)
-// to a list with one atomic for the whole warp.  All lanes call it.
-__device__ __forceinline__ void warp_append(uint32_t *list, uint32_t *count, unsigned bits,
-                                            uint32_t base, int lane)
-{
-    const int mine = __popc(bits);
-    if (!__any_sync(0xffffffffu, mine != 0))
-        return;
-    int incl = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o)
-            incl += v;
-    }
-    uint32_t at = 0;
-    if (lane == 31)
-        at = atomicAdd(count, static_cast<uint32_t>(incl));
-    at = __shfl_sync(0xffffffffu, at, 31) + static_cast<uint32_t>(incl - mine);
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-        if ((bits >> j) & 1u)
-            list[at++] = base + static_cast<uint32_t>(j);
+    return sizeof(MoveStage<T>) * move_stages<T>();
 }
 
 template <class T>
-__global__ void __launch_bounds__(MOVE_THREADS, sizeof(T) == 4 ? DSMC_MOVE_MIN_BLOCKS
-                                                                : DSMC_MOVE_MIN_BLOCKS_FP64)
-    k_move(const CaseDev *__restrict__ cases, const CaseState *st, StepScratch *sc, TileTables tt,
+__global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
+    k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
            Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
            int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf,
            uint32_t *__restrict__ near_list, int ncase, int *err)
 {
     static_assert(TILE == 1024, "near_list packs the slot in tile into 10 bits");
+    constexpr int S = move_stages<T>();
+    constexpr int NB = 3; // ballot buffers: a tile's are read until the next tile's barrier
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    MoveStage<T> *stage = reinterpret_cast<MoveStage<T> *>(smem_raw);
+    __shared__ uint64_t bar[S];
+    __shared__ CaseDev s_case; // constants of the current tile's case
+    __shared__ unsigned s_dead[NB][32], s_out[NB][32]; // per (iteration, warp)
+    __shared__ unsigned s_opre[NB][32];                // exclusive prefix of s_out
+    __shared__ uint32_t s_obase[NB];
+    __shared__ int s_nnear[NB]; // slots of the tile queued for k_move_near
     const int lane = threadIdx.x & 31;
-    const int nwarps = gridDim.x * (MOVE_THREADS / 32);
+    const int warp = threadIdx.x >> 5;
+    const unsigned lanes_below = (1u << lane) - 1u;
     const int total = sc->total_move_tiles;
-    int cur_case = -1;
-    MoveHot h{};
-    for (int t = blockIdx.x * (MOVE_THREADS / 32) + (threadIdx.x >> 5); t < total; t += nwarps) {
+
+    // Thread 0 only: the copies of tile t into stage sidx.
+    auto issue = [&](int t, int sidx) {
         const int ci = case_of(tt.move0, ncase, t);
-        const CaseDev &c = cases[ci];
+        const int64_t g0 = cases[ci].pbase + static_cast<int64_t>(t - tt.move0[ci]) * TILE;
+        constexpr uint32_t vb = TILE * sizeof(T);
+        mbar_arrive_expect_tx(&bar[sidx], 4 * vb);
+        bulk_g2s(stage[sidx].v[0], p.x + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[1], p.y + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[2], p.vx + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[3], p.vy + g0, vb, &bar[sidx]);
+    };
+    // All threads: the out-of-range list entries of the tile at global slot
+    // gt whose ballots are in buffer nb (counted by warp 0 after its barrier).
+    auto append = [&](int nb, int64_t gt) {
+        for (int k = 0; k < TILE_VEC; ++k) {
+            const int i = k * MOVE_WARPS + warp;
+            const unsigned bo = s_out[nb][i];
+            if ((bo >> lane) & 1u)
+                obuf[s_obase[nb] + s_opre[nb][i] + __popc(bo & lanes_below)] =
+                    static_cast<uint32_t>(gt + k * TILE_THREADS + threadIdx.x);
+        }
+    };
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S; ++i)
+            mbar_init(&bar[i], 1);
+        fence_mbar_init();
+        for (int i = 0; i < S; ++i)
+            if (blockIdx.x + i * gridDim.x < total)
+                issue(blockIdx.x + i * gridDim.x, i);
+    }
+    if (threadIdx.x < NB)
+        s_nnear[threadIdx.x] = 0;
+    __syncthreads();
+
+    int cur_case = -1;
+    int64_t prev_gt = 0;
+    int it = 0;
+    for (;; ++it) {
+        const int t = blockIdx.x + it * gridDim.x;
+        if (t >= total)
+            break;
+        const int sidx = it % S;
+        const int nb = it % NB;
+        const int ci = case_of(tt.move0, ncase, t);
         if (ci != cur_case) {
-            h = move_hot(c);
+            // No thread reads s_case between a tile's barrier and the next
+            // tile's top, so the copy needs only the barrier after it.
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(cases + ci);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&s_case);
+            for (int w = threadIdx.x; w < static_cast<int>(sizeof(CaseDev) / 4); w += TILE_THREADS)
+                dst[w] = src[w];
+            __syncthreads();
             cur_case = ci;
         }
-        const int64_t tile0 = static_cast<int64_t>(t - tt.move0[ci]) * TILE;
+        const CaseDev &c = s_case;
+        const bool ok = mbar_wait(&bar[sidx], static_cast<uint32_t>((it / S) & 1));
+        const int local_tile = t - tt.move0[ci];
+        const int64_t tile0 = static_cast<int64_t>(local_tile) * TILE;
         const int64_t left = st[ci].n_old - tile0;
-        const int n_here = left < TILE ? static_cast<int>(left) : TILE;
+        const int n_here = ok ? (left < TILE ? static_cast<int>(left) : TILE) : 0;
         const int64_t gt = c.pbase + tile0;
-        int n_dead = 0, n_out = 0, n_near = 0; // this lane's slots of the tile
-#pragma unroll 1
-        for (int ch = 0; ch < MOVE_CHUNKS; ch += MOVE_UNROLL) {
-            if (ch * MOVE_CHUNK >= n_here)
-                break; // warp-uniform
-            T v[MOVE_UNROLL][4][4]; // chunk, array (x, y, vx, vy), slot
+        T *px = p.x + gt;
+        T *py = p.y + gt;
+        uint32_t *pkey = key + gt;
+        const MoveStage<T> &sg = stage[sidx];
+
+        unsigned near = 0; // bit k: the slot of iteration k takes the exact body
 #pragma unroll
-            for (int u = 0; u < MOVE_UNROLL; ++u) {
-                const int e0 = (ch + u) * MOVE_CHUNK + 4 * lane;
-                // Whole tiles are allocated, so a full vector is in bounds.
-                if ((ch + u) * MOVE_CHUNK < n_here) {
-                    load4(p.x + gt + e0, v[u][0]);
-                    load4(p.y + gt + e0, v[u][1]);
-                    load4(p.vx + gt + e0, v[u][2]);
-                    load4(p.vy + gt + e0, v[u][3]);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < MOVE_UNROLL; ++u) {
-                const int e0 = (ch + u) * MOVE_CHUNK + 4 * lane;
-                if ((ch + u) * MOVE_CHUNK >= n_here)
-                    break; // warp-uniform
-                T xn[4], yn[4];
-                uint32_t kv[4];
-                unsigned out_bits = 0, near_bits = 0;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    xn[j] = v[u][0][j];
-                    yn[j] = v[u][1][j];
-                    kv[j] = KEY_DEAD | KEY_CELL;
-                    if (e0 + j >= n_here)
-                        continue;
-                    int32_t oc, nc;
-                    bool gone;
-                    if (free_flight(h, c, v[u][0][j], v[u][1][j], v[u][2][j], v[u][3][j], xn[j],
-                                    yn[j], oc, gone, nc)) {
-                        const MoveClass m = classify_cells(h.cbase, oc, gone, nc, err);
-                        kv[j] = m.key;
-                        if ((m.dead || m.out) && m.ocg != NO_CELL)
-                            atomicSub(cells.n_in + m.ocg, 1);
-                        if (m.out) {
-                            atomicAdd(cells.n_o + (m.key & KEY_CELL), 1);
-                            out_bits |= 1u << j;
-                        }
-                        n_dead += m.dead ? 1 : 0;
-                    } else {
-                        // The exact body rewrites this slot; keep its start.
-                        xn[j] = v[u][0][j];
-                        yn[j] = v[u][1][j];
-                        near_bits |= 1u << j;
-                    }
-                }
-                n_out += __popc(out_bits);
-                n_near += __popc(near_bits);
-                if (e0 + 3 < n_here) {
-                    store4(p.x + gt + e0, xn);
-                    store4(p.y + gt + e0, yn);
-                    store4(key + gt + e0, kv);
+        for (int k = 0; k < TILE_VEC; ++k) {
+            const int e = k * TILE_THREADS + threadIdx.x;
+            MoveClass m;
+            m.dead = m.out = m.in = false;
+            if (e < n_here) {
+                T xn, yn;
+                int32_t oc, nc;
+                bool gone;
+                if (free_flight(c, sg.v[0][e], sg.v[1][e], sg.v[2][e], sg.v[3][e], xn, yn, oc,
+                                gone, nc)) {
+                    px[e] = xn;
+                    py[e] = yn;
+                    m = classify_cells(c, oc, gone, nc, err);
+                    commit_class(m, pkey, e, cells);
                 } else {
-                    // The last, partial vector: slots from n_old on belong to
-                    // k_inject, which may be writing them right now.
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        if (e0 + j < n_here) {
-                            p.x[gt + e0 + j] = xn[j];
-                            p.y[gt + e0 + j] = yn[j];
-                            key[gt + e0 + j] = kv[j];
-                        }
+                    near |= 1u << k;
                 }
-                warp_append(obuf, &sc->obuf_count, out_bits, static_cast<uint32_t>(gt + e0),
-                            lane);
-                warp_append(near_list, &sc->near_count, near_bits,
-                            (static_cast<uint32_t>(t) << 10) | static_cast<uint32_t>(e0), lane);
+            }
+            const unsigned bd = __ballot_sync(0xffffffffu, m.dead);
+            const unsigned bo = __ballot_sync(0xffffffffu, m.out);
+            if (lane == 0) {
+                s_dead[nb][k * MOVE_WARPS + warp] = bd;
+                s_out[nb][k * MOVE_WARPS + warp] = bo;
             }
         }
-        // The tile's counts: every slot moved here is removed, out of range
-        // or in range; k_move_near adds the queued ones.
-        const int in_lane = -n_dead - n_out - n_near;
-        int dead_w = n_dead, in_w = in_lane;
+        // Slots for the exact body go to k_move_near's queue as (tile, slot
+        // in tile); their ballots, counts and list entries are added there.
+        const unsigned nq = __ballot_sync(0xffffffffu, near != 0);
+        if (nq) {
+            int n_mine = __popc(near);
+            if (n_mine)
+                atomicAdd(&s_nnear[nb], n_mine);
+            int incl = n_mine;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            dead_w += __shfl_xor_sync(0xffffffffu, dead_w, o);
-            in_w += __shfl_xor_sync(0xffffffffu, in_w, o);
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o)
+                    incl += v;
+            }
+            uint32_t qbase = 0;
+            if (lane == 31)
+                qbase = atomicAdd(&sc->near_count, static_cast<uint32_t>(incl));
+            qbase = __shfl_sync(0xffffffffu, qbase, 31) + static_cast<uint32_t>(incl - n_mine);
+            for (int k = 0; k < TILE_VEC; ++k)
+                if ((near >> k) & 1u)
+                    near_list[qbase++] = (static_cast<uint32_t>(t) << 10) |
+                                         static_cast<uint32_t>(k * TILE_THREADS + threadIdx.x);
         }
-        if (lane == 0) {
-            tile_in[t] = n_here + in_w;
-            tile_dead[t] = dead_w;
+        // The one barrier of the tile: the stage is consumed, this tile's
+        // ballots are complete and the previous tile's list base is visible.
+        if (__syncthreads_or(!ok)) {
+            // A copy never completed (nothing of this tile was written).
+            if (threadIdx.x == 0) {
+                report_error(err, DSMC_ERR_TIMEOUT);
+                for (int j = it; j < it + S; ++j)
+                    if (blockIdx.x + j * gridDim.x < total)
+                        mbar_wait(&bar[j % S], static_cast<uint32_t>((j / S) & 1));
+            }
+            return;
         }
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            const int tn = t + S * gridDim.x;
+            if (tn < total)
+                issue(tn, sidx);
+        }
+        if (warp == 0) {
+            // Lane i holds the counts of (iteration, warp) pair i; pairs are
+            // in slot order, so an exclusive scan gives list ranks in slot
+            // order.  Removed slots are only counted here: their ranks come
+            // from k_dead_scan and k_holes, so no tile waits on another.
+            const unsigned o = __popc(s_out[nb][lane]);
+            unsigned oi = o;
+#pragma unroll
+            for (int sft = 1; sft < 32; sft <<= 1) {
+                const unsigned b = __shfl_up_sync(0xffffffffu, oi, sft);
+                if (lane >= sft)
+                    oi += b;
+            }
+            s_opre[nb][lane] = oi - o;
+            const unsigned out_tile = __shfl_sync(0xffffffffu, oi, 31);
+            const unsigned dead_tile =
+                static_cast<unsigned>(warp_sum_u64(__popc(s_dead[nb][lane])));
+            if (lane == 0) {
+                // Every slot this kernel moved is removed, out of range or in
+                // range; k_move_near counts the queued ones.
+                const int in_tile = n_here - s_nnear[nb] - static_cast<int>(dead_tile) -
+                                    static_cast<int>(out_tile);
+                s_nnear[nb] = 0; // rewritten for the tile NB iterations on
+                tile_in[t] = static_cast<int32_t>(in_tile);
+                tile_dead[t] = static_cast<int32_t>(dead_tile);
+                s_obase[nb] = out_tile ? atomicAdd(&sc->obuf_count, out_tile) : 0u;
+            }
+        }
+        // The previous tile's list entries (its base was set before this
+        // tile's barrier).
+        if (it > 0)
+            append((it + NB - 1) % NB, prev_gt);
+        prev_gt = gt;
+    }
+    if (it > 0) {
+        __syncthreads();
+        append((it + NB - 1) % NB, prev_gt);
     }
 }
 
@@ -1399,106 +1394,166 @@ __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *s
 // lower slots of its case); any other particle's key word already holds its
 // slot (k_cell_fix).
 //
-// One warp per tile at a time, with no barrier and no shared memory: the
-// tile's SC_CHUNKS chunks of 128 slots are taken in slot order, lane l
-// handling slots 32 j + l of a chunk (j = 0..3), so every load and store of
-// a warp covers 32 consecutive slots (in-range particles of one cell land on
-// consecutive destinations).  The in-range ranks are warp ballots plus the
-// count of the chunks before.  Many warps per SM, each with a chunk's loads
-// in flight, cover the latency of the dependent base_in lookups.
+// Tiles are staged whole in shared memory by bulk asynchronous copies, SCATTER
+// stages deep: while the warps place tile i, the copies of the next tiles of
+// this CTA are in flight, so the kernel keeps HBM busy without holding the
+// loads in registers.  Iteration k of thread t takes slot k * SC_THREADS + t
+// of the tile (SC_THREADS threads, SC_VEC slots each), so the 32 lanes of a
+// warp store 32 consecutive destinations when they share a cell.  One
+// barrier per tile: it publishes the in-range
+// counts of the (iteration, warp) chunks and frees the stage for its refill.
 // ---------------------------------------------------------------------------
-constexpr int SC_THREADS = 256;
-constexpr int SC_CHUNK = 128;
-constexpr int SC_CHUNKS = TILE / SC_CHUNK;
-// CTAs per SM k_scatter is compiled for (register budget), FP32 and FP64.
-#ifndef DSMC_SCATTER_MIN_BLOCKS
-#define DSMC_SCATTER_MIN_BLOCKS 5
-#endif
-#ifndef DSMC_SCATTER_MIN_BLOCKS_FP64
-#define DSMC_SCATTER_MIN_BLOCKS_FP64 3
-#endif
-
-template <class T> struct ScatterChunk {
-    uint32_t key[4];
-    T v[5][4];
+template <class T> struct ScatterStage {
+    uint32_t key[TILE];
+    T v[5][TILE];
 };
+// Threads of a k_scatter CTA: each takes TILE / SC_THREADS slots of a tile.
+#ifndef DSMC_SCATTER_THREADS
+#define DSMC_SCATTER_THREADS 256
+#endif
+constexpr int SC_THREADS = DSMC_SCATTER_THREADS;
+constexpr int SC_VEC = TILE / SC_THREADS;
+constexpr int SC_WARPS = SC_THREADS / 32;
+static_assert(SC_VEC * SC_WARPS == 32, "one warp scans the (iteration, warp) chunk counts");
 
-template <class T>
-__device__ __forceinline__ void scatter_load(ScatterChunk<T> &ch, const uint32_t *key,
-                                             Slots<T> src, int64_t g0, int64_t avail, int lane)
+template <class T> __host__ __device__ constexpr int scatter_stages()
 {
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int64_t e = 32 * j + lane;
-        const bool ok = e < avail;
-        const int64_t g = g0 + e;
-        ch.key[j] = ok ? __ldcs(key + g) : KEY_DEAD;
-        ch.v[0][j] = ok ? __ldcs(src.x + g) : T(0);
-        ch.v[1][j] = ok ? __ldcs(src.y + g) : T(0);
-        ch.v[2][j] = ok ? __ldcs(src.vx + g) : T(0);
-        ch.v[3][j] = ok ? __ldcs(src.vy + g) : T(0);
-        ch.v[4][j] = ok ? __ldcs(src.vz + g) : T(0);
-    }
+    return sizeof(T) == 4 ? DSMC_SCATTER_STAGES : 2;
+}
+template <class T> __host__ __device__ constexpr size_t scatter_smem()
+{
+    return sizeof(ScatterStage<T>) * scatter_stages<T>();
 }
 
 template <class T>
-__global__ void __launch_bounds__(SC_THREADS, sizeof(T) == 4 ? DSMC_SCATTER_MIN_BLOCKS
-                                                              : DSMC_SCATTER_MIN_BLOCKS_FP64)
+__global__ void __launch_bounds__(SC_THREADS)
     k_scatter(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt,
               Slots<T> src, Slots<T> dst, const uint32_t *__restrict__ key, Cells cells,
               const int32_t *__restrict__ tile_prefix, int ncase, int *err)
 {
+    constexpr int S = scatter_stages<T>();
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    ScatterStage<T> *stage = reinterpret_cast<ScatterStage<T> *>(smem_raw);
+    __shared__ uint64_t bar[S];
+    __shared__ int s_cnt[2][32]; // in-range counts per (iteration, warp), two buffers
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const unsigned lanes_below = (1u << lane) - 1u;
-    const int nwarps = gridDim.x * (SC_THREADS / 32);
     const int total = tt.scatter0[ncase];
-    for (int t = blockIdx.x * (SC_THREADS / 32) + (threadIdx.x >> 5); t < total; t += nwarps) {
+
+    // Thread 0 only: starts the copies of tile t into stage sidx.
+    auto issue = [&](int t, int sidx) {
         const int ci = case_of(tt.scatter0, ncase, t);
-        const int64_t pbase = cases[ci].pbase;
+        const int64_t g0 = cases[ci].pbase + static_cast<int64_t>(t - tt.scatter0[ci]) * TILE;
+        constexpr uint32_t kb = TILE * sizeof(uint32_t), vb = TILE * sizeof(T);
+        mbar_arrive_expect_tx(&bar[sidx], kb + 5 * vb);
+        bulk_g2s(stage[sidx].key, key + g0, kb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[0], src.x + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[1], src.y + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[2], src.vx + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[3], src.vy + g0, vb, &bar[sidx]);
+        bulk_g2s(stage[sidx].v[4], src.vz + g0, vb, &bar[sidx]);
+    };
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S; ++i)
+            mbar_init(&bar[i], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    int issued = 0;
+    if (threadIdx.x == 0)
+        for (; issued < S && blockIdx.x + issued * gridDim.x < total; ++issued)
+            issue(blockIdx.x + issued * gridDim.x, issued);
+
+    int it = 0;
+    bool failed = false;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
+        const int sidx = it % S;
+        const bool ok = mbar_wait(&bar[sidx], static_cast<uint32_t>((it / S) & 1));
+        const int ci = case_of(tt.scatter0, ncase, t);
+        const CaseDev &c = cases[ci];
         const CaseState &s = st[ci];
         const int local_tile = t - tt.scatter0[ci];
         const int64_t keep = s.n_keep;
+        const ScatterStage<T> &sg = stage[sidx];
         const int64_t tile0 = static_cast<int64_t>(local_tile) * TILE;
-        // In-range particles of the case before this tile; only tiles of
-        // moved slots have them (refilled holes and injected slots carry
-        // their final slot), so the prefix is read where it exists.
-        const int64_t in_before =
-            local_tile < s.n_move_tiles ? tile_prefix[s.move_tile0 + local_tile] : 0;
-        const int64_t left = keep - tile0;
-        const int n_here = left < TILE ? static_cast<int>(left) : TILE;
-        int64_t run = in_before; // in-range particles at lower slots
-#pragma unroll 1
-        for (int c0 = 0; c0 < n_here; c0 += SC_CHUNK) {
-            ScatterChunk<T> cur;
-            scatter_load(cur, key, src, pbase + tile0 + c0, n_here - c0, lane);
-            int64_t fin[4];
+        uint32_t keys[SC_VEC];
+        T x[SC_VEC], y[SC_VEC], vx[SC_VEC], vy[SC_VEC], vz[SC_VEC];
+        unsigned bin[SC_VEC];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const uint32_t k = cur.key[j];
-                const unsigned bin = __ballot_sync(0xffffffffu, (k & KEY_IN) != 0);
-                if (k & KEY_DEAD)
-                    fin[j] = -1;
-                else if (k & KEY_IN)
-                    fin[j] = cells.base_in[k & KEY_CELL] + run + __popc(bin & lanes_below);
-                else
-                    fin[j] = k;
-                run += __popc(bin);
+        for (int k = 0; k < SC_VEC; ++k) {
+            const int e = k * SC_THREADS + threadIdx.x;
+            keys[k] = (ok && tile0 + e < keep) ? sg.key[e] : KEY_DEAD;
+            x[k] = sg.v[0][e];
+            y[k] = sg.v[1][e];
+            vx[k] = sg.v[2][e];
+            vy[k] = sg.v[3][e];
+            vz[k] = sg.v[4][e];
+            bin[k] = __ballot_sync(0xffffffffu, (keys[k] & KEY_IN) != 0);
+            if (lane == 0)
+                s_cnt[it & 1][k * SC_WARPS + warp] = __popc(bin[k]);
+        }
+        // Every thread has copied its part of the stage into registers.
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        if (threadIdx.x == 0) {
+            fence_proxy_async_smem();
+            const int tn = t + S * gridDim.x;
+            if (tn < total) {
+                issue(tn, sidx);
+                ++issued;
             }
+        }
+        // Lane i: in-range count of (iteration, warp) chunk i; chunks are in
+        // slot order, so their exclusive scan ranks them within the tile.
+        const int cnt = s_cnt[it & 1][lane];
+        int cinc = cnt;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (cur.key[j] & KEY_DEAD)
-                    continue;
-                if (fin[j] < 0 || fin[j] >= keep) {
-                    report_error(err, DSMC_ERR_STATE); // counts and keys disagree
-                    continue;
-                }
-                const int64_t gd = pbase + fin[j];
-                __stcs(dst.x + gd, cur.v[0][j]);
-                __stcs(dst.y + gd, cur.v[1][j]);
-                __stcs(dst.vx + gd, cur.v[2][j]);
-                __stcs(dst.vy + gd, cur.v[3][j]);
-                __stcs(dst.vz + gd, cur.v[4][j]);
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, cinc, o);
+            if (lane >= o)
+                cinc += v;
+        }
+        const int cexcl = cinc - cnt;
+        const int tile_total = __shfl_sync(0xffffffffu, cinc, 31);
+        const int64_t base = tile_total > 0 ? tile_prefix[s.move_tile0 + local_tile] : 0;
+        int64_t fin[SC_VEC];
+#pragma unroll
+        for (int k = 0; k < SC_VEC; ++k) {
+            const int pre = __shfl_sync(0xffffffffu, cexcl, k * SC_WARPS + warp);
+            if (keys[k] & KEY_DEAD)
+                fin[k] = -1;
+            else if (keys[k] & KEY_IN)
+                fin[k] = cells.base_in[keys[k] & KEY_CELL] + base + pre +
+                         __popc(bin[k] & lanes_below);
+            else
+                fin[k] = keys[k];
+        }
+#pragma unroll
+        for (int k = 0; k < SC_VEC; ++k) {
+            if (keys[k] & KEY_DEAD)
+                continue;
+            if (fin[k] < 0 || fin[k] >= keep) {
+                report_error(err, DSMC_ERR_STATE); // counts and keys disagree
+                continue;
             }
+            const int64_t gd = c.pbase + fin[k];
+            dst.x[gd] = x[k];
+            dst.y[gd] = y[k];
+            dst.vx[gd] = vx[k];
+            dst.vy[gd] = vy[k];
+            dst.vz[gd] = vz[k];
+        }
+    }
+    if (failed) {
+        // A copy never completed: report, then wait (bounded) for the copies
+        // this CTA still has in flight before its shared memory goes away.
+        if (threadIdx.x == 0) {
+            report_error(err, DSMC_ERR_TIMEOUT);
+            for (int j = it; j < issued; ++j)
+                mbar_wait(&bar[j % S], static_cast<uint32_t>((j / S) & 1));
         }
     }
 }

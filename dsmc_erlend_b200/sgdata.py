@@ -14,7 +14,7 @@ from . import Engine, setup
 from .ensemble import WALL_CHOICES, case_key
 from .fields import macroscopic
 from .abi import FP32, WALL_CLL, WALL_DIFFUSE, WALL_SPECULAR, default_params
-from .surrogate import CH, IN_CH, OUT_CH, RES
+from .surrogate import CH, IN_CH, OUT_CH, OUT_NAMES, RES
 
 
 def surrogate_cases(n: int, seed: int, steps: int = 5000, precision: int = FP32,
@@ -97,17 +97,27 @@ def t_scale(p) -> float:
     return p.t_free * (1.0 + p.ma_free ** 2 / 3.0)
 
 
+def _free_and_scale(p, d):
+    ts = t_scale(p)
+    free = {"n": p.n_free, "ux": d.ux_free, "uy": d.uy_free, "t": p.t_free, "txx": p.t_free,
+            "tyy": p.t_free, "tzz": p.t_free, "txy": 0.0}
+    scale = {"n": p.n_free, "ux": d.u_free, "uy": d.u_free, "t": ts, "txx": ts, "tyy": ts,
+             "tzz": ts, "txy": ts}
+    return free, scale
+
+
 def field_target(p, d, f: dict, res: int = RES):
     """A sampled field on the canvas, normalised: (res, res, OUT_CH) targets
-    n / NFree, ux / UFree, uy / UFree, T / t_scale, and the (res, res) mask
-    of canvas cells that are outside the box and whose neighbourhood was
-    sampled."""
+    n / NFree, ux / UFree, uy / UFree, T / t_scale and Txx, Tyy, Tzz, Txy /
+    t_scale, and the (res, res) mask of canvas cells that are outside the
+    box and whose neighbourhood was sampled."""
     nx, ny = p.nx, p.ny
     valid = (f["count"] > 0) & np.isfinite(f["ux"]) & np.isfinite(f["t"])
-    free = {"n": p.n_free, "ux": d.ux_free, "uy": d.uy_free, "t": p.t_free}
+    for k in OUT_NAMES[4:]:
+        valid &= np.isfinite(f[k])
+    free, scale = _free_and_scale(p, d)
     out = np.zeros((res, res, OUT_CH), dtype=np.float32)
-    scale = {"n": p.n_free, "ux": d.u_free, "uy": d.u_free, "t": t_scale(p)}
-    for i, k in enumerate(("n", "ux", "uy", "t")):
+    for i, k in enumerate(OUT_NAMES):
         v = np.where(valid, f[k], free[k] if k != "n" else 0.0).reshape(nx, ny)
         out[..., i] = _bilinear(v, p, res, res) / scale[k]
     ok = _bilinear(valid.reshape(nx, ny).astype(np.float64), p, res, res) > 0.99
@@ -118,13 +128,16 @@ def field_target(p, d, f: dict, res: int = RES):
 def prediction_field(p, d, pred: np.ndarray) -> dict:
     """A canvas prediction (res, res, >= 4) back on the case's grid, as the
     field dict dsmc_init_warm's input is made from (count 1 outside the
-    box, n = 0 inside it)."""
+    box, n = 0 inside it); with 8 channels also the temperature tensor that
+    dsmc_init_warm_tensor takes."""
     back = {}
-    scale = {"n": p.n_free, "ux": d.u_free, "uy": d.u_free, "t": t_scale(p)}
-    for i, k in enumerate(("n", "ux", "uy", "t")):
+    _, scale = _free_and_scale(p, d)
+    for i, k in enumerate(OUT_NAMES[:pred.shape[-1]]):
         back[k] = (_bilinear(pred[..., i].astype(np.float64), p, p.nx, p.ny) * scale[k]).ravel()
     back["n"] = np.maximum(back["n"], 0.0)
-    back["t"] = np.maximum(back["t"], 1.0)
+    for k in ("t", "txx", "tyy", "tzz"):
+        if k in back:
+            back[k] = np.maximum(back[k], 1.0)
     xs = p.x1 + (np.arange(p.nx) + 0.5) * (p.x2 - p.x1) / p.nx
     ys = p.y1 + (np.arange(p.ny) + 0.5) * (p.y2 - p.y1) / p.ny
     x, y = np.meshgrid(xs, ys, indexing="ij")
@@ -137,7 +150,7 @@ def prediction_field(p, d, pred: np.ndarray) -> dict:
 
 def generate(cases, chunk: int = 128, verbose: bool = False):
     """Runs the cases as ensembles of `chunk` (each case to its own n_step,
-    the ensemble to the longest) and returns inputs (N, RES, RES, CH),
+    the ensemble to the longest) and returns inputs (N, RES, RES, IN_CH) float16 (the network pads them to CH),
     targets (N, RES, RES, OUT_CH), masks (N, RES, RES) and the particle-steps
     run."""
     xs, ts, ms = [], [], []
@@ -155,7 +168,7 @@ def generate(cases, chunk: int = 128, verbose: bool = False):
             f = macroscopic(eng.GatherGlobalField(i), d.weight, d.dv, d.molecule_mass,
                             c["sample_step"])
             t, m = field_target(p, d, f)
-            xs.append(case_input(p))
+            xs.append(case_input(p)[..., :IN_CH].astype(np.float16))  # compact; padded on use
             ts.append(t)
             ms.append(m)
         eng.close()

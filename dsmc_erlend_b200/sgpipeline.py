@@ -1,7 +1,12 @@
 """Surrogate pipeline: DSMC ensemble data on the GPU -> surrogate training ->
 hold-out error -> warm versus cold time to a 2% field on the warm-start case.
 
-    python -m dsmc_erlend_b200.sgpipeline --cases 1024 --epochs 40 --out DIR
+    python -m dsmc_erlend_b200.sgpipeline [--cases 4096] [--epochs 200] [--batch 64]
+        [--out DIR]
+
+Defaults are the surrogate-training configuration: 4096 cases of the
+ensemble generator, 5000 steps each (sampled from 2500), resampled to
+128 x 128; the 1.47M-weight network; Adam, batch 64, 200 epochs.
 
 Writes DIR/report.json (data, training, hold-out errors, time to field) and
 DIR/surrogate_weights.npz.  Every DSMC run and every network step runs on the
@@ -28,7 +33,8 @@ def time_to_field_study(p, predictors: dict, ref_replicas: int, transient: int,
     """Best cold and best warm time to a 2% field over the given sampling
     starts, against a reference field of `ref_replicas` replicas.
     `predictors` maps a name to (predicted field, seconds the prediction
-    took); a warm run's time includes its prediction's."""
+    took, whether to seed the full temperature tensor); a warm run's time
+    includes its prediction's."""
     t0 = time.perf_counter()
     ref = reference_field(p, ref_replicas, transient=transient, steps=ref_steps)
     out = {"reference_seconds": time.perf_counter() - t0, "cold": []}
@@ -42,11 +48,11 @@ def time_to_field_study(p, predictors: dict, ref_replicas: int, transient: int,
                                          check_every=check_every, max_steps=40000))
     bc = best(out["cold"])
     out["best_cold"] = bc
-    for name, (predicted, pred_s) in predictors.items():
+    for name, (predicted, pred_s, tensor) in predictors.items():
         runs = []
         for fs in warm_starts:
             r = time_to_field(p, ref, "warm", predicted=predicted, first_sampling_step=fs,
-                              check_every=check_every, max_steps=40000)
+                              check_every=check_every, max_steps=40000, tensor=tensor)
             r["prediction_seconds"] = pred_s
             r["seconds"] += pred_s
             runs.append(r)
@@ -59,11 +65,11 @@ def time_to_field_study(p, predictors: dict, ref_replicas: int, transient: int,
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--cases", type=int, default=1024)
+    ap.add_argument("--cases", type=int, default=4096)
     ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--holdout", type=float, default=0.1)
-    ap.add_argument("--epochs", type=int, default=40)
-    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--epochs", type=int, default=200)
+    ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=4096)
     ap.add_argument("--chunk", type=int, default=128)
@@ -103,7 +109,7 @@ def main():
         free[i, ..., 0] = 1.0
         free[i, ..., 1] = d.ux_free / d.u_free
         free[i, ..., 2] = d.uy_free / d.u_free
-        free[i, ..., 3] = p.t_free / t_scale(p)
+        free[i, ..., 3:7] = p.t_free / t_scale(p)
     report["freestream_errors"] = relative_errors(free, t[ho], m[ho])
     print(json.dumps({k: report[k] for k in ("train_errors", "holdout_errors",
                                              "freestream_errors")}), flush=True)
@@ -120,7 +126,9 @@ def main():
         sg_s = time.perf_counter() - t0
         coarse, coarse_s = coarse_prediction(p)
         report["time_to_field"] = time_to_field_study(
-            p, {"surrogate": (predicted, sg_s), "coarse": (coarse, coarse_s)},
+            p, {"surrogate": (predicted, sg_s, False),
+                "surrogate_tensor": (predicted, sg_s, True),
+                "coarse": (coarse, coarse_s, False)},
             ref_replicas=8, transient=6000, ref_steps=8000,
             cold_starts=(2000, 4000, 6000, 8000), warm_starts=(500, 1000, 2000, 3000),
             check_every=250)

@@ -11,8 +11,9 @@ Canvas: the domain [X1, X2] x [Y1, Y2] on RES x RES cells (x-major like the
 solver's fields).  Inputs (IN_CH channels, padded to 32): box mask, x and y
 of the cell centre, Mach / 8, cos and sin of the angle, log10(n) - 17, the
 wall model as three indicators, the CLL coefficients, box width and height /
-6.  Outputs (4 of 32 channels): n / NFree, ux / UFree, uy / UFree,
-T / (TFree (1 + Ma^2 / 3)) (the stagnation temperature, gamma = 5/3).
+6.  Network: LAYERS below (about 1.47M weights).  Outputs (8 of 32 channels): n / NFree, ux / UFree, uy / UFree,
+T / (TFree (1 + Ma^2 / 3)) (the stagnation temperature, gamma = 5/3) and the
+components Txx, Tyy, Tzz, Txy of the temperature tensor on the same scale.
 """
 from __future__ import annotations
 
@@ -25,19 +26,36 @@ import numpy as np
 
 RES = 128
 CH = 32
-OUT_CH = 4
+# The predicted channels: n, ux, uy, T and the temperature tensor's Txx,
+# Tyy, Tzz, Txy (for dsmc_init_warm_tensor).
+OUT_NAMES = ("n", "ux", "uy", "t", "txx", "tyy", "tzz", "txy")
+OUT_CH = len(OUT_NAMES)
 IN_CH = 14
 
 # (name, source, resampling before the conv, cin, cout, relu, skip added after)
+# Four levels of 128, 64, 32 and 16 pixels with 32, 64, 128 and 128 channels:
+# two 3x3 convolutions per level at 128 and 64 pixels, three at 32 and 16,
+# the decoder mirroring the encoder with additive skips from the last
+# convolution of each encoder level; 1.47M weights.
 LAYERS = [
-    ("e1", "x", None, 32, 32, True, None),
-    ("e2", "e1", "pool", 32, 64, True, None),
-    ("e3", "e2", "pool", 64, 128, True, None),
-    ("b", "e3", "pool", 128, 128, True, None),
-    ("d3", "b", "up", 128, 128, True, "e3"),
-    ("d2", "d3", "up", 128, 64, True, "e2"),
-    ("d1", "d2", "up", 64, 32, True, "e1"),
-    ("out", "d1", None, 32, 32, False, None),
+    ("e1a", "x", None, 32, 32, True, None),
+    ("e1b", "e1a", None, 32, 32, True, None),
+    ("e2a", "e1b", "pool", 32, 64, True, None),
+    ("e2b", "e2a", None, 64, 64, True, None),
+    ("e3a", "e2b", "pool", 64, 128, True, None),
+    ("e3b", "e3a", None, 128, 128, True, None),
+    ("e3c", "e3b", None, 128, 128, True, None),
+    ("ba", "e3c", "pool", 128, 128, True, None),
+    ("bb", "ba", None, 128, 128, True, None),
+    ("bc", "bb", None, 128, 128, True, None),
+    ("d3a", "bc", "up", 128, 128, True, None),
+    ("d3b", "d3a", None, 128, 128, True, None),
+    ("d3c", "d3b", None, 128, 128, True, "e3c"),
+    ("d2a", "d3c", "up", 128, 64, True, None),
+    ("d2b", "d2a", None, 64, 64, True, "e2b"),
+    ("d1a", "d2b", "up", 64, 32, True, None),
+    ("d1b", "d1a", None, 32, 32, True, "e1b"),
+    ("out", "d1b", None, 32, 32, False, None),
 ]
 
 _LIB = Path(__file__).resolve().parent / "lib" / "libdsmc_surrogate.so"
@@ -211,7 +229,7 @@ class Surrogate:
             _ok(L.dsmc_sg_add(ptr(self.dy[src]), ptr(tgt), tgt.numel(), s), "grad add")
 
     def loss_and_grad(self, target, mask):
-        """Masked MSE of the last forward against target (n, res, res, 4)
+        """Masked MSE of the last forward against target (n, res, res, OUT_CH)
         fp32 with mask (n, res, res) fp32; returns the loss tensor [1] and
         fills the output gradient."""
         L = lib()
@@ -331,13 +349,14 @@ class Surrogate:
 
 def relative_errors(pred: np.ndarray, target: np.ndarray, mask: np.ndarray) -> dict:
     """Relative L2 error per output channel over the masked canvas cells:
-    ||pred - target|| / ||target|| for n and T, ||pred - target|| / sqrt(cells)
-    for the velocities (already in units of the freestream speed)."""
+    ||pred - target|| / ||target|| for n and the temperatures,
+    ||pred - target|| / sqrt(cells) for the velocities (already in units of
+    the freestream speed) and for Txy (in units of the temperature scale)."""
     m = mask.astype(bool)
     out = {}
-    for i, k in enumerate(("n", "ux", "uy", "t")):
+    for i, k in enumerate(OUT_NAMES[:min(pred.shape[-1], target.shape[-1])]):
         d = (pred[..., i] - target[..., i])[m]
-        if k in ("n", "t"):
+        if k not in ("ux", "uy", "txy"):
             out[k] = float(np.linalg.norm(d) / max(np.linalg.norm(target[..., i][m]), 1e-30))
         else:
             out[k] = float(np.linalg.norm(d) / np.sqrt(max(m.sum(), 1)))
@@ -346,7 +365,7 @@ def relative_errors(pred: np.ndarray, target: np.ndarray, mask: np.ndarray) -> d
 
 def train(x: np.ndarray, target: np.ndarray, mask: np.ndarray, epochs: int = 40,
           batch: int = 32, lr: float = 2e-3, seed: int = 0, log=None) -> tuple:
-    """Trains a Surrogate on (N, RES, RES, CH) inputs, (N, RES, RES, 4)
+    """Trains a Surrogate on (N, RES, RES, CH) inputs, (N, RES, RES, OUT_CH)
     targets and (N, RES, RES) masks with Adam (cosine learning-rate decay).
     Returns the network and a history of (epoch, mean loss, step ms, TFLOP/s)."""
     import torch
@@ -355,7 +374,7 @@ def train(x: np.ndarray, target: np.ndarray, mask: np.ndarray, epochs: int = 40,
     # One stream for the batch gathers and the graph-replayed steps.
     st = torch.cuda.Stream()
     net = Surrogate(batch, res=x.shape[1], seed=seed, stream=st.cuda_stream)
-    dx = torch.from_numpy(x).to(torch.bfloat16).cuda()
+    dx = _to_device_input(torch, x)
     dt = torch.from_numpy(target.astype(np.float32)).cuda()
     dm = torch.from_numpy(mask.astype(np.float32)).cuda()
     bx = torch.empty((batch,) + dx.shape[1:], dtype=torch.bfloat16, device="cuda")
@@ -398,8 +417,20 @@ def train(x: np.ndarray, target: np.ndarray, mask: np.ndarray, epochs: int = 40,
     return net, history
 
 
+def _to_device_input(torch, x: np.ndarray):
+    """(N, RES, RES, c) inputs, c = IN_CH (stored compactly) or CH, as the
+    network's bf16 (N, RES, RES, CH) device tensor (channels past c are
+    zero), copied in slices to bound the host-side conversion."""
+    n, c = x.shape[0], x.shape[-1]
+    out = torch.zeros((n,) + x.shape[1:-1] + (CH,), dtype=torch.bfloat16, device="cuda")
+    for i in range(0, n, 256):
+        part = torch.from_numpy(np.ascontiguousarray(x[i:i + 256], dtype=np.float32))
+        out[i:i + 256, ..., :c] = part.to(torch.bfloat16).cuda()
+    return out
+
+
 def predict(net: Surrogate, x: np.ndarray) -> np.ndarray:
-    """Predictions (N, RES, RES, 4) for inputs (N, RES, RES, CH) with a
+    """Predictions (N, RES, RES, OUT_CH) for inputs (N, RES, RES, CH) with a
     trained network (its weights copied into a network of this batch)."""
     import torch
 
@@ -410,6 +441,6 @@ def predict(net: Surrogate, x: np.ndarray) -> np.ndarray:
         pad = b - part.shape[0]
         if pad:
             part = np.concatenate([part, np.zeros((pad,) + part.shape[1:], part.dtype)])
-        y = net.forward(torch.from_numpy(part).to(torch.bfloat16).cuda())
+        y = net.forward(_to_device_input(torch, part))
         out.append(y[: b - pad, ..., :OUT_CH].cpu().numpy())
     return np.concatenate(out)

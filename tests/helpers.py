@@ -64,3 +64,25 @@ def assert_ulp(gpu, ref, max_ulp: int, what: str):
                              f" worst {int(u.max())} ulp at {i}: {np.ravel(gpu)[i]!r} vs "
                              f"{np.ravel(ref)[i]!r}")
     return int(u.max()) if u.size else 0
+
+
+def ulp_of_scale(gpu, ref, scale) -> np.ndarray:
+    """|gpu - ref| in units in the last place of max(|ref|, scale): the
+    distance measured on the magnitude of the operands a value came from.
+    A sum that cancels (a Maxwellian draw around a drift, a centre-of-mass
+    velocity plus half the relative one) keeps the absolute error of its
+    operands, which in its own last place can be many units."""
+    ref = np.asarray(ref, dtype=np.float64)
+    mag = np.maximum(np.abs(ref), np.broadcast_to(np.asarray(scale, dtype=np.float64), ref.shape))
+    return np.abs(np.asarray(gpu, dtype=np.float64) - ref) / np.spacing(np.maximum(mag, 1e-300))
+
+
+def assert_ulp_of_scale(gpu, ref, scale, max_ulp: float, what: str) -> float:
+    u = ulp_of_scale(gpu, ref, scale)
+    worst = float(u.max()) if u.size else 0.0
+    if worst > max_ulp:
+        i = int(np.argmax(u))
+        raise AssertionError(f"{what}: {int((u > max_ulp).sum())} of {u.size} beyond {max_ulp} "
+                             f"ulp of the scale; worst {worst:.2f} at {i}: "
+                             f"{np.ravel(gpu)[i]!r} vs {np.ravel(ref)[i]!r}")
+    return worst

@@ -95,19 +95,21 @@ def test_fp32_state_matches_fp64(cuda, engine_lib):
 def test_fp32_state_matches_fp64_large_case_geometry(cuda, engine_lib, wall):
     """The large single instance's flow (angle 10, NPCFree 20, diffuse Tw 300
     K or CLL 0.8/0.8) on a 250 x 250 grid, Dt scaled with the cell to keep the
-    1000 x 1000 case's cell transit time: FP32 state against all-FP64, each
-    field within 2% relative L2 outside the wall cells, and within twice the
-    FP64 run-to-run difference plus 0.5% (FP32 adds no error above noise)."""
+    1000 x 1000 case's cell transit time, 8000 steps sampled after 4000: FP32
+    state against all-FP64, each field's relative L2 difference outside the
+    wall cells within 1.5 times the FP64 run-to-run difference (two keys)
+    plus 0.2%: FP32 adds no error above the Monte Carlo noise.  (The noise of
+    this short window is itself 2-4%; the full-size runs are in
+    dsmc_erlend_b200.precision.)"""
     from dsmc_erlend_b200.abi import WALL_CLL, WALL_DIFFUSE, large_case
     from dsmc_erlend_b200.precision import compare
 
     p = large_case(wall_model=WALL_DIFFUSE if wall == "diffuse" else WALL_CLL)
     p.nx = p.ny = 250
     p.dt = 4e-6
-    p.n_step, p.first_sampling_step = 3000, 1500
+    p.n_step, p.first_sampling_step = 8000, 4000
     r = compare(p, key_a=11, key_b=12)
     e32, e64 = r["fp32_vs_fp64"], r["fp64_vs_fp64_other_key"]
     print(wall, "fp32 vs fp64", e32, "fp64 vs fp64", e64)
     for k in ("n", "ux", "uy", "t"):
-        assert e32[k] <= 0.02, (k, e32)
-        assert e32[k] <= 2 * e64[k] + 0.005, (k, e32, e64)
+        assert e32[k] <= 1.5 * e64[k] + 0.002, (k, e32, e64)
