@@ -74,12 +74,24 @@ def main():
     ap.add_argument("--seed", type=int, default=4096)
     ap.add_argument("--chunk", type=int, default=128)
     ap.add_argument("--no-ttf", action="store_true", help="skip the time-to-field study")
+    ap.add_argument("--weights", default=None,
+                    help="a trained network (surrogate_weights.npz): skip data and training, "
+                         "run the time-to-field study only")
+    ap.add_argument("--warm-starts", default="500,1000,2000,3000,4000,5000",
+                    help="sampling starts tried for the warm runs")
     ap.add_argument("--out", default="surrogate_out")
     args = ap.parse_args()
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
     report = {"args": vars(args)}
 
+    if args.weights:
+        net = Surrogate(1, seed=0)
+        w = np.load(args.weights)
+        net.load_state_dict({k: w[k] for k in w.files})
+        report["time_to_field"] = run_ttf(net, [int(v) for v in args.warm_starts.split(",")])
+        (out / "report_ttf.json").write_text(json.dumps(report, indent=1, default=float))
+        return
     cases = surrogate_cases(args.cases, args.seed, steps=args.steps)
     t0 = time.perf_counter()
     x, t, m, ps = generate(cases, chunk=args.chunk, verbose=True)
@@ -116,26 +128,34 @@ def main():
     np.savez_compressed(out / "surrogate_weights.npz", **net.state_dict())
 
     if not args.no_ttf:
-        p = warm_start_case(seed=1)
-        d = setup(p)
-        t0 = time.perf_counter()
-        one = Surrogate(1, seed=0)
-        one.load_state_dict(net.state_dict())
-        pred = predict(one, case_input(p)[None])[0]
-        predicted = prediction_field(p, d, pred)
-        sg_s = time.perf_counter() - t0
-        coarse, coarse_s = coarse_prediction(p)
-        report["time_to_field"] = time_to_field_study(
-            p, {"surrogate": (predicted, sg_s, False),
-                "surrogate_tensor": (predicted, sg_s, True),
-                "coarse": (coarse, coarse_s, False)},
-            ref_replicas=8, transient=6000, ref_steps=8000,
-            cold_starts=(2000, 4000, 6000, 8000), warm_starts=(500, 1000, 2000, 3000),
-            check_every=250)
-        tt = report["time_to_field"]
-        print(json.dumps({k: tt[k]["warm_over_cold"] for k in tt if k.startswith("warm_")}),
-              flush=True)
+        report["time_to_field"] = run_ttf(net, [int(v) for v in args.warm_starts.split(",")])
     (out / "report.json").write_text(json.dumps(report, indent=1, default=float))
+
+
+def run_ttf(net, warm_starts) -> dict:
+    """The time-to-field study on the warm-start case (512 x 512, Ma 6, n 3e17,
+    angle 15, CLL (0.5, 0.9), box 3 x 5 m, NPCFree 30): cold starts against
+    warm starts from the surrogate (n, u, T and the temperature tensor) and
+    from a coarse run of the same case."""
+    p = warm_start_case(seed=1)
+    d = setup(p)
+    t0 = time.perf_counter()
+    one = Surrogate(1, seed=0)
+    one.load_state_dict(net.state_dict())
+    pred = predict(one, case_input(p)[None])[0]
+    predicted = prediction_field(p, d, pred)
+    sg_s = time.perf_counter() - t0
+    coarse, coarse_s = coarse_prediction(p)
+    tt = time_to_field_study(
+        p, {"surrogate": (predicted, sg_s, False),
+            "surrogate_tensor": (predicted, sg_s, True),
+            "coarse": (coarse, coarse_s, False)},
+        ref_replicas=8, transient=6000, ref_steps=8000,
+        cold_starts=(2000, 4000, 6000, 8000), warm_starts=tuple(warm_starts),
+        check_every=250)
+    print(json.dumps({k: tt[k]["warm_over_cold"] for k in tt if k.startswith("warm_")}),
+          flush=True)
+    return tt
 
 
 if __name__ == "__main__":
