@@ -230,12 +230,19 @@ def test_network_gradients_match_restatement(cuda):
     dout = _bf16(torch, _rand(rng, n, res, res, 32, scale=1e-2))
     net.backward(dout)
     torch.cuda.synchronize()
-    grads = ref.network_backward(params, acts, _np(dout), LAYERS)
-    # Through 18 layers of bf16 activations the gradients of the first
-    # layers carry the roundings of every layer above them: each weight
-    # tensor is held to 4% relative L2, each bias (a sum over every pixel,
-    # where terms cancel) to 8%, and every element to 10% of its tensor's
-    # scale.
+    # The backward is checked on the kernels' own forward activations (bf16,
+    # as stored): with the restatement's, the few pre-activations within a
+    # rounding of zero would switch ReLU masks between the two sides and
+    # their differences, not the backward kernels', would dominate 18 layers
+    # down.
+    gpu_acts = {"x": _np(x)}
+    for name, src, op, *_ in LAYERS:
+        gpu_acts[name + ".relu"] = _np(net.relu_out[name])
+        gpu_acts[name + ".in"] = _np(net.a_in[name]) if op else _np(net._acts[src])
+    grads = ref.network_backward(params, gpu_acts, _np(dout), LAYERS)
+    # Each weight tensor is held to 4% relative L2, each bias (a sum over
+    # every pixel, where terms cancel) to 8%, and every element to 10% of its
+    # tensor's scale.
     errs = {}
     for name in net.w32:
         for kind, got in (("w", net.gw[name]), ("b", net.gb[name])):
