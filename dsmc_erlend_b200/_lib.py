@@ -58,6 +58,12 @@ SIGNATURES = {
                                          C.POINTER(C.c_char_p)]),
     "dsmc_set_launch_config": (C.c_int, [C.c_void_p, _I32, C.c_int]),
     "dsmc_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "dsmc_set_step_mode": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dsmc_get_step_mode": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "dsmc_grid_sync_probe": (C.c_int, [C.c_void_p, C.c_int64]),
+    "dsmc_get_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int,
+                                       C.POINTER(C.c_int), C.POINTER(C.c_char_p), C.c_int]),
     "dsmc_get_kernel_times": (C.c_int, [C.c_void_p, _D, _I64, C.c_int, C.POINTER(C.c_int),
                                         C.POINTER(C.c_char_p)]),
     "dsmc_k_intersect": (C.c_int, [_P, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,

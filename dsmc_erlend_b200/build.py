@@ -28,7 +28,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler",
 
 LIB_SOURCES = ["dsmc_capi.cu", "host_api.cpp", "surface.cpp"]
 DEPENDS = ["dsmc_device.cuh", "dsmc_scan.cuh", "dsmc_kernels.cuh", "dsmc_bulk.cuh",
-           "dsmc_units.cuh"]
+           "dsmc_units.cuh", "dsmc_persist.cuh"]
 
 # The surrogate's kernels: ordinary FP32 contraction is fine there (a neural
 # network, not the reference's arithmetic).

@@ -21,6 +21,13 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
                  : "memory");
 }
 
+// Ends the life of an mbarrier whose phases are all complete, so that its
+// word can be initialised again (the next step of a persistent launch).
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // Makes the mbarrier initialisation visible to the async proxy.
 __device__ __forceinline__ void fence_mbar_init()
 {

@@ -9,10 +9,12 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/dsmc.h"
 #include "dsmc_kernels.cuh"
+#include "dsmc_persist.cuh"
 #include "dsmc_units.cuh"
 
 using namespace dsmc;
@@ -105,6 +107,25 @@ struct dsmc_ctx {
     bool sampled = false;
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+
+    // The persistent step (DSMC_STEP_PERSISTENT): one cooperative launch of
+    // k_persistent for all steps of a dsmc_step call, the kernel node of a
+    // graph (memset of the barrier state, then the kernel); one instantiated
+    // graph per (steps, buffer side) pair met, the most recent few kept.
+    int step_mode = DSMC_STEP_GRAPH;
+    GridSync *d_gsync = nullptr;
+    int *d_probe_err = nullptr;
+    unsigned long long *d_phase_ns = nullptr; // PERSIST_PHASES sums
+    int p_ctas = 0, p_ctas_max = 0; // CTAs per SM of k_persistent
+    bool coop = false;              // the device supports cooperative launches
+    bool p_graph = true;            // launched through graphs (else directly)
+    uint64_t p_wait_ns = 2000000000ull;
+    struct PGraph {
+        int n_steps, side;
+        cudaGraph_t g;
+        cudaGraphExec_t exec;
+    };
+    std::vector<PGraph> pgraphs;
 
     // CTAs per SM of each kernel's grid (the tunable launch shape), and the
     // most that fit (occupancy); zero for kernels with a fixed grid.
@@ -421,6 +442,131 @@ int build_graphs(dsmc_ctx *c)
     return DSMC_OK;
 }
 
+// ---- the persistent step ---------------------------------------------------
+
+template <class T> StepArgs<T> step_args(dsmc_ctx *c)
+{
+    StepArgs<T> a{};
+    a.cases = c->d_cases;
+    a.st = c->d_state;
+    a.sc = c->d_scratch;
+    a.tt = c->tt;
+    a.buf0 = slots<T>(c, 0);
+    a.buf1 = slots<T>(c, 1);
+    a.key = c->key;
+    a.cells = c->cells;
+    a.tile_in = c->tile_in;
+    a.tile_prefix = c->tile_prefix;
+    a.tile_dead = c->tile_dead;
+    a.tile_dprefix = c->tile_dprefix;
+    a.itile_dead = c->itile_dead;
+    a.itile_dprefix = c->itile_dprefix;
+    a.tail_chain = lb_chain(c, 2);
+    a.cell_chain = lb_chain(c, 3);
+    a.hole_pos = c->hole_pos;
+    a.hole_oc = c->hole_oc;
+    a.obuf = c->obuf;
+    a.near_list = c->near_list;
+    a.olist = c->olist;
+    a.coll_list = c->coll_list;
+    a.rec = c->d_counters;
+    a.tmp = c->d_tmp;
+    a.pbases = c->d_pbases;
+    a.total_cells = c->total_cells;
+    a.ncase = c->ncase;
+    constexpr int64_t chunk = PERSIST_THREADS * SCAN_VEC;
+    a.scan_chunks = static_cast<int>((c->max_case_tiles + chunk - 1) / chunk);
+    a.err = c->d_err;
+    a.gsync = c->d_gsync;
+    a.wait_ns = c->p_wait_ns;
+    a.phase_ns = c->d_phase_ns;
+    return a;
+}
+
+// The graph of one persistent launch: zero the barrier state, then the
+// cooperative kernel for n_steps steps from buffer `side`.
+template <class T> int persistent_graph(dsmc_ctx *c, int n_steps, int side, cudaGraphExec_t *out)
+{
+    for (const auto &pg : c->pgraphs)
+        if (pg.n_steps == n_steps && pg.side == side) {
+            *out = pg.exec;
+            return DSMC_OK;
+        }
+    StepArgs<T> a = step_args<T>(c);
+    void *args[] = {&a, &n_steps, &side};
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaMemsetParams mp{};
+    mp.dst = c->d_gsync;
+    mp.value = 0;
+    mp.elementSize = 4;
+    mp.width = sizeof(GridSync) / 4;
+    mp.height = 1;
+    mp.pitch = sizeof(GridSync);
+    cudaGraphNode_t mn = nullptr, kn = nullptr;
+    cudaKernelNodeParams kp{};
+    kp.func = reinterpret_cast<void *>(k_persistent<T>);
+    kp.gridDim = dim3(c->p_ctas * c->sms);
+    kp.blockDim = dim3(PERSIST_THREADS);
+    kp.sharedMemBytes = static_cast<unsigned>(persist_smem<T>());
+    kp.kernelParams = args;
+    cudaLaunchAttributeValue v{};
+    v.cooperative = 1;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaGraphAddMemsetNode(&mn, g, nullptr, 0, &mp);
+    if (e == cudaSuccess)
+        e = cudaGraphAddKernelNode(&kn, g, &mn, 1, &kp);
+    if (e == cudaSuccess)
+        e = cudaGraphKernelNodeSetAttribute(kn, cudaLaunchAttributeCooperative, &v);
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&exec, g, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        return DSMC_ERR_UNSUPPORTED;
+    }
+    if (c->pgraphs.size() >= 8) { // keep the most recent few
+        cudaGraphExecDestroy(c->pgraphs.front().exec);
+        cudaGraphDestroy(c->pgraphs.front().g);
+        c->pgraphs.erase(c->pgraphs.begin());
+    }
+    c->pgraphs.push_back({n_steps, side, g, exec});
+    *out = exec;
+    return DSMC_OK;
+}
+
+// n_steps full steps of every case in one persistent launch.
+template <class T> int persistent_steps(dsmc_ctx *c, int n_steps)
+{
+    if (n_steps == 0)
+        return DSMC_OK;
+    if (c->p_graph) {
+        cudaGraphExec_t exec = nullptr;
+        const int s = persistent_graph<T>(c, n_steps, c->cur, &exec);
+        if (s == DSMC_OK) {
+            CK(cudaGraphLaunch(exec, c->stream));
+            c->cur = (c->cur + n_steps) & 1;
+            return DSMC_OK;
+        }
+        c->p_graph = false; // graphs of cooperative kernels refused: launch directly
+    }
+    const StepArgs<T> a = step_args<T>(c);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(c->p_ctas * c->sms);
+    cfg.blockDim = dim3(PERSIST_THREADS);
+    cfg.dynamicSmemBytes = persist_smem<T>();
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaMemsetAsync(c->d_gsync, 0, sizeof(GridSync), c->stream));
+    CK(cudaLaunchKernelEx(&cfg, k_persistent<T>, a, n_steps, c->cur));
+    c->cur = (c->cur + n_steps) & 1;
+    return DSMC_OK;
+}
+
 // Constants of one case, computed on the host with the reference expressions.
 // Largest float <= v and smallest float >= v.
 float float_down(double v)
@@ -598,6 +744,16 @@ template <class T> int occupancy_grids(dsmc_ctx *c)
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cell_fix, 256, 0));
     occ(KID_CELL_FIX, b);
     c->ctas[KID_CELL_FIX] = std::min(8, c->ctas_max[KID_CELL_FIX]);
+    // The persistent step: every CTA of its grid must be resident at once.
+    int coop = 0;
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
+    c->coop = coop != 0;
+    CK(cudaFuncSetAttribute(k_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(persist_smem<T>())));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_persistent<T>, PERSIST_THREADS,
+                                                     persist_smem<T>()));
+    c->p_ctas_max = b;
+    c->p_ctas = b;
     return DSMC_OK;
 }
 
@@ -606,6 +762,10 @@ void free_ctx(dsmc_ctx *c)
     for (auto &g : c->graph)
         if (g)
             cudaGraphExecDestroy(g);
+    for (auto &pg : c->pgraphs) {
+        cudaGraphExecDestroy(pg.exec);
+        cudaGraphDestroy(pg.g);
+    }
     for (auto e : c->branch_ev)
         if (e)
             cudaEventDestroy(e);
@@ -1012,6 +1172,11 @@ void drop_graphs(dsmc_ctx *c)
             cudaGraphExecDestroy(g);
             g = nullptr;
         }
+    for (auto &pg : c->pgraphs) {
+        cudaGraphExecDestroy(pg.exec);
+        cudaGraphDestroy(pg.g);
+    }
+    c->pgraphs.clear();
 }
 
 } // namespace
@@ -1158,6 +1323,11 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
     ok &= alloc(reinterpret_cast<void **>(&c->olist), sizeof(int32_t) * slot);
     ok &= alloc(reinterpret_cast<void **>(&c->coll_list), sizeof(uint32_t) * cell);
     ok &= alloc(reinterpret_cast<void **>(&c->d_counters), sizeof(dsmc_counters) * n_cases);
+    ok &= alloc(reinterpret_cast<void **>(&c->d_gsync), sizeof(GridSync));
+    ok &= alloc(reinterpret_cast<void **>(&c->d_probe_err), sizeof(int));
+    ok &= alloc(reinterpret_cast<void **>(&c->d_phase_ns),
+                sizeof(unsigned long long) * PERSIST_PHASES);
+
     size_t arena_bytes = 0;
     for (const auto &b : carve)
         arena_bytes += b.second;
@@ -1199,11 +1369,13 @@ int dsmc_ctx_create(const dsmc_params *cases, const dsmc_derived *derived, int n
         cudaMemset(c->cells.o_fill, 0, sizeof(int32_t) * cell) != cudaSuccess ||
         cudaMemset(c->cells.start[0], 0, sizeof(int32_t) * cell) != cudaSuccess ||
         cudaMemset(c->cells.start[1], 0, sizeof(int32_t) * cell) != cudaSuccess ||
-        cudaMemset(c->cells.acc, 0, sizeof(double) * ACC_COUNT * cell) != cudaSuccess)
+        cudaMemset(c->cells.acc, 0, sizeof(double) * ACC_COUNT * cell) != cudaSuccess ||
+        cudaMemset(c->d_phase_ns, 0, sizeof(unsigned long long) * PERSIST_PHASES) != cudaSuccess)
         return fail();
     const int g = c->precision == DSMC_FP32 ? occupancy_grids<float>(c) : occupancy_grids<double>(c);
     if (g)
         return fail();
+
     *out = c;
     return DSMC_OK;
 }
@@ -1313,6 +1485,9 @@ int dsmc_step(dsmc_ctx *c, int n_steps)
         }
         return DSMC_OK;
     }
+    if (c->step_mode == DSMC_STEP_PERSISTENT)
+        return c->precision == DSMC_FP32 ? persistent_steps<float>(c, n_steps)
+                                         : persistent_steps<double>(c, n_steps);
     if (c->graph[0] == nullptr) {
         const int s = build_graphs(c);
         if (s)
@@ -1892,6 +2067,81 @@ int dsmc_set_launch_config(dsmc_ctx *c, const int32_t *ctas_per_sm, int n)
             c->ctas[k] = std::min(ctas_per_sm[k], c->ctas_max[k]);
     drop_graphs(c); // rebuilt with the new shapes at the next dsmc_step
     return DSMC_OK;
+}
+
+int dsmc_set_step_mode(dsmc_ctx *c, int mode, int ctas_per_sm)
+{
+    if (c == nullptr || (mode != DSMC_STEP_GRAPH && mode != DSMC_STEP_PERSISTENT) ||
+        ctas_per_sm < 0)
+        return DSMC_ERR_ARGUMENT;
+    if (c->stage != 0)
+        return DSMC_ERR_STATE;
+    if (mode == DSMC_STEP_PERSISTENT) {
+        if (!c->coop || c->p_ctas_max < 1)
+            return DSMC_ERR_UNSUPPORTED;
+        const int want = ctas_per_sm == 0 ? c->p_ctas_max : std::min(ctas_per_sm, c->p_ctas_max);
+        if (want != c->p_ctas)
+            drop_graphs(c);
+        c->p_ctas = want;
+    }
+    c->step_mode = mode;
+    return DSMC_OK;
+}
+
+int dsmc_get_step_mode(dsmc_ctx *c, int *mode, int *ctas_per_sm, int *max_ctas_per_sm,
+                       int *graph_launch)
+{
+    if (c == nullptr)
+        return DSMC_ERR_ARGUMENT;
+    if (mode)
+        *mode = c->step_mode;
+    if (ctas_per_sm)
+        *ctas_per_sm = c->p_ctas;
+    if (max_ctas_per_sm)
+        *max_ctas_per_sm = c->coop ? c->p_ctas_max : 0;
+    if (graph_launch)
+        *graph_launch = c->p_graph ? 1 : 0;
+    return DSMC_OK;
+}
+
+const char *kPhaseNames[PERSIST_PHASES] = {
+    "plan", "move+inject", "move_near", "dead_scan", "holes", "tail",
+    "cell_scan+tile_scan", "olist+collide_select", "cell_fix", "scatter", "collide_pairs",
+    "sample"};
+
+int dsmc_get_phase_times(dsmc_ctx *c, double *ms_out, int max_phases, int *n_phases,
+                         const char **names_out, int reset)
+{
+    if (c == nullptr || n_phases == nullptr || max_phases < 0)
+        return DSMC_ERR_ARGUMENT;
+    unsigned long long ns[PERSIST_PHASES];
+    CK(cudaMemcpyAsync(ns, c->d_phase_ns, sizeof(ns), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (reset)
+        CK(cudaMemsetAsync(c->d_phase_ns, 0, sizeof(ns), c->stream));
+    *n_phases = PERSIST_PHASES;
+    for (int k = 0; k < PERSIST_PHASES && k < max_phases; ++k) {
+        if (ms_out)
+            ms_out[k] = static_cast<double>(ns[k]) * 1e-6;
+        if (names_out)
+            names_out[k] = kPhaseNames[k];
+    }
+    return DSMC_OK;
+}
+
+int dsmc_grid_sync_probe(dsmc_ctx *c, int64_t wait_ns)
+{
+    if (c == nullptr || wait_ns < 0)
+        return DSMC_ERR_ARGUMENT;
+    CK(cudaMemsetAsync(c->d_gsync, 0, sizeof(GridSync), c->stream));
+    CK(cudaMemsetAsync(c->d_probe_err, 0, sizeof(int), c->stream));
+    k_grid_sync_probe<<<1, 32, 0, c->stream>>>(c->d_gsync, 1, static_cast<uint64_t>(wait_ns),
+                                               c->d_probe_err);
+    CK(cudaGetLastError());
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, c->d_probe_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return err;
 }
 
 int dsmc_autotune(dsmc_ctx *c, int steps_per_trial)

@@ -116,10 +116,11 @@ __device__ __forceinline__ void case_scan(int32_t *base, const int32_t *count_of
 // ---------------------------------------------------------------------------
 // It first clears the step's scratch counters and the look-back status
 // words of the cell scan (the first kernel of a step: nothing reads them
-// before), so the step needs no memset of its own.
-__global__ void k_plan(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
-                       int32_t *tmp, int32_t *itile_dead, uint64_t *cell_chain, int ncase,
-                       int init_mode, int *err)
+// before), so the step needs no memset of its own.  One CTA, any width.
+__device__ __forceinline__ void plan_step(const CaseDev *cases, CaseState *st, StepScratch *sc,
+                                          TileTables tt, int32_t *tmp, int32_t *itile_dead,
+                                          uint64_t *cell_chain, int ncase, int init_mode,
+                                          int *err)
 {
     {
         uint32_t *words = reinterpret_cast<uint32_t *>(sc);
@@ -198,6 +199,13 @@ __global__ void k_plan(const CaseDev *cases, CaseState *st, StepScratch *sc, Til
         st[i].move_tile0 = tt.move0[i];
         st[i].inject_tile0 = tt.inject0[i];
     }
+}
+
+__global__ void k_plan(const CaseDev *cases, CaseState *st, StepScratch *sc, TileTables tt,
+                       int32_t *tmp, int32_t *itile_dead, uint64_t *cell_chain, int ncase,
+                       int init_mode, int *err)
+{
+    plan_step(cases, st, sc, tt, tmp, itile_dead, cell_chain, ncase, init_mode, err);
 }
 
 // The impact branch of MoveParticles (Boundary.cpp:301-326) for slot q (global
@@ -462,17 +470,20 @@ template <class T> __host__ __device__ constexpr size_t move_smem()
     return sizeof(MoveStage<T>) * move_stages<T>();
 }
 
-template <class T>
-__global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
-    k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
-           Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
-           int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf,
-           uint32_t *__restrict__ near_list, int ncase, int *err)
+// The move tiles of block bx of nbx (tiles bx, bx + nbx, ...); smem_raw holds
+// S * sizeof(MoveStage<T>) bytes.  False when a staged copy never completed (reported;
+// the block's copies in flight were waited for, its barriers stay live).
+template <class T, int S = move_stages<T>()>
+__device__ __forceinline__ bool
+    move_tiles(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+               Slots<T> p, uint32_t *__restrict__ key, Cells cells,
+               int32_t *__restrict__ tile_in, int32_t *__restrict__ tile_dead,
+               uint32_t *__restrict__ obuf, uint32_t *__restrict__ near_list, int ncase, int *err,
+               unsigned char *smem_raw, int bx, int nbx)
 {
     static_assert(TILE == 1024, "near_list packs the slot in tile into 10 bits");
-    constexpr int S = move_stages<T>();
+    static_assert(S >= 2, "see the stage rule above");
     constexpr int NB = 3; // ballot buffers: a tile's are read until the next tile's barrier
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     MoveStage<T> *stage = reinterpret_cast<MoveStage<T> *>(smem_raw);
     __shared__ uint64_t bar[S];
     __shared__ CaseDev s_case; // constants of the current tile's case
@@ -512,8 +523,8 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
             mbar_init(&bar[i], 1);
         fence_mbar_init();
         for (int i = 0; i < S; ++i)
-            if (blockIdx.x + i * gridDim.x < total)
-                issue(blockIdx.x + i * gridDim.x, i);
+            if (bx + i * nbx < total)
+                issue(bx + i * nbx, i);
     }
     if (threadIdx.x < NB)
         s_nnear[threadIdx.x] = 0;
@@ -523,7 +534,7 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
     int64_t prev_gt = 0;
     int it = 0;
     for (;; ++it) {
-        const int t = blockIdx.x + it * gridDim.x;
+        const int t = bx + it * nbx;
         if (t >= total)
             break;
         const int sidx = it % S;
@@ -608,14 +619,14 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
             if (threadIdx.x == 0) {
                 report_error(err, DSMC_ERR_TIMEOUT);
                 for (int j = it; j < it + S; ++j)
-                    if (blockIdx.x + j * gridDim.x < total)
+                    if (bx + j * nbx < total)
                         mbar_wait(&bar[j % S], static_cast<uint32_t>((j / S) & 1));
             }
-            return;
+            return false;
         }
         if (threadIdx.x == 0) {
             fence_proxy_async_smem();
-            const int tn = t + S * gridDim.x;
+            const int tn = t + S * nbx;
             if (tn < total)
                 issue(tn, sidx);
         }
@@ -657,21 +668,38 @@ __global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
         __syncthreads();
         append((it + NB - 1) % NB, prev_gt);
     }
+    // Every copy issued was consumed: the barriers can be retired.
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < S; ++i)
+            mbar_inval(&bar[i]);
+    return true;
+}
+
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS, DSMC_MOVE_MIN_BLOCKS)
+    k_move(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+           Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
+           int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf,
+           uint32_t *__restrict__ near_list, int ncase, int *err)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    (void)move_tiles<T>(cases, st, sc, tt, p, key, cells, tile_in, tile_dead, obuf, near_list,
+                        ncase, err, smem_raw, blockIdx.x, gridDim.x);
 }
 
 // k_move_near: the exact MoveParticles body for the slots k_move queued
 // (near the box, or a cell index not certain from its estimate), then their
 // share of the tile counts, the out-of-range list and the drag diagnostics.
 template <class T>
-__global__ void __launch_bounds__(TILE_THREADS)
-    k_move_near(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc,
-                TileTables tt, Slots<T> p, uint32_t *__restrict__ key, Cells cells,
-                int32_t *__restrict__ tile_in, int32_t *__restrict__ tile_dead,
-                uint32_t *__restrict__ obuf, const uint32_t *__restrict__ near_list, int ncase,
-                int *err)
+__device__ __forceinline__ void
+    move_near(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+              Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
+              int32_t *__restrict__ tile_dead, uint32_t *__restrict__ obuf,
+              const uint32_t *__restrict__ near_list, int ncase, int *err, int bx, int nbx)
 {
     const uint32_t n = sc->near_count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = bx * blockDim.x + threadIdx.x; i < n; i += nbx * blockDim.x) {
         const uint32_t w = near_list[i];
         const int t = static_cast<int>(w >> 10);
         const int e = static_cast<int>(w & 1023u);
@@ -699,6 +727,18 @@ __global__ void __launch_bounds__(TILE_THREADS)
     }
 }
 
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_move_near(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc,
+                TileTables tt, Slots<T> p, uint32_t *__restrict__ key, Cells cells,
+                int32_t *__restrict__ tile_in, int32_t *__restrict__ tile_dead,
+                uint32_t *__restrict__ obuf, const uint32_t *__restrict__ near_list, int ncase,
+                int *err)
+{
+    move_near<T>(cases, st, sc, tt, p, key, cells, tile_in, tile_dead, obuf, near_list, ncase,
+                 err, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // k_inject: GenerateNewParticles (Boundary.cpp:60-92) for every strip of every
 // case, written after the case's n_old slots.  In init mode the single strip
@@ -706,11 +746,13 @@ __global__ void __launch_bounds__(TILE_THREADS)
 // without the pre-move, and the removal predicate is InsideBox
 // (RemoveParticlesInsideBox, Geometry.cpp:231-247).
 // ---------------------------------------------------------------------------
+// Inject units are dealt by ticket: any number of CTAs of TILE_THREADS.
 template <class T>
-__global__ void __launch_bounds__(TILE_THREADS)
-    k_inject(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
-             Slots<T> p, uint32_t *__restrict__ key, Cells cells,
-             int32_t *__restrict__ itile_dead, uint32_t *__restrict__ obuf, int ncase, int *err)
+__device__ __forceinline__ void
+    inject_units(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+                 Slots<T> p, uint32_t *__restrict__ key, Cells cells,
+                 int32_t *__restrict__ itile_dead, uint32_t *__restrict__ obuf, int ncase,
+                 int *err)
 {
     __shared__ int s_unit;
     const int init_mode = sc->init_mode;
@@ -804,6 +846,15 @@ __global__ void __launch_bounds__(TILE_THREADS)
     }
 }
 
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_inject(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+             Slots<T> p, uint32_t *__restrict__ key, Cells cells,
+             int32_t *__restrict__ itile_dead, uint32_t *__restrict__ obuf, int ncase, int *err)
+{
+    inject_units<T>(cases, st, sc, tt, p, key, cells, itile_dead, obuf, ncase, err);
+}
+
 // ---------------------------------------------------------------------------
 // Threads of a CTA of the per-case scans (also k_warm_scan).
 constexpr int SCAN_THREADS = 1024;
@@ -823,26 +874,28 @@ __device__ __forceinline__ int32_t seq_count(const int32_t *a, int na, const int
 }
 
 // Sum of counts [0, c0) of the sequence, in every thread.
+template <int NT = SCAN_THREADS>
 __device__ __forceinline__ int32_t seq_before(const int32_t *a, int na, const int32_t *b, int c0)
 {
     int32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0; // four loads in flight per round
     int i = threadIdx.x;
-    for (; i + 3 * SCAN_THREADS < c0; i += 4 * SCAN_THREADS) {
+    for (; i + 3 * NT < c0; i += 4 * NT) {
         s0 += seq_count(a, na, b, i);
-        s1 += seq_count(a, na, b, i + SCAN_THREADS);
-        s2 += seq_count(a, na, b, i + 2 * SCAN_THREADS);
-        s3 += seq_count(a, na, b, i + 3 * SCAN_THREADS);
+        s1 += seq_count(a, na, b, i + NT);
+        s2 += seq_count(a, na, b, i + 2 * NT);
+        s3 += seq_count(a, na, b, i + 3 * NT);
     }
-    for (; i < c0; i += SCAN_THREADS)
+    for (; i < c0; i += NT)
         s0 += seq_count(a, na, b, i);
     int32_t tot;
-    (void)block_exclusive<int32_t, SCAN_THREADS>(s0 + s1 + s2 + s3, tot);
+    (void)block_exclusive<int32_t, NT>(s0 + s1 + s2 + s3, tot);
     return tot;
 }
 
-// Exclusive prefixes of chunk [c0, c0 + SCAN_CHUNK) of the sequence of
+// Exclusive prefixes of chunk [c0, c0 + NT * SCAN_VEC) of the sequence of
 // length n (from `carry`) into oa / ob; returns the prefix of each of this
 // thread's counts in pre[] and carry plus the chunk's total.
+template <int NT = SCAN_THREADS>
 __device__ __forceinline__ int32_t seq_chunk(const int32_t *a, int32_t *oa, int na,
                                              const int32_t *b, int32_t *ob, int n, int c0,
                                              int32_t carry, int32_t pre[SCAN_VEC])
@@ -856,7 +909,7 @@ __device__ __forceinline__ int32_t seq_chunk(const int32_t *a, int32_t *oa, int 
         sum += v[k];
     }
     int32_t tot;
-    int32_t run = carry + block_exclusive<int32_t, SCAN_THREADS>(sum, tot);
+    int32_t run = carry + block_exclusive<int32_t, NT>(sum, tot);
 #pragma unroll
     for (int k = 0; k < SCAN_VEC; ++k) {
         const int i = i0 + k;
@@ -875,32 +928,43 @@ __device__ __forceinline__ int32_t seq_chunk(const int32_t *a, int32_t *oa, int 
 // k_dead_scan: grid (chunks, cases).  Exclusive prefix of the removed-slot
 // counts of a case's move tiles, then of its inject tiles (their ranks
 // continue the count, in slot order); sets dead_old and dead_total.
+// dead_scan_chunk: chunk `chunk` of case `ci` by a CTA of NT threads.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(SCAN_THREADS)
-    k_dead_scan(CaseState *st, const int32_t *tile_dead, int32_t *tile_dprefix,
-                const int32_t *itile_dead, int32_t *itile_dprefix)
+template <int NT>
+__device__ __forceinline__ void dead_scan_chunk(CaseState *st, const int32_t *tile_dead,
+                                                int32_t *tile_dprefix, const int32_t *itile_dead,
+                                                int32_t *itile_dprefix, int chunk, int ci)
 {
-    CaseState &s = st[blockIdx.y];
+    constexpr int CHUNK = NT * SCAN_VEC;
+    CaseState &s = st[ci];
     const int na = s.n_move_tiles;
     const int n = na + s.n_inject_tiles;
-    const int c0 = static_cast<int>(blockIdx.x) * SCAN_CHUNK;
+    const int c0 = chunk * CHUNK;
     if (c0 >= n)
         return; // uniform over the CTA
     const int32_t *a = tile_dead + s.move_tile0, *b = itile_dead + s.inject_tile0;
-    const int32_t carry = seq_before(a, na, b, c0);
+    const int32_t carry = seq_before<NT>(a, na, b, c0);
     int32_t pre[SCAN_VEC];
-    const int32_t total = seq_chunk(a, tile_dprefix + s.move_tile0, na, b,
-                                    itile_dprefix + s.inject_tile0, n, c0, carry, pre);
+    const int32_t total = seq_chunk<NT>(a, tile_dprefix + s.move_tile0, na, b,
+                                        itile_dprefix + s.inject_tile0, n, c0, carry, pre);
     const int i0 = c0 + static_cast<int>(threadIdx.x) * SCAN_VEC;
 #pragma unroll
     for (int k = 0; k < SCAN_VEC; ++k)
         if (i0 + k == na && na < n) // the first inject tile: all move tiles before it
             s.dead_old = pre[k];
-    if (c0 + SCAN_CHUNK >= n && threadIdx.x == 0) { // the last chunk
+    if (c0 + CHUNK >= n && threadIdx.x == 0) { // the last chunk
         s.dead_total = total;
         if (na == n)
             s.dead_old = total;
     }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS)
+    k_dead_scan(CaseState *st, const int32_t *tile_dead, int32_t *tile_dprefix,
+                const int32_t *itile_dead, int32_t *itile_dprefix)
+{
+    dead_scan_chunk<SCAN_THREADS>(st, tile_dead, tile_dprefix, itile_dead, itile_dprefix,
+                                  blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -957,21 +1021,22 @@ __device__ void plan_tail(const CaseDev *cases, CaseState *st, StepScratch *sc, 
 // k_holes: the removed-slot list in slot order (hole_pos, and the old cell of
 // each removed slot in hole_oc), from the tiles that have removed slots.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TILE_THREADS)
-    k_holes(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
-            const uint32_t *__restrict__ key, const int32_t *tile_dead,
-            const int32_t *tile_dprefix, const int32_t *itile_dead, const int32_t *itile_dprefix,
-            int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc, int32_t *tmp,
-            uint64_t *tail_chain, int ncase)
+__device__ __forceinline__ void
+    holes_blocks(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+                 const uint32_t *__restrict__ key, const int32_t *tile_dead,
+                 const int32_t *tile_dprefix, const int32_t *itile_dead,
+                 const int32_t *itile_dprefix, int32_t *__restrict__ hole_pos,
+                 int32_t *__restrict__ hole_oc, int32_t *tmp, uint64_t *tail_chain, int ncase,
+                 int bx, int nbx)
 {
     __shared__ bool s_last;
     __shared__ int s_list[TILE_THREADS];
     const int n_move = sc->total_move_tiles;
     const int total = n_move + sc->total_inject_tiles;
-    for (int T0 = blockIdx.x; T0 < total; T0 += gridDim.x * TILE_THREADS) {
+    for (int T0 = bx; T0 < total; T0 += nbx * TILE_THREADS) {
         // The counts of this CTA's next TILE_THREADS tiles are read at once
         // and the tiles with removed slots listed: most tiles have none.
-        const int Tm = T0 + static_cast<int>(threadIdx.x) * gridDim.x;
+        const int Tm = T0 + static_cast<int>(threadIdx.x) * nbx;
         int cnt = 0;
         if (Tm < total)
             cnt = Tm < n_move ? tile_dead[Tm] : itile_dead[Tm - n_move];
@@ -1018,7 +1083,7 @@ __global__ void __launch_bounds__(TILE_THREADS)
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0)
-        s_last = atomicAdd(&sc->holes_done, 1u) == gridDim.x - 1;
+        s_last = atomicAdd(&sc->holes_done, 1u) == static_cast<unsigned>(nbx - 1);
     __syncthreads();
     if (!s_last)
         return;
@@ -1026,17 +1091,30 @@ __global__ void __launch_bounds__(TILE_THREADS)
     plan_tail(cases, st, sc, tt, hole_pos, tmp, tail_chain, ncase);
 }
 
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_holes(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+            const uint32_t *__restrict__ key, const int32_t *tile_dead,
+            const int32_t *tile_dprefix, const int32_t *itile_dead, const int32_t *itile_dprefix,
+            int32_t *__restrict__ hole_pos, int32_t *__restrict__ hole_oc, int32_t *tmp,
+            uint64_t *tail_chain, int ncase)
+{
+    holes_blocks(cases, st, sc, tt, key, tile_dead, tile_dprefix, itile_dead, itile_dprefix,
+                 hole_pos, hole_oc, tmp, tail_chain, ncase, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // k_tail: the swap-with-last removal (Boundary.cpp:181-202) as a permutation.
 // The r-th surviving slot of the tail [K, n_total), counted from its end,
 // moves into the r-th hole.
 // ---------------------------------------------------------------------------
+// Tail tiles are dealt by ticket: any number of CTAs of TILE_THREADS.
 template <class T>
-__global__ void __launch_bounds__(TILE_THREADS)
-    k_tail(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
-           Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
-           uint64_t *lb, const int32_t *__restrict__ hole_pos,
-           const int32_t *__restrict__ hole_oc, uint32_t *__restrict__ obuf, int ncase, int *err)
+__device__ __forceinline__ void
+    tail_tiles(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+               Slots<T> p, uint32_t *__restrict__ key, Cells cells,
+               int32_t *__restrict__ tile_in, uint64_t *lb, const int32_t *__restrict__ hole_pos,
+               const int32_t *__restrict__ hole_oc, uint32_t *__restrict__ obuf, int ncase,
+               int *err)
 {
     __shared__ int s_tile;
     __shared__ uint64_t s_excl;
@@ -1128,6 +1206,17 @@ __global__ void __launch_bounds__(TILE_THREADS)
     }
 }
 
+template <class T>
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_tail(const CaseDev *__restrict__ cases, CaseState *st, StepScratch *sc, TileTables tt,
+           Slots<T> p, uint32_t *__restrict__ key, Cells cells, int32_t *__restrict__ tile_in,
+           uint64_t *lb, const int32_t *__restrict__ hole_pos,
+           const int32_t *__restrict__ hole_oc, uint32_t *__restrict__ obuf, int ncase, int *err)
+{
+    tail_tiles<T>(cases, st, sc, tt, p, key, cells, tile_in, lb, hole_pos, hole_oc, obuf, ncase,
+                  err);
+}
+
 // ---------------------------------------------------------------------------
 // k_cell_scan: per case, exclusive sums over its cells of the in-range and
 // out-of-range counts (Fin, ostart) and the new cell starts.
@@ -1141,9 +1230,10 @@ __global__ void __launch_bounds__(TILE_THREADS)
 constexpr int CELL_VEC = DSMC_CELL_VEC;
 constexpr int CELL_TILE = TILE_THREADS * CELL_VEC;
 
-__global__ void __launch_bounds__(TILE_THREADS)
-    k_cell_scan(const CaseDev *__restrict__ cases, StepScratch *sc, TileTables tt, Cells cells,
-                int new_side, uint64_t *lb, int ncase, int *err)
+// Cell tiles are dealt by ticket: any number of CTAs of TILE_THREADS.
+__device__ __forceinline__ void cell_scan_tiles(const CaseDev *__restrict__ cases,
+                                                StepScratch *sc, TileTables tt, Cells cells,
+                                                int new_side, uint64_t *lb, int ncase, int *err)
 {
     __shared__ int s_tile;
     int32_t *start = start_of(cells, new_side);
@@ -1207,23 +1297,37 @@ __global__ void __launch_bounds__(TILE_THREADS)
     }
 }
 
+__global__ void __launch_bounds__(TILE_THREADS)
+    k_cell_scan(const CaseDev *__restrict__ cases, StepScratch *sc, TileTables tt, Cells cells,
+                int new_side, uint64_t *lb, int ncase, int *err)
+{
+    cell_scan_tiles(cases, sc, tt, cells, new_side, lb, ncase, err);
+}
+
 // ---------------------------------------------------------------------------
 // k_tile_scan: grid (chunks, cases).  Exclusive prefix of the in-range
 // counts of a case's move tiles into tile_prefix.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(SCAN_THREADS)
-    k_tile_scan(const CaseState *st, const int32_t *tile_in, int32_t *tile_prefix)
+template <int NT>
+__device__ __forceinline__ void tile_scan_chunk(const CaseState *st, const int32_t *tile_in,
+                                                int32_t *tile_prefix, int chunk, int ci)
 {
-    const CaseState &s = st[blockIdx.y];
+    const CaseState &s = st[ci];
     const int n = s.n_move_tiles;
-    const int c0 = static_cast<int>(blockIdx.x) * SCAN_CHUNK;
+    const int c0 = chunk * NT * SCAN_VEC;
     if (c0 >= n)
         return; // uniform over the CTA
     const int32_t *a = tile_in + s.move_tile0;
-    const int32_t carry = seq_before(a, n, a, c0);
+    const int32_t carry = seq_before<NT>(a, n, a, c0);
     int32_t pre[SCAN_VEC];
-    (void)seq_chunk(a, tile_prefix + s.move_tile0, n, a, tile_prefix + s.move_tile0, n, c0,
-                    carry, pre);
+    (void)seq_chunk<NT>(a, tile_prefix + s.move_tile0, n, a, tile_prefix + s.move_tile0, n, c0,
+                        carry, pre);
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS)
+    k_tile_scan(const CaseState *st, const int32_t *tile_in, int32_t *tile_prefix)
+{
+    tile_scan_chunk<SCAN_THREADS>(st, tile_in, tile_prefix, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -1234,15 +1338,17 @@ __global__ void __launch_bounds__(SCAN_THREADS)
 // accesses (list entry, key, counter, list slot) for all of them before the
 // next, so that their memory latencies overlap.
 constexpr int OLIST_BATCH = 4;
-__global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
-                        const StepScratch *sc, const uint32_t *__restrict__ obuf,
-                        const uint32_t *__restrict__ key, Cells cells,
-                        int32_t *__restrict__ olist, const int64_t *__restrict__ pbases,
-                        int ncase, int *err)
+__device__ __forceinline__ void olist_blocks(const CaseDev *__restrict__ cases,
+                                             const CaseState *st, const StepScratch *sc,
+                                             const uint32_t *__restrict__ obuf,
+                                             const uint32_t *__restrict__ key, Cells cells,
+                                             int32_t *__restrict__ olist,
+                                             const int64_t *__restrict__ pbases, int ncase,
+                                             int *err, int bx, int nbx)
 {
     const uint32_t n = sc->obuf_count;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n;
+    const uint32_t stride = nbx * blockDim.x;
+    for (uint32_t i0 = bx * blockDim.x + threadIdx.x; i0 < n;
          i0 += OLIST_BATCH * stride) {
         uint32_t g[OLIST_BATCH], kw[OLIST_BATCH];
         int64_t q[OLIST_BATCH];
@@ -1295,6 +1401,16 @@ __global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
     }
 }
 
+__global__ void k_olist(const CaseDev *__restrict__ cases, const CaseState *st,
+                        const StepScratch *sc, const uint32_t *__restrict__ obuf,
+                        const uint32_t *__restrict__ key, Cells cells,
+                        int32_t *__restrict__ olist, const int64_t *__restrict__ pbases,
+                        int ncase, int *err)
+{
+    olist_blocks(cases, st, sc, obuf, key, cells, olist, pbases, ncase, err, blockIdx.x,
+                 gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // k_cell_fix: per cell, orders its out-of-range list by slot, gives each of
 // those particles its final slot (written into its key word, bit 31 clear),
@@ -1320,14 +1436,15 @@ __device__ __forceinline__ int fix_place(int32_t q, int j, int32_t start, int32_
 // per step) are sorted in registers; longer ones in place.
 constexpr int FIX_REG = 8;
 
-__global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *st,
-                           TileTables tt, Cells cells, int old_side, uint32_t *__restrict__ key,
-                           int32_t *__restrict__ olist, int total_cells, int ncase, int *err)
+__device__ __forceinline__ void cell_fix_blocks(const CaseDev *__restrict__ cases,
+                                                const CaseState *st, TileTables tt, Cells cells,
+                                                int old_side, uint32_t *__restrict__ key,
+                                                int32_t *__restrict__ olist, int total_cells,
+                                                int ncase, int *err, int bx, int nbx)
 {
     const int32_t *os = start_of(cells, old_side);
     const int32_t *ns = start_of(cells, old_side ^ 1);
-    for (int cg = blockIdx.x * blockDim.x + threadIdx.x; cg < total_cells;
-         cg += gridDim.x * blockDim.x) {
+    for (int cg = bx * blockDim.x + threadIdx.x; cg < total_cells; cg += nbx * blockDim.x) {
         const int ci = case_of(tt.cellbase, ncase, cg);
         const CaseDev &c = cases[ci];
         const int cl = cg - c.cbase;
@@ -1388,6 +1505,14 @@ __global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *s
     }
 }
 
+__global__ void k_cell_fix(const CaseDev *__restrict__ cases, const CaseState *st,
+                           TileTables tt, Cells cells, int old_side, uint32_t *__restrict__ key,
+                           int32_t *__restrict__ olist, int total_cells, int ncase, int *err)
+{
+    cell_fix_blocks(cases, st, tt, cells, old_side, key, olist, total_cells, ncase, err,
+                    blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // k_scatter: moves every particle of slots [0, K) to its sorted slot.  An
 // in-range particle goes to base_in[cell] + (number of in-range particles at
@@ -1425,14 +1550,17 @@ template <class T> __host__ __device__ constexpr size_t scatter_smem()
     return sizeof(ScatterStage<T>) * scatter_stages<T>();
 }
 
-template <class T>
-__global__ void __launch_bounds__(SC_THREADS)
-    k_scatter(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt,
-              Slots<T> src, Slots<T> dst, const uint32_t *__restrict__ key, Cells cells,
-              const int32_t *__restrict__ tile_prefix, int ncase, int *err)
+// The scatter tiles of block bx of nbx; smem_raw holds
+// S * sizeof(ScatterStage<T>) bytes.  False when a staged copy never completed (reported; the copies in
+// flight were waited for, the barriers stay live).
+template <class T, int S = scatter_stages<T>()>
+__device__ __forceinline__ bool
+    scatter_tiles(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt,
+                  Slots<T> src, Slots<T> dst, const uint32_t *__restrict__ key, Cells cells,
+                  const int32_t *__restrict__ tile_prefix, int ncase, int *err,
+                  unsigned char *smem_raw, int bx, int nbx)
 {
-    constexpr int S = scatter_stages<T>();
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    static_assert(S >= 2, "see the stage rule above");
     ScatterStage<T> *stage = reinterpret_cast<ScatterStage<T> *>(smem_raw);
     __shared__ uint64_t bar[S];
     __shared__ int s_cnt[2][32]; // in-range counts per (iteration, warp), two buffers
@@ -1462,12 +1590,12 @@ __global__ void __launch_bounds__(SC_THREADS)
     __syncthreads();
     int issued = 0;
     if (threadIdx.x == 0)
-        for (; issued < S && blockIdx.x + issued * gridDim.x < total; ++issued)
-            issue(blockIdx.x + issued * gridDim.x, issued);
+        for (; issued < S && bx + issued * nbx < total; ++issued)
+            issue(bx + issued * nbx, issued);
 
     int it = 0;
     bool failed = false;
-    for (int t = blockIdx.x; t < total; t += gridDim.x, ++it) {
+    for (int t = bx; t < total; t += nbx, ++it) {
         const int sidx = it % S;
         const bool ok = mbar_wait(&bar[sidx], static_cast<uint32_t>((it / S) & 1));
         const int ci = case_of(tt.scatter0, ncase, t);
@@ -1500,7 +1628,7 @@ __global__ void __launch_bounds__(SC_THREADS)
         }
         if (threadIdx.x == 0) {
             fence_proxy_async_smem();
-            const int tn = t + S * gridDim.x;
+            const int tn = t + S * nbx;
             if (tn < total) {
                 issue(tn, sidx);
                 ++issued;
@@ -1555,7 +1683,25 @@ __global__ void __launch_bounds__(SC_THREADS)
             for (int j = it; j < issued; ++j)
                 mbar_wait(&bar[j % S], static_cast<uint32_t>((j / S) & 1));
         }
+        return false;
     }
+    // Every copy issued was consumed: the barriers can be retired.
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < S; ++i)
+            mbar_inval(&bar[i]);
+    return true;
+}
+
+template <class T>
+__global__ void __launch_bounds__(SC_THREADS)
+    k_scatter(const CaseDev *__restrict__ cases, const CaseState *st, TileTables tt,
+              Slots<T> src, Slots<T> dst, const uint32_t *__restrict__ key, Cells cells,
+              const int32_t *__restrict__ tile_prefix, int ncase, int *err)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    (void)scatter_tiles<T>(cases, st, tt, src, dst, key, cells, tile_prefix, ncase, err,
+                           smem_raw, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1657,13 +1803,14 @@ __device__ __forceinline__ int ntc_candidates(const CaseDev &c, int n, int nn, d
     return ncc;
 }
 
-__global__ void __launch_bounds__(256)
-    k_collide_select(const CaseDev *__restrict__ cases, const CaseState *st, StepScratch *sc,
-                     TileTables tt, Cells cells, int side, uint32_t *__restrict__ coll_list,
-                     int total_cells, int ncase)
+__device__ __forceinline__ void
+    collide_select_blocks(const CaseDev *__restrict__ cases, const CaseState *st,
+                          StepScratch *sc, TileTables tt, Cells cells, int side,
+                          uint32_t *__restrict__ coll_list, int total_cells, int ncase, int bx,
+                          int nbx)
 {
     const int32_t *start = start_of(cells, side);
-    for (int base = blockIdx.x * blockDim.x; base < total_cells; base += gridDim.x * blockDim.x) {
+    for (int base = bx * blockDim.x; base < total_cells; base += nbx * blockDim.x) {
         const int cg = base + threadIdx.x;
         bool listed = false;
         if (cg < total_cells) {
@@ -1692,16 +1839,24 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+__global__ void __launch_bounds__(256)
+    k_collide_select(const CaseDev *__restrict__ cases, const CaseState *st, StepScratch *sc,
+                     TileTables tt, Cells cells, int side, uint32_t *__restrict__ coll_list,
+                     int total_cells, int ncase)
+{
+    collide_select_blocks(cases, st, sc, tt, cells, side, coll_list, total_cells, ncase,
+                          blockIdx.x, gridDim.x);
+}
+
 template <class T>
-__global__ void __launch_bounds__(128)
-    k_collide_pairs(const CaseDev *__restrict__ cases, CaseState *st, const StepScratch *sc,
-                    TileTables tt, Slots<T> p, Cells cells, int side,
-                    const uint32_t *__restrict__ coll_list, int ncase)
+__device__ __forceinline__ void
+    collide_pairs_blocks(const CaseDev *__restrict__ cases, CaseState *st,
+                         const StepScratch *sc, TileTables tt, Slots<T> p, Cells cells, int side,
+                         const uint32_t *__restrict__ coll_list, int ncase, int bx, int nbx)
 {
     const int32_t *start = start_of(cells, side);
     const uint32_t count = sc->coll_count;
-    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count;
-         w += gridDim.x * blockDim.x) {
+    for (uint32_t w = bx * blockDim.x + threadIdx.x; w < count; w += nbx * blockDim.x) {
         const int cg = static_cast<int>(coll_list[w]);
         const int ci = case_of(tt.cellbase, ncase, cg);
         const CaseDev &c = cases[ci];
@@ -1723,43 +1878,69 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+template <class T>
+__global__ void __launch_bounds__(128)
+    k_collide_pairs(const CaseDev *__restrict__ cases, CaseState *st, const StepScratch *sc,
+                    TileTables tt, Slots<T> p, Cells cells, int side,
+                    const uint32_t *__restrict__ coll_list, int ncase)
+{
+    collide_pairs_blocks<T>(cases, st, sc, tt, p, cells, side, coll_list, ncase, blockIdx.x,
+                            gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // k_sample: Sampling's accumulation (Sampling.cpp:14-31) in the reference's
 // order: each sum of a cell is made by one thread that walks the cell's
 // particles sequentially, so every FP64 sum is bit-identical to the
-// reference's.  The velocities of a block of SAMPLE_CELLS cells are one
-// contiguous slot range, staged in shared memory
-// by bulk asynchronous copies (SAMPLE_STAGES per CTA; with one stage, which
-// measured fastest, more CTAs fit on an SM and overlap each other's copies).
-// A block whose range exceeds a stage is read from global memory directly.
+// reference's.  A sample block is CELLS consecutive cells of one case with
+// SPLIT threads per cell: thread t takes cell t % CELLS and part t / CELLS
+// of its sums (each part a fixed set of sums, so a thread's chains are
+// short and independent).  The velocities of a block are one contiguous
+// slot range, staged in shared memory by bulk asynchronous copies, S stages
+// per CTA; a block whose range exceeds a stage is read from global memory
+// directly.  The step graph's k_sample: SAMPLE_CELLS x SAMPLE_SPLIT threads,
+// SAMPLE_STAGES stages (one stage measured fastest: more CTAs fit on an SM
+// and overlap each other's copies); the persistent step uses its own shape.
 // ---------------------------------------------------------------------------
 constexpr int SAMPLE_STAGES = DSMC_SAMPLE_STAGES;
 constexpr int SAMPLE_UNROLL = DSMC_SAMPLE_UNROLL;
-// Sample blocks of SAMPLE_CELLS cells (a half of a collision block), two
-// threads per cell: the warps of the first half of the CTA sum NP, V and
-// VV00 .. VV11 of their cells, those of the second half VV12, VV22 and V2V.
-// Every sum stays with one thread, in slot order; the split halves the chain
-// each thread walks.
-constexpr int SAMPLE_CELLS = 64;
-constexpr int SAMPLE_SUB = COLLIDE_CELLS / SAMPLE_CELLS; // sample blocks per collision block
-constexpr int SAMPLE_THREADS = 2 * SAMPLE_CELLS;
-static_assert(SAMPLE_CELLS % 32 == 0 && COLLIDE_CELLS % SAMPLE_CELLS == 0,
-              "whole warps per half, whole sample blocks per collision block");
-template <class T> __host__ __device__ constexpr int sample_pcl()
+#ifndef DSMC_SAMPLE_CELLS
+#define DSMC_SAMPLE_CELLS 64
+#endif
+#ifndef DSMC_SAMPLE_SPLIT
+#define DSMC_SAMPLE_SPLIT 2
+#endif
+constexpr int SAMPLE_CELLS = DSMC_SAMPLE_CELLS;
+constexpr int SAMPLE_SPLIT = DSMC_SAMPLE_SPLIT;
+constexpr int SAMPLE_THREADS = SAMPLE_SPLIT * SAMPLE_CELLS;
+#ifndef DSMC_SAMPLE_MIN_BLOCKS // k_sample's register budget: 1024 threads per SM
+#define DSMC_SAMPLE_MIN_BLOCKS (1024 / SAMPLE_THREADS)
+#endif
+template <int CELLS> __host__ __device__ constexpr int sample_sub()
 {
-    return 12288 / sizeof(T) / SAMPLE_SUB;
+    static_assert(CELLS % 32 == 0 && COLLIDE_CELLS % CELLS == 0,
+                  "whole warps per part, whole sample blocks per collision block");
+    return COLLIDE_CELLS / CELLS; // sample blocks per collision block
+}
+// Staging capacity of a block: 24 (FP32) or 12 (FP64) particles per cell.
+template <class T, int CELLS = SAMPLE_CELLS> __host__ __device__ constexpr int sample_pcl()
+{
+    return 12288 / sizeof(T) / sample_sub<CELLS>();
 }
 // First cell (in its case) of sample block b of case ci.
+template <int CELLS>
 __device__ __forceinline__ int sample_cell0(const TileTables &tt, int ci, int b)
 {
-    return (b / SAMPLE_SUB - tt.cblock0[ci]) * COLLIDE_CELLS + (b % SAMPLE_SUB) * SAMPLE_CELLS;
+    constexpr int SUB = sample_sub<CELLS>();
+    return (b / SUB - tt.cblock0[ci]) * COLLIDE_CELLS + (b % SUB) * CELLS;
 }
-template <class T> struct SampleStage {
-    T v[3][sample_pcl<T>() + 16 / sizeof(T)];
+template <class T, int CELLS = SAMPLE_CELLS> struct SampleStage {
+    T v[3][sample_pcl<T, CELLS>() + 16 / sizeof(T)];
 };
-template <class T> __host__ __device__ constexpr size_t sample_smem()
+template <class T, int CELLS = SAMPLE_CELLS, int S = SAMPLE_STAGES>
+__host__ __device__ constexpr size_t sample_smem()
 {
-    return sizeof(SampleStage<T>) * SAMPLE_STAGES;
+    return sizeof(SampleStage<T, CELLS>) * S;
 }
 
 // End of the step (Simulation.cpp:160-161) and Sampling's counters
@@ -1805,88 +1986,144 @@ __device__ __forceinline__ void finish_cases(const CaseDev *cases, CaseState *st
     }
 }
 
-// One particle's terms of the moment sums (Sampling.cpp:24-30), split into
-// the two halves of a cell's threads (add0: NP's partner sums V, VV00, VV01,
-// VV02, VV11; add1: V2V, VV12, VV22).  FP64 velocities: products rounded,
-// then added.
-__device__ __forceinline__ void sample_add0(double a[ACC_NC], double v0, double v1, double v2)
+// The part of a cell's threads that owns moment m, SPLIT threads per cell:
+//   2: NP, V, VV00, VV01, VV02, VV11 | VV12, VV22, V2V
+//   4: NP, V | VV00, VV01, VV02 | VV11, VV12, VV22 | V2V
+__host__ __device__ constexpr int sample_part_of(int split, int m)
 {
-    a[ACC_V0] += v0;
-    a[ACC_V1] += v1;
-    a[ACC_V2] += v2;
-    a[ACC_VV00] += v0 * v0;
-    a[ACC_VV01] += v0 * v1;
-    a[ACC_VV02] += v0 * v2;
-    a[ACC_VV11] += v1 * v1;
-}
-__device__ __forceinline__ void sample_add1(double a[ACC_NC], double v0, double v1, double v2)
-{
-    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
-    a[ACC_V2V0] += vv * v0;
-    a[ACC_V2V1] += vv * v1;
-    a[ACC_V2V2] += vv * v2;
-    a[ACC_VV12] += v1 * v2;
-    a[ACC_VV22] += v2 * v2;
-}
-// FP32 velocities: the product of two floats is exact in FP64 (24 + 24
-// significand bits), so s + u * v rounds once either way and a fused
-// multiply-add gives the same bits as the separate product and sum, with one
-// FP64 operation instead of two.  vv * v is not exact and keeps its rounding.
-__device__ __forceinline__ void sample_add0(double a[ACC_NC], float f0, float f1, float f2)
-{
-    const double v0 = f0, v1 = f1, v2 = f2;
-    a[ACC_V0] += v0;
-    a[ACC_V1] += v1;
-    a[ACC_V2] += v2;
-    a[ACC_VV00] += v0 * v0;
-    a[ACC_VV01] = __fma_rn(v0, v1, a[ACC_VV01]);
-    a[ACC_VV02] = __fma_rn(v0, v2, a[ACC_VV02]);
-    a[ACC_VV11] = __fma_rn(v1, v1, a[ACC_VV11]);
-}
-__device__ __forceinline__ void sample_add1(double a[ACC_NC], float f0, float f1, float f2)
-{
-    const double v0 = f0, v1 = f1, v2 = f2;
-    const double vv = __fma_rn(v2, v2, __fma_rn(v1, v1, v0 * v0));
-    a[ACC_V2V0] += vv * v0;
-    a[ACC_V2V1] += vv * v1;
-    a[ACC_V2V2] += vv * v2;
-    a[ACC_VV12] = __fma_rn(v1, v2, a[ACC_VV12]);
-    a[ACC_VV22] = __fma_rn(v2, v2, a[ACC_VV22]);
+    return split == 2 ? (m <= ACC_VV11 ? 0 : 1)
+                      : (m <= ACC_V2 ? 0 : m <= ACC_VV02 ? 1 : m <= ACC_VV22 ? 2 : 3);
 }
 
-template <class T>
-__global__ void __launch_bounds__(SAMPLE_THREADS)
-    k_sample(const CaseDev *__restrict__ cases, CaseState *st, TileTables tt, Slots<T> p,
-             Cells cells, int side, int ncase, int finish, dsmc_counters *rec, int *err)
+// One particle's terms (Sampling.cpp:24-30) of the sums that part P owns.
+// FP64 velocities: products rounded, then added.  FP32 velocities: the
+// product of two floats is exact in FP64 (24 + 24 significand bits), so
+// s + u * v rounds once either way and a fused multiply-add gives the same
+// bits as the separate product and sum, with one FP64 operation instead of
+// two; vv * v is not exact and keeps its rounding.  Either way every sum has
+// the same bits whichever part layout computes it.
+template <int SPLIT, int P>
+__device__ __forceinline__ void sample_add(double a[ACC_NC], double v0, double v1, double v2)
 {
-    if (finish && blockIdx.x == 0)
+#define DSMC_OWN(m) (sample_part_of(SPLIT, m) == P)
+    if (DSMC_OWN(ACC_V0)) {
+        a[ACC_V0] += v0;
+        a[ACC_V1] += v1;
+        a[ACC_V2] += v2;
+    }
+    if (DSMC_OWN(ACC_VV00))
+        a[ACC_VV00] += v0 * v0;
+    if (DSMC_OWN(ACC_VV01))
+        a[ACC_VV01] += v0 * v1;
+    if (DSMC_OWN(ACC_VV02))
+        a[ACC_VV02] += v0 * v2;
+    if (DSMC_OWN(ACC_VV11))
+        a[ACC_VV11] += v1 * v1;
+    if (DSMC_OWN(ACC_VV12))
+        a[ACC_VV12] += v1 * v2;
+    if (DSMC_OWN(ACC_VV22))
+        a[ACC_VV22] += v2 * v2;
+    if (DSMC_OWN(ACC_V2V0)) {
+        const double vv = v0 * v0 + v1 * v1 + v2 * v2;
+        a[ACC_V2V0] += vv * v0;
+        a[ACC_V2V1] += vv * v1;
+        a[ACC_V2V2] += vv * v2;
+    }
+}
+template <int SPLIT, int P>
+__device__ __forceinline__ void sample_add(double a[ACC_NC], float f0, float f1, float f2)
+{
+    const double v0 = f0, v1 = f1, v2 = f2;
+    if (DSMC_OWN(ACC_V0)) {
+        a[ACC_V0] += v0;
+        a[ACC_V1] += v1;
+        a[ACC_V2] += v2;
+    }
+    if (DSMC_OWN(ACC_VV00))
+        a[ACC_VV00] += v0 * v0;
+    if (DSMC_OWN(ACC_VV01))
+        a[ACC_VV01] = __fma_rn(v0, v1, a[ACC_VV01]);
+    if (DSMC_OWN(ACC_VV02))
+        a[ACC_VV02] = __fma_rn(v0, v2, a[ACC_VV02]);
+    if (DSMC_OWN(ACC_VV11))
+        a[ACC_VV11] = __fma_rn(v1, v1, a[ACC_VV11]);
+    if (DSMC_OWN(ACC_VV12))
+        a[ACC_VV12] = __fma_rn(v1, v2, a[ACC_VV12]);
+    if (DSMC_OWN(ACC_VV22))
+        a[ACC_VV22] = __fma_rn(v2, v2, a[ACC_VV22]);
+    if (DSMC_OWN(ACC_V2V0)) {
+        const double vv = __fma_rn(v2, v2, __fma_rn(v1, v1, v0 * v0));
+        a[ACC_V2V0] += vv * v0;
+        a[ACC_V2V1] += vv * v1;
+        a[ACC_V2V2] += vv * v2;
+    }
+#undef DSMC_OWN
+}
+
+// Part P's sums of one cell of n particles (velocities vx, vy, vz, in slot
+// order): read, accumulated in order, written back.  The count NP is a sum
+// of n ones: exact, so one add of n.
+template <class T, int SPLIT, int P>
+__device__ __forceinline__ void sample_cell(Cells cells, int cg, int n, const T *vx,
+                                            const T *vy, const T *vz)
+{
+    double a[ACC_NC];
+#pragma unroll
+    for (int m = 0; m < ACC_NC; ++m)
+        if (sample_part_of(SPLIT, m) == P)
+            a[m] = cells.acc[m * cells.acc_stride + cg];
+    if (sample_part_of(SPLIT, ACC_NP) == P)
+        a[ACC_NP] += static_cast<double>(n);
+    // Unrolled so that the loads and products of the next particles overlap
+    // the adds of this one (the sums keep their order: only the adds chain).
+#pragma unroll SAMPLE_UNROLL
+    for (int i = 0; i < n; ++i)
+        sample_add<SPLIT, P>(a, vx[i], vy[i], vz[i]);
+#pragma unroll
+    for (int m = 0; m < ACC_NC; ++m)
+        if (sample_part_of(SPLIT, m) == P)
+            cells.acc[m * cells.acc_stride + cg] = a[m];
+}
+
+// The sample blocks bx, bx + nbx, ... (CELLS cells, SPLIT x CELLS threads,
+// S stages); smem_raw holds sample_smem<T, CELLS, S>() bytes.  Its block
+// bx == 0 also ends the step when `finish` is set.  False when a staged copy
+// never completed (reported; copies in flight waited for).
+template <class T, int CELLS, int SPLIT, int S>
+__device__ __forceinline__ bool sample_blocks(const CaseDev *__restrict__ cases, CaseState *st,
+                                              TileTables tt, Slots<T> p, Cells cells, int side,
+                                              int ncase, int finish, dsmc_counters *rec,
+                                              int *err, unsigned char *smem_raw, int bx,
+                                              int nbx)
+{
+    static_assert(SPLIT == 2 || SPLIT == 4, "two or four threads per cell");
+    if (finish && bx == 0)
         finish_cases(cases, st, ncase, 0, 1, 1, rec);
-    constexpr int S = SAMPLE_STAGES;
     constexpr int A = 16 / sizeof(T); // elements per 16 bytes
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    SampleStage<T> *stage = reinterpret_cast<SampleStage<T> *>(smem_raw);
+    constexpr int SUB = sample_sub<CELLS>();
+    SampleStage<T, CELLS> *stage = reinterpret_cast<SampleStage<T, CELLS> *>(smem_raw);
     __shared__ uint64_t bar[S];
     __shared__ int s_staged[S];
     __shared__ int64_t s_r0[S]; // first staged slot (rounded down to A)
     const int32_t *start = start_of(cells, side);
-    const int nblocks = tt.cblock0[ncase] * SAMPLE_SUB;
+    const int nblocks = tt.cblock0[ncase] * SUB;
 
     // Thread 0 only: stages the velocities of block b in stage sidx when its
     // case samples this step and the range fits.
     auto issue = [&](int b, int sidx) {
         s_staged[sidx] = 0;
-        const int ci = case_of(tt.cblock0, ncase, b / SAMPLE_SUB);
+        const int ci = case_of(tt.cblock0, ncase, b / SUB);
         if (st[ci].sampling_mode != 1)
             return;
         const CaseDev &c = cases[ci];
-        const int cl0 = sample_cell0(tt, ci, b);
+        const int cl0 = sample_cell0<CELLS>(tt, ci, b);
         if (cl0 >= c.ncell)
             return;
-        const int cl1 = min(cl0 + SAMPLE_CELLS, c.ncell);
+        const int cl1 = min(cl0 + CELLS, c.ncell);
         const int64_t r0 = start[c.cbase + cl0] & ~static_cast<int64_t>(A - 1);
         const int64_t r1 = (start[c.cbase + cl1] + A - 1) & ~static_cast<int64_t>(A - 1);
         const int64_t n = r1 - r0;
-        if (n <= 0 || n > sample_pcl<T>() + A)
+        if (n <= 0 || n > sample_pcl<T, CELLS>() + A)
             return;
         const uint32_t bytes = static_cast<uint32_t>(n * sizeof(T));
         mbar_arrive_expect_tx(&bar[sidx], 3 * bytes);
@@ -1901,36 +2138,31 @@ __global__ void __launch_bounds__(SAMPLE_THREADS)
             mbar_init(&bar[i], 1);
         fence_mbar_init();
         for (int i = 0; i < S; ++i)
-            if (blockIdx.x + i * gridDim.x < nblocks)
-                issue(blockIdx.x + i * gridDim.x, i);
+            if (bx + i * nbx < nblocks)
+                issue(bx + i * nbx, i);
     }
     __syncthreads();
 
     uint32_t phase = 0; // bit i: parity of the next completion of stage i
     for (int it = 0;; ++it) {
-        const int b = blockIdx.x + it * gridDim.x;
+        const int b = bx + it * nbx;
         if (b >= nblocks)
-            return;
+            break;
         const int sidx = it % S;
-        const int ci = case_of(tt.cblock0, ncase, b / SAMPLE_SUB);
+        const int ci = case_of(tt.cblock0, ncase, b / SUB);
         const bool staged = s_staged[sidx] != 0;
-        const int half = threadIdx.x / SAMPLE_CELLS; // uniform over a warp
+        const int part = threadIdx.x / CELLS; // uniform over a warp
         bool ok = true;
         if (st[ci].sampling_mode == 1) {
             const CaseDev &c = cases[ci];
-            const int cl = sample_cell0(tt, ci, b) + static_cast<int>(threadIdx.x % SAMPLE_CELLS);
+            const int cl = sample_cell0<CELLS>(tt, ci, b) + static_cast<int>(threadIdx.x % CELLS);
             const int cg = c.cbase + cl;
             const bool mine = cl < c.ncell;
             int64_t a0 = 0;
             int n = 0;
-            double a[ACC_NC];
             if (mine) {
                 a0 = start[cg];
                 n = static_cast<int>(start[cg + 1] - a0);
-#pragma unroll
-                for (int m = 0; m < ACC_NC; ++m)
-                    if ((m <= ACC_VV11) == (half == 0))
-                        a[m] = cells.acc[m * cells.acc_stride + cg];
             }
             const T *vx = p.vx + c.pbase + a0, *vy = p.vy + c.pbase + a0,
                     *vz = p.vz + c.pbase + a0;
@@ -1943,26 +2175,14 @@ __global__ void __launch_bounds__(SAMPLE_THREADS)
                 vz = stage[sidx].v[2] + off;
             }
             if (mine && n > 0 && ok) {
-                // Unrolled so that the loads and products of the next
-                // particles overlap the adds of this one (the sums keep
-                // their order: only the adds into a[] chain).
-                if (half == 0) {
-                    // The count is a sum of n ones: exact, so one add of n.
-                    a[ACC_NP] += static_cast<double>(n);
-#pragma unroll SAMPLE_UNROLL
-                    for (int i = 0; i < n; ++i)
-                        sample_add0(a, vx[i], vy[i], vz[i]);
-#pragma unroll
-                    for (int m = 0; m <= ACC_VV11; ++m)
-                        cells.acc[m * cells.acc_stride + cg] = a[m];
-                } else {
-#pragma unroll SAMPLE_UNROLL
-                    for (int i = 0; i < n; ++i)
-                        sample_add1(a, vx[i], vy[i], vz[i]);
-#pragma unroll
-                    for (int m = ACC_VV12; m < ACC_NC; ++m)
-                        cells.acc[m * cells.acc_stride + cg] = a[m];
-                }
+                if (part == 0)
+                    sample_cell<T, SPLIT, 0>(cells, cg, n, vx, vy, vz);
+                else if (part == 1)
+                    sample_cell<T, SPLIT, 1>(cells, cg, n, vx, vy, vz);
+                else if (SPLIT == 4 && part == 2)
+                    sample_cell<T, SPLIT, 2>(cells, cg, n, vx, vy, vz);
+                else if (SPLIT == 4)
+                    sample_cell<T, SPLIT, 3>(cells, cg, n, vx, vy, vz);
             }
         }
         // The stage is consumed: refill it with this CTA's block it + S.
@@ -1973,11 +2193,11 @@ __global__ void __launch_bounds__(SAMPLE_THREADS)
                     if (s_staged[j])
                         mbar_wait(&bar[j], (phase >> j) & 1u);
             }
-            return;
+            return false;
         }
         if (threadIdx.x == 0) {
             fence_proxy_async_smem();
-            const int bn = b + S * gridDim.x;
+            const int bn = b + S * nbx;
             s_staged[sidx] = 0;
             if (bn < nblocks)
                 issue(bn, sidx);
@@ -1985,6 +2205,23 @@ __global__ void __launch_bounds__(SAMPLE_THREADS)
         if (S == 1) // the next block reads this stage's flags: publish them first
             __syncthreads();
     }
+    // No copy is in flight after the last block (each issued stage was
+    // consumed): the barriers can be retired.
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < S; ++i)
+            mbar_inval(&bar[i]);
+    return true;
+}
+
+template <class T>
+__global__ void __launch_bounds__(SAMPLE_THREADS, DSMC_SAMPLE_MIN_BLOCKS)
+    k_sample(const CaseDev *__restrict__ cases, CaseState *st, TileTables tt, Slots<T> p,
+             Cells cells, int side, int ncase, int finish, dsmc_counters *rec, int *err)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    (void)sample_blocks<T, SAMPLE_CELLS, SAMPLE_SPLIT, SAMPLE_STAGES>(
+        cases, st, tt, p, cells, side, ncase, finish, rec, err, smem_raw, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------

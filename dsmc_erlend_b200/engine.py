@@ -241,6 +241,37 @@ class Engine:
         check(self._lib.dsmc_autotune(self._h, int(steps_per_trial)), "dsmc_autotune")
         return self.launch_config()
 
+    # -- step mode ------------------------------------------------------------
+    def set_step_mode(self, persistent: bool, ctas_per_sm: int = 0):
+        """dsmc_step as one graph launch per step (persistent=False, the
+        default) or as ONE persistent cooperative kernel for all steps of a
+        call (persistent=True; grid ctas_per_sm x SMs, 0 = the most that
+        fit).  Results are identical."""
+        check(self._lib.dsmc_set_step_mode(self._h, 1 if persistent else 0, int(ctas_per_sm)),
+              "dsmc_set_step_mode")
+
+    def step_mode(self) -> dict:
+        """{"persistent", "ctas_per_sm", "max_ctas_per_sm", "graph_launch"}."""
+        v = [C.c_int() for _ in range(4)]
+        check(self._lib.dsmc_get_step_mode(self._h, *[C.byref(x) for x in v]),
+              "dsmc_get_step_mode")
+        return {"persistent": bool(v[0].value), "ctas_per_sm": v[1].value,
+                "max_ctas_per_sm": v[2].value, "graph_launch": bool(v[3].value)}
+
+    def phase_times(self, reset: bool = False) -> dict:
+        """{phase: ms} of the persistent step, summed since the last reset."""
+        ms = (C.c_double * 32)()
+        names = (C.c_char_p * 32)()
+        n = C.c_int()
+        check(self._lib.dsmc_get_phase_times(self._h, ms, 32, C.byref(n), names,
+                                             1 if reset else 0), "dsmc_get_phase_times")
+        return {names[i].decode(): ms[i] for i in range(n.value)}
+
+    def grid_sync_probe(self, wait_ns: int) -> int:
+        """Status of a grid-barrier wait that can never complete, bounded by
+        wait_ns (DSMC_ERR_TIMEOUT expected)."""
+        return int(self._lib.dsmc_grid_sync_probe(self._h, int(wait_ns)))
+
     def _all_kernel_names(self):
         names = (C.c_char_p * 32)()
         n = C.c_int()

@@ -1,10 +1,12 @@
 """Throughput of the batched ensemble: the 256 cases of ensemble_cases() (grid
-side U[64, 400], Ma U[2, 8], ...) advanced together in one context, one CUDA
-graph per step; particle-steps/s summed over the cases, CUDA events on the
-context's stream.
+side U[64, 400], Ma U[2, 8], ...) advanced together in one context, either
+one CUDA graph per step or (--persistent) one persistent cooperative kernel
+for all timed steps; particle-steps/s summed over the cases, CUDA events on
+the context's stream.
 
     python -m dsmc_erlend_b200.ensemble_bench [--cases 256] [--steps 200]
-        [--warmup 20] [--autotune] [--precision fp32|fp64]
+        [--warmup 20] [--autotune] [--precision fp32|fp64] [--persistent]
+        [--ctas-per-sm N]
 
 Prints one JSON line.  The full protocol is 5000 steps per case; the timed
 window here is a bounded slice of it after the cold start and warm-up.
@@ -28,6 +30,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--persistent", action="store_true")
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
     args = ap.parse_args()
 
     import torch
@@ -47,6 +51,9 @@ def main():
         if args.autotune:
             shapes = eng.autotune(steps_per_trial=2)
             eng.InitialConditions()
+        if args.persistent:
+            eng.set_step_mode(True, args.ctas_per_sm)
+        mode = eng.step_mode()
         eng.step(args.warmup)
         eng.synchronize()
         before = sum(eng.counters(i)["particle_steps"] for i in range(len(cases)))
@@ -70,7 +77,8 @@ def main():
                                "grid side U[64,400], Ma U[2,8], angle U[-30,30], "
                                "n log-U[1e16,1e18], box U[2,6], walls S/D/CLL, NPCFree U[5,20]",
                    "precision": args.precision, "sampling": "every timed step"},
-        "cold_start_s": init_s, "launch_shapes": shapes}))
+        "launch": ("persistent" if mode["persistent"] else "graph per step"),
+        "step_mode": mode, "cold_start_s": init_s, "launch_shapes": shapes}))
 
 
 if __name__ == "__main__":

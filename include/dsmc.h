@@ -349,6 +349,42 @@ int dsmc_set_launch_config(dsmc_ctx *ctx, const int32_t *ctas_per_sm, int n);
  * afterwards for a run from step 0 with the tuned shapes. */
 int dsmc_autotune(dsmc_ctx *ctx, int steps_per_trial);
 
+/* How dsmc_step runs the steps of every case of the context (no counterpart
+ * in the reference, whose ranks loop over MoveParticles .. Sampling):
+ *   DSMC_STEP_GRAPH       one CUDA graph launch per step, the step's kernels
+ *                         as its nodes (the default);
+ *   DSMC_STEP_PERSISTENT  ONE cooperative kernel for all n_steps steps of a
+ *                         dsmc_step call, launched as the kernel node of a
+ *                         CUDA graph: every CTA stays resident and the
+ *                         stages of a step are separated by grid barriers.
+ * Both give identical particles, cell lists, counters and moments.  The
+ * persistent grid is ctas_per_sm x SMs CTAs (0: the most that fit); every
+ * barrier wait is bounded (about 2 s), after which the launch ends and
+ * DSMC_ERR_TIMEOUT is reported.  DSMC_ERR_UNSUPPORTED when the device has
+ * no cooperative launch; DSMC_ERR_STATE in the middle of a staged step.
+ * dsmc_set_profiling's per-kernel timing always uses the graph sequence. */
+enum { DSMC_STEP_GRAPH = 0, DSMC_STEP_PERSISTENT = 1 };
+int dsmc_set_step_mode(dsmc_ctx *ctx, int mode, int ctas_per_sm);
+/* The mode, the persistent grid's CTAs per SM and their maximum (0 without
+ * cooperative launch), and whether persistent launches go through CUDA
+ * graphs (1) or, where the driver refuses graphs of cooperative kernels,
+ * are launched directly (0). */
+int dsmc_get_step_mode(dsmc_ctx *ctx, int *mode, int *ctas_per_sm, int *max_ctas_per_sm,
+                       int *graph_launch);
+/* Device time of each phase of the persistent step (the stages between two
+ * grid barriers: plan, move+inject, move_near, dead_scan, holes, tail,
+ * cell_scan+tile_scan, olist+collide_select, cell_fix, scatter,
+ * collide_pairs, sample), summed over the persistent steps run since the
+ * last reset, in milliseconds, with the phase names; reset != 0 zeroes the
+ * sums after reading them. */
+int dsmc_get_phase_times(dsmc_ctx *ctx, double *ms_out, int max_phases, int *n_phases,
+                         const char **names_out, int reset);
+/* Test of the bounded grid-barrier wait: one CTA waits at a barrier that
+ * one more CTA would have to reach (none does) and gives up after wait_ns
+ * nanoseconds.  Returns DSMC_ERR_TIMEOUT, the status the kernel reported;
+ * the context's own error word is untouched and it stays usable. */
+int dsmc_grid_sync_probe(dsmc_ctx *ctx, int64_t wait_ns);
+
 /* Per-kernel device time of the stages, for profiling.  When enabled,
  * dsmc_step brackets every kernel with CUDA events; dsmc_get_kernel_times
  * returns the summed milliseconds per kernel since the last reset and the
