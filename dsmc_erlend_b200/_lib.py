@@ -32,6 +32,7 @@ SIGNATURES = {
     "dsmc_init_cold": (C.c_int, [C.c_void_p]),
     "dsmc_init_warm": (C.c_int, [C.c_void_p, _D]),
     "dsmc_init_warm_tensor": (C.c_int, [C.c_void_p, _D]),
+    "dsmc_init_warm_mixture": (C.c_int, [C.c_void_p, _D]),
     "dsmc_step": (C.c_int, [C.c_void_p, C.c_int]),
     "dsmc_step_read": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dsmc_stage_move": (C.c_int, [C.c_void_p]),

@@ -95,6 +95,56 @@ def warm_input(f: dict, tensor: bool = False) -> np.ndarray:
     return out
 
 
+def mixture_input(f: dict, ux_free: float, uy_free: float, t_free: float,
+                  molecule_mass: float, alpha_max: float = 0.9,
+                  t_floor: float = 0.05, reg: float = 0.05) -> np.ndarray:
+    """dsmc_init_warm_mixture's (n, alpha, ux_r, uy_r, T_r) per cell from a
+    field with the temperature tensor (n, ux, uy, txx, tyy, tzz): each cell's
+    gas as a fraction alpha of freestream molecules (the case's freestream
+    Maxwellian, U = (ux_free, uy_free), T = t_free) and 1 - alpha of a second,
+    isotropic population (u_r, T_r), with n, u and Tzz matched exactly and
+    Txx + Tyy matched when alpha is not clipped.
+
+    For such a mixture, with c = k / m:
+        u   = alpha U + (1 - alpha) u_r
+        Tzz = alpha T_free + (1 - alpha) T_r
+        c (Txx + Tyy - 2 Tzz) = alpha (1 - alpha) |U - u_r|^2
+                              = alpha / (1 - alpha) |U - u|^2,
+    so R = c (Txx + Tyy - 2 Tzz) / |U - u|^2 gives alpha = R / (1 + R), then
+    u_r = (u - alpha U) / (1 - alpha) and T_r = (Tzz - alpha T_free) /
+    (1 - alpha).  |U - u|^2 is regularised by (reg |U|)^2 so that a cell
+    at freestream conditions (both terms near zero) takes alpha near 0 (one
+    Maxwellian of its own moments); alpha is capped at alpha_max (u_r
+    amplifies errors in u by 1 / (1 - alpha)) and lowered where T_r would
+    fall below t_floor T_free."""
+    c = K_BOLTZMANN / molecule_mass
+    n = np.asarray(f["n"], dtype=np.float64)
+    ux, uy = np.asarray(f["ux"], np.float64), np.asarray(f["uy"], np.float64)
+    txx, tyy, tzz = (np.asarray(f[k], np.float64) for k in ("txx", "tyy", "tzz"))
+    ok = np.isfinite(ux) & np.isfinite(uy) & np.isfinite(txx) & np.isfinite(tyy) & \
+        np.isfinite(tzz) & (n > 0) & (np.asarray(f.get("count", np.ones_like(n))) > 0)
+    u2 = ux_free * ux_free + uy_free * uy_free
+    e = (ux_free - ux) ** 2 + (uy_free - uy) ** 2 + reg * reg * u2
+    with np.errstate(invalid="ignore", divide="ignore"):
+        r = np.maximum(c * (txx + tyy - 2.0 * tzz), 0.0) / e
+        alpha = np.minimum(r / (1.0 + r), alpha_max)
+        tfl = t_floor * t_free
+        # T_r >= tfl  <=>  alpha <= (Tzz - tfl) / (T_free - tfl)
+        cap = np.where(t_free > tfl, (tzz - tfl) / (t_free - tfl), 0.0)
+        alpha = np.clip(np.minimum(alpha, cap), 0.0, alpha_max)
+        alpha = np.where(ok, alpha, 0.0)
+        uxr = (ux - alpha * ux_free) / (1.0 - alpha)
+        uyr = (uy - alpha * uy_free) / (1.0 - alpha)
+        tr = np.maximum((tzz - alpha * t_free) / (1.0 - alpha), 0.0)
+    out = np.zeros((len(n), 5), dtype=np.float64)
+    out[ok, 0] = n[ok]
+    out[ok, 1] = alpha[ok]
+    out[ok, 2] = uxr[ok]
+    out[ok, 3] = uyr[ok]
+    out[ok, 4] = tr[ok]
+    return out
+
+
 def coarsen(f: dict, nx: int, ny: int, b: int) -> dict:
     """Field on blocks of b x b cells (nx, ny multiples of b): n averaged,
     velocity and temperature weighted by the sample counts."""

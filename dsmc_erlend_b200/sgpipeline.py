@@ -29,12 +29,15 @@ from .timetofield import coarse_prediction, reference_field, time_to_field
 
 
 def time_to_field_study(p, predictors: dict, ref_replicas: int, transient: int,
-                        ref_steps: int, cold_starts, warm_starts, check_every: int) -> dict:
+                        ref_steps: int, cold_starts, warm_starts, check_every: int,
+                        ceiling: bool = False) -> dict:
     """Best cold and best warm time to a 2% field over the given sampling
     starts, against a reference field of `ref_replicas` replicas.
     `predictors` maps a name to (predicted field, seconds the prediction
-    took, whether to seed the full temperature tensor); a warm run's time
-    includes its prediction's."""
+    took, the warm-start kind of timetofield.warm_array); a warm run's time
+    includes its prediction's.  With `ceiling`, warm runs from the
+    reference field itself (as one Maxwellian and as the mixture) show what
+    a perfect prediction of the moments would give."""
     t0 = time.perf_counter()
     ref = reference_field(p, ref_replicas, transient=transient, steps=ref_steps)
     out = {"reference_seconds": time.perf_counter() - t0, "cold": []}
@@ -48,11 +51,14 @@ def time_to_field_study(p, predictors: dict, ref_replicas: int, transient: int,
                                          check_every=check_every, max_steps=40000))
     bc = best(out["cold"])
     out["best_cold"] = bc
-    for name, (predicted, pred_s, tensor) in predictors.items():
+    if ceiling:
+        predictors = {**predictors, "ceiling_moments": (ref, 0.0, "moments"),
+                      "ceiling_mixture": (ref, 0.0, "mixture")}
+    for name, (predicted, pred_s, kind) in predictors.items():
         runs = []
         for fs in warm_starts:
             r = time_to_field(p, ref, "warm", predicted=predicted, first_sampling_step=fs,
-                              check_every=check_every, max_steps=40000, tensor=tensor)
+                              check_every=check_every, max_steps=40000, kind=kind)
             r["prediction_seconds"] = pred_s
             r["seconds"] += pred_s
             runs.append(r)
@@ -79,6 +85,8 @@ def main():
                          "run the time-to-field study only")
     ap.add_argument("--warm-starts", default="500,1000,2000,3000,4000,5000",
                     help="sampling starts tried for the warm runs")
+    ap.add_argument("--ceiling", action="store_true",
+                    help="add warm runs from the reference field itself")
     ap.add_argument("--out", default="surrogate_out")
     args = ap.parse_args()
     out = Path(args.out)
@@ -89,7 +97,8 @@ def main():
         net = Surrogate(1, seed=0)
         w = np.load(args.weights)
         net.load_state_dict({k: w[k] for k in w.files})
-        report["time_to_field"] = run_ttf(net, [int(v) for v in args.warm_starts.split(",")])
+        report["time_to_field"] = run_ttf(net, [int(v) for v in args.warm_starts.split(",")],
+                                          ceiling=args.ceiling)
         (out / "report_ttf.json").write_text(json.dumps(report, indent=1, default=float))
         return
     cases = surrogate_cases(args.cases, args.seed, steps=args.steps)
@@ -128,11 +137,12 @@ def main():
     np.savez_compressed(out / "surrogate_weights.npz", **net.state_dict())
 
     if not args.no_ttf:
-        report["time_to_field"] = run_ttf(net, [int(v) for v in args.warm_starts.split(",")])
+        report["time_to_field"] = run_ttf(net, [int(v) for v in args.warm_starts.split(",")],
+                                          ceiling=args.ceiling)
     (out / "report.json").write_text(json.dumps(report, indent=1, default=float))
 
 
-def run_ttf(net, warm_starts) -> dict:
+def run_ttf(net, warm_starts, ceiling: bool = False) -> dict:
     """The time-to-field study on the warm-start case (512 x 512, Ma 6, n 3e17,
     angle 15, CLL (0.5, 0.9), box 3 x 5 m, NPCFree 30): cold starts against
     warm starts from the surrogate (n, u, T and the temperature tensor) and
@@ -147,12 +157,13 @@ def run_ttf(net, warm_starts) -> dict:
     sg_s = time.perf_counter() - t0
     coarse, coarse_s = coarse_prediction(p)
     tt = time_to_field_study(
-        p, {"surrogate": (predicted, sg_s, False),
-            "surrogate_tensor": (predicted, sg_s, True),
-            "coarse": (coarse, coarse_s, False)},
+        p, {"surrogate": (predicted, sg_s, "moments"),
+            "surrogate_tensor": (predicted, sg_s, "tensor"),
+            "surrogate_mixture": (predicted, sg_s, "mixture"),
+            "coarse": (coarse, coarse_s, "moments")},
         ref_replicas=8, transient=6000, ref_steps=8000,
         cold_starts=(2000, 4000, 6000, 8000), warm_starts=tuple(warm_starts),
-        check_every=250)
+        check_every=250, ceiling=ceiling)
     print(json.dumps({k: tt[k]["warm_over_cold"] for k in tt if k.startswith("warm_")}),
           flush=True)
     return tt

@@ -18,7 +18,19 @@ import numpy as np
 
 from . import Engine, setup
 from .ensemble import replicas
-from .fields import field_errors, macroscopic, warm_input
+from .fields import field_errors, macroscopic, mixture_input, warm_input
+
+
+def warm_array(p, d, predicted: dict, kind: str = "moments") -> np.ndarray:
+    """The warm-start input of a predicted field: "moments" (n, u, T: one
+    local Maxwellian), "tensor" (n, u and the temperature tensor: one
+    anisotropic Maxwellian) or "mixture" (freestream plus a second
+    population, fields.mixture_input)."""
+    if kind == "mixture":
+        return mixture_input(predicted, d.ux_free, d.uy_free, p.t_free, d.molecule_mass)
+    if kind not in ("moments", "tensor"):
+        raise ValueError(kind)
+    return warm_input(predicted, tensor=kind == "tensor")
 
 
 def merged_field(eng: Engine, n_cases: int) -> dict:
@@ -44,10 +56,10 @@ def reference_field(p, replicas_n: int, transient: int, steps: int, seed: int = 
 
 def time_to_field(p, ref: dict, start: str, predicted: dict | None = None,
                   first_sampling_step: int = 0, tol: float = 0.02, check_every: int = 250,
-                  max_steps: int = 200000, tensor: bool = False) -> dict:
+                  max_steps: int = 200000, kind: str = "moments") -> dict:
     """Runs one case from `start` ("cold" or "warm") with sampling after
     `first_sampling_step`, checking the sampled field every `check_every`
-    steps; returns the steps and the wall time of the run itself (start and
+    steps (a warm start seeds `predicted` as warm_array's `kind`); returns the steps and the wall time of the run itself (start and
     steps, device synchronised; the field checks are measurement and their
     time is left out) at the first check within `tol`."""
     q = p.copy(first_sampling_step=first_sampling_step)
@@ -55,7 +67,7 @@ def time_to_field(p, ref: dict, start: str, predicted: dict | None = None,
     eng = Engine(q)
     t0 = time.perf_counter()
     if start == "warm":
-        eng.init_warm(warm_input(predicted, tensor=tensor))
+        eng.init_warm(warm_array(q, d, predicted, kind))
     else:
         eng.InitialConditions()
     eng.synchronize()

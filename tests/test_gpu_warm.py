@@ -7,7 +7,9 @@ drawn from the local Maxwellian of a given field.
   * a field varying from cell to cell is reproduced cell by cell;
   * the fill is deterministic for a seed and differs between seeds;
   * the residual check of warm.warm_start keeps a good prediction and falls
-    back to the cold start for a wrong one.
+    back to the cold start for a wrong one;
+  * the two-population fill (dsmc_init_warm_mixture) draws the freestream
+    fraction and the second population with the mixture's moments.
 """
 from __future__ import annotations
 
@@ -131,3 +133,44 @@ def test_residual_check_keeps_good_and_rejects_bad_prediction(cuda, engine_lib):
     mode, res = warm_start(e, [huge], check_steps=300, tol=0.05, block=2)
     assert mode == "cold" and e.counters()["step"] == 0
     e.close()
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32])
+def test_mixture_fill_has_the_mixture_moments(cuda, engine_lib, precision):
+    p = small_case(WALL_DIFFUSE, seed=21, precision=precision, npc_free=40.0)
+    d = setup(p)
+    alpha, ur, tr = 0.4, (-150.0, 60.0), 700.0
+    f = np.zeros((p.nx * p.ny, 5))
+    f[:, 0] = p.n_free
+    f[:, 1] = alpha
+    f[:, 2], f[:, 3] = ur
+    f[:, 4] = tr
+    e = Engine(p)
+    e.init_warm(f)
+    st = e.particles()
+    n = len(st["x"])
+    c = K_BOLTZMANN / d.molecule_mass
+    s_free, s_r = c * p.t_free, c * tr
+    mx = alpha * d.ux_free + (1 - alpha) * ur[0]
+    my = alpha * d.uy_free + (1 - alpha) * ur[1]
+    dx, dy = d.ux_free - ur[0], d.uy_free - ur[1]
+    var = {"vx": alpha * s_free + (1 - alpha) * s_r + alpha * (1 - alpha) * dx * dx,
+           "vy": alpha * s_free + (1 - alpha) * s_r + alpha * (1 - alpha) * dy * dy,
+           "vz": alpha * s_free + (1 - alpha) * s_r}
+    for k, mean in (("vx", mx), ("vy", my), ("vz", 0.0)):
+        assert abs(st[k].mean() - mean) < 5 * np.sqrt(var[k] / n), k
+        assert abs(st[k].var() / var[k] - 1) < 0.03, k
+    # The two populations: the share of particles within one freestream
+    # thermal speed of the freestream velocity (in the x-y plane) is alpha
+    # times 1 - exp(-1/2) = 0.39, plus the second population's small overlap.
+    near = np.hypot(st["vx"] - d.ux_free, st["vy"] - d.uy_free) < np.sqrt(s_free)
+    share = near.mean()
+    assert alpha * 0.39 - 0.02 < share < alpha * 0.39 + 0.05, share
+    again = Engine(p)
+    again.init_warm(f)
+    st2 = again.particles()
+    assert all(np.array_equal(st[k], st2[k]) for k in st)
+    e.step(3)
+    e.synchronize()
+    e.close()
+    again.close()
