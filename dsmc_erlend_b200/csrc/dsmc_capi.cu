@@ -983,10 +983,11 @@ __global__ void __launch_bounds__(SCAN_THREADS)
 // variance k T / m; with stride 7 the field gives the temperature tensor
 // (Txx, Tyy, Tzz, Txy) and the Gaussians are correlated through its
 // Cholesky factor (the xz and yz entries vanish in this 2-D flow).  With
-// stride 5 the field is (n, alpha, ux_r, uy_r, T_r), a mixture of two
-// populations: with probability alpha (one uniform of the velocity stream
-// first) a particle is drawn from the case's freestream Maxwellian, else
-// from the Maxwellian of (ux_r, uy_r, 0) and T_r.
+// stride 8 the field is (n, alpha, ux_r, uy_r, Txx_r, Tyy_r, Tzz_r, Txy_r),
+// a mixture of two populations: with probability alpha (one uniform of the
+// velocity stream first) a particle is drawn from the case's freestream
+// Maxwellian, else from the Gaussian of mean (ux_r, uy_r, 0) whose
+// covariance is k / m times that temperature tensor (Cholesky as above).
 template <class T>
 __global__ void k_warm_fill(const CaseDev *cases, const CaseState *st, int ncase,
                             const double *field, int stride, const int32_t *off, Slots<T> p)
@@ -1001,17 +1002,18 @@ __global__ void k_warm_fill(const CaseDev *cases, const CaseState *st, int ncase
             const int nc = warm_candidates(c, f, cl);
             if (nc == 0)
                 continue;
-            const bool mix = stride == 5;
+            const bool mix = stride == 8;
             const double ux = mix ? f[2] : f[1], uy = mix ? f[3] : f[2];
-            const double var = K_BOLTZMANN * fmax(mix ? f[4] : f[3], 0.0) / c.mass;
+            const double var = K_BOLTZMANN * fmax(f[3], 0.0) / c.mass;
             const double alpha = mix ? f[1] : 0.0;
             double l11 = 0.0, l21 = 0.0, l22 = 0.0, l33 = 0.0;
-            if (stride == 7) {
+            if (stride == 7 || mix) {
+                const double *tt = f + (mix ? 4 : 3); // Txx, Tyy, Tzz, Txy
                 const double kb = K_BOLTZMANN / c.mass;
-                l11 = sqrt(fmax(kb * f[3], 0.0));
-                l21 = l11 > 0.0 ? kb * f[6] / l11 : 0.0;
-                l22 = sqrt(fmax(kb * f[4] - l21 * l21, 0.0));
-                l33 = sqrt(fmax(kb * f[5], 0.0));
+                l11 = sqrt(fmax(kb * tt[0], 0.0));
+                l21 = l11 > 0.0 ? kb * tt[3] / l11 : 0.0;
+                l22 = sqrt(fmax(kb * tt[1] - l21 * l21, 0.0));
+                l33 = sqrt(fmax(kb * tt[2], 0.0));
             }
             dsmc_stream r, rv;
             open_stream(r, c, DSMC_RNG_WARM, 0, static_cast<uint32_t>(cl));
@@ -1022,12 +1024,11 @@ __global__ void k_warm_fill(const CaseDev *cases, const CaseState *st, int ncase
                 T x, y;
                 warm_position<T>(c, cl, r, x, y);
                 double vx, vy, vz;
-                if (mix) {
-                    const bool free = uniform(rv) < alpha;
-                    vx = frand_gaussian(rv, free ? c.ux_free : ux, free ? c.rt_free : var);
-                    vy = frand_gaussian(rv, free ? c.uy_free : uy, free ? c.rt_free : var);
-                    vz = frand_gaussian(rv, 0.0, free ? c.rt_free : var);
-                } else if (stride == 7) {
+                if (mix && uniform(rv) < alpha) { // the freestream population
+                    vx = frand_gaussian(rv, c.ux_free, c.rt_free);
+                    vy = frand_gaussian(rv, c.uy_free, c.rt_free);
+                    vz = frand_gaussian(rv, 0.0, c.rt_free);
+                } else if (stride == 7 || mix) {
                     const double z1 = frand_gaussian(rv, 0.0, 1.0);
                     const double z2 = frand_gaussian(rv, 0.0, 1.0);
                     const double z3 = frand_gaussian(rv, 0.0, 1.0);
@@ -1470,7 +1471,7 @@ int dsmc_init_warm_tensor(dsmc_ctx *c, const double *host_field)
 
 int dsmc_init_warm_mixture(dsmc_ctx *c, const double *host_field)
 {
-    return init_warm(c, host_field, 5);
+    return init_warm(c, host_field, 8);
 }
 
 int dsmc_step_read(dsmc_ctx *c, int n_steps, dsmc_counters *host_out)

@@ -99,17 +99,17 @@ class Engine:
         """Fills every case from the local Maxwellian of `field`: (n, ux, uy,
         T) per cell, cells x-major, cases one after another (dsmc_init_warm),
         (n, ux, uy, Txx, Tyy, Tzz, Txy) (dsmc_init_warm_tensor), or the
-        two-population (n, alpha, ux_r, uy_r, T_r) (dsmc_init_warm_mixture,
-        fields.mixture_input)."""
+        two-population (n, alpha, ux_r, uy_r, Txx_r, Tyy_r, Tzz_r, Txy_r)
+        (dsmc_init_warm_mixture, fields.mixture_input)."""
         f = np.ascontiguousarray(field, dtype=np.float64)
         need = sum(p.nx * p.ny for p in self.params)
-        if f.shape not in ((need, 4), (need, 5), (need, 7)):
-            raise ValueError(f"field must have shape ({need}, 4), ({need}, 5) or ({need}, 7), "
+        if f.shape not in ((need, 4), (need, 7), (need, 8)):
+            raise ValueError(f"field must have shape ({need}, 4), ({need}, 7) or ({need}, 8), "
                              f"not {f.shape}")
         if f.shape[1] == 7:  # n, ux, uy, Txx, Tyy, Tzz, Txy: dsmc_init_warm_tensor
             check(self._lib.dsmc_init_warm_tensor(self._h, f.ctypes.data_as(_D)),
                   "dsmc_init_warm_tensor")
-        elif f.shape[1] == 5:  # n, alpha, ux_r, uy_r, T_r: dsmc_init_warm_mixture
+        elif f.shape[1] == 8:  # n, alpha, u_r, T_r tensor: dsmc_init_warm_mixture
             check(self._lib.dsmc_init_warm_mixture(self._h, f.ctypes.data_as(_D)),
                   "dsmc_init_warm_mixture")
         else:

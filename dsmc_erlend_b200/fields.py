@@ -96,16 +96,15 @@ def warm_input(f: dict, tensor: bool = False) -> np.ndarray:
 
 
 def mixture_input(f: dict, ux_free: float, uy_free: float, t_free: float,
-                  molecule_mass: float, alpha_max: float = 0.9,
+                  molecule_mass: float, tensor: bool = False, alpha_max: float = 0.9,
                   t_floor: float = 0.05, reg: float = 0.05) -> np.ndarray:
-    """dsmc_init_warm_mixture's (n, alpha, ux_r, uy_r, T_r) per cell from a
-    field with the temperature tensor (n, ux, uy, txx, tyy, tzz): each cell's
-    gas as a fraction alpha of freestream molecules (the case's freestream
-    Maxwellian, U = (ux_free, uy_free), T = t_free) and 1 - alpha of a second,
-    isotropic population (u_r, T_r), with n, u and Tzz matched exactly and
-    Txx + Tyy matched when alpha is not clipped.
+    """dsmc_init_warm_mixture's (n, alpha, ux_r, uy_r, Txx_r, Tyy_r, Tzz_r,
+    Txy_r) per cell from a field with the temperature tensor (n, ux, uy, txx,
+    tyy, tzz, txy): each cell's gas as a fraction alpha of freestream
+    molecules (the case's freestream Maxwellian, U = (ux_free, uy_free),
+    T = t_free) and 1 - alpha of a second population (u_r and its tensor).
 
-    For such a mixture, with c = k / m:
+    For such a mixture, with c = k / m and an isotropic second population T_r:
         u   = alpha U + (1 - alpha) u_r
         Tzz = alpha T_free + (1 - alpha) T_r
         c (Txx + Tyy - 2 Tzz) = alpha (1 - alpha) |U - u_r|^2
@@ -116,19 +115,29 @@ def mixture_input(f: dict, ux_free: float, uy_free: float, t_free: float,
     at freestream conditions (both terms near zero) takes alpha near 0 (one
     Maxwellian of its own moments); alpha is capped at alpha_max (u_r
     amplifies errors in u by 1 / (1 - alpha)) and lowered where T_r would
-    fall below t_floor T_free."""
+    fall below t_floor T_free.  That matches n, u and Tzz exactly, and
+    Txx + Tyy when alpha is not capped.  With `tensor` the second
+    population keeps that alpha but takes the whole remaining tensor,
+        T_r,ij = (T_ij - alpha T_free d_ij - alpha (1 - alpha) dU_i dU_j / c)
+                 / (1 - alpha),   dU = U - u_r,
+    so that the mixture matches Txx, Tyy, Tzz and Txy one by one (its
+    diagonal kept at t_floor T_free or more, its xy entry within 0.95 of
+    the geometric mean of the diagonal)."""
     c = K_BOLTZMANN / molecule_mass
     n = np.asarray(f["n"], dtype=np.float64)
     ux, uy = np.asarray(f["ux"], np.float64), np.asarray(f["uy"], np.float64)
     txx, tyy, tzz = (np.asarray(f[k], np.float64) for k in ("txx", "tyy", "tzz"))
+    txy = np.asarray(f.get("txy", np.zeros_like(n)), np.float64)
     ok = np.isfinite(ux) & np.isfinite(uy) & np.isfinite(txx) & np.isfinite(tyy) & \
         np.isfinite(tzz) & (n > 0) & (np.asarray(f.get("count", np.ones_like(n))) > 0)
+    if tensor:
+        ok &= np.isfinite(txy)
     u2 = ux_free * ux_free + uy_free * uy_free
     e = (ux_free - ux) ** 2 + (uy_free - uy) ** 2 + reg * reg * u2
+    tfl = t_floor * t_free
     with np.errstate(invalid="ignore", divide="ignore"):
         r = np.maximum(c * (txx + tyy - 2.0 * tzz), 0.0) / e
         alpha = np.minimum(r / (1.0 + r), alpha_max)
-        tfl = t_floor * t_free
         # T_r >= tfl  <=>  alpha <= (Tzz - tfl) / (T_free - tfl)
         cap = np.where(t_free > tfl, (tzz - tfl) / (t_free - tfl), 0.0)
         alpha = np.clip(np.minimum(alpha, cap), 0.0, alpha_max)
@@ -136,12 +145,21 @@ def mixture_input(f: dict, ux_free: float, uy_free: float, t_free: float,
         uxr = (ux - alpha * ux_free) / (1.0 - alpha)
         uyr = (uy - alpha * uy_free) / (1.0 - alpha)
         tr = np.maximum((tzz - alpha * t_free) / (1.0 - alpha), 0.0)
-    out = np.zeros((len(n), 5), dtype=np.float64)
-    out[ok, 0] = n[ok]
-    out[ok, 1] = alpha[ok]
-    out[ok, 2] = uxr[ok]
-    out[ok, 3] = uyr[ok]
-    out[ok, 4] = tr[ok]
+        if tensor:
+            dx, dy = ux_free - uxr, uy_free - uyr
+            w = alpha * (1.0 - alpha) / c
+            rxx = np.maximum((txx - alpha * t_free - w * dx * dx) / (1.0 - alpha), tfl)
+            ryy = np.maximum((tyy - alpha * t_free - w * dy * dy) / (1.0 - alpha), tfl)
+            rzz = np.maximum(tr, tfl)
+            rxy = (txy - w * dx * dy) / (1.0 - alpha)
+            lim = 0.95 * np.sqrt(rxx * ryy)
+            rxy = np.clip(rxy, -lim, lim)
+        else:
+            rxx = ryy = rzz = tr
+            rxy = np.zeros_like(tr)
+    out = np.zeros((len(n), 8), dtype=np.float64)
+    for i, v in enumerate((n, alpha, uxr, uyr, rxx, ryy, rzz, rxy)):
+        out[ok, i] = np.broadcast_to(v, n.shape)[ok]
     return out
 
 

@@ -53,7 +53,8 @@ def time_to_field_study(p, predictors: dict, ref_replicas: int, transient: int,
     out["best_cold"] = bc
     if ceiling:
         predictors = {**predictors, "ceiling_moments": (ref, 0.0, "moments"),
-                      "ceiling_mixture": (ref, 0.0, "mixture")}
+                      "ceiling_mixture": (ref, 0.0, "mixture"),
+                      "ceiling_mixture_tensor": (ref, 0.0, "mixture_tensor")}
     for name, (predicted, pred_s, kind) in predictors.items():
         runs = []
         for fs in warm_starts:
@@ -160,6 +161,7 @@ def run_ttf(net, warm_starts, ceiling: bool = False) -> dict:
         p, {"surrogate": (predicted, sg_s, "moments"),
             "surrogate_tensor": (predicted, sg_s, "tensor"),
             "surrogate_mixture": (predicted, sg_s, "mixture"),
+            "surrogate_mixture_tensor": (predicted, sg_s, "mixture_tensor"),
             "coarse": (coarse, coarse_s, "moments")},
         ref_replicas=8, transient=6000, ref_steps=8000,
         cold_starts=(2000, 4000, 6000, 8000), warm_starts=tuple(warm_starts),

@@ -24,10 +24,12 @@ from .fields import field_errors, macroscopic, mixture_input, warm_input
 def warm_array(p, d, predicted: dict, kind: str = "moments") -> np.ndarray:
     """The warm-start input of a predicted field: "moments" (n, u, T: one
     local Maxwellian), "tensor" (n, u and the temperature tensor: one
-    anisotropic Maxwellian) or "mixture" (freestream plus a second
-    population, fields.mixture_input)."""
-    if kind == "mixture":
-        return mixture_input(predicted, d.ux_free, d.uy_free, p.t_free, d.molecule_mass)
+    anisotropic Maxwellian), "mixture" (freestream plus an isotropic second
+    population, fields.mixture_input) or "mixture_tensor" (the second
+    population with the remaining temperature tensor)."""
+    if kind in ("mixture", "mixture_tensor"):
+        return mixture_input(predicted, d.ux_free, d.uy_free, p.t_free, d.molecule_mass,
+                             tensor=kind == "mixture_tensor")
     if kind not in ("moments", "tensor"):
         raise ValueError(kind)
     return warm_input(predicted, tensor=kind == "tensor")

@@ -223,12 +223,14 @@ int dsmc_init_warm(dsmc_ctx *ctx, const double *host_field);
  * the moments give it): the velocities are Gaussians with that covariance,
  * which keeps the anisotropy of shock layers and wakes. */
 int dsmc_init_warm_tensor(dsmc_ctx *ctx, const double *host_field);
-/* The same from 5 doubles per cell: n, alpha, ux_r, uy_r, T_r.  Each
- * particle belongs with probability alpha to the case's freestream
- * Maxwellian (UxFree, UyFree, TFree) and otherwise to the Maxwellian of
- * (ux_r, uy_r, 0) at T_r: a two-population gas such as the mix of freestream
- * and wall-reflected molecules ahead of a body in a rarefied flow, whose
- * distribution no single Maxwellian matches. */
+/* The same from 8 doubles per cell: n, alpha, ux_r, uy_r, Txx_r, Tyy_r,
+ * Tzz_r, Txy_r.  Each particle belongs with probability alpha to the case's
+ * freestream Maxwellian (UxFree, UyFree, TFree) and otherwise to the
+ * Gaussian of mean (ux_r, uy_r, 0) with that temperature tensor (an
+ * isotropic T_r: Txx_r = Tyy_r = Tzz_r = T_r, Txy_r = 0): a two-population
+ * gas such as the mix of freestream and wall-reflected molecules ahead of a
+ * body in a rarefied flow, whose distribution no single Maxwellian
+ * matches. */
 int dsmc_init_warm_mixture(dsmc_ctx *ctx, const double *host_field);
 
 /* Runs n_steps complete time steps (Simulation.cpp:138-199) for every case:

@@ -39,7 +39,9 @@ def test_recovers_a_known_mixture():
     np.testing.assert_allclose(out[:, 1], alpha, rtol=1e-10)
     np.testing.assert_allclose(out[:, 2], ur[0], rtol=1e-9)
     np.testing.assert_allclose(out[:, 3], ur[1], rtol=1e-9)
-    np.testing.assert_allclose(out[:, 4], tr, rtol=1e-9)
+    for col in (4, 5, 6):  # Txx_r = Tyy_r = Tzz_r = T_r, Txy_r = 0
+        np.testing.assert_allclose(out[:, col], tr, rtol=1e-9)
+    assert np.all(out[:, 7] == 0.0)
     np.testing.assert_allclose(out[:, 0], 1e17)
 
 
@@ -51,7 +53,35 @@ def test_freestream_cells_take_one_maxwellian():
     np.testing.assert_allclose(out[:, 1], 0.0, atol=1e-12)
     np.testing.assert_allclose(out[:, 2], U[0])
     np.testing.assert_allclose(out[:, 3], U[1])
-    np.testing.assert_allclose(out[:, 4], f["tzz"])
+    np.testing.assert_allclose(out[:, 6], f["tzz"])
+
+
+def mixture_tensor(out):
+    """n, u and the temperature tensor of dsmc_init_warm_mixture's input."""
+    a, uxr, uyr, rxx, ryy, rzz, rxy = (out[:, k] for k in range(1, 8))
+    dx, dy = U[0] - uxr, U[1] - uyr
+    w = a * (1 - a) / C
+    return {"ux": a * U[0] + (1 - a) * uxr, "uy": a * U[1] + (1 - a) * uyr,
+            "txx": a * TF + (1 - a) * rxx + w * dx * dx,
+            "tyy": a * TF + (1 - a) * ryy + w * dy * dy,
+            "tzz": a * TF + (1 - a) * rzz, "txy": (1 - a) * rxy + w * dx * dy}
+
+
+def test_tensor_second_population_matches_every_moment():
+    # An anisotropic cell: the isotropic form matches n, u, Tzz and the
+    # trace Txx + Tyy only; the tensor form matches each entry.
+    f = mixture_moments(np.array([0.2, 0.5, 0.7]), (-250.0, 100.0), 800.0)
+    f["txx"] = f["txx"] + np.array([120.0, -60.0, 40.0])
+    f["tyy"] = f["tyy"] - np.array([120.0, -60.0, 40.0])
+    f["txy"] = f["txy"] + np.array([30.0, -20.0, 10.0])
+    iso = mixture_tensor(mixture_input(f, U[0], U[1], TF, M, reg=0.0))
+    full = mixture_tensor(mixture_input(f, U[0], U[1], TF, M, tensor=True, reg=0.0))
+    for k in ("ux", "uy", "tzz"):
+        np.testing.assert_allclose(iso[k], f[k], rtol=1e-9)
+    np.testing.assert_allclose(iso["txx"] + iso["tyy"], f["txx"] + f["tyy"], rtol=1e-9)
+    assert np.abs(iso["txx"] - f["txx"]).max() > 10.0
+    for k in ("ux", "uy", "txx", "tyy", "tzz", "txy"):
+        np.testing.assert_allclose(full[k], f[k], rtol=1e-9, atol=1e-6)
 
 
 def test_caps_keep_a_valid_second_population():
@@ -62,9 +92,9 @@ def test_caps_keep_a_valid_second_population():
     out = mixture_input(f, U[0], U[1], TF, M, alpha_max=0.9, t_floor=0.05)
     a = out[:, 1]
     assert np.all(a <= 0.9 + 1e-12) and np.all(a >= 0.0)
-    assert np.all(out[:, 4] >= 0.05 * TF - 1e-9)
+    assert np.all(out[:, 6] >= 0.05 * TF - 1e-9)
     np.testing.assert_allclose(a * U[0] + (1 - a) * out[:, 2], f["ux"], rtol=1e-12)
-    np.testing.assert_allclose(a * TF + (1 - a) * out[:, 4], f["tzz"], rtol=1e-12)
+    np.testing.assert_allclose(a * TF + (1 - a) * out[:, 6], f["tzz"], rtol=1e-12)
 
 
 def test_empty_and_invalid_cells_stay_empty():

@@ -139,27 +139,33 @@ def test_residual_check_keeps_good_and_rejects_bad_prediction(cuda, engine_lib):
 def test_mixture_fill_has_the_mixture_moments(cuda, engine_lib, precision):
     p = small_case(WALL_DIFFUSE, seed=21, precision=precision, npc_free=40.0)
     d = setup(p)
-    alpha, ur, tr = 0.4, (-150.0, 60.0), 700.0
-    f = np.zeros((p.nx * p.ny, 5))
+    alpha, ur = 0.4, (-150.0, 60.0)
+    rxx, ryy, rzz, rxy = 900.0, 500.0, 700.0, 150.0  # the second population's tensor [K]
+    f = np.zeros((p.nx * p.ny, 8))
     f[:, 0] = p.n_free
     f[:, 1] = alpha
     f[:, 2], f[:, 3] = ur
-    f[:, 4] = tr
+    f[:, 4:8] = (rxx, ryy, rzz, rxy)
     e = Engine(p)
     e.init_warm(f)
     st = e.particles()
     n = len(st["x"])
     c = K_BOLTZMANN / d.molecule_mass
-    s_free, s_r = c * p.t_free, c * tr
-    mx = alpha * d.ux_free + (1 - alpha) * ur[0]
-    my = alpha * d.uy_free + (1 - alpha) * ur[1]
+    s_free = c * p.t_free
+    mean = {"vx": alpha * d.ux_free + (1 - alpha) * ur[0],
+            "vy": alpha * d.uy_free + (1 - alpha) * ur[1], "vz": 0.0}
     dx, dy = d.ux_free - ur[0], d.uy_free - ur[1]
-    var = {"vx": alpha * s_free + (1 - alpha) * s_r + alpha * (1 - alpha) * dx * dx,
-           "vy": alpha * s_free + (1 - alpha) * s_r + alpha * (1 - alpha) * dy * dy,
-           "vz": alpha * s_free + (1 - alpha) * s_r}
-    for k, mean in (("vx", mx), ("vy", my), ("vz", 0.0)):
-        assert abs(st[k].mean() - mean) < 5 * np.sqrt(var[k] / n), k
-        assert abs(st[k].var() / var[k] - 1) < 0.03, k
+    w = alpha * (1 - alpha)
+    cov = {("vx", "vx"): alpha * s_free + (1 - alpha) * c * rxx + w * dx * dx,
+           ("vy", "vy"): alpha * s_free + (1 - alpha) * c * ryy + w * dy * dy,
+           ("vz", "vz"): alpha * s_free + (1 - alpha) * c * rzz,
+           ("vx", "vy"): (1 - alpha) * c * rxy + w * dx * dy}
+    for k, m in mean.items():
+        assert abs(st[k].mean() - m) < 5 * np.sqrt(cov[(k, k)] / n), k
+    for (a, b), v in cov.items():
+        got = np.mean((st[a] - st[a].mean()) * (st[b] - st[b].mean()))
+        scale = np.sqrt(cov[(a, a)] * cov[(b, b)])
+        assert abs(got - v) < 0.03 * scale, (a, b, got, v)
     # The two populations: the share of particles within one freestream
     # thermal speed of the freestream velocity (in the x-y plane) is alpha
     # times 1 - exp(-1/2) = 0.39, plus the second population's small overlap.
