@@ -15,13 +15,24 @@ from typing import Sequence
 import numpy as np
 
 from ._lib import DsmcError
-from .fields import coarsen, macroscopic, warm_input, weighted_errors
+from .fields import coarsen, macroscopic, mixture_input, warm_input, weighted_errors
 
 
-def predicted_input(fields: Sequence[dict]) -> np.ndarray:
-    """dsmc_init_warm's array for the cases of a context, from one predicted
-    field dict (n, ux, uy, t, count) per case."""
-    return np.concatenate([warm_input(f) for f in fields], axis=0)
+def predicted_input(fields: Sequence[dict], kind: str = "moments",
+                    engine=None) -> np.ndarray:
+    """The warm-start array for the cases of a context, from one predicted
+    field dict per case: "moments" (n, ux, uy, t, count: dsmc_init_warm),
+    "tensor" (with txx, tyy, tzz, txy: dsmc_init_warm_tensor), or "mixture"
+    / "mixture_tensor" (freestream plus a second population,
+    dsmc_init_warm_mixture; needs the engine for each case's freestream)."""
+    if kind in ("mixture", "mixture_tensor"):
+        parts = []
+        for i, f in enumerate(fields):
+            p, d = engine.params[i], engine.derived[i]
+            parts.append(mixture_input(f, d.ux_free, d.uy_free, p.t_free, d.molecule_mass,
+                                       tensor=kind == "mixture_tensor"))
+        return np.concatenate(parts, axis=0)
+    return np.concatenate([warm_input(f, tensor=kind == "tensor") for f in fields], axis=0)
 
 
 def sampled_field(engine, case: int = 0) -> dict:
@@ -47,14 +58,14 @@ def residual(engine, case: int, predicted: dict, block: int = 4) -> dict:
 
 
 def warm_start(engine, predicted: Sequence[dict], check_steps: int = 200, tol: float = 0.05,
-               block: int = 4):
-    """Warm-starts every case of `engine` from `predicted` (one field per case)
-    and checks the early residual.  Returns ("warm" | "cold", residuals per
-    case).  On fallback the engine is cold-started (InitialConditions) and
-    has run no steps; a prediction with more particles than a case's
-    capacity falls back at once."""
+               block: int = 4, kind: str = "moments"):
+    """Warm-starts every case of `engine` from `predicted` (one field per case,
+    seeded as predicted_input's `kind`) and checks the early residual.
+    Returns ("warm" | "cold", residuals per case).  On fallback the engine
+    is cold-started (InitialConditions) and has run no steps; a prediction
+    with more particles than a case's capacity falls back at once."""
     try:
-        engine.init_warm(predicted_input(predicted))
+        engine.init_warm(predicted_input(predicted, kind, engine))
     except DsmcError as e:
         if e.status != 31:  # DSMC_ERR_CAPACITY: more particles than the case holds
             raise

@@ -123,6 +123,9 @@ def test_residual_check_keeps_good_and_rejects_bad_prediction(cuda, engine_lib):
     mode, res = warm_start(e, [want], check_steps=300, tol=0.05, block=2)
     assert mode == "warm", res
     assert e.counters()["step"] == 300
+    for kind in ("mixture", "mixture_tensor"):  # the two-population seeds pass too
+        mode, res = warm_start(e, [want], check_steps=300, tol=0.05, block=2, kind=kind)
+        assert mode == "warm", (kind, res)
     bad = dict(want)
     bad["t"] = want["t"] * 1.5
     mode, res = warm_start(e, [bad], check_steps=300, tol=0.05, block=2)
