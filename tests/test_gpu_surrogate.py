@@ -267,8 +267,8 @@ def test_trained_surrogate_beats_freestream_and_shortens_transient(cuda, engine_
     from dsmc_erlend_b200 import Engine, setup
     from dsmc_erlend_b200.sgdata import case_input, generate, prediction_field, surrogate_cases
     from dsmc_erlend_b200.surrogate import Surrogate, predict, relative_errors, train
-    from dsmc_erlend_b200.fields import weighted_errors, warm_input
-    from dsmc_erlend_b200.timetofield import merged_field, reference_field
+    from dsmc_erlend_b200.fields import weighted_errors
+    from dsmc_erlend_b200.timetofield import merged_field, reference_field, warm_array
 
     cases = surrogate_cases(96, seed=77, steps=1500, grid_range=(64, 96))
     x, t, m, _ = generate(cases, chunk=48)
@@ -302,10 +302,11 @@ def test_trained_surrogate_beats_freestream_and_shortens_transient(cuda, engine_
     warm_f = prediction_field(p, d, predict(one, case_input(p)[None])[0])
     window = 300
     errs = {}
-    for start in ("cold", "warm", "warm_tensor"):
+    kinds = {"warm": "moments", "warm_tensor": "tensor", "warm_mixture": "mixture_tensor"}
+    for start in ("cold", *kinds):
         e = Engine(p)
-        if start.startswith("warm"):
-            e.init_warm(warm_input(warm_f, tensor=start == "warm_tensor"))
+        if start in kinds:
+            e.init_warm(warm_array(p, d, warm_f, kinds[start]))
         else:
             e.InitialConditions()
         e.step(window)
@@ -318,6 +319,10 @@ def test_trained_surrogate_beats_freestream_and_shortens_transient(cuda, engine_
         assert errs[w]["n"] < errs["cold"]["n"], errs
         assert errs[w]["t"] < errs["cold"]["t"], errs
         assert sum(errs[w].values()) < sum(errs["cold"].values()), errs
+    # The two-population seed (freestream plus the rest of the predicted
+    # tensor) gains over the cold start as well.
+    assert sum(errs["warm_mixture"].values()) < sum(errs["cold"].values()), errs
+    print("errors after the window:", errs)
 
 
 def test_graph_train_step_matches_eager(cuda):
