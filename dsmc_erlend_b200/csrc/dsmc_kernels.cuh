@@ -2060,18 +2060,24 @@ __device__ __forceinline__ void sample_add(double a[ACC_NC], float f0, float f1,
 #undef DSMC_OWN
 }
 
-// Part P's sums of one cell of n particles (velocities vx, vy, vz, in slot
-// order): read, accumulated in order, written back.  The count NP is a sum
-// of n ones: exact, so one add of n.
-template <class T, int SPLIT, int P>
-__device__ __forceinline__ void sample_cell(Cells cells, int cg, int n, const T *vx,
-                                            const T *vy, const T *vz)
+// The sums that part `part` owns of cell cg, read into a[] (issued before the
+// wait for the staged velocities, so that their latency overlaps it).
+template <int SPLIT>
+__device__ __forceinline__ void sample_load(int part, double a[ACC_NC], Cells cells, int cg)
 {
-    double a[ACC_NC];
 #pragma unroll
     for (int m = 0; m < ACC_NC; ++m)
-        if (sample_part_of(SPLIT, m) == P)
+        if (sample_part_of(SPLIT, m) == part)
             a[m] = cells.acc[m * cells.acc_stride + cg];
+}
+
+// Part P's sums a[] of one cell of n particles (velocities vx, vy, vz, in
+// slot order): accumulated in order and written back.  The count NP is a
+// sum of n ones: exact, so one add of n.
+template <class T, int SPLIT, int P>
+__device__ __forceinline__ void sample_cell(double a[ACC_NC], Cells cells, int cg, int n,
+                                            const T *vx, const T *vy, const T *vz)
+{
     if (sample_part_of(SPLIT, ACC_NP) == P)
         a[ACC_NP] += static_cast<double>(n);
     // Unrolled so that the loads and products of the next particles overlap
@@ -2160,9 +2166,11 @@ __device__ __forceinline__ bool sample_blocks(const CaseDev *__restrict__ cases,
             const bool mine = cl < c.ncell;
             int64_t a0 = 0;
             int n = 0;
+            double a[ACC_NC];
             if (mine) {
                 a0 = start[cg];
                 n = static_cast<int>(start[cg + 1] - a0);
+                sample_load<SPLIT>(part, a, cells, cg);
             }
             const T *vx = p.vx + c.pbase + a0, *vy = p.vy + c.pbase + a0,
                     *vz = p.vz + c.pbase + a0;
@@ -2176,13 +2184,13 @@ __device__ __forceinline__ bool sample_blocks(const CaseDev *__restrict__ cases,
             }
             if (mine && n > 0 && ok) {
                 if (part == 0)
-                    sample_cell<T, SPLIT, 0>(cells, cg, n, vx, vy, vz);
+                    sample_cell<T, SPLIT, 0>(a, cells, cg, n, vx, vy, vz);
                 else if (part == 1)
-                    sample_cell<T, SPLIT, 1>(cells, cg, n, vx, vy, vz);
+                    sample_cell<T, SPLIT, 1>(a, cells, cg, n, vx, vy, vz);
                 else if (SPLIT == 4 && part == 2)
-                    sample_cell<T, SPLIT, 2>(cells, cg, n, vx, vy, vz);
+                    sample_cell<T, SPLIT, 2>(a, cells, cg, n, vx, vy, vz);
                 else if (SPLIT == 4)
-                    sample_cell<T, SPLIT, 3>(cells, cg, n, vx, vy, vz);
+                    sample_cell<T, SPLIT, 3>(a, cells, cg, n, vx, vy, vz);
             }
         }
         // The stage is consumed: refill it with this CTA's block it + S.
