@@ -127,6 +127,14 @@ constexpr int TBM = 128, TBK = 64;
 template <int BN> __host__ __device__ constexpr int tc_stages() { return BN == 64 ? 2 : 3; }
 template <int BN> constexpr int tc_ctas_per_sm() { return BN == 128 ? 2 : (BN == 64 ? 4 : 3); }
 constexpr int TC_THREADS = TBM + 32 + TBM; // gatherers, MMA warp, epilogue
+// AMODE 3 (Cin 32, tiles of 16 pixels x 8 rows): per tile one halo box per
+// tap column (dw), 10 rows x 16 pixels x 32 channels, read once for that
+// column's three taps (dh), whose A operands are the box's rows dh .. dh + 7
+// (1024 bytes apart: whole 64-byte-swizzle atoms); the weights of all 9
+// taps stay in shared memory for the CTA's life.  Per tile 30 KB cross
+// from L2 instead of 80 KB of tap boxes plus the weights.
+constexpr int H3W = 16, H3H = 8;
+constexpr uint32_t A3_BYTES = (H3H + 2) * H3W * 64;
 constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;
 
 __device__ int g_tc_error; // a bounded wait of a tensor-core kernel gave up
@@ -236,6 +244,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
 
 // Stages plus 1 KB to align the first to a swizzle atom.
 template <int BN> constexpr int tc_smem() { return tc_stages<BN>() * (TBM + BN) * TBK * 2 + 1024; }
+template <int BN> constexpr int tc_smem3()
+{
+    return tc_stages<BN>() * static_cast<int>(A3_BYTES) + 9 * BN * 64 + 1024;
+}
 
 // AMODE selects how the stages are filled: 0, the cp.async im2col gather
 // (any shape); 1 and 2, TMA tile loads by one thread, for shapes whose
@@ -246,6 +258,9 @@ template <int BN> constexpr int tc_smem() { return tc_stages<BN>() * (TBM + BN) 
 // chunk, 128-byte swizzle, as the gather lays it out.  AMODE 2 (Cin 32): a
 // chunk is two taps, two boxes of 32 channels in 64-byte-swizzled K-major
 // tiles of 8 KB each (a tenth tap reads a box wholly outside the image).
+// AMODE 3: the halo boxes described at A3_BYTES (Cin 32, Cout = BN, W a
+// multiple of 16, H of 8), the weights through a 2-D map [Cout][9 Cin] in
+// boxes of 32 k (one tap) x BN rows, 64-byte swizzle.
 template <int BN, int AMODE>
 __global__ void __launch_bounds__(TC_THREADS)
     k_conv_fwd_tc(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
@@ -255,21 +270,32 @@ __global__ void __launch_bounds__(TC_THREADS)
                   const __grid_constant__ CUtensorMap tmw, int BW, int BH)
 {
     static_assert(BN == 32 || BN == 64 || BN == 128, "tensor-memory columns: a power of 2");
-    static_assert(AMODE >= 0 && AMODE <= 2, "gather, TMA 128-byte or TMA 64-byte tiles");
+    static_assert(AMODE >= 0 && AMODE <= 3,
+                  "gather, TMA 128-byte, TMA 64-byte tap tiles, TMA halo boxes");
     constexpr int TST = tc_stages<BN>();
     constexpr uint32_t A_BYTES = TBM * TBK * 2, B_BYTES = BN * TBK * 2;
-    constexpr uint32_t STAGE = A_BYTES + B_BYTES;
+    constexpr uint32_t STAGE = AMODE == 3 ? A3_BYTES : A_BYTES + B_BYTES;
     extern __shared__ __align__(1024) unsigned char tc_smem_dyn[];
     __shared__ uint64_t bar_full[TST], bar_empty[TST];
     __shared__ uint64_t bar_acc_full[2], bar_acc_empty[2];
     __shared__ uint64_t bar_done;
+    __shared__ uint64_t bar_w; // AMODE 3: the resident weights have landed
     __shared__ uint32_t s_tmem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int M = N * H * W;
     const int K = 9 * Cin;
-    const int KT = (K + TBK - 1) / TBK;
+    const int KT = AMODE == 3 ? 3 : (K + TBK - 1) / TBK; // AMODE 3: one chunk per tap column
     const int ntiles_n = Cout / BN;
-    const int ntiles = ((M + TBM - 1) / TBM) * ntiles_n;
+    const int ntiles = AMODE == 3 ? N * (H / H3H) * (W / H3W)
+                                  : ((M + TBM - 1) / TBM) * ntiles_n;
+    // AMODE 3: image and top-left pixel of tile t (row-major over 16 x 8 tiles).
+    auto tile3 = [&](int t, int &img, int &th, int &tw) {
+        const int tx = W / H3W, per = tx * (H / H3H);
+        img = t / per;
+        const int r = t % per;
+        th = (r / tx) * H3H;
+        tw = (r % tx) * H3W;
+    };
 
     if (warp == 4) { // two accumulators: the epilogue of a tile overlaps the next
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -287,6 +313,7 @@ __global__ void __launch_bounds__(TC_THREADS)
             tc_mbar_init(&bar_acc_empty[i], TBM); // every epilogue thread arrives
         }
         tc_mbar_init(&bar_done, 1);
+        tc_mbar_init(&bar_w, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -297,8 +324,33 @@ __global__ void __launch_bounds__(TC_THREADS)
     // The swizzle acts on address bits: stages start on 1024-byte boundaries.
     unsigned char *tc_smem_raw =
         tc_smem_dyn + ((1024u - (smem_u32(tc_smem_dyn) & 1023u)) & 1023u);
+    unsigned char *const w3_smem = tc_smem_raw + TST * A3_BYTES; // AMODE 3 weights
 
-    if (AMODE && warp < 4) {
+    if (AMODE == 3 && warp < 4) {
+        if (tid == 0) { // TMA producer: the weights once, then per tile a box per tap column
+            tc_mbar_expect_tx(&bar_w, 9u * BN * 64u);
+            for (int tap = 0; tap < 9; ++tap)
+                tma_load_2d(w3_smem + tap * BN * 64, &tmw, 32 * tap, 0, &bar_w);
+            int g = 0;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                int img, th, tw;
+                tile3(t, img, th, tw);
+                for (int d = 0; d < 3; ++d, ++g) { // tap column dw = d - 1
+                    const int st = g % TST;
+                    if (g >= TST)
+                        ok = tc_mbar_wait(&bar_empty[st],
+                                          static_cast<uint32_t>(((g - TST) / TST) & 1));
+                    if (!ok)
+                        break;
+                    tc_mbar_expect_tx(&bar_full[st], A3_BYTES);
+                    // Rows th - 1 .. th + 8, pixels tw + d - 1 ..: zeros outside
+                    // the image are the padding.
+                    tma_load_4d(tc_smem_raw + st * A3_BYTES, &tmx, 0, tw + d - 1, th - 1, img,
+                                &bar_full[st]);
+                }
+            }
+        }
+    } else if (AMODE && warp < 4) {
         if (tid == 0) { // TMA producer: chunks in the order the MMA thread takes them
             int g = 0;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
@@ -402,6 +454,8 @@ __global__ void __launch_bounds__(TC_THREADS)
     } else if (warp == 4) {
         if (lane == 0) { // MMA issuer
             int g = 0, i = 0;
+            if (AMODE == 3)
+                ok = tc_mbar_wait(&bar_w, 0);
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
                 const int b = i & 1;
                 if (i >= 2)
@@ -415,17 +469,32 @@ __global__ void __launch_bounds__(TC_THREADS)
                         break;
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t sa = smem_u32(tc_smem_raw + st * STAGE), sb = sa + A_BYTES;
+                    if constexpr (AMODE == 3) {
+                        // Chunk kc is tap column dw = kc - 1; tap (dh, dw) reads
+                        // box rows dh + 1 .. dh + 8, 1024 bytes per row of 16
+                        // pixels, and weight box 3 (dh + 1) + kc.
+                        const uint32_t sw = smem_u32(w3_smem);
 #pragma unroll
-                    for (int kk = 0; kk < TBK / 16; ++kk) {
-                        // AMODE 2: k 0-31 in the first 64-byte-swizzled
-                        // tile, 32-63 in the second.
-                        const uint64_t da =
-                            AMODE == 2
-                                ? umma_desc_sw64(sa + (kk >> 1) * (A_BYTES / 2) + 32 * (kk & 1))
-                                : umma_desc_sw128(sa + 32 * kk);
-                        umma_bf16(tmem + static_cast<uint32_t>(b * BN), da,
-                                  umma_desc_sw128(sb + 32 * kk), umma_idesc<BN>(),
-                                  (kc > 0 || kk > 0) ? 1u : 0u);
+                        for (int r = 0; r < 3; ++r)
+#pragma unroll
+                            for (int kk = 0; kk < 2; ++kk)
+                                umma_bf16(tmem + static_cast<uint32_t>(b * BN),
+                                          umma_desc_sw64(sa + 1024u * r + 32 * kk),
+                                          umma_desc_sw64(sw + (3 * r + kc) * BN * 64 + 32 * kk),
+                                          umma_idesc<BN>(), (kc > 0 || r > 0 || kk > 0) ? 1u : 0u);
+                    } else {
+#pragma unroll
+                        for (int kk = 0; kk < TBK / 16; ++kk) {
+                            // AMODE 2: k 0-31 in the first 64-byte-swizzled
+                            // tile, 32-63 in the second.
+                            const uint64_t da =
+                                AMODE == 2 ? umma_desc_sw64(sa + (kk >> 1) * (A_BYTES / 2) +
+                                                            32 * (kk & 1))
+                                           : umma_desc_sw128(sa + 32 * kk);
+                            umma_bf16(tmem + static_cast<uint32_t>(b * BN), da,
+                                      umma_desc_sw128(sb + 32 * kk), umma_idesc<BN>(),
+                                      (kc > 0 || kk > 0) ? 1u : 0u);
+                        }
                     }
                     umma_commit(&bar_empty[st]);
                 }
@@ -443,8 +512,16 @@ __global__ void __launch_bounds__(TC_THREADS)
             if (ok)
                 ok = tc_mbar_wait(&bar_acc_full[b], static_cast<uint32_t>((i >> 1) & 1));
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int m0 = (t / ntiles_n) * TBM, n0 = (t % ntiles_n) * BN;
-            const int m = m0 + row;
+            int m, n0;
+            if (AMODE == 3) { // accumulator row = pixel (th + row / 16, tw + row % 16)
+                int img, th, tw;
+                tile3(t, img, th, tw);
+                m = (img * H + th + row / H3W) * W + tw + row % H3W;
+                n0 = 0;
+            } else {
+                m = (t / ntiles_n) * TBM + row;
+                n0 = (t % ntiles_n) * BN;
+            }
             const bool am = m < M;
 #pragma unroll
             for (int c = 0; c < BN; c += 16) {
@@ -1140,6 +1217,32 @@ bool conv_tma_maps(const bf16 *x, const bf16 *w, int n, int h, int w_, int cin, 
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The TMA maps of AMODE 3: the input [N][H][W][32] in halo boxes of 32
+// channels x 16 pixels x 10 rows, the weights [Cout][9 x 32] in boxes of one
+// tap (32 k) x bn rows, both with the 64-byte swizzle.
+bool conv_tma_maps3(const bf16 *x, const bf16 *w, int n, int h, int w_, int cout, int bn,
+                    CUtensorMap *mx, CUtensorMap *mw)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(x) & 15u) || (reinterpret_cast<uintptr_t>(w) & 15u))
+        return false;
+    const cuuint64_t xd[4] = {32, cuuint64_t(w_), cuuint64_t(h), cuuint64_t(n)};
+    const cuuint64_t xs[3] = {64, cuuint64_t(w_) * 64, cuuint64_t(h) * w_ * 64};
+    const cuuint32_t xb[4] = {32, H3W, H3H + 2, 1};
+    const cuuint32_t one[4] = {1, 1, 1, 1};
+    if (enc(mx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(x), xd, xs, xb, one,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    const cuuint64_t wd[2] = {9 * 32, cuuint64_t(cout)};
+    const cuuint64_t ws[1] = {9 * 32 * 2};
+    const cuuint32_t wb[2] = {32, cuuint32_t(bn)};
+    return enc(mw, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(w), wd, ws, wb, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int BN, int AMODE>
 int conv_fwd_tc_mode(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
                      float *y32, int n, int h, int w_, int cin, int cout, int relu,
@@ -1147,9 +1250,10 @@ int conv_fwd_tc_mode(const bf16 *x, const bf16 *w, const float *bias, const bf16
 {
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
+    constexpr int smem = AMODE == 3 ? tc_smem3<BN>() : tc_smem<BN>();
     std::call_once(once, [] {
         attr = cudaFuncSetAttribute(k_conv_fwd_tc<BN, AMODE>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<BN>());
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     });
     if (attr != cudaSuccess)
         return ERR_CUDA;
@@ -1163,22 +1267,31 @@ int conv_fwd_tc_mode(const bf16 *x, const bf16 *w, const float *bias, const bf16
     // Persistent: tc_ctas_per_sm CTAs per SM, each taking tiles
     // blockIdx.x + i * gridDim.x.
     const int M = n * h * w_;
-    const int64_t tiles = static_cast<int64_t>((M + TBM - 1) / TBM) * (cout / BN);
+    const int64_t tiles = AMODE == 3 ? int64_t(n) * (h / H3H) * (w_ / H3W)
+                                     : static_cast<int64_t>((M + TBM - 1) / TBM) * (cout / BN);
     const int per_sm = tc_ctas_per_sm<BN>();
     const int grid = static_cast<int>(tiles < int64_t(sms) * per_sm ? tiles : int64_t(sms) * per_sm);
-    k_conv_fwd_tc<BN, AMODE><<<grid, TC_THREADS, tc_smem<BN>(), s>>>(
+    k_conv_fwd_tc<BN, AMODE><<<grid, TC_THREADS, smem, s>>>(
         x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx, mw, bw, bh);
     return status();
 }
 
-// TMA tiles when every 128-pixel tile is a rectangle of one image (W a
-// divisor or a multiple of 128, H W a multiple of 128) and Cin is 32 or a
-// multiple of 64; the cp.async gather otherwise.
+// Halo boxes (AMODE 3) for Cin 32 with one channel tile on 16 x 8-pixel
+// tiles; else TMA tiles when every 128-pixel tile is a rectangle of one
+// image (W a divisor or a multiple of 128, H W a multiple of 128) and Cin is
+// 32 or a multiple of 64; the cp.async gather otherwise.
 template <int BN>
 int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
                 float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
 {
     CUtensorMap mx, mw;
+#ifndef DSMC_CONV_HALO
+#define DSMC_CONV_HALO 1
+#endif
+    if (DSMC_CONV_HALO && cin == 32 && cout == BN && w_ % H3W == 0 && h % H3H == 0 &&
+        conv_tma_maps3(x, w, n, h, w_, cout, BN, &mx, &mw))
+        return conv_fwd_tc_mode<BN, 3>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx,
+                                       mw, H3W, H3H, s);
     const bool rect = (w_ % TBM == 0 || TBM % w_ == 0) && (int64_t(h) * w_) % TBM == 0;
     const int bw = w_ < TBM ? w_ : TBM, bh = TBM / bw;
     if (rect && cin % 64 == 0 &&

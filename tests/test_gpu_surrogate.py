@@ -41,14 +41,19 @@ def _close(got, want, rtol, what):
     assert err <= rtol, f"{what}: max error {err:.3e} of scale {scale:.3e}"
 
 
-# Shapes whose 128-pixel tiles are rectangles of one image take the TMA
+# Cin 32 with one channel tile on images of 16-pixel columns and 8-pixel
+# rows takes the halo boxes (16 x 8-pixel tiles: (1, 32, 32, 32, 64),
+# (2, 16, 32, 32, 32), (3, 8, 16, 32, 32), (2, 128, 128, 32, 128)); other
+# shapes whose 128-pixel tiles are rectangles of one image take the TMA tap
 # loads (Cin 32: two 64-byte-swizzled taps a chunk; Cin a multiple of 64:
 # 128-byte-swizzled boxes); the others, and Cin 96, the cp.async gather.
 @pytest.mark.parametrize("n,h,w,cin,cout", [(2, 8, 8, 32, 32), (1, 12, 20, 64, 96),
                                             (3, 16, 16, 128, 64), (2, 16, 8, 32, 32),
                                             (1, 32, 32, 32, 64), (1, 4, 256, 64, 128),
                                             (2, 8, 16, 96, 32), (1, 2, 128, 256, 32),
-                                            (1, 160, 128, 64, 128), (1, 150, 130, 32, 128)])
+                                            (1, 160, 128, 64, 128), (1, 150, 130, 32, 128),
+                                            (2, 16, 32, 32, 32), (3, 8, 16, 32, 32),
+                                            (2, 128, 128, 32, 128)])
 def test_conv_forward(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
@@ -78,7 +83,7 @@ def test_conv_forward(cuda, n, h, w, cin, cout):
                                             (1, 9, 11, 96, 64), (1, 5, 9, 32, 160),
                                             (1, 6, 10, 128, 256), (2, 16, 16, 64, 32),
                                             (1, 8, 32, 32, 128), (1, 8, 16, 128, 256),
-                                            (2, 4, 64, 32, 160)])
+                                            (2, 4, 64, 32, 160), (2, 16, 32, 32, 32)])
 def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
