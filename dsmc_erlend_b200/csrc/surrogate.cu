@@ -244,6 +244,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16])
 
 // Stages plus 1 KB to align the first to a swizzle atom.
 template <int BN> constexpr int tc_smem() { return tc_stages<BN>() * (TBM + BN) * TBK * 2 + 1024; }
+// CTAs per SM of AMODE 3 (measured: for 64 channels what its shared memory
+// lets reside, 3 instead of the tap-tile form's 4; 4 for 32 channels, which
+// would fit, measured slower than 3).
+template <int BN> constexpr int tc_ctas_per_sm3() { return BN == 128 ? 2 : 3; }
 template <int BN> constexpr int tc_smem3()
 {
     return tc_stages<BN>() * static_cast<int>(A3_BYTES) + 9 * BN * 64 + 1024;
@@ -1269,7 +1273,7 @@ int conv_fwd_tc_mode(const bf16 *x, const bf16 *w, const float *bias, const bf16
     const int M = n * h * w_;
     const int64_t tiles = AMODE == 3 ? int64_t(n) * (h / H3H) * (w_ / H3W)
                                      : static_cast<int64_t>((M + TBM - 1) / TBM) * (cout / BN);
-    const int per_sm = tc_ctas_per_sm<BN>();
+    const int per_sm = AMODE == 3 ? tc_ctas_per_sm3<BN>() : tc_ctas_per_sm<BN>();
     const int grid = static_cast<int>(tiles < int64_t(sms) * per_sm ? tiles : int64_t(sms) * per_sm);
     k_conv_fwd_tc<BN, AMODE><<<grid, TC_THREADS, smem, s>>>(
         x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx, mw, bw, bh);
