@@ -634,7 +634,7 @@ __device__ __forceinline__ uint32_t sw128_mn_off(int m, int k, uint32_t sbo)
 }
 template <int NB> __host__ __device__ constexpr int wg_stage() { return 128 * WG_PIX * 2 + NB * WG_PIX * 2; }
 template <int NB> constexpr int wg_smem() { return WG_ST * wg_stage<NB>() + 1024; }
-template <int NB> constexpr int wg_ctas_per_sm() { return NB == 64 ? 3 : (NB == 128 ? 2 : 1); }
+template <int NB> constexpr int wg_ctas_per_sm() { return NB <= 64 ? 3 : (NB == 128 ? 2 : 1); }
 
 // TMA: the stages are filled by one thread with tile loads for shapes whose
 // 64-pixel chunks are BW x BH rectangles of one image: per tap a box of
@@ -643,7 +643,8 @@ template <int NB> constexpr int wg_ctas_per_sm() { return NB == 64 ? 3 : (NB == 
 // boxes of 64 channels x 64 pixels from a 2-D map of dY [pixels][Cout]
 // (zeros past Cout).  A box is rows of pixels as they sit in memory, which
 // is the MN-major swizzled tile: atoms along M a box apart (LBO), 8-pixel
-// groups one atom row apart (SBO); 64-byte swizzle for Cin 32.
+// groups one atom row apart (SBO); 64-byte swizzle for Cin 32.  NB 32 (Cout
+// 32, TMA only): one dY box of 32 channels, 64-byte swizzle, N = 32.
 template <int CI, int NB, bool TMA>
 __global__ void __launch_bounds__(WG_THREADS)
     k_conv_wgrad_tc(const bf16 *__restrict__ dy, const bf16 *__restrict__ x,
@@ -652,7 +653,9 @@ __global__ void __launch_bounds__(WG_THREADS)
                     const __grid_constant__ CUtensorMap tmy, int BW, int BH)
 {
     static_assert(CI == 32 || CI == 64 || CI == 128, "taps x Cin fill the 128 rows");
-    static_assert(NB == 64 || NB == 128 || NB == 256, "whole 64-channel swizzle atoms");
+    static_assert(NB == 32 || NB == 64 || NB == 128 || NB == 256,
+                  "one 32-channel or whole 64-channel swizzle atoms");
+    static_assert(NB != 32 || TMA, "32 output channels: TMA boxes only");
     constexpr int TAPS = 128 / CI;
     constexpr uint32_t A_BYTES = 128 * WG_PIX * 2;
     constexpr uint32_t STAGE = wg_stage<NB>();
@@ -690,7 +693,8 @@ __global__ void __launch_bounds__(WG_THREADS)
     unsigned char *sm = wg_smem_dyn + ((1024u - (smem_u32(wg_smem_dyn) & 1023u)) & 1023u);
 
     constexpr int CB = CI < 64 ? CI : 64;                  // channels of an X box
-    constexpr uint32_t XBOX = CB * WG_PIX * 2, YBOX = 64 * WG_PIX * 2;
+    constexpr int YC = NB < 64 ? NB : 64;                  // channels of a dY box
+    constexpr uint32_t XBOX = CB * WG_PIX * 2, YBOX = YC * WG_PIX * 2;
     if (TMA && warp < 4) {
         if (tid == 0) {
             for (int kc = 0; kc < KT; ++kc) {
@@ -714,8 +718,8 @@ __global__ void __launch_bounds__(WG_THREADS)
                                 img, &bar_full[st]);
                 }
 #pragma unroll
-                for (int b = 0; b < NB / 64; ++b)
-                    tma_load_2d(sa + A_BYTES + b * YBOX, &tmy, 64 * b, p0, &bar_full[st]);
+                for (int b = 0; b < NB / YC; ++b)
+                    tma_load_2d(sa + A_BYTES + b * YBOX, &tmy, YC * b, p0, &bar_full[st]);
             }
         }
     } else if (warp < 4) {
@@ -803,12 +807,14 @@ __global__ void __launch_bounds__(WG_THREADS)
             const uint32_t sa = smem_u32(sm + st * STAGE);
 #pragma unroll
             for (int kk = 0; kk < WG_PIX / 16; ++kk) {
-                // TMA boxes: 8-pixel groups of CB (X) or 64 (dY) channels.
+                // TMA boxes: 8-pixel groups of CB (X) or YC (dY) channels.
                 const uint64_t da =
                     TMA ? umma_desc_mn(sa + kk * 2 * (CB * 16), XBOX, CB * 16, CB == 64 ? 2 : 4)
                         : umma_desc_sw128_mn(sa + kk * 2 * SBO_A, SBO_A);
-                const uint64_t db = TMA ? umma_desc_mn(sa + A_BYTES + kk * 2 * 1024, YBOX, 1024, 2)
-                                        : umma_desc_sw128_mn(sa + A_BYTES + kk * 2 * SBO_B, SBO_B);
+                const uint64_t db =
+                    TMA ? umma_desc_mn(sa + A_BYTES + kk * 2 * (YC * 16), YBOX, YC * 16,
+                                       YC == 64 ? 2 : 4)
+                        : umma_desc_sw128_mn(sa + A_BYTES + kk * 2 * SBO_B, SBO_B);
                 umma_bf16(tmem, da, db, umma_idesc_mn<NB>(), (kc > 0 || kk > 0) ? 1u : 0u);
             }
             umma_commit(&bar_empty[st]);
@@ -1316,7 +1322,7 @@ int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res
 // channels x bw x bh pixels (128- or 64-byte swizzle), dY [pixels][Cout] in
 // boxes of 64 channels x 64 pixels.  False when they do not suit.
 bool wgrad_tma_maps(const bf16 *dy, const bf16 *x, int n, int h, int w_, int cin, int cout,
-                    int cb, int bw, int bh, CUtensorMap *mx, CUtensorMap *my)
+                    int cb, int bw, int bh, CUtensorMap *mx, CUtensorMap *my, int yc = 64)
 {
     auto enc = tensor_map_encoder();
     if (!enc || (reinterpret_cast<uintptr_t>(x) & 15u) || (reinterpret_cast<uintptr_t>(dy) & 15u))
@@ -1334,12 +1340,17 @@ bool wgrad_tma_maps(const bf16 *dy, const bf16 *x, int n, int h, int w_, int cin
         return false;
     const cuuint64_t yd[2] = {cuuint64_t(cout), cuuint64_t(n) * h * w_};
     const cuuint64_t ys[1] = {cuuint64_t(cout) * 2};
-    const cuuint32_t yb[2] = {64, cuuint32_t(WG_PIX)};
+    const cuuint32_t yb[2] = {cuuint32_t(yc), cuuint32_t(WG_PIX)};
     return enc(my, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(dy), yd, ys, yb, one,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_INTERLEAVE_NONE,
+               yc == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
+
+// NB 32 (Cout 32: N 32 instead of a zero-filled 64, half the MMA work) has
+// no gather form: it returns WG_NOT_TAKEN when the chunks are no rectangles.
+constexpr int WG_NOT_TAKEN = -1;
 
 template <int CI, int NB>
 int wgrad_tc(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int cout,
@@ -1348,8 +1359,10 @@ int wgrad_tc(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_conv_wgrad_tc<CI, NB, false>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, wg_smem<NB>());
+        if constexpr (NB != 32)
+            attr = cudaFuncSetAttribute(k_conv_wgrad_tc<CI, NB, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        wg_smem<NB>());
         if (attr == cudaSuccess)
             attr = cudaFuncSetAttribute(k_conv_wgrad_tc<CI, NB, true>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1376,9 +1389,12 @@ int wgrad_tc(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int
     CUtensorMap mx, my;
     const bool rect = (w_ % WG_PIX == 0 || WG_PIX % w_ == 0) && (int64_t(h) * w_) % WG_PIX == 0;
     const int bw = w_ < WG_PIX ? w_ : WG_PIX, bh = WG_PIX / bw;
-    if (rect && wgrad_tma_maps(dy, x, n, h, w_, CI, cout, CI < 64 ? CI : 64, bw, bh, &mx, &my)) {
+    if (rect && wgrad_tma_maps(dy, x, n, h, w_, CI, cout, CI < 64 ? CI : 64, bw, bh, &mx, &my,
+                               NB < 64 ? NB : 64)) {
         k_conv_wgrad_tc<CI, NB, true><<<dim3(splits, groups), WG_THREADS, wg_smem<NB>(), s>>>(
             dy, x, dw, n, h, w_, cout, per, mx, my, bw, bh);
+    } else if constexpr (NB == 32) {
+        return WG_NOT_TAKEN;
     } else {
         memset(&mx, 0, sizeof(mx));
         memset(&my, 0, sizeof(my));
@@ -1392,6 +1408,11 @@ template <int CI>
 int wgrad_tc_n(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int cout,
                cudaStream_t s)
 {
+    if (cout == 32) {
+        const int st = wgrad_tc<CI, 32>(dy, x, dw, n, h, w_, cout, s);
+        if (st != WG_NOT_TAKEN)
+            return st;
+    }
     if (cout <= 64)
         return wgrad_tc<CI, 64>(dy, x, dw, n, h, w_, cout, s);
     if (cout <= 128)

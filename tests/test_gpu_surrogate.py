@@ -107,7 +107,7 @@ def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     assert L.dsmc_sg_check(None) == 0
 
 
-@pytest.mark.parametrize("cin,cout", [(32, 64), (64, 128), (128, 32)])
+@pytest.mark.parametrize("cin,cout", [(32, 64), (64, 128), (128, 32), (32, 32), (64, 32)])
 def test_wgrad_large_pixel_count_splits(cuda, cin, cout):
     # Enough pixels for several pixel splits, and accumulation into dw.
     from dsmc_erlend_b200.surrogate import lib, ptr
