@@ -851,6 +851,143 @@ __global__ void __launch_bounds__(WG_THREADS)
                      : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// wgrad for Cin 32 on images of 16-pixel columns and 8-pixel rows, Cout = NB
+// (32 or 64): per 16 x 8-pixel tile one halo box of X per tap column (dw),
+// 10 rows x 16 pixels x 32 channels (the forward's AMODE 3 box), and one
+// box of dY, 8 rows x 16 pixels x NB channels.  MMA M = 128 rows (four
+// 32-row atoms: the column's taps dh = -1, 0, 1 and a fourth whose rows are
+// discarded) x N = NB x K = the tile's pixels, both operands MN-major.  The
+// A atom of tap dh is the box shifted by dh + 1 image rows (1024 bytes,
+// whole 64-byte-swizzle atoms), so one descriptor (leading offset 1024,
+// stride 512 between 8-pixel groups) covers the three taps; the fourth atom
+// reads up to a row past the box, inside the slot.  Per tile 38 KB (NB 32)
+// cross from L2 instead of 120 KB for the tap-box form's three tap groups,
+// with the same 3/4 of the MMA rows useful (9 of 12 taps there).  Each tap
+// column accumulates into its own NB tensor-memory columns over all the
+// CTA's tiles; one CTA per SM over a contiguous range of tiles; producer
+// thread 0, MMA thread 32, epilogue warps 0-2 (the tensor-memory lanes of
+// the useful atoms).
+// ---------------------------------------------------------------------------
+constexpr uint32_t WH_XSLOT = (H3H + 3) * H3W * 64; // a box and the fourth atom's extra row
+constexpr int WH_ST = 4;
+template <int NB> __host__ __device__ constexpr uint32_t wh_ybytes() { return H3W * H3H * NB * 2; }
+template <int NB> __host__ __device__ constexpr uint32_t wh_stage()
+{
+    return 3 * WH_XSLOT + wh_ybytes<NB>();
+}
+template <int NB> constexpr int wh_smem() { return WH_ST * static_cast<int>(wh_stage<NB>()) + 1024; }
+
+template <int NB>
+__global__ void __launch_bounds__(128, 1)
+    k_conv_wgrad_halo(float *__restrict__ dw, int N, int H, int W, int per,
+                      const __grid_constant__ CUtensorMap tmx,
+                      const __grid_constant__ CUtensorMap tmy)
+{
+    static_assert(NB == 32 || NB == 64, "one dY box of 32 or 64 channels");
+    constexpr uint32_t STAGE = wh_stage<NB>(), YBYTES = wh_ybytes<NB>();
+    constexpr uint32_t TCOLS = NB == 32 ? 128 : 256; // 3 NB accumulator columns
+    static_assert(STAGE % 1024 == 0 && WH_XSLOT % 1024 == 0, "swizzle atoms stay aligned");
+    extern __shared__ __align__(1024) unsigned char wh_smem_dyn[];
+    __shared__ uint64_t bar_full[WH_ST], bar_empty[WH_ST];
+    __shared__ uint64_t bar_done;
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tx = W / H3W, tpi = tx * (H / H3H);
+    const int ntiles = N * tpi;
+    const int t_begin = blockIdx.x * per;
+    const int KT = max(0, min(ntiles, t_begin + per) - t_begin);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&s_tmem)), "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 32) {
+        for (int i = 0; i < WH_ST; ++i) {
+            tc_mbar_init(&bar_full[i], 1);
+            tc_mbar_init(&bar_empty[i], 1);
+        }
+        tc_mbar_init(&bar_done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    bool ok = true;
+    unsigned char *sm = wh_smem_dyn + ((1024u - (smem_u32(wh_smem_dyn) & 1023u)) & 1023u);
+
+    if (tid == 0) {
+        for (int kc = 0; kc < KT; ++kc) {
+            const int st = kc % WH_ST;
+            if (kc >= WH_ST)
+                ok = tc_mbar_wait(&bar_empty[st], static_cast<uint32_t>(((kc - WH_ST) / WH_ST) & 1));
+            if (!ok)
+                break;
+            const int t = t_begin + kc, img = t / tpi, r = t % tpi;
+            const int th = (r / tx) * H3H, tw = (r % tx) * H3W;
+            unsigned char *sa = sm + st * STAGE;
+            tc_mbar_expect_tx(&bar_full[st], 3 * A3_BYTES + YBYTES);
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                tma_load_4d(sa + d * WH_XSLOT, &tmx, 0, tw + d - 1, th - 1, img, &bar_full[st]);
+            tma_load_4d(sa + 3 * WH_XSLOT, &tmy, 0, tw, th, img, &bar_full[st]);
+        }
+    } else if (tid == 32) {
+        for (int kc = 0; kc < KT && ok; ++kc) {
+            const int st = kc % WH_ST;
+            ok = tc_mbar_wait(&bar_full[st], static_cast<uint32_t>((kc / WH_ST) & 1));
+            if (!ok)
+                break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(sm + st * STAGE), sy = sa + 3 * WH_XSLOT;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+#pragma unroll
+                for (int kk = 0; kk < H3H; ++kk) {
+                    // K step kk: image row kk of the tile (two 8-pixel groups).
+                    const uint64_t da = umma_desc_mn(sa + d * WH_XSLOT + kk * 1024, 1024, 512, 4);
+                    const uint64_t db = umma_desc_mn(sy + kk * 2 * (NB * 16), YBYTES, NB * 16,
+                                                     NB == 64 ? 2 : 4);
+                    umma_bf16(tmem + static_cast<uint32_t>(d * NB), da, db, umma_idesc_mn<NB>(),
+                              (kc > 0 || kk > 0) ? 1u : 0u);
+                }
+            }
+            umma_commit(&bar_empty[st]);
+        }
+        umma_commit(&bar_done);
+    }
+    const bool done = tc_mbar_wait(&bar_done, 0);
+    const bool ok_all = __syncthreads_and(ok && done);
+    if (!ok_all && tid == 0)
+        atomicExch(&g_tc_error, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok_all && warp < 3 && KT > 0) {
+        // Lane 32 a + ci of tap column d: dW[co][3 a + d][ci].
+#pragma unroll 1
+        for (int d = 0; d < 3; ++d) {
+            float *dst = dw + (warp * 3 + d) * 32 + (tid & 31);
+#pragma unroll 1
+            for (int c = 0; c < NB; c += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) +
+                              static_cast<uint32_t>(d * NB + c),
+                          r);
+#pragma unroll
+                for (int e = 0; e < 16; ++e)
+                    atomicAdd(dst + static_cast<int64_t>(c + e) * 9 * 32, __uint_as_float(r[e]));
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS)
+                     : "memory");
+}
+
 // w_rot[ci][tap][co] = w[co][8 - tap][ci]: the weights of the dgrad conv.
 __global__ void k_rotate(const bf16 *__restrict__ w, bf16 *__restrict__ w_rot, int Cin, int Cout)
 {
@@ -1230,20 +1367,29 @@ bool conv_tma_maps(const bf16 *x, const bf16 *w, int n, int h, int w_, int cin, 
 // The TMA maps of AMODE 3: the input [N][H][W][32] in halo boxes of 32
 // channels x 16 pixels x 10 rows, the weights [Cout][9 x 32] in boxes of one
 // tap (32 k) x bn rows, both with the 64-byte swizzle.
-bool conv_tma_maps3(const bf16 *x, const bf16 *w, int n, int h, int w_, int cout, int bn,
-                    CUtensorMap *mx, CUtensorMap *mw)
+// The halo boxes of a [N][H][W][32] input: 32 channels x 16 pixels x 10 rows.
+bool halo_x_map(const bf16 *x, int n, int h, int w_, CUtensorMap *mx)
 {
     auto enc = tensor_map_encoder();
-    if (!enc || (reinterpret_cast<uintptr_t>(x) & 15u) || (reinterpret_cast<uintptr_t>(w) & 15u))
+    if (!enc || (reinterpret_cast<uintptr_t>(x) & 15u))
         return false;
     const cuuint64_t xd[4] = {32, cuuint64_t(w_), cuuint64_t(h), cuuint64_t(n)};
     const cuuint64_t xs[3] = {64, cuuint64_t(w_) * 64, cuuint64_t(h) * w_ * 64};
     const cuuint32_t xb[4] = {32, H3W, H3H + 2, 1};
     const cuuint32_t one[4] = {1, 1, 1, 1};
-    if (enc(mx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(x), xd, xs, xb, one,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return enc(mx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(x), xd, xs, xb, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool conv_tma_maps3(const bf16 *x, const bf16 *w, int n, int h, int w_, int cout, int bn,
+                    CUtensorMap *mx, CUtensorMap *mw)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(w) & 15u) || !halo_x_map(x, n, h, w_, mx))
         return false;
+    const cuuint32_t one[4] = {1, 1, 1, 1};
     const cuuint64_t wd[2] = {9 * 32, cuuint64_t(cout)};
     const cuuint64_t ws[1] = {9 * 32 * 2};
     const cuuint32_t wb[2] = {32, cuuint32_t(bn)};
@@ -1404,10 +1550,65 @@ int wgrad_tc(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int
     return status();
 }
 
+// The halo-box weight gradient (Cin 32, Cout = NB, 16 x 8-pixel tiles); false
+// when the maps do not suit.
+template <int NB>
+bool wgrad_halo(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, cudaStream_t s,
+                int *st)
+{
+    auto enc = tensor_map_encoder();
+    CUtensorMap mx, my;
+    if (!enc || (reinterpret_cast<uintptr_t>(dy) & 15u) || !halo_x_map(x, n, h, w_, &mx))
+        return false;
+    const cuuint64_t yd[4] = {NB, cuuint64_t(w_), cuuint64_t(h), cuuint64_t(n)};
+    const cuuint64_t ys[3] = {NB * 2, cuuint64_t(w_) * NB * 2, cuuint64_t(h) * w_ * NB * 2};
+    const cuuint32_t yb[4] = {NB, H3W, H3H, 1};
+    const cuuint32_t one[4] = {1, 1, 1, 1};
+    if (enc(&my, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(dy), yd, ys, yb, one,
+            CU_TENSOR_MAP_INTERLEAVE_NONE,
+            NB == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_conv_wgrad_halo<NB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, wh_smem<NB>());
+    });
+    static int sms = 0;
+    if (attr == cudaSuccess && sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 0;
+    }
+    if (attr != cudaSuccess || sms == 0) {
+        *st = ERR_CUDA;
+        return true;
+    }
+    // One CTA per SM, each a contiguous range of tiles.
+    const int ntiles = n * (h / H3H) * (w_ / H3W);
+    const int per = (ntiles + sms - 1) / sms;
+    const int splits = (ntiles + per - 1) / per;
+    k_conv_wgrad_halo<NB><<<splits, 128, wh_smem<NB>(), s>>>(dw, n, h, w_, per, mx, my);
+    *st = status();
+    return true;
+}
+
 template <int CI>
 int wgrad_tc_n(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, int cout,
                cudaStream_t s)
 {
+#ifndef DSMC_WGRAD_HALO
+#define DSMC_WGRAD_HALO 1
+#endif
+    if (DSMC_WGRAD_HALO && CI == 32 && h % H3H == 0 && w_ % H3W == 0) {
+        int st = OK;
+        if (cout == 32 && wgrad_halo<32>(dy, x, dw, n, h, w_, s, &st))
+            return st;
+        if (cout == 64 && wgrad_halo<64>(dy, x, dw, n, h, w_, s, &st))
+            return st;
+    }
     if (cout == 32) {
         const int st = wgrad_tc<CI, 32>(dy, x, dw, n, h, w_, cout, s);
         if (st != WG_NOT_TAKEN)

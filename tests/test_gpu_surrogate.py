@@ -83,7 +83,8 @@ def test_conv_forward(cuda, n, h, w, cin, cout):
                                             (1, 9, 11, 96, 64), (1, 5, 9, 32, 160),
                                             (1, 6, 10, 128, 256), (2, 16, 16, 64, 32),
                                             (1, 8, 32, 32, 128), (1, 8, 16, 128, 256),
-                                            (2, 4, 64, 32, 160), (2, 16, 32, 32, 32)])
+                                            (2, 4, 64, 32, 160), (2, 16, 32, 32, 32),
+                                            (1, 8, 16, 32, 64), (3, 16, 16, 32, 32)])
 def test_conv_dgrad_and_wgrad(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
@@ -122,6 +123,25 @@ def test_wgrad_large_pixel_count_splits(cuda, cin, cout):
                                     None) == 0
     torch.cuda.synchronize()
     _close(_np(dw) - 1.0, ref.conv3x3_wgrad(_np(dy), _np(x)), 1e-4, "wgrad split")
+    assert lib().dsmc_sg_check(None) == 0
+
+
+@pytest.mark.parametrize("n,h,w,cout", [(5, 64, 160, 32), (3, 64, 128, 64)])
+def test_wgrad_halo_tile_ranges(cuda, n, h, w, cout):
+    # Cin 32 on 16 x 8-pixel tiles: several tiles a CTA, a short last
+    # range (400 tiles: on 148 SMs 133 CTAs of 3 and one of 1), accumulation
+    # into dw.
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    rng = np.random.default_rng(11)
+    x = _bf16(torch, _rand(rng, n, h, w, 32))
+    dy = _bf16(torch, _rand(rng, n, h, w, cout, scale=0.05))
+    dw = torch.ones(cout, 3, 3, 32, dtype=torch.float32, device="cuda")
+    assert lib().dsmc_sg_conv_wgrad(ptr(dy), ptr(x), ptr(dw), None, n, h, w, 32, cout,
+                                    None) == 0
+    torch.cuda.synchronize()
+    _close(_np(dw) - 1.0, ref.conv3x3_wgrad(_np(dy), _np(x)), 1e-4, "wgrad halo")
     assert lib().dsmc_sg_check(None) == 0
 
 
