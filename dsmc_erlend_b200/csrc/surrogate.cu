@@ -853,30 +853,37 @@ __global__ void __launch_bounds__(WG_THREADS)
 
 // ---------------------------------------------------------------------------
 // wgrad for Cin 32 on images of 16-pixel columns and 8-pixel rows, Cout = NB
-// (32 or 64): per 16 x 8-pixel tile one halo box of X per tap column (dw),
-// 10 rows x 16 pixels x 32 channels (the forward's AMODE 3 box), and one
-// box of dY, 8 rows x 16 pixels x NB channels.  MMA M = 128 rows (four
-// 32-row atoms: the column's taps dh = -1, 0, 1 and a fourth whose rows are
-// discarded) x N = NB x K = the tile's pixels, both operands MN-major.  The
-// A atom of tap dh is the box shifted by dh + 1 image rows (1024 bytes,
-// whole 64-byte-swizzle atoms), so one descriptor (leading offset 1024,
-// stride 512 between 8-pixel groups) covers the three taps; the fourth atom
-// reads up to a row past the box, inside the slot.  Per tile 38 KB (NB 32)
-// cross from L2 instead of 120 KB for the tap-box form's three tap groups,
-// with the same 3/4 of the MMA rows useful (9 of 12 taps there).  Each tap
-// column accumulates into its own NB tensor-memory columns over all the
+// (32 or 64).  Per 16 x 8-pixel tile: one halo box of X, 10 rows (th - 1 ..
+// th + 8) x 16 pixels x 32 channels (the forward's AMODE 3 box), and three
+// boxes of dY, 8 rows x 16 pixels x NB channels, at columns tw + 1, tw,
+// tw - 1.  One MMA per image row of the tile: M = 128 rows (four 32-row
+// atoms, taps dh = -1, 0, 1 and a fourth whose rows are discarded) x N = 3
+// NB (taps dw = -1, 0, 1) x K = 16 pixels, both operands MN-major.  The A
+// atom of dh is the X box shifted by dh + 1 image rows (1024 bytes, whole
+// 64-byte-swizzle atoms: leading offset 1024, stride 512 between 8-pixel
+// groups; the fourth atom reads a row past the box, inside the slot); the B
+// atom of dw is the dY box shifted by -dw columns (leading offset one box).
+// So pixel p pairs X[p + (dh, 0)] with dY[p - (0, dw)]: over a row of tiles
+// each q = p - (0, dw) meets X[q + (dh, dw)] once; the column a shift
+// leaves out meets only padding, the one it brings in reads dY's zero fill.
+// Per tile 34 KB (NB 32) cross from L2 and 8 MMAs of N = 96 issue, against
+// 120 KB and 24 MMAs of N = 32 for the tap-box form's three tap groups; 3/4
+// of the MMA rows are useful in both.  Tap (dh, dw) accumulates into tensor-
+// memory lanes 32 (dh + 1) + ci, columns (dw + 1) NB + co, over all the
 // CTA's tiles; one CTA per SM over a contiguous range of tiles; producer
-// thread 0, MMA thread 32, epilogue warps 0-2 (the tensor-memory lanes of
-// the useful atoms).
+// thread 0, MMA thread 32, epilogue warps 0-2 (the lanes of useful atoms).
 // ---------------------------------------------------------------------------
 constexpr uint32_t WH_XSLOT = (H3H + 3) * H3W * 64; // a box and the fourth atom's extra row
-constexpr int WH_ST = 4;
+template <int NB> __host__ __device__ constexpr int wh_stages() { return NB == 32 ? 6 : 3; }
 template <int NB> __host__ __device__ constexpr uint32_t wh_ybytes() { return H3W * H3H * NB * 2; }
 template <int NB> __host__ __device__ constexpr uint32_t wh_stage()
 {
-    return 3 * WH_XSLOT + wh_ybytes<NB>();
+    return WH_XSLOT + 3 * wh_ybytes<NB>();
 }
-template <int NB> constexpr int wh_smem() { return WH_ST * static_cast<int>(wh_stage<NB>()) + 1024; }
+template <int NB> constexpr int wh_smem()
+{
+    return wh_stages<NB>() * static_cast<int>(wh_stage<NB>()) + 1024;
+}
 
 template <int NB>
 __global__ void __launch_bounds__(128, 1)
@@ -885,6 +892,7 @@ __global__ void __launch_bounds__(128, 1)
                       const __grid_constant__ CUtensorMap tmy)
 {
     static_assert(NB == 32 || NB == 64, "one dY box of 32 or 64 channels");
+    constexpr int WH_ST = wh_stages<NB>();
     constexpr uint32_t STAGE = wh_stage<NB>(), YBYTES = wh_ybytes<NB>();
     constexpr uint32_t TCOLS = NB == 32 ? 128 : 256; // 3 NB accumulator columns
     static_assert(STAGE % 1024 == 0 && WH_XSLOT % 1024 == 0, "swizzle atoms stay aligned");
@@ -929,11 +937,12 @@ __global__ void __launch_bounds__(128, 1)
             const int t = t_begin + kc, img = t / tpi, r = t % tpi;
             const int th = (r / tx) * H3H, tw = (r % tx) * H3W;
             unsigned char *sa = sm + st * STAGE;
-            tc_mbar_expect_tx(&bar_full[st], 3 * A3_BYTES + YBYTES);
+            tc_mbar_expect_tx(&bar_full[st], A3_BYTES + 3 * YBYTES);
+            tma_load_4d(sa, &tmx, 0, tw, th - 1, img, &bar_full[st]);
 #pragma unroll
-            for (int d = 0; d < 3; ++d)
-                tma_load_4d(sa + d * WH_XSLOT, &tmx, 0, tw + d - 1, th - 1, img, &bar_full[st]);
-            tma_load_4d(sa + 3 * WH_XSLOT, &tmy, 0, tw, th, img, &bar_full[st]);
+            for (int d = 0; d < 3; ++d) // tap dw = d - 1: dY shifted by -dw columns
+                tma_load_4d(sa + WH_XSLOT + d * YBYTES, &tmy, 0, tw + 1 - d, th, img,
+                            &bar_full[st]);
         }
     } else if (tid == 32) {
         for (int kc = 0; kc < KT && ok; ++kc) {
@@ -942,18 +951,14 @@ __global__ void __launch_bounds__(128, 1)
             if (!ok)
                 break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(sm + st * STAGE), sy = sa + 3 * WH_XSLOT;
+            const uint32_t sa = smem_u32(sm + st * STAGE), sy = sa + WH_XSLOT;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-#pragma unroll
-                for (int kk = 0; kk < H3H; ++kk) {
-                    // K step kk: image row kk of the tile (two 8-pixel groups).
-                    const uint64_t da = umma_desc_mn(sa + d * WH_XSLOT + kk * 1024, 1024, 512, 4);
-                    const uint64_t db = umma_desc_mn(sy + kk * 2 * (NB * 16), YBYTES, NB * 16,
-                                                     NB == 64 ? 2 : 4);
-                    umma_bf16(tmem + static_cast<uint32_t>(d * NB), da, db, umma_idesc_mn<NB>(),
-                              (kc > 0 || kk > 0) ? 1u : 0u);
-                }
+            for (int kk = 0; kk < H3H; ++kk) {
+                // K step kk: image row kk of the tile (two 8-pixel groups).
+                const uint64_t da = umma_desc_mn(sa + kk * 1024, 1024, 512, 4);
+                const uint64_t db =
+                    umma_desc_mn(sy + kk * 2 * (NB * 16), YBYTES, NB * 16, NB == 64 ? 2 : 4);
+                umma_bf16(tmem, da, db, umma_idesc_mn<3 * NB>(), (kc > 0 || kk > 0) ? 1u : 0u);
             }
             umma_commit(&bar_empty[st]);
         }
@@ -965,7 +970,7 @@ __global__ void __launch_bounds__(128, 1)
         atomicExch(&g_tc_error, 1);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok_all && warp < 3 && KT > 0) {
-        // Lane 32 a + ci of tap column d: dW[co][3 a + d][ci].
+        // Lane 32 a + ci, column d NB + co: dW[co][3 a + d][ci].
 #pragma unroll 1
         for (int d = 0; d < 3; ++d) {
             float *dst = dw + (warp * 3 + d) * 32 + (tid & 31);
