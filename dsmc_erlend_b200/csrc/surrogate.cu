@@ -1139,6 +1139,76 @@ __global__ void k_bias_grad(const bf16 *__restrict__ dy, float *__restrict__ db,
     }
 }
 
+// One pass over a layer's output gradient dy [M][C] for the backward step:
+// skip (when given) receives dy as it comes (skip_acc 0: a copy, the skip
+// source's first gradient; 1: added), then dy = y > 0 ? dy : 0 (when y is
+// given: the ReLU), then db[c] += the sum over pixels of the result.  Lanes
+// and reduction as in k_bias_grad.
+__global__ void k_relu_bias_bwd(bf16 *__restrict__ dy, const bf16 *__restrict__ y,
+                                bf16 *__restrict__ skip, int skip_acc, float *__restrict__ db,
+                                int M, int C)
+{
+    const int c8 = C / 8;
+    const int lanes = blockDim.x / c8;
+    const int g = threadIdx.x % c8, lp = threadIdx.x / c8;
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (lp < lanes)
+        for (int p = blockIdx.x * lanes + lp; p < M; p += gridDim.x * lanes) {
+            const int64_t o = static_cast<int64_t>(p) * C + 8 * g;
+            V8 v = ld8(dy + o);
+            if (skip) {
+                if (skip_acc) {
+                    V8 k = ld8(skip + o);
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        k.v[e] += v.v[e];
+                    st8(skip + o, k);
+                } else {
+                    st8(skip + o, v);
+                }
+            }
+            if (y) {
+                const V8 a = ld8(y + o);
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    v.v[e] = a.v[e] > 0.0f ? v.v[e] : 0.0f;
+                st8(dy + o, v);
+            }
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                s[e] += v.v[e];
+        }
+    __shared__ float part[256][9];
+#pragma unroll
+    for (int e = 0; e < 8; ++e)
+        part[threadIdx.x][e] = s[e];
+    __syncthreads();
+    if (threadIdx.x < C) {
+        const int gg = threadIdx.x / 8, e = threadIdx.x % 8;
+        float t = 0.0f;
+        for (int l = 0; l < lanes; ++l)
+            t += part[l * c8 + gg][e];
+        atomicAdd(db + threadIdx.x, t);
+    }
+}
+
+// Sum of v over the CTA (blockDim.x a multiple of 32, at most 1024), valid
+// in thread 0.
+__device__ __forceinline__ float block_sum(float v)
+{
+    __shared__ float ws[32];
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0)
+        ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float t = 0.0f;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w)
+            t += ws[w];
+    return t;
+}
+
 // ---------------------------------------------------------------------------
 // Elementwise kernels.  Channel counts are multiples of 32, so every kernel
 // moves 8 bf16 (16 bytes) per thread and step, never across a pixel.
@@ -1196,8 +1266,8 @@ __global__ void k_pool_fwd(const bf16 *x, bf16 *y, int N, int H, int W, int C)
     }
 }
 
-// Input-gradient vector i of (n, h, w, c).
-__global__ void k_pool_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
+// Input-gradient vector i of (n, h, w, c); acc: added to dx.
+__global__ void k_pool_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C, int acc)
 {
     const int c8 = C / 8;
     const int64_t n8 = static_cast<int64_t>(N) * H * W * c8;
@@ -1211,6 +1281,12 @@ __global__ void k_pool_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
 #pragma unroll
         for (int k = 0; k < 8; ++k)
             g.v[k] *= 0.25f;
+        if (acc) {
+            const V8 d = ld8(dx + 8 * i);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                g.v[k] = d.v[k] + static_cast<float>(__float2bfloat16(g.v[k]));
+        }
         st8(dx + 8 * i, g);
     }
 }
@@ -1231,8 +1307,9 @@ __global__ void k_up_fwd(const bf16 *x, bf16 *y, int N, int H, int W, int C)
     }
 }
 
-// Input-gradient vector i of (n, h, w, c) from dy of (n, 2h, 2w, c).
-__global__ void k_up_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
+// Input-gradient vector i of (n, h, w, c) from dy of (n, 2h, 2w, c); acc:
+// added to dx.
+__global__ void k_up_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C, int acc)
 {
     const int c8 = C / 8;
     const int64_t n8 = static_cast<int64_t>(N) * H * W * c8;
@@ -1249,43 +1326,58 @@ __global__ void k_up_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
 #pragma unroll
         for (int k = 0; k < 8; ++k)
             r.v[k] = a.v[k] + bb.v[k] + cc.v[k] + dd.v[k];
+        if (acc) {
+            const V8 d = ld8(dx + 8 * i);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                r.v[k] = d.v[k] + static_cast<float>(__float2bfloat16(r.v[k]));
+        }
         st8(dx + 8 * i, r);
     }
 }
 
+// One atomic per CTA.
 __global__ void k_mask_sum(const float *mask, int64_t n, float *sum)
 {
     float s = 0.0f;
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
         s += mask[i];
-    for (int o = 16; o > 0; o >>= 1)
-        s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0)
+    s = block_sum(s);
+    if (threadIdx.x == 0)
         atomicAdd(sum, s);
 }
 
+// Masked MSE over the first K of C channels and its gradient: one thread per
+// (pixel, 8-channel group), a 16-byte store of the gradient; groups past K
+// store zeros and read nothing.  One atomic per CTA for the loss.
 __global__ void k_mse(const float *out, const float *tgt, const float *mask, const float *msum,
                       bf16 *dy, float *loss, int64_t pixels, int C, int K)
 {
     const float scale = 1.0f / (static_cast<float>(K) * fmaxf(*msum, 1.0f));
+    const int c8 = C / 8;
     float l = 0.0f;
-    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < pixels;
-         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const float mk = mask[p];
-        for (int c = 0; c < C; ++c) {
-            float g = 0.0f;
-            if (c < K && mk != 0.0f) {
-                const float d = out[p * C + c] - tgt[p * K + c];
-                l += d * d * scale;
-                g = 2.0f * d * scale;
-            }
-            dy[p * C + c] = __float2bfloat16(g);
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+         i < pixels * c8; i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t p = i / c8;
+        const int c0 = 8 * static_cast<int>(i % c8);
+        V8 r;
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+            r.v[e] = 0.0f;
+        if (c0 < K && mask[p] != 0.0f) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                if (c0 + e < K) {
+                    const float d = out[p * C + c0 + e] - tgt[p * K + c0 + e];
+                    l += d * d * scale;
+                    r.v[e] = 2.0f * d * scale;
+                }
         }
+        st8(dy + p * C + c0, r);
     }
-    for (int o = 16; o > 0; o >>= 1)
-        l += __shfl_xor_sync(0xffffffffu, l, o);
-    if ((threadIdx.x & 31) == 0)
+    l = block_sum(l);
+    if (threadIdx.x == 0)
         atomicAdd(loss, l);
 }
 
@@ -1752,13 +1844,20 @@ int dsmc_sg_pool_fwd(const uint16_t *x, uint16_t *y, int n, int h, int w_, int c
     return status();
 }
 
-int dsmc_sg_pool_bwd(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c, void *stream)
+int dsmc_sg_pool_bwd_acc(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c,
+                         int accumulate, void *stream)
 {
     if (!dy || !dx || n <= 0 || h <= 0 || w_ <= 0 || c <= 0 || h % 2 || w_ % 2 || c % 8)
         return ERR_ARG;
     k_pool_bwd<<<grid_for(int64_t(n) * h * w_ * c / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<const bf16 *>(dy), reinterpret_cast<bf16 *>(dx), n, h, w_, c);
+        reinterpret_cast<const bf16 *>(dy), reinterpret_cast<bf16 *>(dx), n, h, w_, c,
+        accumulate ? 1 : 0);
     return status();
+}
+
+int dsmc_sg_pool_bwd(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c, void *stream)
+{
+    return dsmc_sg_pool_bwd_acc(dy, dx, n, h, w_, c, 0, stream);
 }
 
 int dsmc_sg_up_fwd(const uint16_t *x, uint16_t *y, int n, int h, int w_, int c, void *stream)
@@ -1770,12 +1869,30 @@ int dsmc_sg_up_fwd(const uint16_t *x, uint16_t *y, int n, int h, int w_, int c, 
     return status();
 }
 
-int dsmc_sg_up_bwd(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c, void *stream)
+int dsmc_sg_up_bwd_acc(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c,
+                       int accumulate, void *stream)
 {
     if (!dy || !dx || n <= 0 || h <= 0 || w_ <= 0 || c <= 0 || c % 8)
         return ERR_ARG;
     k_up_bwd<<<grid_for(int64_t(n) * h * w_ * c / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<const bf16 *>(dy), reinterpret_cast<bf16 *>(dx), n, h, w_, c);
+        reinterpret_cast<const bf16 *>(dy), reinterpret_cast<bf16 *>(dx), n, h, w_, c,
+        accumulate ? 1 : 0);
+    return status();
+}
+
+int dsmc_sg_up_bwd(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c, void *stream)
+{
+    return dsmc_sg_up_bwd_acc(dy, dx, n, h, w_, c, 0, stream);
+}
+
+int dsmc_sg_relu_bias_bwd(uint16_t *dy, const uint16_t *y, uint16_t *skip, int skip_accumulate,
+                          float *db, int64_t pixels, int c, void *stream)
+{
+    if (!dy || !db || pixels < 0 || pixels > INT32_MAX || c < 8 || c > 256 || c % 8)
+        return ERR_ARG;
+    k_relu_bias_bwd<<<592, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<bf16 *>(dy), reinterpret_cast<const bf16 *>(y),
+        reinterpret_cast<bf16 *>(skip), skip_accumulate ? 1 : 0, db, static_cast<int>(pixels), c);
     return status();
 }
 
@@ -1793,15 +1910,15 @@ int dsmc_sg_add(uint16_t *a, const uint16_t *b, int64_t count, void *stream)
 int dsmc_sg_mse(const float *out, const float *target, const float *mask, uint16_t *dy,
                 float *loss, int64_t pixels, int c, int k, void *stream)
 {
-    if (!out || !target || !mask || !dy || !loss || pixels <= 0 || k <= 0 || k > c)
+    if (!out || !target || !mask || !dy || !loss || pixels <= 0 || k <= 0 || k > c || c % 8)
         return ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // loss[0] = loss, loss[1] = sum of the mask (scratch).
     if (cudaMemsetAsync(loss, 0, 2 * sizeof(float), s) != cudaSuccess)
         return ERR_CUDA;
-    k_mask_sum<<<grid_for(pixels), 256, 0, s>>>(mask, pixels, loss + 1);
-    k_mse<<<grid_for(pixels), 256, 0, s>>>(out, target, mask, loss + 1,
-                                           reinterpret_cast<bf16 *>(dy), loss, pixels, c, k);
+    k_mask_sum<<<592, 256, 0, s>>>(mask, pixels, loss + 1);
+    k_mse<<<grid_for(pixels * (c / 8) / 4), 256, 0, s>>>(
+        out, target, mask, loss + 1, reinterpret_cast<bf16 *>(dy), loss, pixels, c, k);
     return status();
 }
 

@@ -5,13 +5,15 @@ step: each layer shape of the network at a batch size, forward
 
     python -m dsmc_erlend_b200.sgbench [--batch 32] [--iters 20]
     python -m dsmc_erlend_b200.sgbench --shape 128x128:32:32 --profile
+    python -m dsmc_erlend_b200.sgbench --batch 64 --step-profile
 
 Prints one JSON line: per shape and op, milliseconds per call and TFLOP/s
 (2 Cin Cout 9 H W N), and the training step's milliseconds and TFLOP/s,
 eager and replayed as one CUDA graph.
 `--profile` runs forward, input gradient and weight gradient of one shape
 twice each (in that order) with no timing, for a profiler to capture the
-second round.
+second round.  `--step-profile` runs three eager training steps with no
+timing (a profiler's launch list of the last one is the step's kernels).
 """
 from __future__ import annotations
 
@@ -39,9 +41,22 @@ def main():
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--shape", default=None, help="HxW:Cin:Cout, e.g. 128x128:32:32")
     ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--step-profile", action="store_true")
     args = ap.parse_args()
 
     import torch
+
+    if args.step_profile:
+        net = S.Surrogate(args.batch)
+        x = torch.randn(args.batch, S.RES, S.RES, S.CH, device="cuda").to(torch.bfloat16)
+        tgt = torch.randn(args.batch, S.RES, S.RES, S.OUT_CH, device="cuda")
+        mask = torch.ones(args.batch, S.RES, S.RES, device="cuda")
+        for _ in range(3):
+            net.train_step(x, tgt, mask)
+        torch.cuda.synchronize()
+        S._ok(S.lib().dsmc_sg_check(None), "tensor-core wait")
+        print(json.dumps({"step_profile": args.batch}))
+        return
 
     L = S.lib()
     if args.shape:

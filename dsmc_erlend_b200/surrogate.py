@@ -68,6 +68,9 @@ _SIGS = {
     "dsmc_sg_conv_dgrad": [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
     "dsmc_sg_conv_wgrad": [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
     "dsmc_sg_relu_bwd": [_P, _P, C.c_int64, _P],
+    "dsmc_sg_relu_bias_bwd": [_P, _P, _P, C.c_int, _P, C.c_int64, C.c_int, _P],
+    "dsmc_sg_pool_bwd_acc": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "dsmc_sg_up_bwd_acc": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
     "dsmc_sg_pool_fwd": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P],
     "dsmc_sg_pool_bwd": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P],
     "dsmc_sg_up_fwd": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P],
@@ -118,18 +121,37 @@ class Surrogate:
         self.stream = stream
         g = torch.Generator().manual_seed(seed)
         dev = torch.device("cuda")
+        # All parameters in flat buffers, per layer its weights then its bias
+        # (every segment a multiple of 32 elements, so each view stays 64-byte
+        # aligned): masters, bf16 copies, gradients and Adam moments share the
+        # offsets, so one launch updates all of them and one fill zeroes the
+        # gradients.  The per-layer tensors below are views.
+        segs = []
+        for name, _, _, cin, cout, _, _ in LAYERS:
+            segs += [(name, "w", (cout, 3, 3, cin)), (name, "b", (cout,))]
+        self.n_params = sum(math.prod(shp) for _, _, shp in segs)
+        self.p32 = torch.zeros(self.n_params, device=dev)
+        self.pb = torch.zeros(self.n_params, dtype=torch.bfloat16, device=dev)
+        self.g_all = torch.zeros(self.n_params, device=dev)
+        self.m_all = torch.zeros(self.n_params, device=dev)
+        self.v_all = torch.zeros(self.n_params, device=dev)
         self.w32, self.wb, self.b32, self.m, self.v, self.gw, self.gb = {}, {}, {}, {}, {}, {}, {}
+        off = 0
+        for name, kind, shp in segs:
+            k = math.prod(shp)
+            views = [t[off:off + k].view(shp)
+                     for t in (self.p32, self.pb, self.g_all, self.m_all, self.v_all)]
+            off += k
+            self.m[name + "." + kind], self.v[name + "." + kind] = views[3], views[4]
+            if kind == "w":
+                self.w32[name], self.wb[name], self.gw[name] = views[:3]
+            else:
+                self.b32[name], self.gb[name] = views[0], views[2]
         for name, _, _, cin, cout, _, _ in LAYERS:
             std = math.sqrt(2.0 / (9 * cin))  # He initialisation
             w = torch.randn(cout, 3, 3, cin, generator=g) * std
-            self.w32[name] = w.to(dev)
-            self.wb[name] = w.to(torch.bfloat16).to(dev)
-            self.b32[name] = torch.zeros(cout, device=dev)
-            self.gw[name] = torch.zeros_like(self.w32[name])
-            self.gb[name] = torch.zeros_like(self.b32[name])
-            for d in (self.m, self.v):
-                d[name + ".w"] = torch.zeros_like(self.w32[name])
-                d[name + ".b"] = torch.zeros_like(self.b32[name])
+            self.w32[name].copy_(w)
+            self.wb[name].copy_(w.to(torch.bfloat16))
         self.t = 0
         self.w_rot = torch.empty(9 * 128 * 128, dtype=torch.bfloat16, device=dev)
         self.shape = {"x": (res, CH)}
@@ -150,7 +172,6 @@ class Surrogate:
             self.y[name] = buf(r, cout) if skip else self.relu_out[name]
         self.out32 = buf(res, CH, torch.float32)
         self.dy = {k: buf(*self.shape[k]) for k in self.shape}
-        self.scratch = {k: buf(*self.shape[k]) for k in self.shape}
         self.da_in = {name: buf(self.shape[name][0], cin)
                       for name, _, op, cin, _, _, _ in LAYERS}
         self.loss = torch.zeros(2, device=dev)
@@ -197,43 +218,50 @@ class Surrogate:
         gradient dout (bf16, same shape as the output)."""
         L, s, n = lib(), self._s, self.n
         acts = self._acts
-        for g in list(self.gw.values()) + list(self.gb.values()):
-            g.zero_()
+        self.g_all.zero_()
         last = LAYERS[-1][0]
-        for k in self.dy:
-            if k != last:
-                self.dy[k].zero_()
-        self.dy[last].copy_(dout)
+        if dout.data_ptr() != self.dy[last].data_ptr():
+            self.dy[last].copy_(dout)
+        # A gradient buffer is written by its first contribution and added to
+        # by later ones (a skip source gets the decoder's gradient first, then
+        # its pooled consumer's), so no buffer is zero-filled first.
+        written = {last}
         for name, src, op, cin, cout, relu, skip in reversed(LAYERS):
             r = self.shape[name][0]
             dy = self.dy[name]
+            _ok(L.dsmc_sg_relu_bias_bwd(ptr(dy), ptr(self.relu_out[name]) if relu else None,
+                                        ptr(self.dy[skip]) if skip else None,
+                                        int(skip in written), ptr(self.gb[name]), n * r * r,
+                                        cout, s), f"relu and bias {name}")
             if skip:
-                _ok(L.dsmc_sg_add(ptr(self.dy[skip]), ptr(dy), dy.numel(), s), "skip grad")
-            if relu:
-                _ok(L.dsmc_sg_relu_bwd(ptr(dy), ptr(self.relu_out[name]), dy.numel(), s), "relu")
+                written.add(skip)
             a = self.a_in[name] if op else acts[src]
-            _ok(L.dsmc_sg_conv_wgrad(ptr(dy), ptr(a), ptr(self.gw[name]), ptr(self.gb[name]),
+            _ok(L.dsmc_sg_conv_wgrad(ptr(dy), ptr(a), ptr(self.gw[name]), None,
                                      n, r, r, cin, cout, s), f"wgrad {name}")
             if src == "x":
                 continue
-            da = self.da_in[name]
+            acc = src in written
+            # The input gradient goes straight into dy[src] when it is the
+            # first contribution and needs no resampling.
+            da = self.dy[src] if (op is None and not acc) else self.da_in[name]
             _ok(L.dsmc_sg_conv_dgrad(ptr(dy), ptr(self.wb[name]), ptr(self.w_rot), ptr(da),
                                      n, r, r, cin, cout, s), f"dgrad {name}")
-            tgt = self.scratch[src]
             if op == "pool":
-                _ok(L.dsmc_sg_pool_bwd(ptr(da), ptr(tgt), n, 2 * r, 2 * r, cin, s), "pool bwd")
+                _ok(L.dsmc_sg_pool_bwd_acc(ptr(da), ptr(self.dy[src]), n, 2 * r, 2 * r, cin,
+                                           int(acc), s), "pool bwd")
             elif op == "up":
-                _ok(L.dsmc_sg_up_bwd(ptr(da), ptr(tgt), n, r // 2, r // 2, cin, s), "up bwd")
-            else:
-                tgt = da
-            _ok(L.dsmc_sg_add(ptr(self.dy[src]), ptr(tgt), tgt.numel(), s), "grad add")
+                _ok(L.dsmc_sg_up_bwd_acc(ptr(da), ptr(self.dy[src]), n, r // 2, r // 2, cin,
+                                         int(acc), s), "up bwd")
+            elif acc:
+                _ok(L.dsmc_sg_add(ptr(self.dy[src]), ptr(da), da.numel(), s), "grad add")
+            written.add(src)
 
     def loss_and_grad(self, target, mask):
         """Masked MSE of the last forward against target (n, res, res, OUT_CH)
         fp32 with mask (n, res, res) fp32; returns the loss tensor [1] and
         fills the output gradient."""
         L = lib()
-        dout = self.scratch[LAYERS[-1][0]]
+        dout = self.dy[LAYERS[-1][0]]
         _ok(L.dsmc_sg_mse(ptr(self.out32), ptr(target), ptr(mask), ptr(dout), ptr(self.loss),
                           self.n * self.res * self.res, CH, OUT_CH, self._s), "mse")
         return self.loss[:1], dout
@@ -242,13 +270,10 @@ class Surrogate:
                   eps: float = 1e-8):
         L, s = lib(), self._s
         self.t += 1
-        for name in self.w32:
-            _ok(L.dsmc_sg_adam(ptr(self.w32[name]), ptr(self.wb[name]), ptr(self.gw[name]),
-                               ptr(self.m[name + ".w"]), ptr(self.v[name + ".w"]),
-                               self.w32[name].numel(), lr, beta1, beta2, eps, self.t, s), "adam w")
-            _ok(L.dsmc_sg_adam(ptr(self.b32[name]), None, ptr(self.gb[name]),
-                               ptr(self.m[name + ".b"]), ptr(self.v[name + ".b"]),
-                               self.b32[name].numel(), lr, beta1, beta2, eps, self.t, s), "adam b")
+        # All parameters in one launch (the biases' bf16 copies are unused).
+        _ok(L.dsmc_sg_adam(ptr(self.p32), ptr(self.pb), ptr(self.g_all), ptr(self.m_all),
+                           ptr(self.v_all), self.n_params, lr, beta1, beta2, eps, self.t, s),
+            "adam")
 
     def train_step(self, x, target, mask, lr: float = 1e-3):
         self.forward(x)
@@ -292,15 +317,9 @@ class Surrogate:
                 self.forward(x)
                 _, dout = self.loss_and_grad(target, mask)
                 self.backward(dout)
-                for name in self.w32:
-                    _ok(L.dsmc_sg_adam_dev(ptr(self.w32[name]), ptr(self.wb[name]),
-                                           ptr(self.gw[name]), ptr(self.m[name + ".w"]),
-                                           ptr(self.v[name + ".w"]), self.w32[name].numel(),
-                                           ptr(self._hp), beta1, beta2, eps, self._s), "adam w")
-                    _ok(L.dsmc_sg_adam_dev(ptr(self.b32[name]), None, ptr(self.gb[name]),
-                                           ptr(self.m[name + ".b"]), ptr(self.v[name + ".b"]),
-                                           self.b32[name].numel(), ptr(self._hp), beta1, beta2,
-                                           eps, self._s), "adam b")
+                _ok(L.dsmc_sg_adam_dev(ptr(self.p32), ptr(self.pb), ptr(self.g_all),
+                                       ptr(self.m_all), ptr(self.v_all), self.n_params,
+                                       ptr(self._hp), beta1, beta2, eps, self._s), "adam")
             self._graph, self._graph_key = g, key
         self.t += 1
         # The bias corrections as dsmc_sg_adam forms them (FP32 powf).

@@ -43,21 +43,34 @@ int dsmc_sg_conv_wgrad(const uint16_t *dy, const uint16_t *x, float *dw, float *
 /* dy *= (y > 0): the gradient through a ReLU whose output is y. */
 int dsmc_sg_relu_bwd(uint16_t *dy, const uint16_t *y, int64_t count, void *stream);
 
+/* One pass over a layer's output gradient dy (pixels x c, c a multiple of 8
+ * up to 256): skip, when not NULL, receives dy as it comes (a copy, or
+ * added when skip_accumulate); then dy *= (y > 0) when y is not NULL; then
+ * db[ch] += the sum over pixels of dy[.][ch].  The relu, skip-gradient and
+ * bias-gradient passes of a layer's backward step in one. */
+int dsmc_sg_relu_bias_bwd(uint16_t *dy, const uint16_t *y, uint16_t *skip, int skip_accumulate,
+                          float *db, int64_t pixels, int c, void *stream);
+
 /* 2 x 2 average pooling (h, w even) and its gradient. */
 int dsmc_sg_pool_fwd(const uint16_t *x, uint16_t *y, int n, int h, int w_, int c, void *stream);
 int dsmc_sg_pool_bwd(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c,
                      void *stream);
+/* The gradient added to dx (rounded to bf16 first) when accumulate. */
+int dsmc_sg_pool_bwd_acc(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c,
+                         int accumulate, void *stream);
 
 /* Nearest 2x upsampling of an (n, h, w, c) tensor and its gradient. */
 int dsmc_sg_up_fwd(const uint16_t *x, uint16_t *y, int n, int h, int w_, int c, void *stream);
 int dsmc_sg_up_bwd(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c,
                    void *stream);
+int dsmc_sg_up_bwd_acc(const uint16_t *dy, uint16_t *dx, int n, int h, int w_, int c,
+                       int accumulate, void *stream);
 
 /* a += b elementwise (bf16). */
 int dsmc_sg_add(uint16_t *a, const uint16_t *b, int64_t count, void *stream);
 
 /* Masked mean squared error of the first `k` channels of out (fp32, c
- * channels) against target (fp32, k channels), weighted by mask (n*h*w,
+ * channels, a multiple of 8) against target (fp32, k channels), weighted by mask (n*h*w,
  * 0 or 1); dy (bf16, c channels) receives its gradient (zero beyond k) and
  * loss[0] (device fp32) the loss.  Scaled by 1 / (k * sum of mask). */
 int dsmc_sg_mse(const float *out, const float *target, const float *mask, uint16_t *dy,

@@ -206,6 +206,60 @@ def test_resampling_and_loss_kernels(cuda):
     _close(_np(dy), gw, 2 ** -8, "mse grad")
 
 
+def _round_bf16(torch, a):
+    return torch.from_numpy(np.asarray(a, np.float32)).to(torch.bfloat16).float().numpy()
+
+
+@pytest.mark.parametrize("c", [32, 128])
+def test_fused_backward_passes(cuda, c):
+    # dsmc_sg_relu_bias_bwd (skip copy or add, ReLU mask, bias gradient) and
+    # the accumulating pooling / upsampling gradients, against the separate
+    # passes they replace.
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    L = lib()
+    rng = np.random.default_rng(c)
+    n, h, w = 2, 8, 12
+    y = _bf16(torch, _rand(rng, n, h, w, c))
+    g = _bf16(torch, _rand(rng, n, h, w, c))
+    s0 = _bf16(torch, _rand(rng, n, h, w, c))
+    g0, y0, s00 = _np(g), _np(y), _np(s0)
+    masked = g0 * (y0 > 0)
+    # ReLU with the skip source's first gradient (a copy).
+    skip = torch.empty_like(g)
+    db = torch.ones(c, device="cuda")
+    assert L.dsmc_sg_relu_bias_bwd(ptr(g), ptr(y), ptr(skip), 0, ptr(db), n * h * w, c,
+                                   None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(_np(skip), g0)
+    assert np.array_equal(_np(g), masked)
+    _close(db.cpu().numpy() - 1.0, masked.sum(axis=(0, 1, 2)), 1e-5, "bias grad")
+    # No ReLU, the skip gradient added.
+    g2 = _bf16(torch, g0)
+    db2 = torch.zeros(c, device="cuda")
+    assert L.dsmc_sg_relu_bias_bwd(ptr(g2), None, ptr(s0), 1, ptr(db2), n * h * w, c,
+                                   None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(_np(g2), g0)
+    assert np.array_equal(_np(s0), _round_bf16(torch, s00 + g0))
+    _close(db2.cpu().numpy(), g0.sum(axis=(0, 1, 2)), 1e-5, "bias grad, no relu")
+    # Pooling and upsampling gradients added to what dx holds.
+    p = _bf16(torch, _rand(rng, n, h // 2, w // 2, c))
+    u = _bf16(torch, _rand(rng, n, 2 * h, 2 * w, c))
+    d0 = _rand(rng, n, h, w, c)
+    pb, ub = _bf16(torch, d0), _bf16(torch, d0)
+    base = _np(pb)
+    assert L.dsmc_sg_pool_bwd_acc(ptr(p), ptr(pb), n, h, w, c, 1, None) == 0
+    assert L.dsmc_sg_up_bwd_acc(ptr(u), ptr(ub), n, h, w, c, 1, None) == 0
+    pw, uw = torch.empty_like(pb), torch.empty_like(ub)
+    assert L.dsmc_sg_pool_bwd(ptr(p), ptr(pw), n, h, w, c, None) == 0
+    assert L.dsmc_sg_up_bwd(ptr(u), ptr(uw), n, h, w, c, None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(_np(pb), _round_bf16(torch, base + _np(pw)))
+    assert np.array_equal(_np(ub), _round_bf16(torch, base + _np(uw)))
+
+
 def test_adam_step(cuda):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
