@@ -253,6 +253,58 @@ template <int BN> constexpr int tc_smem3()
     return tc_stages<BN>() * static_cast<int>(A3_BYTES) + 9 * BN * 64 + 1024;
 }
 
+// The forward epilogue of 16 channels co .. co + 15 at element offset o
+// (pixel * Cout + co): bias and ReLU on the accumulators v, then the residual
+// (added to y, or as the skip sum ysum = bf16(y) + res, y kept for the
+// ReLU's gradient) and the bf16 / FP32 stores.
+__device__ __forceinline__ void fwd_store16(float v[16], int64_t o, int co,
+                                            const float *__restrict__ bias, int relu,
+                                            const bf16 *__restrict__ res, bf16 *__restrict__ y,
+                                            bf16 *__restrict__ ysum, float *__restrict__ y32)
+{
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        v[e] += bias ? bias[co + e] : 0.0f;
+        if (relu)
+            v[e] = fmaxf(v[e], 0.0f);
+    }
+    if (ysum) {
+#pragma unroll
+        for (int h8 = 0; h8 < 2; ++h8) {
+            const V8 rr = ld8(res + o + 8 * h8);
+            V8 out;
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                out.v[e] = static_cast<float>(__float2bfloat16(v[8 * h8 + e])) + rr.v[e];
+            st8(ysum + o + 8 * h8, out);
+        }
+    } else if (res) {
+#pragma unroll
+        for (int h8 = 0; h8 < 2; ++h8) {
+            const V8 rr = ld8(res + o + 8 * h8);
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                v[8 * h8 + e] += rr.v[e];
+        }
+    }
+    if (y) {
+#pragma unroll
+        for (int h8 = 0; h8 < 2; ++h8) {
+            V8 out;
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                out.v[e] = v[8 * h8 + e];
+            st8(y + o + 8 * h8, out);
+        }
+    }
+    if (y32) {
+#pragma unroll
+        for (int e4 = 0; e4 < 4; ++e4)
+            *reinterpret_cast<float4 *>(y32 + o + 4 * e4) =
+                make_float4(v[4 * e4], v[4 * e4 + 1], v[4 * e4 + 2], v[4 * e4 + 3]);
+    }
+}
+
 // AMODE selects how the stages are filled: 0, the cp.async im2col gather
 // (any shape); 1 and 2, TMA tile loads by one thread, for shapes whose
 // 128-pixel tile is a BW x BH rectangle of one image: the input through a
@@ -269,7 +321,8 @@ template <int BN, int AMODE>
 __global__ void __launch_bounds__(TC_THREADS)
     k_conv_fwd_tc(const bf16 *__restrict__ x, const bf16 *__restrict__ w,
                   const float *__restrict__ bias, const bf16 *__restrict__ res,
-                  bf16 *__restrict__ y, float *__restrict__ y32, int N, int H, int W, int Cin,
+                  bf16 *__restrict__ y, bf16 *__restrict__ ysum, float *__restrict__ y32, int N,
+                  int H, int W, int Cin,
                   int Cout, int relu, const __grid_constant__ CUtensorMap tmx,
                   const __grid_constant__ CUtensorMap tmw, int BW, int BH)
 {
@@ -538,37 +591,10 @@ __global__ void __launch_bounds__(TC_THREADS)
                     continue;
                 float v[16];
 #pragma unroll
-                for (int e = 0; e < 16; ++e) {
-                    v[e] = __uint_as_float(r[e]) + (bias ? bias[co + e] : 0.0f);
-                    if (relu)
-                        v[e] = fmaxf(v[e], 0.0f);
-                }
-                const int64_t o = static_cast<int64_t>(m) * Cout + co;
-                if (res) {
-#pragma unroll
-                    for (int h8 = 0; h8 < 2; ++h8) {
-                        const V8 rr = ld8(res + o + 8 * h8);
-#pragma unroll
-                        for (int e = 0; e < 8; ++e)
-                            v[8 * h8 + e] += rr.v[e];
-                    }
-                }
-                if (y) {
-#pragma unroll
-                    for (int h8 = 0; h8 < 2; ++h8) {
-                        V8 out;
-#pragma unroll
-                        for (int e = 0; e < 8; ++e)
-                            out.v[e] = v[8 * h8 + e];
-                        st8(y + o + 8 * h8, out);
-                    }
-                }
-                if (y32) {
-#pragma unroll
-                    for (int e4 = 0; e4 < 4; ++e4)
-                        *reinterpret_cast<float4 *>(y32 + o + 4 * e4) = make_float4(
-                            v[4 * e4], v[4 * e4 + 1], v[4 * e4 + 2], v[4 * e4 + 3]);
-                }
+                for (int e = 0; e < 16; ++e)
+                    v[e] = __uint_as_float(r[e]);
+                fwd_store16(v, static_cast<int64_t>(m) * Cout + co, co, bias, relu, res, y, ysum,
+                            y32);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             tc_mbar_arrive(&bar_acc_empty[b]); // this buffer may be reused
@@ -1003,6 +1029,31 @@ __global__ void k_rotate(const bf16 *__restrict__ w, bf16 *__restrict__ w_rot, i
         const int tap = static_cast<int>((i / Cin) % 9);
         const int co = static_cast<int>(i / (9 * static_cast<int64_t>(Cin)));
         w_rot[(static_cast<int64_t>(ci) * 9 + (8 - tap)) * Cout + co] = w[i];
+    }
+}
+
+// The rotation of several layers' weights in one launch: layer blockIdx.y
+// starts at element off[l] of both w and w_rot.
+constexpr int ROT_MAX_LAYERS = 32;
+struct RotTable {
+    int64_t off[ROT_MAX_LAYERS];
+    int cin[ROT_MAX_LAYERS], cout[ROT_MAX_LAYERS];
+};
+
+__global__ void k_rotate_layers(const bf16 *__restrict__ w, bf16 *__restrict__ w_rot,
+                                const RotTable t)
+{
+    const int l = blockIdx.y;
+    const int Cin = t.cin[l], Cout = t.cout[l];
+    const bf16 *src = w + t.off[l];
+    bf16 *dst = w_rot + t.off[l];
+    const int64_t total = static_cast<int64_t>(Cout) * 9 * Cin;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int ci = static_cast<int>(i % Cin);
+        const int tap = static_cast<int>((i / Cin) % 9);
+        const int co = static_cast<int>(i / (9 * static_cast<int64_t>(Cin)));
+        dst[(static_cast<int64_t>(ci) * 9 + (8 - tap)) * Cout + co] = src[i];
     }
 }
 
@@ -1498,7 +1549,7 @@ bool conv_tma_maps3(const bf16 *x, const bf16 *w, int n, int h, int w_, int cout
 
 template <int BN, int AMODE>
 int conv_fwd_tc_mode(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
-                     float *y32, int n, int h, int w_, int cin, int cout, int relu,
+                     bf16 *ysum, float *y32, int n, int h, int w_, int cin, int cout, int relu,
                      const CUtensorMap &mx, const CUtensorMap &mw, int bw, int bh, cudaStream_t s)
 {
     static std::once_flag once;
@@ -1525,7 +1576,7 @@ int conv_fwd_tc_mode(const bf16 *x, const bf16 *w, const float *bias, const bf16
     const int per_sm = AMODE == 3 ? tc_ctas_per_sm3<BN>() : tc_ctas_per_sm<BN>();
     const int grid = static_cast<int>(tiles < int64_t(sms) * per_sm ? tiles : int64_t(sms) * per_sm);
     k_conv_fwd_tc<BN, AMODE><<<grid, TC_THREADS, smem, s>>>(
-        x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx, mw, bw, bh);
+        x, w, bias, res, y, ysum, y32, n, h, w_, cin, cout, relu, mx, mw, bw, bh);
     return status();
 }
 
@@ -1535,28 +1586,30 @@ int conv_fwd_tc_mode(const bf16 *x, const bf16 *w, const float *bias, const bf16
 // 32 or a multiple of 64; the cp.async gather otherwise.
 template <int BN>
 int conv_fwd_tc(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
-                float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
+                bf16 *ysum, float *y32, int n, int h, int w_, int cin, int cout, int relu,
+                cudaStream_t s)
 {
     CUtensorMap mx, mw;
 #ifndef DSMC_CONV_HALO
 #define DSMC_CONV_HALO 1
 #endif
+
     if (DSMC_CONV_HALO && cin == 32 && cout == BN && w_ % H3W == 0 && h % H3H == 0 &&
         conv_tma_maps3(x, w, n, h, w_, cout, BN, &mx, &mw))
-        return conv_fwd_tc_mode<BN, 3>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx,
+        return conv_fwd_tc_mode<BN, 3>(x, w, bias, res, y, ysum, y32, n, h, w_, cin, cout, relu, mx,
                                        mw, H3W, H3H, s);
     const bool rect = (w_ % TBM == 0 || TBM % w_ == 0) && (int64_t(h) * w_) % TBM == 0;
     const int bw = w_ < TBM ? w_ : TBM, bh = TBM / bw;
     if (rect && cin % 64 == 0 &&
         conv_tma_maps(x, w, n, h, w_, cin, cout, BN, 64, bw, bh, &mx, &mw))
-        return conv_fwd_tc_mode<BN, 1>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx,
+        return conv_fwd_tc_mode<BN, 1>(x, w, bias, res, y, ysum, y32, n, h, w_, cin, cout, relu, mx,
                                        mw, bw, bh, s);
     if (rect && cin == 32 && conv_tma_maps(x, w, n, h, w_, cin, cout, BN, 32, bw, bh, &mx, &mw))
-        return conv_fwd_tc_mode<BN, 2>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx,
+        return conv_fwd_tc_mode<BN, 2>(x, w, bias, res, y, ysum, y32, n, h, w_, cin, cout, relu, mx,
                                        mw, bw, bh, s);
     memset(&mx, 0, sizeof(mx));
     memset(&mw, 0, sizeof(mw));
-    return conv_fwd_tc_mode<BN, 0>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, mx, mw,
+    return conv_fwd_tc_mode<BN, 0>(x, w, bias, res, y, ysum, y32, n, h, w_, cin, cout, relu, mx, mw,
                                    0, 0, s);
 }
 // Weight gradient on the tensor cores: groups of 128 / Cin taps x splits of
@@ -1719,7 +1772,8 @@ int wgrad_tc_n(const bf16 *dy, const bf16 *x, float *dw, int n, int h, int w_, i
 }
 
 int conv_fwd_launch(const bf16 *x, const bf16 *w, const float *bias, const bf16 *res, bf16 *y,
-                    float *y32, int n, int h, int w_, int cin, int cout, int relu, cudaStream_t s)
+                    bf16 *ysum, float *y32, int n, int h, int w_, int cin, int cout, int relu,
+                    cudaStream_t s)
 {
     // The widest channel tile that divides Cout and still gives every SM a
     // tile; for small images (16x16 x 32 is 64 pixel tiles) 64 channels.
@@ -1732,10 +1786,10 @@ int conv_fwd_launch(const bf16 *x, const bf16 *w, const float *bias, const bf16 
     }
     const int64_t mt = (int64_t(n) * h * w_ + TBM - 1) / TBM;
     if (cout % 128 == 0 && mt * (cout / 128) >= sms)
-        return conv_fwd_tc<128>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, s);
+        return conv_fwd_tc<128>(x, w, bias, res, y, ysum, y32, n, h, w_, cin, cout, relu, s);
     if (cout % 64 == 0)
-        return conv_fwd_tc<64>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, s);
-    return conv_fwd_tc<32>(x, w, bias, res, y, y32, n, h, w_, cin, cout, relu, s);
+        return conv_fwd_tc<64>(x, w, bias, res, y, ysum, y32, n, h, w_, cin, cout, relu, s);
+    return conv_fwd_tc<32>(x, w, bias, res, y, ysum, y32, n, h, w_, cin, cout, relu, s);
 }
 
 bool conv_shape_ok(int n, int h, int w, int cin, int cout)
@@ -1756,7 +1810,20 @@ int dsmc_sg_conv_fwd(const uint16_t *x, const uint16_t *w, const float *bias, co
         return ERR_ARG;
     return conv_fwd_launch(reinterpret_cast<const bf16 *>(x), reinterpret_cast<const bf16 *>(w),
                            bias, reinterpret_cast<const bf16 *>(res), reinterpret_cast<bf16 *>(y),
-                           y32, n, h, w_, cin, cout, relu, static_cast<cudaStream_t>(stream));
+                           nullptr, y32, n, h, w_, cin, cout, relu,
+                           static_cast<cudaStream_t>(stream));
+}
+
+int dsmc_sg_conv_fwd_skip(const uint16_t *x, const uint16_t *w, const float *bias,
+                          const uint16_t *skip, uint16_t *y, uint16_t *ysum, int n, int h, int w_,
+                          int cin, int cout, int relu, void *stream)
+{
+    if (!x || !w || !skip || !y || !ysum || !conv_shape_ok(n, h, w_, cin, cout))
+        return ERR_ARG;
+    return conv_fwd_launch(reinterpret_cast<const bf16 *>(x), reinterpret_cast<const bf16 *>(w),
+                           bias, reinterpret_cast<const bf16 *>(skip),
+                           reinterpret_cast<bf16 *>(y), reinterpret_cast<bf16 *>(ysum), nullptr,
+                           n, h, w_, cin, cout, relu, static_cast<cudaStream_t>(stream));
 }
 
 int dsmc_sg_check(void *stream)
@@ -1785,6 +1852,30 @@ int dsmc_sg_conv_dgrad(const uint16_t *dy, const uint16_t *w, uint16_t *w_rot, u
         reinterpret_cast<const bf16 *>(w), reinterpret_cast<bf16 *>(w_rot), cin, cout);
     return dsmc_sg_conv_fwd(dy, w_rot, nullptr, nullptr, dx, nullptr, n, h, w_, cout, cin, 0,
                             stream);
+}
+
+int dsmc_sg_rotate_layers(const uint16_t *w, uint16_t *w_rot, const int64_t *offsets,
+                          const int *cin, const int *cout, int layers, void *stream)
+{
+    if (!w || !w_rot || !offsets || !cin || !cout || layers < 0 || layers > ROT_MAX_LAYERS)
+        return ERR_ARG;
+    RotTable t;
+    int64_t most = 0;
+    for (int l = 0; l < layers; ++l) {
+        if (offsets[l] < 0 || offsets[l] % 8 || cin[l] <= 0 || cout[l] <= 0)
+            return ERR_ARG;
+        t.off[l] = offsets[l];
+        t.cin[l] = cin[l];
+        t.cout[l] = cout[l];
+        const int64_t k = int64_t(9) * cin[l] * cout[l];
+        most = k > most ? k : most;
+    }
+    if (layers == 0)
+        return OK;
+    const int bx = static_cast<int>(most / 256 + 1 < 256 ? most / 256 + 1 : 256);
+    k_rotate_layers<<<dim3(bx, layers), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const bf16 *>(w), reinterpret_cast<bf16 *>(w_rot), t);
+    return status();
 }
 
 int dsmc_sg_conv_wgrad(const uint16_t *dy, const uint16_t *x, float *dw, float *db, int n, int h,

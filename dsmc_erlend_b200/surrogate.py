@@ -67,6 +67,9 @@ _SIGS = {
                          C.c_int, _P],
     "dsmc_sg_conv_dgrad": [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
     "dsmc_sg_conv_wgrad": [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "dsmc_sg_conv_fwd_skip": [_P, _P, _P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int,
+                              C.c_int, C.c_int, _P],
+    "dsmc_sg_rotate_layers": [_P, _P, _P, _P, _P, C.c_int, _P],
     "dsmc_sg_relu_bwd": [_P, _P, C.c_int64, _P],
     "dsmc_sg_relu_bias_bwd": [_P, _P, _P, C.c_int, _P, C.c_int64, C.c_int, _P],
     "dsmc_sg_pool_bwd_acc": [_P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
@@ -135,12 +138,22 @@ class Surrogate:
         self.g_all = torch.zeros(self.n_params, device=dev)
         self.m_all = torch.zeros(self.n_params, device=dev)
         self.v_all = torch.zeros(self.n_params, device=dev)
+        # The input-gradient weights (each layer's rotated bf16 copy at its
+        # weights' offsets), made for all layers by one launch per backward.
+        self.prot = torch.zeros(self.n_params, dtype=torch.bfloat16, device=dev)
         self.w32, self.wb, self.b32, self.m, self.v, self.gw, self.gb = {}, {}, {}, {}, {}, {}, {}
+        self.wrot = {}
+        rot_off, rot_cin, rot_cout = [], [], []
         off = 0
         for name, kind, shp in segs:
             k = math.prod(shp)
             views = [t[off:off + k].view(shp)
                      for t in (self.p32, self.pb, self.g_all, self.m_all, self.v_all)]
+            if kind == "w":
+                self.wrot[name] = self.prot[off:off + k]
+                rot_off.append(off)
+                rot_cout.append(shp[0])
+                rot_cin.append(shp[3])
             off += k
             self.m[name + "." + kind], self.v[name + "." + kind] = views[3], views[4]
             if kind == "w":
@@ -153,7 +166,9 @@ class Surrogate:
             self.w32[name].copy_(w)
             self.wb[name].copy_(w.to(torch.bfloat16))
         self.t = 0
-        self.w_rot = torch.empty(9 * 128 * 128, dtype=torch.bfloat16, device=dev)
+        nl = len(rot_off)
+        self._rot = ((C.c_int64 * nl)(*rot_off), (C.c_int * nl)(*rot_cin),
+                     (C.c_int * nl)(*rot_cout), nl)
         self.shape = {"x": (res, CH)}
         for name, src, op, cin, cout, _, _ in LAYERS:
             r = self.shape[src][0]
@@ -201,13 +216,16 @@ class Surrogate:
                     "up")
                 a = self.a_in[name]
             last = name == LAYERS[-1][0]
-            _ok(L.dsmc_sg_conv_fwd(ptr(a), ptr(self.wb[name]), ptr(self.b32[name]), None,
-                                   ptr(self.relu_out[name]), ptr(self.out32) if last else None,
-                                   n, r, r, cin, cout, int(relu), s), f"conv {name}")
-            if skip:
-                self.y[name].copy_(self.relu_out[name])
-                _ok(L.dsmc_sg_add(ptr(self.y[name]), ptr(acts[skip]), self.y[name].numel(), s),
-                    "skip")
+            if skip:  # relu_out for the ReLU's gradient, y = relu_out + skip
+                _ok(L.dsmc_sg_conv_fwd_skip(ptr(a), ptr(self.wb[name]), ptr(self.b32[name]),
+                                            ptr(acts[skip]), ptr(self.relu_out[name]),
+                                            ptr(self.y[name]), n, r, r, cin, cout, int(relu), s),
+                    f"conv {name}")
+            else:
+                _ok(L.dsmc_sg_conv_fwd(ptr(a), ptr(self.wb[name]), ptr(self.b32[name]), None,
+                                       ptr(self.relu_out[name]),
+                                       ptr(self.out32) if last else None,
+                                       n, r, r, cin, cout, int(relu), s), f"conv {name}")
             acts[name] = self.y[name]
         self._acts = acts
         return self.out32
@@ -226,6 +244,9 @@ class Surrogate:
         # by later ones (a skip source gets the decoder's gradient first, then
         # its pooled consumer's), so no buffer is zero-filled first.
         written = {last}
+        offs, cins, couts, nl = self._rot
+        _ok(L.dsmc_sg_rotate_layers(ptr(self.pb), ptr(self.prot), offs, cins, couts, nl, s),
+            "rotate weights")
         for name, src, op, cin, cout, relu, skip in reversed(LAYERS):
             r = self.shape[name][0]
             dy = self.dy[name]
@@ -244,8 +265,10 @@ class Surrogate:
             # The input gradient goes straight into dy[src] when it is the
             # first contribution and needs no resampling.
             da = self.dy[src] if (op is None and not acc) else self.da_in[name]
-            _ok(L.dsmc_sg_conv_dgrad(ptr(dy), ptr(self.wb[name]), ptr(self.w_rot), ptr(da),
-                                     n, r, r, cin, cout, s), f"dgrad {name}")
+            # The input gradient: the forward convolution of dy with the
+            # rotated weights (Cout in, Cin out).
+            _ok(L.dsmc_sg_conv_fwd(ptr(dy), ptr(self.wrot[name]), None, None, ptr(da), None,
+                                   n, r, r, cout, cin, 0, s), f"dgrad {name}")
             if op == "pool":
                 _ok(L.dsmc_sg_pool_bwd_acc(ptr(da), ptr(self.dy[src]), n, 2 * r, 2 * r, cin,
                                            int(acc), s), "pool bwd")

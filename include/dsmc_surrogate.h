@@ -29,10 +29,24 @@ int dsmc_sg_conv_fwd(const uint16_t *x, const uint16_t *w, const float *bias,
                      const uint16_t *res, uint16_t *y, float *y32, int n, int h, int w_,
                      int cin, int cout, int relu, void *stream);
 
+/* A convolution with a skip connection: y = act(conv(x, w) + bias) and
+ * ysum = y + skip, both bf16 (ysum from y as stored), in one pass. */
+int dsmc_sg_conv_fwd_skip(const uint16_t *x, const uint16_t *w, const float *bias,
+                          const uint16_t *skip, uint16_t *y, uint16_t *ysum, int n, int h,
+                          int w_, int cin, int cout, int relu, void *stream);
+
 /* dx = conv_transpose(dy, w): the input gradient of dsmc_sg_conv_fwd.
  * w_rot is scratch for the rotated weights, 9 * cin * cout elements. */
 int dsmc_sg_conv_dgrad(const uint16_t *dy, const uint16_t *w, uint16_t *w_rot, uint16_t *dx,
                        int n, int h, int w_, int cin, int cout, void *stream);
+
+/* The rotated weights dsmc_sg_conv_dgrad makes (w_rot[ci][8 - tap][co] =
+ * w[co][tap][ci]) for `layers` (at most 32) layers in one launch: layer l
+ * occupies elements offsets[l] (a multiple of 8) .. + 9 cin[l] cout[l] of
+ * both w and w_rot.  dsmc_sg_conv_fwd(dy, w_rot + offsets[l], ..., cout[l],
+ * cin[l], relu 0) is then that layer's input gradient. */
+int dsmc_sg_rotate_layers(const uint16_t *w, uint16_t *w_rot, const int64_t *offsets,
+                          const int *cin, const int *cout, int layers, void *stream);
 
 /* dw += sum over pixels of dy (x) shifted x, FP32 [Cout][3][3][Cin];
  * db += sum over pixels of dy (db may be NULL; cout <= 256 with db).

@@ -53,7 +53,9 @@ def _close(got, want, rtol, what):
                                             (2, 8, 16, 96, 32), (1, 2, 128, 256, 32),
                                             (1, 160, 128, 64, 128), (1, 150, 130, 32, 128),
                                             (2, 16, 32, 32, 32), (3, 8, 16, 32, 32),
-                                            (2, 128, 128, 32, 128)])
+                                            (2, 128, 128, 32, 128), (1, 24, 40, 32, 64),
+                                            (2, 8, 130, 32, 32), (1, 16, 14, 32, 32),
+                                            (1, 8, 3, 32, 32)])
 def test_conv_forward(cuda, n, h, w, cin, cout):
     from dsmc_erlend_b200.surrogate import lib, ptr
 
@@ -204,6 +206,58 @@ def test_resampling_and_loss_kernels(cuda):
                      mask.cpu().numpy(), 4)
     assert abs(loss[0].item() - lw) <= 1e-5 * lw
     _close(_np(dy), gw, 2 ** -8, "mse grad")
+
+
+def test_conv_forward_with_skip(cuda):
+    # y and y + skip from one pass equal the convolution followed by the add.
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    L = lib()
+    rng = np.random.default_rng(21)
+    for n, h, w, cin, cout in [(2, 16, 32, 32, 32), (1, 8, 16, 64, 64), (1, 16, 16, 128, 128)]:
+        x = _bf16(torch, _rand(rng, n, h, w, cin))
+        wt = _bf16(torch, _rand(rng, cout, 3, 3, cin, scale=0.1))
+        b = torch.from_numpy(rng.standard_normal(cout).astype(np.float32)).cuda()
+        skip = _bf16(torch, _rand(rng, n, h, w, cout))
+        y = torch.empty(n, h, w, cout, dtype=torch.bfloat16, device="cuda")
+        ysum, y0, ysum0 = torch.empty_like(y), torch.empty_like(y), torch.empty_like(y)
+        assert L.dsmc_sg_conv_fwd_skip(ptr(x), ptr(wt), ptr(b), ptr(skip), ptr(y), ptr(ysum),
+                                       n, h, w, cin, cout, 1, None) == 0
+        assert L.dsmc_sg_conv_fwd(ptr(x), ptr(wt), ptr(b), None, ptr(y0), None, n, h, w, cin,
+                                  cout, 1, None) == 0
+        ysum0.copy_(y0)
+        assert L.dsmc_sg_add(ptr(ysum0), ptr(skip), ysum0.numel(), None) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(y, y0) and torch.equal(ysum, ysum0)
+    assert L.dsmc_sg_check(None) == 0
+
+
+def test_rotate_layers(cuda):
+    # Several layers' rotated weights in one launch, at their offsets.
+    import ctypes as C
+
+    from dsmc_erlend_b200.surrogate import lib, ptr
+
+    torch = cuda
+    rng = np.random.default_rng(8)
+    shapes = [(32, 32), (64, 32), (128, 64)]  # (cout, cin)
+    offs, off = [], 16
+    for co, ci in shapes:
+        offs.append(off)
+        off += 9 * co * ci + 32
+    w = _bf16(torch, _rand(rng, off))
+    rot = torch.zeros(off, dtype=torch.bfloat16, device="cuda")
+    n = len(shapes)
+    assert lib().dsmc_sg_rotate_layers(
+        ptr(w), ptr(rot), (C.c_int64 * n)(*offs), (C.c_int * n)(*[ci for _, ci in shapes]),
+        (C.c_int * n)(*[co for co, _ in shapes]), n, None) == 0
+    torch.cuda.synchronize()
+    wn, rn = _np(w), _np(rot)
+    for (co, ci), o in zip(shapes, offs):
+        k = 9 * co * ci
+        want = wn[o:o + k].reshape(co, 9, ci)[:, ::-1, :].transpose(2, 1, 0).ravel()
+        assert np.array_equal(rn[o:o + k], want)
 
 
 def _round_bf16(torch, a):
