@@ -580,7 +580,9 @@ __global__ void __launch_bounds__(TC_THREADS)
                 n0 = (t % ntiles_n) * BN;
             }
             const bool am = m < M;
-#pragma unroll
+            // Rolled: each load waits for its tensor-memory read anyway, and
+            // unrolled copies of the store paths spill.
+#pragma unroll 1
             for (int c = 0; c < BN; c += 16) {
                 uint32_t r[16];
                 tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) +
